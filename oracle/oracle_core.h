@@ -1,0 +1,191 @@
+// ORACLE -- TEST INFRASTRUCTURE ONLY.
+//
+// A literal C++ restatement of the reference's THERMACOND job=1 path
+// (KeivanS/Anharmonic-lattice-dynamics, Fortran).  It is the checker for
+// the CUDA library: only tests/, __graft_entry__.smoke() and bench.py's
+// CPU-baseline leg may load it.  Nothing in the product links it.
+//
+// Parity status: the mesh, IBZ, phonon, group-velocity, Bose and RHS
+// stages are pinned against outputs the reference itself shipped
+// (THERMACOND/Ge-example/kappa and GeSe-example/kappa; see
+// tests/golden/make_golden.py).  The V3, tetrahedron, linewidth,
+// collision-matrix, CG and kappa stages are PARITY UNPINNED: no shipped
+// example carries an fc3.dat, and no Fortran compiler exists here to run
+// the reference; they follow the cited source line by line.
+//
+// Conventions: arrays keep the reference's Fortran layout (column-major,
+// 1-based index *values*); F2/F3/... helpers below give the addressing.
+#pragma once
+#include <atomic>
+#include <cmath>
+#include <stdexcept>
+#include <complex>
+#include <cstdint>
+#include <cstdio>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace orc {
+
+// parallel loop over [lo, hi] (inclusive) with dynamic scheduling; the
+// reference splits the same loops over MPI ranks
+template <class F>
+void parfor(int lo, int hi, int nthreads, F f) {
+  if (nthreads <= 1 || hi <= lo) {
+    for (int i = lo; i <= hi; ++i) f(i);
+    return;
+  }
+  std::atomic<int> next{lo};
+  std::vector<std::thread> th;
+  for (int t = 0; t < nthreads; ++t)
+    th.emplace_back([&]() {
+      for (;;) {
+        int i = next.fetch_add(1);
+        if (i > hi) break;
+        f(i);
+      }
+    });
+  for (auto& x : th) x.join();
+}
+
+typedef std::complex<double> cplx;
+
+// complex product written out so the operation order is fixed
+inline cplx cmul(cplx a, cplx b) {
+  return cplx(a.real() * b.real() - a.imag() * b.imag(), a.real() * b.imag() + a.imag() * b.real());
+}
+
+struct vec3 {
+  double x, y, z;
+};
+
+// ---------------------------------------------------------------- constants
+// THERMACOND/modules.f90:4-23.  cnst is declared real(8) but initialised
+// from a default-real (FP32) literal, so its value is the FP32 rounding.
+struct Consts {
+  double pi = 3.14159265358979323846;
+  double h_plank = 6.62606896e-34;
+  double k_b = 1.3806504e-23;
+  double c_light = 2.99792458e+8;
+  double hbar = 1.054571628e-34;
+  double ee = 1.60217653e-19;
+  double uma = 1.66053878e-27;
+  double cnst = (double)521.1098918f;
+  double const33 = 0;  // kappa.f90:182
+  Consts() {
+    const33 = 1e30 * std::pow(hbar / uma, 1.5) / std::pow(std::sqrt(ee * 1e20 / uma), 1.5) * ee /
+              h_plank / 100 / c_light;
+  }
+};
+
+struct Tetra {
+  int i[4];
+  double w[4];
+  double c[4];
+};
+
+struct State {
+  Consts K;
+  // ---- latdyn.params (rest.f90:13-51)
+  int nc[3] = {0, 0, 0};
+  bool dos_bs_only = false;
+  double shft[3] = {0, 0, 0};
+  double normald[3] = {0, 0, 0};
+  int wmesh = 0;
+  double wmax = 0, width = 0, etaz = 0;
+  bool verbose = false;
+  double tmin = 0, tmax = 0;
+  int ntemp = 0, job = 0, ksub_size = 0, iso = 0, classical = 0;
+  // ---- structure.params (rest.f90:87-130)
+  double latticeparameters[6] = {0};
+  double primitivelattice[9] = {0};  // (3,3) column-major
+  double lattice_parameter = 0;
+  int include_fc[4] = {0};
+  int natom_type = 0;
+  std::vector<double> mas;
+  int natoms0 = 0;
+  std::vector<int> atom_type;   // per primitive atom (1-based type)
+  std::vector<double> mass0;    // atom0(i)%mass
+  // ---- lat_fc.dat (rest.f90:164-289)
+  double r1[3], r2[3], r3[3], g1[3], g2[3], g3[3];
+  double volume_r = 0, volume_g = 0;
+  int nterms[4] = {0};
+  int natoms = 0;
+  std::vector<double> atompos;   // (3,natoms)
+  std::vector<int> iatomcell0;   // (natoms)
+  std::vector<int> iatomcell;    // (3,natoms)
+  // ---- symmetry (force_constants.f90:3-186)
+  int lattpgcount = 0;
+  double op_kmatrix[48][9];      // (3,3) column-major per op
+  // ---- fc2/fc3 (rest.f90:303-443)
+  std::vector<int> iatomterm_2, ixyzterm_2;   // (2,nt2)
+  std::vector<double> fcs_2;
+  std::vector<int> iatomterm_3, ixyzterm_3;   // (3,nt3)
+  std::vector<double> fcs_3;
+  int born_flag = 0;
+  double epsil[9] = {0};          // (3,3) column-major
+  std::vector<double> charge;     // (3,3,natoms0) column-major: charge(i,j) of atom k
+  // ---- mesh and IBZ
+  int nkc = 0, ndyn = 0, nibz = 0;
+  std::vector<double> kpc;       // (3,nkc)
+  std::vector<int> mappos;       // get_negatives map
+  int npos = 0;
+  std::vector<int> mapibz, mapinv;  // 1-based
+  std::vector<double> kibz, wibz;   // (3,nibz)
+  // ---- phonons (module eigen)
+  std::vector<double> eigenval;     // (ndyn,nkc)
+  std::vector<cplx> eigenvec;       // (ndyn,ndyn,nkc)
+  std::vector<double> veloc;        // (3,ndyn,nkc)
+  // ---- tetrahedra
+  std::vector<Tetra> tet;           // 6*nkc
+  // ---- exactBTE2
+  std::vector<double> frequency, dist;  // (nkc,ndyn)
+};
+
+// Fortran column-major addressing helpers (1-based index values)
+inline size_t F2(int i, int j, int n1) { return (size_t)(i - 1) + (size_t)(j - 1) * n1; }
+inline size_t F3(int i, int j, int k, int n1, int n2) {
+  return (size_t)(i - 1) + (size_t)n1 * ((size_t)(j - 1) + (size_t)n2 * (size_t)(k - 1));
+}
+inline size_t F5(int a, int b, int c, int d, int e, int n1, int n2, int n3, int n4) {
+  return (size_t)(a - 1) + (size_t)n1 * ((size_t)(b - 1) + (size_t)n2 * ((size_t)(c - 1) +
+         (size_t)n3 * ((size_t)(d - 1) + (size_t)n4 * (size_t)(e - 1))));
+}
+
+// ----------------------------------------------------------------- routines
+std::string read_inputs(State& S, const std::string& dir);
+void make_kp_reg(State& S);
+void get_negatives(State& S);
+void getstar(const State& S, const double kvec[3], int& narms, double kvecstar[][3], int kvecop[]);
+void get_weights(State& S);
+void get_k_info(const State& S, const double q[3], int& nk, int& i, int& j, int& k, int& inside);
+void set_dynamical_matrix(const State& S, const double kpt[3], cplx* dynmat);
+void hermitian_eigen(int n, const cplx* upper, double* eival, cplx* eivec);
+void get_freq(const State& S, const double kp[3], double* eival, cplx* eivec);
+void finitedif_vel(const State& S, const double q0[3], double* vgr, double* evl0, cplx* evc0);
+void get_frequencies(State& S, int nthreads);
+void subst_eivecs(State& S);
+void make_kp_reg_tet(State& S);
+void weight_tet_one(Tetra& t, double e);
+void calculate_w3_ibz_split_sq(State& S, int k1, int k2, double* v33s8, int nthreads);
+void calculate_FGR_mpi2(State& S, int k1, int k2, const double* v33s8, double* P1smpi, double* P2smpi,
+                        int nthreads);
+void calculate_FGR_gauss(State& S, int k1, int k2, const double* v33s8, double* P1smpi, double* P2smpi,
+                         int nthreads);
+double nbe(double w, double t, int m, int* err);
+int distribution(State& S, double tempk);
+void calculate_tauRTA_mpi2(State& S, int k1, int k2, double tempk, const double* P1smpi,
+                           const double* P2smpi, double* Q, double* QN, double* QU, double* P1, double* P2,
+                           int nthreads);
+void calculate_RTA_distributionfunction(State& S, double tempk, const double* Q, double* FFF);
+int mode_kappa(State& S, double tempk, const double* FFF, double* kappa);
+void kstarsinfbz1(const State& S, const double q[3], int& ds, double kvecstars[][3], int kvecops[]);
+void CollisionMatrix_mpi(State& S, int k1, int k2, const double* P1, const double* P2, double* CM,
+                         int nthreads);
+void cal_RHS_IBZ(State& S, double tempk, double* RHS);
+int cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
+                 int n_dig_accur, int nthreads);
+int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa);
+
+}  // namespace orc

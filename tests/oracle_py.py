@@ -1,0 +1,275 @@
+"""ctypes access to the C++ oracle (oracle/_build/liboracle.so).
+
+Test infrastructure: the oracle restates the reference's Fortran routines
+and is used only as the checker (tests, smoke, bench CPU baseline).
+Arrays follow the reference's Fortran layout; numpy arrays are created
+with order='F' so indices read like the Fortran source.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "oracle", "_build", "liboracle.so")
+_lib = None
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int)
+
+
+def build():
+    subprocess.check_call(["make", "-s", "-C", os.path.join(ROOT, "oracle")])
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB):
+            build()
+        L = C.CDLL(LIB)
+        L.orc_load.restype = C.c_void_p
+        L.orc_load.argtypes = [C.c_char_p, C.c_char_p, C.c_int]
+        L.orc_free.argtypes = [C.c_void_p]
+        for name in ["orc_sizes", "orc_lattice", "orc_op_kmatrix", "orc_mesh", "orc_get_kpc", "orc_get_ibz",
+                     "orc_get_k_info", "orc_getstar", "orc_kstars", "orc_dynmat", "orc_get_freq", "orc_phonons",
+                     "orc_get_phonons", "orc_set_phonons", "orc_tet", "orc_v3", "orc_fgr", "orc_distribution",
+                     "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d"]:
+            getattr(L, name).restype = C.c_int
+        L.orc_weight_tet_nonperm.restype = C.c_long
+        _lib = L
+    return _lib
+
+
+def _p(a, t=dp):
+    return a.ctypes.data_as(t) if a is not None else None
+
+
+class Oracle:
+    def __init__(self, d: str, nthreads: int = 0):
+        L = lib()
+        err = C.create_string_buffer(512)
+        h = L.orc_load(d.encode(), err, 512)
+        if not h:
+            raise RuntimeError("oracle load failed: " + err.value.decode())
+        self.h = C.c_void_p(h)
+        self.nthreads = nthreads or (os.cpu_count() or 1)
+        self._sizes()
+
+    def __del__(self):
+        try:
+            lib().orc_free(self.h)
+        except Exception:
+            pass
+
+    def _sizes(self):
+        s = np.zeros(12, dtype=np.int32)
+        lib().orc_sizes(self.h, _p(s, ip))
+        (self.ndyn, self.nkc, self.nibz, self.nt2, self.nt3, self.natoms, self.npg,
+         n1, n2, n3, self.nat0, self.npos) = [int(x) for x in s]
+        self.nc = (n1, n2, n3)
+
+    def lattice(self):
+        o = np.zeros(22)
+        lib().orc_lattice(self.h, _p(o))
+        return {"r": o[0:9].reshape(3, 3), "g": o[9:18].reshape(3, 3), "volume_r": o[18], "volume_g": o[19],
+                "const33": o[20], "cnst": o[21]}
+
+    def op_kmatrix(self):
+        o = np.zeros((48, 3, 3))
+        n = lib().orc_op_kmatrix(self.h, _p(o))
+        # stored column-major per op -> transpose to (row, col)
+        return np.array([o[i].T for i in range(n)])
+
+    def mesh(self):
+        n = lib().orc_mesh(self.h)
+        self._sizes()
+        return n
+
+    def kpc(self):
+        k = np.zeros((3, self.nkc), order="F")
+        lib().orc_get_kpc(self.h, _p(k))
+        return k
+
+    def ibz(self):
+        mapibz = np.zeros(self.nkc, dtype=np.int32)
+        mapinv = np.zeros(self.nibz, dtype=np.int32)
+        kibz = np.zeros((3, self.nibz), order="F")
+        wibz = np.zeros(self.nibz)
+        mappos = np.zeros(self.nkc, dtype=np.int32)
+        lib().orc_get_ibz(self.h, _p(mapibz, ip), _p(mapinv, ip), _p(kibz), _p(wibz), _p(mappos, ip))
+        return {"mapibz": mapibz, "mapinv": mapinv, "kibz": kibz, "wibz": wibz, "mappos": mappos}
+
+    def get_k_info(self, q):
+        o = np.zeros(5, dtype=np.int32)
+        q = np.ascontiguousarray(q, dtype=float)
+        lib().orc_get_k_info(self.h, _p(q), _p(o, ip))
+        return tuple(int(x) for x in o)  # nk, i, j, k, inside
+
+    def getstar(self, q, fbz=False):
+        st = np.zeros((48, 3))
+        ops = np.zeros(48, dtype=np.int32)
+        q = np.ascontiguousarray(q, dtype=float)
+        f = lib().orc_kstars if fbz else lib().orc_getstar
+        n = f(self.h, _p(q), _p(st), _p(ops, ip))
+        return st[:n].copy(), ops[:n].copy()
+
+    def dynmat(self, q):
+        d = np.zeros((self.ndyn, self.ndyn), dtype=complex, order="F")
+        q = np.ascontiguousarray(q, dtype=float)
+        lib().orc_dynmat(self.h, _p(q), d.ctypes.data_as(dp))
+        return d
+
+    def get_freq(self, q):
+        ev = np.zeros(self.ndyn)
+        vec = np.zeros((self.ndyn, self.ndyn), dtype=complex, order="F")
+        q = np.ascontiguousarray(q, dtype=float)
+        lib().orc_get_freq(self.h, _p(q), _p(ev), vec.ctypes.data_as(dp))
+        return ev, vec
+
+    def phonons(self):
+        lib().orc_phonons(self.h, self.nthreads)
+
+    def get_phonons(self):
+        n, nk = self.ndyn, self.nkc
+        ev = np.zeros((n, nk), order="F")
+        vec = np.zeros((n, n, nk), dtype=complex, order="F")
+        vel = np.zeros((3, n, nk), order="F")
+        lib().orc_get_phonons(self.h, _p(ev), vec.ctypes.data_as(dp), _p(vel))
+        return ev, vec, vel
+
+    def set_phonons(self, ev, vec, vel):
+        ev = np.asfortranarray(ev, dtype=float)
+        vec = np.asfortranarray(vec, dtype=complex)
+        vel = np.asfortranarray(vel, dtype=float)
+        lib().orc_set_phonons(self.h, _p(ev), vec.ctypes.data_as(dp), _p(vel))
+
+    def tet(self):
+        c = np.zeros((4, 6 * self.nkc), dtype=np.int32, order="F")
+        lib().orc_tet(self.h, _p(c, ip))
+        return c
+
+    def v3(self, k1, k2):
+        n, nk = self.ndyn, self.nkc
+        out = np.zeros((k2 - k1 + 1, nk, n, n, n), order="F")
+        err = C.create_string_buffer(256)
+        r = lib().orc_v3(self.h, k1, k2, _p(out), self.nthreads, err, 256)
+        if r:
+            raise RuntimeError(err.value.decode())
+        return out
+
+    def fgr(self, k1, k2, v33, gauss=False):
+        P1 = np.zeros_like(v33, order="F")
+        P2 = np.zeros_like(v33, order="F")
+        v33 = np.asfortranarray(v33)
+        lib().orc_fgr(self.h, k1, k2, _p(v33), _p(P1), _p(P2), int(gauss), self.nthreads)
+        return P1, P2
+
+    def distribution(self, tempk):
+        f = np.zeros((self.nkc, self.ndyn), order="F")
+        d = np.zeros((self.nkc, self.ndyn), order="F")
+        e = lib().orc_distribution(self.h, C.c_double(tempk), _p(f), _p(d))
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return f, d
+
+    def tau(self, k1, k2, tempk, P1s, P2s, want_p=True):
+        ns = k2 - k1 + 1
+        Q = np.zeros((ns, self.ndyn), order="F")
+        QN = np.zeros_like(Q)
+        QU = np.zeros_like(Q)
+        P1 = np.zeros_like(P1s, order="F") if want_p else None
+        P2 = np.zeros_like(P1s, order="F") if want_p else None
+        lib().orc_tau(self.h, k1, k2, C.c_double(tempk), _p(np.asfortranarray(P1s)), _p(np.asfortranarray(P2s)),
+                      _p(Q), _p(QN), _p(QU), _p(P1), _p(P2), self.nthreads)
+        return Q, QN, QU, P1, P2
+
+    def rta(self, tempk, Q):
+        FFF = np.zeros((self.nibz, self.ndyn, 3), order="F")
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        Q = np.asfortranarray(Q)
+        e = lib().orc_rta(self.h, C.c_double(tempk), _p(Q), _p(FFF), _p(kap))
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return FFF, kap
+
+    def collision(self, k1, k2, P1, P2):
+        ns = k2 - k1 + 1
+        CM = np.zeros((ns * self.ndyn * 3, self.nibz * self.ndyn * 3), order="F")
+        lib().orc_collision(self.h, k1, k2, _p(np.asfortranarray(P1)), _p(np.asfortranarray(P2)), _p(CM),
+                            self.nthreads)
+        return CM
+
+    def rhs(self, tempk):
+        r = np.zeros(self.nibz * self.ndyn * 3)
+        lib().orc_rhs(self.h, C.c_double(tempk), _p(r))
+        return r
+
+    def cg(self, A, b, x0, max_iter=100, ndig=2):
+        A = np.asfortranarray(A, dtype=float)
+        x = np.array(x0, dtype=float)
+        fmin = C.c_double(0)
+        it = lib().orc_cg(A.shape[0], _p(A), _p(np.ascontiguousarray(b, dtype=float)), _p(x), C.byref(fmin),
+                          max_iter, ndig, self.nthreads)
+        return x, fmin.value, it
+
+    def kappa_d(self, tempk, x):
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        e = lib().orc_kappa_d(self.h, C.c_double(tempk), _p(np.ascontiguousarray(x, dtype=float)), _p(kap))
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return kap
+
+
+def weight_tet(w, e):
+    c = np.zeros(4)
+    w = np.ascontiguousarray(w, dtype=float)
+    lib().orc_weight_tet(_p(w), C.c_double(e), _p(c))
+    return c
+
+
+def weight_tet_nonperm() -> int:
+    return int(lib().orc_weight_tet_nonperm())
+
+
+def run_job1(d: str, tempk=None, gauss=None, k1=1, k2=None, phonons=None, nthreads=0):
+    """The whole job=1 sequence of kappa.f90:389-871 on the oracle.
+
+    Returns a dict with every intermediate array.  `phonons` =
+    (eigenval, eigenvec, veloc) injects eigenpairs in place of the oracle's
+    own eigensolver.  `gauss` switches the delta to the Gaussian extension.
+    """
+    O = Oracle(d, nthreads)
+    O.mesh()
+    if phonons is None:
+        O.phonons()
+    else:
+        O.set_phonons(*phonons)
+    O.tet()
+    k2 = k2 or O.nibz
+    if tempk is None:
+        tempk = float(open(os.path.join(d, "latdyn.params")).read().split("\n")[6].split()[0])
+    if gauss is None:
+        gauss = False
+        bp = os.path.join(d, "b200.params")
+        if os.path.exists(bp):
+            gauss = "delta gauss" in open(bp).read()
+    v33 = O.v3(k1, k2)
+    P1s, P2s = O.fgr(k1, k2, v33, gauss=gauss)
+    freq, dist = O.distribution(tempk)
+    Q, QN, QU, P1, P2 = O.tau(k1, k2, tempk, P1s, P2s)
+    out = {"O": O, "v33": v33, "P1s": P1s, "P2s": P2s, "freq": freq, "dist": dist, "Q": Q, "QN": QN, "QU": QU,
+           "P1": P1, "P2": P2, "tempk": tempk}
+    if k1 == 1 and k2 == O.nibz:
+        FFF, krta = O.rta(tempk, Q)
+        CM = O.collision(k1, k2, P1, P2)
+        RHS = O.rhs(tempk)
+        x0 = np.array([FFF[i, j, k] for i in range(O.nibz) for j in range(O.ndyn) for k in range(3)])
+        x, fmin, it = O.cg(CM, RHS, x0)
+        kd = O.kappa_d(tempk, x)
+        out.update({"FFF": FFF, "kappa_rta": krta, "CM": CM, "RHS": RHS, "x0": x0, "x": x, "cg_iters": it,
+                    "kappa_cg": kd})
+    return out
