@@ -1,0 +1,397 @@
+// Boltzmann-equation stage on the device.
+//
+//   calculate_RTA_distributionfunction  THERMACOND/sub.f90:1238-1289
+//   mode_kappa / mode_kappa_d           THERMACOND/sub.f90:1292-1401, 1407-1530
+//   veloc_avergeIBZ_invsyFBZ            THERMACOND/sub.f90:5479-5537
+//   cal_RHS_IBZ                         THERMACOND/sub.f90:2618-2691
+//   CollisionMatrix_mpi                 THERMACOND/sub.f90:3034-3210
+//   cg_quadratic                        THERMACOND/cg.f90:19-61
+//
+// Vectors indexed like the reference's DirectSolution / RHS:
+// s = 3*((ibz)*ndyn + l) + xyz (0-based).  The collision matrix is kept
+// row-major on the device (row s1 contiguous) so that the CG matrix-vector
+// product reads each row with coalesced loads; HBM bandwidth bounds it.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <vector>
+
+#include "ald_internal.h"
+
+namespace ald {
+
+namespace {
+
+__device__ __forceinline__ int wrapm(int v, int n) {
+  v %= n;
+  return v < 0 ? v + n : v;
+}
+__device__ __forceinline__ void decompose(const Geometry& g, int n, int* m) {
+  m[0] = n / (g.nc[1] * g.nc[2]);
+  m[1] = (n / g.nc[2]) % g.nc[1];
+  m[2] = n % g.nc[2];
+}
+__device__ __forceinline__ int compose(const Geometry& g, const int* m) { return m[2] + g.nc[2] * (m[1] + g.nc[1] * m[0]); }
+
+__device__ __forceinline__ double nbe_dev(double w, double t, int m, int* err) {
+  if (t <= 0 || w <= 0) {
+    atomicOr(err, 1);
+    return 0.0;
+  }
+  double z = w / t;
+  if (m == 0) {
+    if (z > 60) return 0.0;
+    if (z < (double)0.0010f) return 1 / (z * (1 + z / 2 * (1 + z / 3)));
+    return 1 / (exp(z) - 1);
+  }
+  return 1 / z;
+}
+
+__device__ __forceinline__ void opmul(const double* op, const double* v, double* out) {  // column-major 3x3
+  for (int i = 0; i < 3; ++i) {
+    double x = 0;
+    for (int j = 0; j < 3; ++j) x = x + op[i + 3 * j] * v[j];
+    out[i] = x;
+  }
+}
+
+__global__ void rta_F_kernel(KappaArgs a, const double* Q, double* F) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = a.geo.b;
+  if (idx >= a.nibz * b) return;
+  int i = idx / b, l = idx % b;
+  int n0 = a.mapinv[i];
+  double omega = a.freq[(size_t)n0 * b + l], nb = a.dist[(size_t)n0 * b + l];
+  const double c = PhysConst::c_light, h = PhysConst::h_plank, kb = PhysConst::k_b;
+  for (int x = 0; x < 3; ++x) {
+    double v = a.vel[((size_t)n0 * b + l) * 3 + x];
+    F[(size_t)idx * 3 + x] = -((((((c * v) * h) * ((omega * c) * 100)) * nb) * (nb + 1)) / (kb * (a.tempk * a.tempk)) /
+                               ((Q[idx] * c) * 100));
+  }
+}
+
+__global__ void rhs_kernel(KappaArgs a, double* rhs) {
+  int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  int b = a.geo.b;
+  if (idx >= a.nibz * b) return;
+  int i = idx / b, l = idx % b;
+  int n0 = a.mapinv[i];
+  double omega = a.freq[(size_t)n0 * b + l], nb0 = a.dist[(size_t)n0 * b + l];
+  const double c = PhysConst::c_light, h = PhysConst::h_plank, kb = PhysConst::k_b;
+  for (int x = 0; x < 3; ++x) {
+    double v = a.vel[((size_t)n0 * b + l) * 3 + x];
+    rhs[(size_t)idx * 3 + x] =
+        ((((((c * v) * h) * ((omega * c) * 100)) * nb0) * (nb0 + 1)) / (kb * (a.tempk * a.tempk))) / (c * 100);
+  }
+}
+
+// one CTA per band l; threads over IBZ points; 9 sums reduced in the block
+__global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double* kappa_modes, int* err) {
+  __shared__ double red[9][32];
+  const int b = a.geo.b, l = blockIdx.x;
+  double acc[9];
+  for (int k = 0; k < 9; ++k) acc[k] = 0.0;
+  for (int i = threadIdx.x; i < a.nibz; i += blockDim.x) {
+    double f[3] = {F[((size_t)i * b + l) * 3], F[((size_t)i * b + l) * 3 + 1], F[((size_t)i * b + l) * 3 + 2]};
+    double vv[3];
+    if (averaged) {
+      // star average with inverse operations (veloc_avergeIBZ_invsyFBZ)
+      int s0 = a.star_off[i], s1 = a.star_off[i + 1];
+      double narms = (double)(s1 - s0);
+      double va[3] = {0, 0, 0};
+      for (int s = s0; s < s1; ++s) {
+        const double* vq = a.vel + ((size_t)a.star_q[s] * b + l) * 3;
+        double vin[3] = {vq[0], vq[1], vq[2]}, vr[3];
+        opmul(a.opk_inv + 9 * a.star_op[s], vin, vr);
+        for (int x = 0; x < 3; ++x) va[x] = va[x] + (vr[x] / narms);
+      }
+      for (int x = 0; x < 3; ++x) vv[x] = va[x];
+    } else {
+      const double* vq = a.vel + ((size_t)a.mapinv[i] * b + l) * 3;
+      vv[0] = vq[0];
+      vv[1] = vq[1];
+      vv[2] = vq[2];
+    }
+    for (int s = a.arm_off[i]; s < a.arm_off[i + 1]; ++s) {
+      const double* op = a.opk + 9 * a.arm_op[s];
+      double F12[3], velocc[3];
+      opmul(op, f, F12);
+      opmul(op, vv, velocc);
+      int n0 = a.arm_q[s];
+      double omega = sqrt(a.w2[(size_t)n0 * b + l]) * PhysConst::cnst();
+      double nb0 = nbe_dev(omega, a.temp, a.classical, err);
+      for (int j = 0; j < 3; ++j)
+        for (int jj = 0; jj < 3; ++jj)
+          acc[j + 3 * jj] -= ((((a.const1 * omega) * velocc[j]) * nb0) * (nb0 + 1)) * F12[jj];
+    }
+  }
+  for (int k = 0; k < 9; ++k) {
+    double v = acc[k];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 9) {
+    double s = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
+    int j = threadIdx.x % 3, jj = threadIdx.x / 3;
+    kappa_modes[l + b * (j + 3 * jj)] = s;  // kappa(ndyn,3,3) column-major
+  }
+}
+
+// collision matrix: thread per (row group (n1,l1), column group (n2,l2))
+__global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* mapinv, const int* arm_off,
+                                 const int* arm_q, const int* arm_op, const double* opk, const double* Q,
+                                 const double* R1, const double* R2, double* CM, int ld) {
+  const int b = g.b, nkc = g.nkc;
+  int col = blockIdx.x * blockDim.x + threadIdx.x;  // n2*b + l2
+  if (col >= nibz * b) return;
+  int rowg = blockIdx.y;                             // local row group: nl*b + l1
+  int n1 = n1_first + rowg / b, l1 = rowg % b;
+  int n2 = col / b, l2 = col % b;
+  int q1 = mapinv[n1];
+  int m1[3];
+  decompose(g, q1, m1);
+  double blk[9];
+  for (int k = 0; k < 9; ++k) blk[k] = 0.0;
+  for (int s = arm_off[n2]; s < arm_off[n2 + 1]; ++s) {
+    int n0 = arm_q[s];
+    double C;
+    if (n0 == q1 && l1 == l2) {
+      C = -Q[(size_t)(rowg / b) * b + l1];
+    } else {
+      int m0[3], mp1[3], mp2[3];
+      decompose(g, n0, m0);
+      for (int a = 0; a < 3; ++a) {
+        int sh = g.shifted ? g.nc[a] / 2 : 0;
+        mp1[a] = wrapm(m1[a] - m0[a] + sh, g.nc[a]);  // q1 - arm
+        mp2[a] = wrapm(m0[a] - m1[a] + sh, g.nc[a]);  // arm - q1
+      }
+      int nk3_p1 = compose(g, mp1), nk3_p2 = compose(g, mp2);
+      size_t base = (size_t)(rowg / b) * nkc;  // R arrays are local to the row range
+      C = -R1[((base + n0) * b + l1) * b + l2] + R1[((base + nk3_p2) * b + l1) * b + l2] +
+          0.5 * R2[((base + n0) * b + l1) * b + l2] + 0.5 * R2[((base + nk3_p1) * b + l1) * b + l2];
+    }
+    const double* op = opk + 9 * arm_op[s];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) blk[i + 3 * j] = blk[i + 3 * j] + (C * op[i + 3 * j]);
+  }
+  size_t r0 = 3 * ((size_t)rowg);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + 3 * (size_t)col + j] = blk[i + 3 * j];
+}
+
+// ---------------------------------------------------------------- CG
+constexpr int kGemvWarps = 8;
+constexpr int kVecThreads = 1024;
+
+struct CgDev {
+  double num, den, err;
+  int done, iters;
+  double bnorm;
+};
+
+// y = A x (row-major), partial[blk] = sum over the block's rows of y*x
+__global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, const double* __restrict__ A,
+                                                               const double* __restrict__ x, double* __restrict__ y,
+                                                               double* partial, const CgDev* st) {
+  if (st && st->done) return;
+  __shared__ double wsum[kGemvWarps];
+  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int row = blockIdx.x * kGemvWarps + warp;
+  double dot = 0.0;
+  if (row < n) {
+    const double* Ar = A + (size_t)row * n;
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    int j = lane;
+    for (; j + 96 < n; j += 128) {
+      s0 += Ar[j] * x[j];
+      s1 += Ar[j + 32] * x[j + 32];
+      s2 += Ar[j + 64] * x[j + 64];
+      s3 += Ar[j + 96] * x[j + 96];
+    }
+    for (; j < n; j += 32) s0 += Ar[j] * x[j];
+    double s = (s0 + s1) + (s2 + s3);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) {
+      y[row] = s;
+      dot = s * x[row];
+    }
+  }
+  if (lane == 0) wsum[warp] = dot;
+  __syncthreads();
+  if (threadIdx.x == 0 && partial) {
+    double t = 0;
+    for (int w = 0; w < kGemvWarps; ++w) t += wsum[w];
+    partial[blockIdx.x] = t;
+  }
+}
+
+__device__ double vblock_sum(double v) {
+  __shared__ double red[kVecThreads / 32];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = v;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double t = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_down_sync(0xffffffffu, t, o);
+    if (threadIdx.x == 0) red[0] = t;
+  }
+  __syncthreads();
+  double r = red[0];
+  __syncthreads();
+  return r;
+}
+
+// grad = A x - b ; conj = -grad  (y holds A x)
+__global__ void cg_init_kernel(int n, const double* y, const double* b, double* grad, double* conj, CgDev* st) {
+  double bb = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double gr = y[i] - b[i];
+    grad[i] = gr;
+    conj[i] = -gr;
+    bb += b[i] * b[i];
+  }
+  bb = vblock_sum(bb);
+  if (threadIdx.x == 0) {
+    st->done = 0;
+    st->iters = 0;
+    st->err = 9999;
+    st->bnorm = sqrt(bb);
+  }
+}
+
+// one CG update after aux = A conj (cg.f90:37-55)
+__global__ void cg_step_kernel(int n, const double* aux, const double* partial, int nparts, double* grad,
+                               double* conj, double* v0, double* x, CgDev* st, int mode, double tol) {
+  if (st->done) return;
+  double num = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) num += grad[i] * conj[i];
+  num = vblock_sum(num);
+  double den = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) den += partial[i];
+  den = vblock_sum(den);
+  double alpha = num / den;
+  double v2 = 0, cc = 0, gg = 0, g2 = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    double gi = grad[i];
+    v0[i] = gi;
+    double xi = x[i] - alpha * conj[i];
+    x[i] = xi;
+    double gn = gi - alpha * aux[i];
+    grad[i] = gn;
+    v2 += xi * xi;
+    cc += conj[i] * conj[i];
+    gg += gn * gn;
+    g2 += gi * gi;
+  }
+  v2 = vblock_sum(v2);
+  cc = vblock_sum(cc);
+  gg = vblock_sum(gg);
+  g2 = vblock_sum(g2);
+  double err = mode == ALD_CG_REFERENCE ? (num * num / den / den) * cc / v2 : sqrt(gg) / st->bnorm;
+  bool stop = err < tol;
+  if (!stop) {
+    double beta = gg / g2;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) conj[i] = -grad[i] + beta * conj[i];
+  }
+  if (threadIdx.x == 0) {
+    st->iters += 1;
+    st->err = err;
+    if (stop) st->done = 1;
+  }
+}
+
+__global__ void cg_fmin_kernel(int n, const double* x, const double* Ax, const double* b, double* out) {
+  double s1 = 0, s2 = 0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    s1 += x[i] * Ax[i];
+    s2 += x[i] * b[i];
+  }
+  s1 = vblock_sum(s1);
+  s2 = vblock_sum(s2);
+  if (threadIdx.x == 0) *out = 0.5 * s1 - s2;
+}
+
+}  // namespace
+
+cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaStream_t s) {
+  int n = a.nibz * a.geo.b;
+  rta_F_kernel<<<(n + 255) / 256, 256, 0, s>>>(a, Q, FFF);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
+                         cudaStream_t s) {
+  kappa_kernel<<<a.geo.b, 256, 0, s>>>(a, F, averaged, kappa_modes, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s) {
+  int n = a.nibz * a.geo.b;
+  rhs_kernel<<<(n + 255) / 256, 256, 0, s>>>(a, rhs);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
+                             const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
+                             const double* Q, const double* R1, const double* R2, double* CM, int ld,
+                             cudaStream_t s) {
+  int ncolg = nibz * geo.b;
+  dim3 grid((ncolg + 127) / 128, nrows * geo.b);
+  collision_kernel<<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2, CM,
+                                         ld);
+  return cudaGetLastError();
+}
+
+// Conjugate gradients of cg_quadratic on a device matrix.  The max_iter
+// iterations are captured once into a CUDA graph; a device flag turns the
+// remaining launches into no-ops after the stop rule fires.
+int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
+              double* err_out, double* funcmin, cudaStream_t s, std::string& msg) {
+  int nblk = (n + kGemvWarps - 1) / kGemvWarps;
+  DevBuf<double> grad, conj, aux, v0, partial, fmin;
+  DevBuf<CgDev> st;
+  if (grad.alloc(n) || conj.alloc(n) || aux.alloc(n) || v0.alloc(n) || partial.alloc(nblk) || fmin.alloc(1) ||
+      st.alloc(1)) {
+    msg = "cg: device allocation failed";
+    return ALD_ERR_NOMEM;
+  }
+  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, aux.p, nullptr, nullptr);
+  cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, aux.p, db, grad.p, conj.p, st.p);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    for (int it = 0; it < max_iter; ++it) {
+      gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, conj.p, aux.p, partial.p, st.p);
+      cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, aux.p, partial.p, nblk, grad.p, conj.p, v0.p, dx, st.p, mode, tol);
+    }
+    e = cudaStreamEndCapture(s, &graph);
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (e != cudaSuccess) {
+    msg = std::string("cg: ") + cudaGetErrorString(e);
+    return ALD_ERR_CUDA;
+  }
+  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, aux.p, nullptr, nullptr);
+  cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, aux.p, db, fmin.p);
+  CgDev h;
+  e = cudaMemcpyAsync(&h, st.p, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(funcmin, fmin.p, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    msg = std::string("cg: ") + cudaGetErrorString(e);
+    return ALD_ERR_CUDA;
+  }
+  *iters = h.iters;
+  *err_out = h.err;
+  return h.done ? ALD_OK : ALD_WARN_CG_MAXITER;
+}
+
+}  // namespace ald

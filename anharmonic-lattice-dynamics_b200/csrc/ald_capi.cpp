@@ -1,0 +1,709 @@
+// C ABI of libald (include/ald.h): context lifecycle, the per-stage entry
+// points that stand in for THERMACOND's job=1 subroutines, and the fused
+// device pipeline.  All compute runs in CUDA kernels on the context's
+// stream; host code only parses inputs, builds index tables and moves
+// buffers across the boundary.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <string>
+
+#include "ald_internal.h"
+
+using namespace ald;
+
+#include "ald_ctx.h"
+
+
+namespace ald {
+namespace capi {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(call)                                                                        \
+  do {                                                                                  \
+    cudaError_t _e = (call);                                                            \
+    if (_e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
+  } while (0)
+#define CKA(call)                                                                       \
+  do {                                                                                  \
+    cudaError_t _e = (call);                                                            \
+    if (_e == cudaErrorMemoryAllocation) return fail(ALD_ERR_NOMEM, "device allocation failed: " #call); \
+    if (_e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e)); \
+  } while (0)
+
+double g_h2d = 0;  // bytes uploaded by the create call in progress
+
+template <class T>
+cudaError_t upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
+  cudaError_t e = d.alloc(std::max<size_t>(h.size(), 1));
+  if (e != cudaSuccess) return e;
+  if (h.empty()) return cudaSuccess;
+  g_h2d += (double)h.size() * sizeof(T);
+  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+double temp_cm(double tempk) {
+  return tempk * PhysConst::k_b / (100 * PhysConst::h_plank * PhysConst::c_light);
+}
+
+int check_err_flags(ald_ctx* c) {
+  int h = 0;
+  CK(cudaMemcpyAsync(&h, c->err.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (h) {
+    CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    if (h & 2) return fail(ALD_ERR_DEN_ZERO, "MATRIX_ELT: den=0 (an eigenvalue is exactly zero)");
+    if (h & 1) return fail(ALD_ERR_NBE, "ERROR in N_BE: w=<0 or t=<0");
+  }
+  return ALD_OK;
+}
+
+int ensure_phonons(ald_ctx* c) {
+  if (c->have_phonons) return ALD_OK;
+  const int b = c->geo.b, nkc = c->geo.nkc;
+  if (b > 64) return fail(ALD_ERR_UNSUPPORTED, "eigensolver: more than 64 bands is not supported by this build");
+  CKA(c->w2_all.alloc((size_t)nkc * 7 * b));
+  CKA(c->w2.alloc((size_t)nkc * b));
+  CKA(c->evec.alloc((size_t)nkc * b * b * 2));
+  CKA(c->vel.alloc((size_t)nkc * b * 3));
+  PhononArgs a;
+  a.geo = c->geo;
+  a.kpc32 = c->kpc32.p;
+  a.g = nullptr;
+  a.fc2_off = c->fc2_off.p;
+  a.fc2_atom = c->fc2_atom.p;
+  a.fc2_val = c->fc2_val.p;
+  a.fc2_sqm = c->fc2_sqm.p;
+  a.rr = c->rr.p;
+  a.born_flag = c->S.born_flag;
+  a.born = c->born.p;
+  a.dq = (double)0.001f;  // finitedif_vel: dq=0.001 is a default-REAL literal
+  a.w2_all = c->w2_all.p;
+  a.w2 = c->w2.p;
+  a.evec = c->evec.p;
+  a.err = c->err.p;
+  CK(launch_phonons(a, c->stream));
+  CK(launch_phonon_post(c->geo, c->w2_all.p, a.dq, PhysConst::cnst(), c->vel.p, c->stream));
+  CK(launch_subst_eivecs(c->geo, c->neg_src.p, c->neg_dst.p, (int)c->T.neg_src.size(), c->evec.p, c->stream));
+  c->have_phonons = true;
+  c->dist_tempk = -1;
+  return ALD_OK;
+}
+
+int ensure_dist(ald_ctx* c, double tempk) {
+  if (c->dist_tempk == tempk) return ALD_OK;
+  const size_t n = (size_t)c->geo.nkc * c->geo.b;
+  CKA(c->freq.alloc(n));
+  CKA(c->dist.alloc(n));
+  CK(launch_freq_dist(c->geo, c->w2.p, PhysConst::cnst(), temp_cm(tempk), c->S.classical, c->freq.p, c->dist.p,
+                      c->err.p, c->stream));
+  int r = check_err_flags(c);
+  if (r) return r;
+  c->dist_tempk = tempk;
+  return ALD_OK;
+}
+
+bool ksub_ok(ald_ctx* c, const int* k) { return k && k[0] >= 1 && k[1] >= k[0] && k[1] <= c->T.nibz; }
+
+V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
+  V3Args a;
+  a.geo = c->geo;
+  a.n1_first = first;
+  a.nrows = nrows;
+  a.mapinv = c->mapinv.p;
+  a.evec = c->evec.p;
+  a.w2 = c->w2.p;
+  a.ntrip = c->F3.ntrip;
+  a.natoms = c->S.natoms;
+  a.blk_off = c->blk_off.p;
+  a.trip_j = c->trip_j.p;
+  a.trip_k = c->trip_k.p;
+  a.fc3w = c->fc3w.p;
+  a.phase_coef = c->phase_coef.p;
+  a.roots = c->roots.p;
+  a.const33 = PhysConst::const33();
+  a.v3sq = out;
+  a.err = c->err.p;
+  return a;
+}
+
+int run_v3(ald_ctx* c, const V3Args& a) {
+  if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
+  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "V3: more than 12 bands is not supported by this build");
+  cudaError_t e = (c->opt.precision == ALD_MIXED) ? launch_v3_mixed(a, c->stream) : launch_v3_fp64(a, c->stream);
+  if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 launch: ") + cudaGetErrorString(e));
+  return ALD_OK;
+}
+
+KappaArgs kappa_args(ald_ctx* c, double tempk) {
+  KappaArgs k;
+  k.geo = c->geo;
+  k.nibz = c->T.nibz;
+  k.mapinv = c->mapinv.p;
+  k.freq = c->freq.p;
+  k.dist = c->dist.p;
+  k.vel = c->vel.p;
+  k.w2 = c->w2.p;
+  k.arm_off = c->arm_off.p;
+  k.arm_q = c->arm_q.p;
+  k.arm_op = c->arm_op.p;
+  k.star_off = c->star_off.p;
+  k.star_q = c->star_q.p;
+  k.star_op = c->star_op.p;
+  k.opk = c->opk.p;
+  k.opk_inv = c->opk_inv.p;
+  k.tempk = tempk;
+  k.temp = temp_cm(tempk);
+  k.const1 = PhysConst::h_plank * PhysConst::c_light * 100 * PhysConst::c_light /
+             (c->T.nkc * c->S.volume_r / 1e30);
+  k.classical = c->S.classical;
+  return k;
+}
+
+int delta_mode(ald_ctx* c) { return c->opt.delta; }
+double gauss_width(ald_ctx* c) { return c->opt.width_cm > 0 ? c->opt.width_cm : c->S.width; }
+
+// |V3|^2 rows per chunk within the byte budget
+int rows_per_chunk(ald_ctx* c) {
+  size_t per_row = (size_t)c->T.nkc * c->geo.b * c->geo.b * c->geo.b * sizeof(double);
+  size_t budget = c->opt.chunk_bytes ? c->opt.chunk_bytes : (size_t)512 << 20;
+  return (int)std::max<size_t>(1, std::min<size_t>(budget / per_row, (size_t)c->T.nibz));
+}
+
+}  // namespace capi
+}  // namespace ald
+
+using namespace ald::capi;
+
+// =====================================================================
+extern "C" {
+
+void ald_default_options(ald_options* o) {
+  std::memset(o, 0, sizeof *o);
+  o->delta = ALD_DELTA_TETRA;
+  o->precision = ALD_FP64;
+  o->cg_stop = ALD_CG_REFERENCE;
+  o->cg_max_iter = 100;
+  o->cg_ndig = 2;
+  o->cg_tol = 1e-8;
+  o->width_cm = -1;
+  o->device = 0;
+  o->chunk_bytes = 0;
+}
+
+const char* ald_last_error(void) { return g_err.c_str(); }
+
+int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) {
+  if (!dir || !out) return fail(ALD_ERR_ARG, "null argument");
+  *out = nullptr;
+  std::unique_ptr<ald_ctx> c(new ald_ctx());
+  if (opt) c->opt = *opt;
+  else ald_default_options(&c->opt);
+  std::string e = read_system(dir, c->S);
+  if (!e.empty()) return fail(ALD_ERR_IO, e);
+  // b200.params knobs apply where the caller left the defaults
+  if (!opt) {
+    if (c->S.delta >= 0) c->opt.delta = c->S.delta;
+    if (c->S.precision >= 0) c->opt.precision = c->S.precision;
+    if (c->S.cg_stop >= 0) c->opt.cg_stop = c->S.cg_stop;
+    if (c->S.cg_tol > 0) c->opt.cg_tol = c->S.cg_tol;
+    if (c->S.width_cm > 0) c->opt.width_cm = c->S.width_cm;
+  }
+  e = build_tables(c->S, c->T);
+  if (!e.empty()) return fail(e.find("not a kpoint") != std::string::npos ? ALD_ERR_NOT_KPOINT : ALD_ERR_IO, e);
+  if (c->S.include_fc[2] == 1) {
+    e = build_fc3(c->S, c->F3);
+    if (!e.empty()) return fail(ALD_ERR_IO, e);
+  }
+  e = build_fc2(c->S, c->F2);
+  if (!e.empty()) return fail(ALD_ERR_IO, e);
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return fail(ALD_ERR_CUDA, "no CUDA device");
+  c->device = c->opt.device;
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+  c->stream = c->own_stream;
+  Geometry& g = c->geo;
+  for (int a = 0; a < 3; ++a) g.nc[a] = c->S.nc[a];
+  g.nkc = c->T.nkc;
+  g.b = c->T.b;
+  g.nat0 = c->S.nat0;
+  g.shifted = c->T.shifted ? 1 : 0;
+  g.L = c->T.L;
+  cudaStream_t s = c->stream;
+  g_h2d = 0;
+  // tables
+  CKA(upload(c->kpc32, c->T.kpc32, s));
+  std::vector<double> rr(3 * (size_t)c->S.natoms);
+  for (int j = 0; j < c->S.natoms; ++j) {
+    int j0 = c->S.cell0[j] - 1;
+    for (int x = 0; x < 3; ++x) rr[3 * j + x] = c->S.atompos[3 * j + x] - c->S.atompos[3 * j0 + x];
+  }
+  CKA(upload(c->rr, rr, s));
+  CKA(upload(c->fc2_off, c->F2.off, s));
+  CKA(upload(c->fc2_atom, c->F2.atom, s));
+  CKA(upload(c->fc2_val, c->F2.val, s));
+  CKA(upload(c->fc2_sqm, c->F2.sqm, s));
+  {
+    // epsil(9), charge(9*nat0), masses(nat0), eps_scale, rho2, om0
+    std::vector<double> bo(9 + 10 * c->S.nat0 + 4, 0.0);
+    std::memcpy(bo.data(), c->S.epsil, 9 * sizeof(double));
+    std::copy(c->S.charge.begin(), c->S.charge.end(), bo.begin() + 9);
+    std::copy(c->S.mass0.begin(), c->S.mass0.end(), bo.begin() + 9 + 9 * c->S.nat0);
+    auto len = [](const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); };
+    double gg = std::pow(len(c->S.g[0]) * len(c->S.g[1]) * len(c->S.g[2]), (double)0.33f);
+    double rho = gg / 4.0;
+    double* sc = bo.data() + 9 + 10 * c->S.nat0;
+    sc[0] = 8.8541878176e-12 / 1e10 / PhysConst::ee;
+    sc[1] = rho * rho;
+    sc[2] = c->S.volume_r;
+    CKA(upload(c->born, bo, s));
+  }
+  if (c->S.include_fc[2] == 1) {
+    CKA(upload(c->blk_off, c->F3.blk_off, s));
+    CKA(upload(c->trip_j, c->F3.trip_j, s));
+    CKA(upload(c->trip_k, c->F3.trip_k, s));
+    CKA(upload(c->fc3w, c->F3.w, s));
+  }
+  {
+    std::vector<double> rt(2 * (size_t)c->T.L);
+    for (int t = 0; t < c->T.L; ++t) {
+      double ang = 2.0 * PhysConst::pi * (double)t / (double)c->T.L;
+      rt[2 * t] = std::cos(ang);
+      rt[2 * t + 1] = std::sin(ang);
+    }
+    // exact values on the axes
+    for (int t = 0; t < c->T.L; ++t) {
+      if ((4L * t) % c->T.L == 0) {
+        long k = (4L * t) / c->T.L;
+        rt[2 * t] = k == 0 ? 1.0 : (k == 2 ? -1.0 : 0.0);
+        rt[2 * t + 1] = k == 1 ? 1.0 : (k == 3 ? -1.0 : 0.0);
+      }
+    }
+    CKA(upload(c->roots, rt, s));
+  }
+  CKA(upload(c->phase_coef, c->T.phase_coef, s));
+  std::vector<int> mi(c->T.nibz);
+  for (int i = 0; i < c->T.nibz; ++i) mi[i] = c->T.mapinv[i] - 1;
+  CKA(upload(c->mapinv, mi, s));
+  CKA(upload(c->neg_src, c->T.neg_src, s));
+  CKA(upload(c->neg_dst, c->T.neg_dst, s));
+  CKA(upload(c->arm_off, c->T.arm_off, s));
+  CKA(upload(c->arm_q, c->T.arm_q, s));
+  CKA(upload(c->arm_op, c->T.arm_op, s));
+  CKA(upload(c->star_off, c->T.star_off, s));
+  CKA(upload(c->star_q, c->T.star_q, s));
+  CKA(upload(c->star_op, c->T.star_op, s));
+  CKA(upload(c->tet_corner, c->T.tet_corner, s));
+  CKA(upload(c->tet_inc, c->T.tet_inc, s));
+  {
+    std::vector<double> op(48 * 9, 0.0), opi(48 * 9, 0.0);
+    for (int o = 0; o < c->T.npg; ++o) {
+      const double* m = c->T.opk[o];
+      std::memcpy(&op[9 * o], m, 9 * sizeof(double));
+      // exact inverse of an integer matrix with |det| = 1
+      auto M = [&](int i, int j) { return m[i + 3 * j]; };
+      double det = M(0, 0) * (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1)) - M(0, 1) * (M(1, 0) * M(2, 2) - M(1, 2) * M(2, 0)) +
+                   M(0, 2) * (M(1, 0) * M(2, 1) - M(1, 1) * M(2, 0));
+      double* r = &opi[9 * o];
+      r[0 + 3 * 0] = (M(1, 1) * M(2, 2) - M(1, 2) * M(2, 1)) / det;
+      r[0 + 3 * 1] = (M(0, 2) * M(2, 1) - M(0, 1) * M(2, 2)) / det;
+      r[0 + 3 * 2] = (M(0, 1) * M(1, 2) - M(0, 2) * M(1, 1)) / det;
+      r[1 + 3 * 0] = (M(1, 2) * M(2, 0) - M(1, 0) * M(2, 2)) / det;
+      r[1 + 3 * 1] = (M(0, 0) * M(2, 2) - M(0, 2) * M(2, 0)) / det;
+      r[1 + 3 * 2] = (M(0, 2) * M(1, 0) - M(0, 0) * M(1, 2)) / det;
+      r[2 + 3 * 0] = (M(1, 0) * M(2, 1) - M(1, 1) * M(2, 0)) / det;
+      r[2 + 3 * 1] = (M(0, 1) * M(2, 0) - M(0, 0) * M(2, 1)) / det;
+      r[2 + 3 * 2] = (M(0, 0) * M(1, 1) - M(0, 1) * M(1, 0)) / det;
+    }
+    CKA(upload(c->opk, op, s));
+    CKA(upload(c->opk_inv, opi, s));
+  }
+  CKA(c->err.alloc(4));
+  CK(cudaMemsetAsync(c->err.p, 0, 4 * sizeof(int), s));
+  CK(cudaStreamSynchronize(s));
+  c->h2d_bytes = g_h2d;
+  *out = c.release();
+  return ALD_OK;
+}
+
+void ald_destroy(ald_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+int ald_set_stream(ald_ctx* c, void* stream) {
+  if (!c) return fail(ALD_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  CK(cudaStreamSynchronize(c->stream));
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return ALD_OK;
+}
+
+double ald_h2d_bytes(ald_ctx* c) { return c ? c->h2d_bytes : 0.0; }
+
+int ald_get_info(ald_ctx* c, ald_info* info) {
+  if (!c || !info) return fail(ALD_ERR_ARG, "null argument");
+  info->ndyn = c->geo.b;
+  info->natoms0 = c->S.nat0;
+  for (int a = 0; a < 3; ++a) info->nc[a] = c->S.nc[a];
+  info->nkc = c->T.nkc;
+  info->nibz = c->T.nibz;
+  info->nterms2 = c->S.nterms[1];
+  info->nterms3 = c->S.nterms[2];
+  info->natoms = c->S.natoms;
+  info->lattpgcount = c->T.npg;
+  info->born_flag = c->S.born_flag;
+  info->tempk = c->S.tmin;
+  info->width_cm = c->S.width;
+  info->volume_r = c->S.volume_r;
+  return ALD_OK;
+}
+
+int ald_read_mesh(const char* dir, ald_info* info, double* kpc, int* mapibz, int* mapinv, double* kibz,
+                  double* wibz) {
+  if (!dir || !info) return fail(ALD_ERR_ARG, "null argument");
+  System S;
+  Tables T;
+  std::string e = read_system(dir, S);
+  if (!e.empty()) return fail(ALD_ERR_IO, e);
+  e = build_tables(S, T);
+  if (!e.empty()) return fail(e.find("not a kpoint") != std::string::npos ? ALD_ERR_NOT_KPOINT : ALD_ERR_IO, e);
+  info->ndyn = T.b;
+  info->natoms0 = S.nat0;
+  for (int a = 0; a < 3; ++a) info->nc[a] = S.nc[a];
+  info->nkc = T.nkc;
+  info->nibz = T.nibz;
+  info->nterms2 = S.nterms[1];
+  info->nterms3 = S.nterms[2];
+  info->natoms = S.natoms;
+  info->lattpgcount = T.npg;
+  info->born_flag = S.born_flag;
+  info->tempk = S.tmin;
+  info->width_cm = S.width;
+  info->volume_r = S.volume_r;
+  if (kpc) std::memcpy(kpc, T.kpc32.data(), T.kpc32.size() * sizeof(double));
+  if (mapibz) std::memcpy(mapibz, T.mapibz.data(), T.mapibz.size() * sizeof(int));
+  if (mapinv) std::memcpy(mapinv, T.mapinv.data(), T.mapinv.size() * sizeof(int));
+  if (kibz) std::memcpy(kibz, T.kibz.data(), T.kibz.size() * sizeof(double));
+  if (wibz) std::memcpy(wibz, T.wibz.data(), T.wibz.size() * sizeof(double));
+  return ALD_OK;
+}
+
+int ald_get_mesh(ald_ctx* c, double* kpc, int* mapibz, int* mapinv, double* kibz, double* wibz) {
+  if (!c) return fail(ALD_ERR_ARG, "null context");
+  if (kpc) std::memcpy(kpc, c->T.kpc32.data(), c->T.kpc32.size() * sizeof(double));
+  if (mapibz) std::memcpy(mapibz, c->T.mapibz.data(), c->T.mapibz.size() * sizeof(int));
+  if (mapinv) std::memcpy(mapinv, c->T.mapinv.data(), c->T.mapinv.size() * sizeof(int));
+  if (kibz) std::memcpy(kibz, c->T.kibz.data(), c->T.kibz.size() * sizeof(double));
+  if (wibz) std::memcpy(wibz, c->T.wibz.data(), c->T.wibz.size() * sizeof(double));
+  return ALD_OK;
+}
+
+int ald_get_frequencies(ald_ctx* c, double* eigenval, double* eigenvec, double* veloc) {
+  if (!c) return fail(ALD_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  c->have_phonons = false;
+  int r = ensure_phonons(c);
+  if (r) return r;
+  const size_t nkc = c->T.nkc, b = c->geo.b;
+  if (eigenval) CK(cudaMemcpyAsync(eigenval, c->w2.p, nkc * b * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (eigenvec)
+    CK(cudaMemcpyAsync(eigenvec, c->evec.p, nkc * b * b * 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (veloc) CK(cudaMemcpyAsync(veloc, c->vel.p, nkc * b * 3 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err_flags(c);
+}
+
+int ald_set_phonons(ald_ctx* c, const double* eigenval, const double* eigenvec, const double* veloc) {
+  if (!c || !eigenval || !eigenvec || !veloc) return fail(ALD_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  const size_t nkc = c->T.nkc, b = c->geo.b;
+  CKA(c->w2.alloc(nkc * b));
+  CKA(c->evec.alloc(nkc * b * b * 2));
+  CKA(c->vel.alloc(nkc * b * 3));
+  CK(cudaMemcpyAsync(c->w2.p, eigenval, nkc * b * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->evec.p, eigenvec, nkc * b * b * 2 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->vel.p, veloc, nkc * b * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->have_phonons = true;
+  c->dist_tempk = -1;
+  return ALD_OK;
+}
+
+int ald_calculate_w3_ibz_split_sq(ald_ctx* c, const int ksubset[2], double* v33s8) {
+  if (!c || !v33s8) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  const int nr = ksubset[1] - ksubset[0] + 1;
+  const size_t n = (size_t)nr * c->T.nkc * c->geo.b * c->geo.b * c->geo.b;
+  DevBuf<double> v, f;
+  CKA(v.alloc(n));
+  CKA(f.alloc(n));
+  r = run_v3(c, v3_args(c, ksubset[0] - 1, nr, v.p));
+  if (r) return r;
+  CK(launch_to_fortran5(v.p, f.p, nr, c->T.nkc, c->geo.b, c->stream));
+  CK(cudaMemcpyAsync(v33s8, f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err_flags(c);
+}
+
+int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, double* P1smpi, double* P2smpi) {
+  if (!c || !v33s8 || !P1smpi || !P2smpi) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "delta stage: more than 12 bands is not supported by this build");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, c->S.tmin);
+  if (r) return r;
+  const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc;
+  const size_t n = (size_t)nr * nkc * b * b * b;
+  DevBuf<double> vf, v, p1, p2, R1, R2;
+  DevBuf<float> scratch;
+  CKA(vf.alloc(n));
+  CKA(v.alloc(n));
+  CKA(p1.alloc(n));
+  CKA(p2.alloc(n));
+  CKA(R1.alloc((size_t)nr * nkc * b * b));
+  CKA(R2.alloc((size_t)nr * nkc * b * b));
+  CKA(scratch.alloc(std::max<size_t>(1, combine_scratch_bytes(c->geo, nr, 0) / sizeof(float))));
+  CK(cudaMemcpyAsync(vf.p, v33s8, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(vf.p, v.p, nr, nkc, b, c->stream));
+  CombineArgs a;
+  a.geo = c->geo;
+  a.n1_first = ksubset[0] - 1;
+  a.nrows = nr;
+  a.mapinv = c->mapinv.p;
+  a.v3sq = v.p;
+  a.freq = c->freq.p;
+  a.dist = c->dist.p;
+  a.tet_corner = c->tet_corner.p;
+  a.tet_inc = c->tet_inc.p;
+  a.gauss = delta_mode(c) == ALD_DELTA_GAUSS;
+  a.sigma = gauss_width(c);
+  a.R1 = R1.p;
+  a.R2 = R2.p;
+  a.P1s = p1.p;
+  a.P2s = p2.p;
+  a.P1 = nullptr;
+  a.P2 = nullptr;
+  CK(launch_combine(a, scratch.p, c->stream));
+  CK(launch_to_fortran5(p1.p, vf.p, nr, nkc, b, c->stream));
+  CK(cudaMemcpyAsync(P1smpi, vf.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  CK(launch_to_fortran5(p2.p, vf.p, nr, nkc, b, c->stream));
+  CK(cudaMemcpyAsync(P2smpi, vf.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err_flags(c);
+}
+
+int ald_distribution(ald_ctx* c, double tempk, double* frequency, double* dist) {
+  if (!c) return fail(ALD_ERR_ARG, "null context");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  const int nkc = c->T.nkc, b = c->geo.b;
+  std::vector<double> f((size_t)nkc * b), d((size_t)nkc * b);
+  CK(cudaMemcpyAsync(f.data(), c->freq.p, f.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(d.data(), c->dist.p, d.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int q = 0; q < nkc; ++q)  // (nkc, ndyn) Fortran layout
+    for (int l = 0; l < b; ++l) {
+      if (frequency) frequency[q + (size_t)nkc * l] = f[(size_t)q * b + l];
+      if (dist) dist[q + (size_t)nkc * l] = d[(size_t)q * b + l];
+    }
+  return ALD_OK;
+}
+
+int ald_calculate_tau_rta(ald_ctx* c, const int ksubset[2], double tempk, const double* P1smpi,
+                          const double* P2smpi, double* Q, double* QN, double* QU, double* P1, double* P2) {
+  if (!c || !P1smpi || !P2smpi || !Q || !QN || !QU) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc;
+  const size_t n = (size_t)nr * nkc * b * b * b;
+  DevBuf<double> tmp, s1, s2, o1, o2, q;
+  CKA(tmp.alloc(n));
+  CKA(s1.alloc(n));
+  CKA(s2.alloc(n));
+  if (P1) CKA(o1.alloc(n));
+  if (P2) CKA(o2.alloc(n));
+  CKA(q.alloc((size_t)3 * nr * b));
+  CK(cudaMemcpyAsync(tmp.p, P1smpi, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, s1.p, nr, nkc, b, c->stream));
+  CK(cudaMemcpyAsync(tmp.p, P2smpi, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, s2.p, nr, nkc, b, c->stream));
+  CK(launch_tau(c->geo, ksubset[0] - 1, nr, c->mapinv.p, s1.p, s2.p, c->dist.p, q.p, q.p + nr * b,
+                q.p + 2 * nr * b, o1.p, o2.p, c->stream));
+  std::vector<double> hq((size_t)3 * nr * b);
+  CK(cudaMemcpyAsync(hq.data(), q.p, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (P1) {
+    CK(launch_to_fortran5(o1.p, tmp.p, nr, nkc, b, c->stream));
+    CK(cudaMemcpyAsync(P1, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  }
+  if (P2) {
+    CK(launch_to_fortran5(o2.p, tmp.p, nr, nkc, b, c->stream));
+    CK(cudaMemcpyAsync(P2, tmp.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  }
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < nr; ++i)  // Q(nk1, ndyn)
+    for (int l = 0; l < b; ++l) {
+      Q[i + (size_t)nr * l] = hq[(size_t)i * b + l];
+      QN[i + (size_t)nr * l] = hq[(size_t)nr * b + (size_t)i * b + l];
+      QU[i + (size_t)nr * l] = hq[(size_t)2 * nr * b + (size_t)i * b + l];
+    }
+  return ALD_OK;
+}
+
+int ald_rta_kappa(ald_ctx* c, double tempk, const double* Q, double* FFF, double* kappa) {
+  if (!c || !Q) return fail(ALD_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  const int nibz = c->T.nibz, b = c->geo.b;
+  std::vector<double> hq((size_t)nibz * b);
+  for (int i = 0; i < nibz; ++i)
+    for (int l = 0; l < b; ++l) hq[(size_t)i * b + l] = Q[i + (size_t)nibz * l];
+  DevBuf<double> dq, dF, dk;
+  CKA(dq.alloc(hq.size()));
+  CKA(dF.alloc(hq.size() * 3));
+  CKA(dk.alloc((size_t)b * 9));
+  CK(cudaMemcpyAsync(dq.p, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  KappaArgs k = kappa_args(c, tempk);
+  CK(launch_rta_F(k, dq.p, dF.p, c->stream));
+  CK(launch_kappa(k, dF.p, 0, dk.p, c->err.p, c->stream));
+  std::vector<double> hF(hq.size() * 3);
+  CK(cudaMemcpyAsync(hF.data(), dF.p, hF.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  if (kappa) CK(cudaMemcpyAsync(kappa, dk.p, (size_t)b * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (FFF)
+    for (int i = 0; i < nibz; ++i)
+      for (int l = 0; l < b; ++l)
+        for (int x = 0; x < 3; ++x) FFF[i + (size_t)nibz * (l + (size_t)b * x)] = hF[((size_t)i * b + l) * 3 + x];
+  return check_err_flags(c);
+}
+
+int ald_collision_matrix(ald_ctx* c, const int ksubset[2], const double* P1, const double* P2, double* CM) {
+  if (!c || !P1 || !P2 || !CM) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  CK(cudaSetDevice(c->device));
+  const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc, nibz = c->T.nibz;
+  const size_t n = (size_t)nr * nkc * b * b * b;
+  DevBuf<double> tmp, p1, p2, R1, R2, Qd, cm, cmt;
+  CKA(tmp.alloc(n));
+  CKA(p1.alloc(n));
+  CKA(p2.alloc(n));
+  CKA(R1.alloc((size_t)nr * nkc * b * b));
+  CKA(R2.alloc((size_t)nr * nkc * b * b));
+  CKA(Qd.alloc((size_t)nr * b));
+  const int rows = 3 * b * nr, cols = 3 * b * nibz;
+  CKA(cm.alloc((size_t)rows * cols));
+  CKA(cmt.alloc((size_t)rows * cols));
+  CK(cudaMemcpyAsync(tmp.p, P1, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, p1.p, nr, nkc, b, c->stream));
+  CK(cudaMemcpyAsync(tmp.p, P2, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, p2.p, nr, nkc, b, c->stream));
+  CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
+  CK(launch_collision(c->geo, nibz, ksubset[0] - 1, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p,
+                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, cols, c->stream));
+  CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
+  CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ALD_OK;
+}
+
+int ald_rhs(ald_ctx* c, double tempk, double* RHS) {
+  if (!c || !RHS) return fail(ALD_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  size_t n = (size_t)c->T.nibz * c->geo.b * 3;
+  DevBuf<double> d;
+  CKA(d.alloc(n));
+  KappaArgs k = kappa_args(c, tempk);
+  CK(launch_rhs(k, d.p, c->stream));
+  CK(cudaMemcpyAsync(RHS, d.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ALD_OK;
+}
+
+int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
+                     int n_dig_accur, int* iters) {
+  if (n <= 0 || !a || !b || !vmin) return fail(ALD_ERR_ARG, "bad argument");
+  cudaStream_t s;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SG {
+    cudaStream_t s;
+    ~SG() { cudaStreamDestroy(s); }
+  } guard{s};
+  DevBuf<double> A, At, db, dx;
+  CKA(A.alloc((size_t)n * n));
+  CKA(At.alloc((size_t)n * n));
+  CKA(db.alloc(n));
+  CKA(dx.alloc(n));
+  CK(cudaMemcpyAsync(A.p, a, (size_t)n * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  // a(n,n) column-major == A^T row-major: transpose to row-major
+  CK(launch_transpose(A.p, At.p, n, n, s));
+  CK(cudaMemcpyAsync(db.p, b, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(dx.p, vmin, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  int it = 0;
+  double err = 0, fm = 0;
+  std::string msg;
+  double tol = 1.0 / std::pow(10.0, 2 * n_dig_accur);
+  int r = cg_device(n, At.p, db.p, dx.p, max_iter, ALD_CG_REFERENCE, tol, &it, &err, &fm, s, msg);
+  if (r != ALD_OK && r != ALD_WARN_CG_MAXITER) return fail(r, msg);
+  CK(cudaMemcpyAsync(vmin, dx.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  if (funcmin) *funcmin = fm;
+  if (iters) *iters = it;
+  return r;
+}
+
+int ald_mode_kappa_d(ald_ctx* c, double tempk, const double* Fi_x, double* kappa) {
+  if (!c || !Fi_x || !kappa) return fail(ALD_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  const int b = c->geo.b;
+  size_t n = (size_t)c->T.nibz * b * 3;
+  DevBuf<double> dF, dk;
+  CKA(dF.alloc(n));
+  CKA(dk.alloc((size_t)b * 9));
+  CK(cudaMemcpyAsync(dF.p, Fi_x, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  KappaArgs k = kappa_args(c, tempk);
+  CK(launch_kappa(k, dF.p, 1, dk.p, c->err.p, c->stream));
+  CK(cudaMemcpyAsync(kappa, dk.p, (size_t)b * 9 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return check_err_flags(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,59 @@
+// The context object behind ald_ctx* and the helpers shared by the C ABI
+// translation units (ald_capi.cpp, ald_pipeline.cpp).
+#pragma once
+#include <string>
+
+#include "ald_internal.h"
+
+using namespace ald;
+
+struct ald_ctx {
+  System S;
+  Tables T;
+  Fc3Blocks F3;
+  Fc2Csr F2;
+  ald_options opt;
+  int device = 0;
+  cudaStream_t stream = nullptr;      // stream the work is issued on
+  cudaStream_t own_stream = nullptr;  // the context's own stream
+  double h2d_bytes = 0;
+  Geometry geo;
+  // device tables
+  DevBuf<double> kpc32, rr, fc2_val, fc2_sqm, born, fc3w, roots, opk, opk_inv;
+  DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,
+      arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
+  // phonons and occupations
+  DevBuf<double> w2_all, w2, evec, vel, freq, dist;
+  bool have_phonons = false;
+  double dist_tempk = -1;
+};
+
+namespace ald {
+namespace capi {
+int fail(int code, const std::string& msg);
+int check_err_flags(ald_ctx* c);
+int ensure_phonons(ald_ctx* c);
+int ensure_dist(ald_ctx* c, double tempk);
+V3Args v3_args(ald_ctx* c, int first, int nrows, double* out);
+int run_v3(ald_ctx* c, const V3Args& a);
+KappaArgs kappa_args(ald_ctx* c, double tempk);
+int delta_mode(ald_ctx* c);
+double gauss_width(ald_ctx* c);
+int rows_per_chunk(ald_ctx* c);
+}  // namespace capi
+}  // namespace ald
+
+#define ALD_CK(call)                                                                            \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e != cudaSuccess)                                                                      \
+      return ald::capi::fail(ALD_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e));   \
+  } while (0)
+#define ALD_CKA(call)                                                                           \
+  do {                                                                                          \
+    cudaError_t _e = (call);                                                                    \
+    if (_e == cudaErrorMemoryAllocation)                                                        \
+      return ald::capi::fail(ALD_ERR_NOMEM, "device allocation failed: " #call);               \
+    if (_e != cudaSuccess)                                                                      \
+      return ald::capi::fail(ALD_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(_e));   \
+  } while (0)

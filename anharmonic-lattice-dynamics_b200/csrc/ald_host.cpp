@@ -1,0 +1,783 @@
+// Host side of libald: input readers, lattice point group, q-mesh, IBZ,
+// star arms and tetrahedra.  Everything here runs once per context; the
+// tables it builds are integer-indexed so the device never searches a
+// mesh by floating-point comparison.
+//
+// Reference routines mirrored (file:line in THERMACOND/):
+//   read_params rest.f90:2-76, read_input_fit rest.f90:78-149,
+//   read_lattice rest.f90:152-289, read_fc234 rest.f90:303-443,
+//   read_born rest.f90:3580-3601,
+//   force_constants_init force_constants.f90:3-186 (point group, op_kmatrix),
+//   dlatmat2 force_constants.f90:1379-1545,
+//   make_kp_reg modules.f90:1721-1784, get_k_info rest.f90:3024-3058,
+//   get_negatives rest.f90:3208-3260, getstar force_constants.f90:1748-1784,
+//   get_weights modules.f90:2006-2160, kstarsinfbz1 sub.f90:5551-5590,
+//   make_kp_reg_tet tetrahedron.f90:2-142.
+#include <algorithm>
+#include <array>
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <numeric>
+#include <unordered_map>
+
+#include "ald_internal.h"
+
+namespace ald {
+
+double PhysConst::const33() {
+  return 1e30 * std::pow(hbar / uma, 1.5) / std::pow(std::sqrt(ee * 1e20 / uma), 1.5) * ee / h_plank / 100 /
+         c_light;
+}
+
+namespace {
+
+// ---------------------------------------------------------------- records
+// Fortran list-directed input: a READ takes values from the next record
+// on, spanning records when a list is longer than one line, and discards
+// what is left of the last record.  Blank/comma separate values; '/' ends.
+class Records {
+ public:
+  bool load(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) return false;
+    std::string l;
+    while (std::getline(f, l)) rec_.push_back(l);
+    return true;
+  }
+  bool next(size_t n, std::vector<std::string>& out) {
+    out.clear();
+    while (out.size() < n) {
+      if (at_ >= rec_.size()) return false;
+      split(rec_[at_++], out, n);
+    }
+    return true;
+  }
+  bool line(std::string& s) {
+    if (at_ >= rec_.size()) return false;
+    s = rec_[at_++];
+    return true;
+  }
+  size_t remaining_nonblank() const {
+    size_t c = 0;
+    std::vector<std::string> t;
+    for (size_t i = at_; i < rec_.size(); ++i) {
+      t.clear();
+      split(rec_[i], t, 1);
+      if (!t.empty()) ++c;
+    }
+    return c;
+  }
+
+ private:
+  static void split(const std::string& l, std::vector<std::string>& out, size_t cap) {
+    std::string tok;
+    auto flush = [&]() {
+      if (!tok.empty() && out.size() < cap) out.push_back(tok);
+      tok.clear();
+    };
+    for (char c : l) {
+      if (c == '/') break;
+      if (c == ' ' || c == '\t' || c == ',' || c == '\r') {
+        flush();
+      } else {
+        tok += c;
+      }
+    }
+    flush();
+  }
+  std::vector<std::string> rec_;
+  size_t at_ = 0;
+};
+
+double dval(const std::string& s) {
+  std::string t(s);
+  for (char& c : t)
+    if (c == 'd' || c == 'D') c = 'e';
+  return std::strtod(t.c_str(), nullptr);
+}
+int ival(const std::string& s) { return (int)std::strtol(s.c_str(), nullptr, 10); }
+
+inline int cm(int i, int j) { return i + 3 * j; }  // 0-based column-major 3x3
+
+void mat3mul(const double* a, const double* b, double* c) {  // c = a*b (column-major)
+  double t[9];
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0;
+      for (int k = 0; k < 3; ++k) s += a[cm(i, k)] * b[cm(k, j)];
+      t[cm(i, j)] = s;
+    }
+  std::memcpy(c, t, sizeof t);
+}
+
+bool mat3inv(const double* a, double* out) {
+  double det = a[cm(0, 0)] * (a[cm(1, 1)] * a[cm(2, 2)] - a[cm(1, 2)] * a[cm(2, 1)]) -
+               a[cm(0, 1)] * (a[cm(1, 0)] * a[cm(2, 2)] - a[cm(1, 2)] * a[cm(2, 0)]) +
+               a[cm(0, 2)] * (a[cm(1, 0)] * a[cm(2, 1)] - a[cm(1, 1)] * a[cm(2, 0)]);
+  if (std::fabs(det) < 1e-12) return false;
+  double r[9];
+  r[cm(0, 0)] = (a[cm(1, 1)] * a[cm(2, 2)] - a[cm(1, 2)] * a[cm(2, 1)]) / det;
+  r[cm(0, 1)] = (a[cm(0, 2)] * a[cm(2, 1)] - a[cm(0, 1)] * a[cm(2, 2)]) / det;
+  r[cm(0, 2)] = (a[cm(0, 1)] * a[cm(1, 2)] - a[cm(0, 2)] * a[cm(1, 1)]) / det;
+  r[cm(1, 0)] = (a[cm(1, 2)] * a[cm(2, 0)] - a[cm(1, 0)] * a[cm(2, 2)]) / det;
+  r[cm(1, 1)] = (a[cm(0, 0)] * a[cm(2, 2)] - a[cm(0, 2)] * a[cm(2, 0)]) / det;
+  r[cm(1, 2)] = (a[cm(0, 2)] * a[cm(1, 0)] - a[cm(0, 0)] * a[cm(1, 2)]) / det;
+  r[cm(2, 0)] = (a[cm(1, 0)] * a[cm(2, 1)] - a[cm(1, 1)] * a[cm(2, 0)]) / det;
+  r[cm(2, 1)] = (a[cm(0, 1)] * a[cm(2, 0)] - a[cm(0, 0)] * a[cm(2, 1)]) / det;
+  r[cm(2, 2)] = (a[cm(0, 0)] * a[cm(1, 1)] - a[cm(0, 1)] * a[cm(1, 0)]) / det;
+  std::memcpy(out, r, sizeof r);
+  return true;
+}
+
+double norm3(const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// Lattice point group in the order dlatmat2 enumerates it (the order sets
+// which operation is attached to each star arm): integer matrices mapping
+// the three basis vectors onto lattice vectors of equal length, found
+// shell by shell, identity first, then closed under multiplication.
+std::string lattice_point_group(const double* prim_to_cart, std::vector<std::array<int, 9>>& ops) {
+  const double eps = 1e-5;
+  double len[3], dif[3][3];
+  const double* col[3] = {prim_to_cart, prim_to_cart + 3, prim_to_cart + 6};
+  for (int i = 0; i < 3; ++i) len[i] = norm3(col[i]);
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      double v[3] = {col[i][0] - col[j][0], col[i][1] - col[j][1], col[i][2] - col[j][2]};
+      dif[i][j] = norm3(v);
+    }
+  struct Cand {
+    int n[3];
+    double v[3];
+  };
+  std::vector<Cand> cand[3];
+  double lmax = std::max(std::max(len[0], len[1]), len[2]) + eps;
+  for (int shell = 1;; ++shell) {
+    bool any_short = false;
+    for (int a = -shell; a <= shell; ++a)
+      for (int b = -shell; b <= shell; ++b)
+        for (int c = -shell; c <= shell; ++c) {
+          if (std::abs(a) != shell && std::abs(b) != shell && std::abs(c) != shell) continue;
+          Cand k;
+          k.n[0] = a;
+          k.n[1] = b;
+          k.n[2] = c;
+          for (int x = 0; x < 3; ++x) k.v[x] = a * col[0][x] + b * col[1][x] + c * col[2][x];
+          double d = norm3(k.v);
+          if (d < lmax) any_short = true;
+          for (int i = 0; i < 3; ++i)
+            if (std::fabs(d - len[i]) < eps) {
+              cand[i].push_back(k);
+              if (cand[i].size() > 400) return "point group search: too many lattice vectors";
+            }
+        }
+    if (!any_short) break;
+  }
+  ops.clear();
+  std::array<int, 9> ident{};
+  bool have_ident = false;
+  std::vector<std::array<int, 9>> rest;
+  for (auto& c0 : cand[0])
+    for (auto& c1 : cand[1])
+      for (auto& c2 : cand[2]) {
+        std::array<int, 9> m;
+        const Cand* cc[3] = {&c0, &c1, &c2};
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) m[cm(i, j)] = cc[j]->n[i];
+        int det = m[cm(0, 0)] * (m[cm(1, 1)] * m[cm(2, 2)] - m[cm(1, 2)] * m[cm(2, 1)]) -
+                  m[cm(0, 1)] * (m[cm(1, 0)] * m[cm(2, 2)] - m[cm(1, 2)] * m[cm(2, 0)]) +
+                  m[cm(0, 2)] * (m[cm(1, 0)] * m[cm(2, 1)] - m[cm(1, 1)] * m[cm(2, 0)]);
+        if (std::abs(det) != 1) continue;
+        bool ok = true;
+        for (int i = 1; i < 3 && ok; ++i)
+          for (int j = 0; j < i; ++j) {
+            double v[3] = {cc[i]->v[0] - cc[j]->v[0], cc[i]->v[1] - cc[j]->v[1], cc[i]->v[2] - cc[j]->v[2]};
+            if (std::fabs(norm3(v) - dif[i][j]) > eps) {
+              ok = false;
+              break;
+            }
+          }
+        if (!ok) continue;
+        if (m[0] + m[4] + m[8] == 3) {
+          ident = m;
+          have_ident = true;
+        } else {
+          rest.push_back(m);
+        }
+      }
+  if (!have_ident) return "point group search: identity not found";
+  ops.push_back(ident);
+  for (auto& m : rest) ops.push_back(m);
+  if (ops.size() > 48) return "more than 48 point operations";
+  // closure under products, visiting pairs in the reference's order
+  std::vector<std::vector<char>> tried(48, std::vector<char>(48, 0));
+  bool grew = true;
+  while (grew) {
+    grew = false;
+    size_t na = ops.size();
+    for (size_t a = 0; a < na; ++a) {
+      size_t nb = ops.size();
+      for (size_t b = 0; b < nb; ++b) {
+        if (tried[a][b]) continue;
+        tried[a][b] = 1;
+        std::array<int, 9> p{};
+        for (int j = 0; j < 3; ++j)
+          for (int i = 0; i < 3; ++i) {
+            int s = 0;
+            for (int k = 0; k < 3; ++k) s += ops[a][cm(i, k)] * ops[b][cm(k, j)];
+            p[cm(i, j)] = s;
+          }
+        if (std::find(ops.begin(), ops.end(), p) == ops.end()) {
+          if (ops.size() == 48) return "more than 48 point operations";
+          ops.push_back(p);
+          grew = true;
+        }
+      }
+    }
+  }
+  return "";
+}
+
+}  // namespace
+
+// ======================================================================
+std::string read_system(const std::string& dir, System& S) {
+  std::vector<std::string> t;
+  {  // ------------------------------------------------- latdyn.params
+    Records R;
+    if (!R.load(dir + "/latdyn.params")) return "cannot open latdyn.params";
+    std::string dummy;
+    bool ok = R.next(4, t);
+    if (ok) {
+      for (int i = 0; i < 3; ++i) S.nc[i] = ival(t[i]);
+    }
+    ok = ok && R.next(3, t);
+    if (ok)
+      for (int i = 0; i < 3; ++i) S.shft[i] = dval(t[i]);
+    ok = ok && R.next(3, t);  // normald
+    ok = ok && R.next(2, t);  // wmesh wmax
+    ok = ok && R.next(2, t);
+    if (ok) {
+      S.width = dval(t[0]);
+      S.etaz = dval(t[1]);
+    }
+    ok = ok && R.next(1, t);  // verbose
+    ok = ok && R.next(3, t);
+    if (ok) {
+      S.tmin = dval(t[0]);
+      S.tmax = dval(t[1]);
+    }
+    ok = ok && R.next(1, t);
+    if (ok) S.job = ival(t[0]);
+    ok = ok && R.next(1, t);  // ksub_size
+    ok = ok && R.line(dummy);  // v3path, read with (a)
+    ok = ok && R.next(1, t);
+    if (ok) S.iso = ival(t[0]);
+    ok = ok && R.next(1, t);
+    if (ok) S.classical = ival(t[0]);
+    ok = ok && R.next(4, t);
+    ok = ok && R.next(1, t);
+    if (!ok) return "latdyn.params: premature end of file";
+  }
+  {  // ---------------------------------------------- structure.params
+    Records R;
+    if (!R.load(dir + "/structure.params")) return "cannot open structure.params";
+    bool ok = R.next(6, t);
+    if (ok)
+      for (int i = 0; i < 6; ++i) S.latp[i] = dval(t[i]);
+    ok = ok && R.next(9, t);
+    if (ok)
+      for (int i = 0; i < 9; ++i) S.primlatt[i] = dval(t[i]);
+    ok = ok && R.next(1, t);
+    if (ok) {
+      S.scale = dval(t[0]);
+      for (int i = 0; i < 3; ++i) S.latp[i] *= S.scale;
+    }
+    ok = ok && R.next(4, t);
+    for (int i = 0; i < 3 && ok; ++i) ok = R.next(1, t);
+    int ntype = 0;
+    ok = ok && R.next(1, t);
+    if (ok) ntype = ival(t[0]);
+    if (ok && (ntype < 1 || ntype > 100000)) return "structure.params: bad natom_type";
+    ok = ok && R.next(ntype, t);
+    if (ok)
+      for (int i = 0; i < ntype; ++i) S.mas.push_back(dval(t[i]));
+    ok = ok && R.next(ntype, t);
+    ok = ok && R.next(1, t);
+    if (ok) S.nat0 = ival(t[0]);
+    if (ok && (S.nat0 < 1 || S.nat0 > 4096)) return "structure.params: bad natoms0";
+    for (int i = 0; i < 8 && ok; ++i) ok = R.next(1, t);
+    S.atype.assign(S.nat0, 0);
+    for (int i = 0; i < S.nat0 && ok; ++i) {
+      ok = R.next(5, t);
+      if (!ok) break;
+      int lab = ival(t[0]);
+      if (lab < 1 || lab > S.nat0) return "structure.params: atom label out of range";
+      S.atype[lab - 1] = ival(t[1]);
+    }
+    if (!ok) return "structure.params: premature end of file";
+    for (int i = 0; i < S.nat0; ++i) {
+      if (S.atype[i] < 1 || S.atype[i] > ntype) return "structure.params: atom type out of range";
+      S.mass0.push_back(S.mas[S.atype[i] - 1]);
+    }
+  }
+  {  // ---------------------------------------------------- lat_fc.dat
+    Records R;
+    if (!R.load(dir + "/lat_fc.dat")) return "cannot open lat_fc.dat";
+    std::string l;
+    for (;;) {
+      if (!R.line(l)) return "lat_fc.dat: no '  Crystal data: transl' record";
+      if (l.compare(0, 22, "  Crystal data: transl") == 0) break;
+    }
+    for (int a = 0; a < 3; ++a) {
+      if (!R.next(3, t)) return "lat_fc.dat: truncated lattice vectors";
+      for (int x = 0; x < 3; ++x) S.r[a][x] = dval(t[x]);
+    }
+    auto cross = [](const double* u, const double* v, double* w) {
+      w[0] = u[1] * v[2] - u[2] * v[1];
+      w[1] = u[2] * v[0] - u[0] * v[2];
+      w[2] = u[0] * v[1] - u[1] * v[0];
+    };
+    double c23[3], c31[3], c12[3];
+    cross(S.r[1], S.r[2], c23);
+    cross(S.r[2], S.r[0], c31);
+    cross(S.r[0], S.r[1], c12);
+    double om = S.r[0][0] * c23[0] + S.r[0][1] * c23[1] + S.r[0][2] * c23[2];
+    for (int x = 0; x < 3; ++x) {
+      S.g[0][x] = 2 * PhysConst::pi * c23[x] / om;
+      S.g[1][x] = 2 * PhysConst::pi * c31[x] / om;
+      S.g[2][x] = 2 * PhysConst::pi * c12[x] / om;
+    }
+    S.volume_r = std::fabs(c12[0] * S.r[2][0] + c12[1] * S.r[2][1] + c12[2] * S.r[2][2]);
+    double gc[3];
+    cross(S.g[0], S.g[1], gc);
+    S.volume_g = std::fabs(gc[0] * S.g[2][0] + gc[1] * S.g[2][1] + gc[2] * S.g[2][2]);
+    bool ok = R.next(1, t) && R.next(1, t);
+    if (!ok) return "lat_fc.dat: truncated";
+    if (ival(t[0]) != S.nat0) return "lat_fc.dat: natoms0 incompatible with structure.params";
+    for (int i = 0; i < S.nat0; ++i) {
+      if (!R.next(7, t)) return "lat_fc.dat: truncated atom list";
+      if (ival(t[0]) != i + 1 || ival(t[2]) != S.atype[i] || dval(t[6]) != S.mass0[i])
+        return "READ_LATTICE: structure.params and lat_fc.dat are not compatible";
+    }
+    ok = R.next(1, t) && R.next(4, t);
+    if (ok)
+      for (int i = 0; i < 4; ++i) S.include_fc[i] = ival(t[i]);
+    for (int i = 0; i < 8 && ok; ++i) ok = R.next(1, t);
+    ok = ok && R.next(1, t) && R.next(4, t) && R.next(1, t) && R.next(4, t);
+    if (ok)
+      for (int i = 0; i < 4; ++i) S.nterms[i] = ival(t[i]);
+    ok = ok && R.next(1, t) && R.next(1, t) && R.next(1, t) && R.next(2, t);
+    if (!ok) return "lat_fc.dat: truncated header";
+    S.natoms = ival(t[1]);
+    if (S.natoms < S.nat0 || S.natoms > 10000000) return "lat_fc.dat: bad atom count";
+    S.atompos.assign(3 * S.natoms, 0.0);
+    S.cell0.assign(S.natoms, 0);
+    S.cell.assign(3 * S.natoms, 0);
+    for (int n = 0; n < S.natoms; ++n) {
+      if (!R.next(8, t)) return "End of lat_fc.dat file reached";
+      int i = ival(t[0]);
+      if (i < 1 || i > S.natoms) return "lat_fc.dat: atom index out of range";
+      for (int x = 0; x < 3; ++x) S.atompos[3 * (i - 1) + x] = dval(t[1 + x]);
+      S.cell0[i - 1] = ival(t[4]);
+      for (int x = 0; x < 3; ++x) S.cell[3 * (i - 1) + x] = ival(t[5 + x]);
+    }
+    for (int n = 0; n < S.natoms; ++n)
+      if (S.cell0[n] < 1 || S.cell0[n] > S.nat0) return "lat_fc.dat: iatomcell0 out of range";
+  }
+  // ------------------------------------------------------- fc2.dat / fc3.dat
+  for (int rank = 2; rank <= 3; ++rank) {
+    if (rank == 3 && S.include_fc[2] != 1) break;
+    std::string fn = dir + (rank == 2 ? "/fc2.dat" : "/fc3.dat");
+    Records R;
+    if (!R.load(fn)) return "READ_FC234: file " + std::string(rank == 2 ? "fc2.dat" : "fc3.dat") + " does not exist";
+    std::string hdr;
+    R.line(hdr);
+    size_t mx = R.remaining_nonblank();
+    if ((int)mx != S.nterms[rank - 1])
+      return "READ_FC" + std::to_string(rank) + ": number of lines read inconsistent with lat_fc.dat";
+    int nv = 2 + 2 * rank + 1;
+    auto& idx = rank == 2 ? S.t2 : S.t3;
+    auto& val = rank == 2 ? S.f2 : S.f3;
+    idx.resize(mx * 2 * rank);
+    val.resize(mx);
+    for (size_t j = 0; j < mx; ++j) {
+      if (!R.next(nv, t)) return "fc file truncated";
+      for (int c = 0; c < 2 * rank; ++c) idx[j * 2 * rank + c] = ival(t[2 + c]);
+      val[j] = dval(t[nv - 1]);
+      for (int c = 0; c < rank; ++c) {
+        int at = idx[j * 2 * rank + 2 * c], xyz = idx[j * 2 * rank + 2 * c + 1];
+        if (at < 1 || at > S.natoms || xyz < 1 || xyz > 3) return "fc file: atom or xyz index out of range";
+      }
+    }
+  }
+  {  // ------------------------------------------------ dielectric.params
+    Records R;
+    if (!R.load(dir + "/dielectric.params")) return "cannot open dielectric.params";
+    if (!R.next(1, t)) return "dielectric.params: empty";
+    S.born_flag = ival(t[0]);
+    for (int i = 0; i < 3; ++i) {
+      if (!R.next(3, t)) return "dielectric.params: truncated";
+      for (int j = 0; j < 3; ++j) S.epsil[i + 3 * j] = dval(t[j]);
+    }
+    S.charge.assign(9 * S.nat0, 0.0);
+    for (int k = 0; k < S.nat0; ++k)
+      for (int i = 0; i < 3; ++i) {
+        if (!R.next(3, t)) {
+          if (S.born_flag != 0) return "dielectric.params: truncated Born charges";
+          break;
+        }
+        for (int j = 0; j < 3; ++j) S.charge[9 * k + i + 3 * j] = dval(t[j]);
+      }
+  }
+  {  // --------------------------------------------------- b200.params
+    std::ifstream f(dir + "/b200.params");
+    std::string key, v;
+    while (f >> key >> v) {
+      if (key == "delta") S.delta = (v == "gauss") ? ALD_DELTA_GAUSS : ALD_DELTA_TETRA;
+      else if (key == "precision") S.precision = (v == "mixed") ? ALD_MIXED : ALD_FP64;
+      else if (key == "cg_stop") S.cg_stop = (v == "residual") ? ALD_CG_RESIDUAL : ALD_CG_REFERENCE;
+      else if (key == "cg_tol") S.cg_tol = dval(v);
+      else if (key == "width_cm") S.width_cm = dval(v);
+    }
+  }
+  if (S.nc[0] < 1 || S.nc[1] < 1 || S.nc[2] < 1) return "latdyn.params: bad mesh";
+  return "";
+}
+
+// ======================================================================
+std::string build_tables(const System& S, Tables& T) {
+  const int N0 = S.nc[0], N1 = S.nc[1], N2 = S.nc[2];
+  T.nkc = N0 * N1 * N2;
+  T.b = 3 * S.nat0;
+  T.shifted = (N0 % 2 == 0 && N1 % 2 == 0 && N2 % 2 == 0);
+  // ---- conventional / primitive frames and the lattice point group
+  double latp[6];
+  std::memcpy(latp, S.latp, sizeof latp);
+  double d2r = 4.0 * std::atan(1.0) / 180.0;
+  for (int i = 3; i < 6; ++i) latp[i] *= d2r;
+  double conv_to_cart[9] = {0};
+  conv_to_cart[cm(0, 0)] = latp[0];
+  conv_to_cart[cm(0, 1)] = latp[1] * std::cos(latp[5]);
+  conv_to_cart[cm(1, 1)] = latp[1] * std::sin(latp[5]);
+  conv_to_cart[cm(0, 2)] = latp[2] * std::cos(latp[4]);
+  conv_to_cart[cm(1, 2)] = latp[2] * (std::cos(latp[3]) - std::cos(latp[5]) * std::cos(latp[4])) / std::sin(latp[5]);
+  conv_to_cart[cm(2, 2)] = std::sqrt(latp[2] * latp[2] - conv_to_cart[cm(0, 2)] * conv_to_cart[cm(0, 2)] -
+                                     conv_to_cart[cm(1, 2)] * conv_to_cart[cm(1, 2)]);
+  double prim_to_cart[9], conv_to_prim[9];
+  mat3mul(conv_to_cart, S.primlatt, prim_to_cart);
+  if (!mat3inv(S.primlatt, conv_to_prim)) return "primitive_lattice is singular";
+  std::vector<std::array<int, 9>> ops;
+  std::string e = lattice_point_group(prim_to_cart, ops);
+  if (!e.empty()) return e;
+  T.npg = (int)ops.size();
+  for (int o = 0; o < T.npg; ++o) {
+    // k transformation in the conventional frame: ((P I P^-1)^-1)^T, entries rounded
+    double m[9], t1[9], t2[9], inv[9];
+    for (int i = 0; i < 9; ++i) m[i] = ops[o][i];
+    mat3mul(m, conv_to_prim, t1);
+    mat3mul(S.primlatt, t1, t2);
+    if (!mat3inv(t2, inv)) return "singular point operation";
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) T.opk[o][cm(i, j)] = (double)std::lround(inv[cm(j, i)]);
+  }
+  // ---- the mesh of make_kp_reg: fractions are default-REAL quotients
+  T.kpc32.assign(3 * (size_t)T.nkc, 0.0);
+  for (int i = 0; i < N0; ++i)
+    for (int j = 0; j < N1; ++j)
+      for (int k = 0; k < N2; ++k) {
+        size_t n = (size_t)k + (size_t)N2 * (j + (size_t)N1 * i);
+        double f0 = (double)((float)i / (float)N0), f1 = (double)((float)j / (float)N1),
+               f2 = (double)((float)k / (float)N2);
+        for (int x = 0; x < 3; ++x) {
+          double q = ((f0 * S.g[0][x] + f1 * S.g[1][x]) + f2 * S.g[2][x]);
+          if (T.shifted) q += (-0.5) * ((S.g[0][x] + S.g[1][x]) + S.g[2][x]);
+          T.kpc32[3 * n + x] = q;
+        }
+      }
+  auto mesh_index = [&](int a, int b, int c) { return c + N2 * (b + N1 * a); };
+  auto wrap = [](int v, int n) { return ((v % n) + n) % n; };
+  // reduced k-coordinates of mesh point m are (m_a/N_a - s/2): keep twice-N integers
+  // h_a = 2*m_a - s*N_a so that f_a = h_a / (2 N_a) exactly
+  auto h_of = [&](int n, int* h) {
+    int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
+    for (int a = 0; a < 3; ++a) h[a] = 2 * m[a] - (T.shifted ? S.nc[a] : 0);
+  };
+  // point-group action on reduced k coordinates: Rk = G^-1 OPK G with G = [g1 g2 g3]
+  double G[9], Ginv[9];
+  for (int a = 0; a < 3; ++a)
+    for (int x = 0; x < 3; ++x) G[cm(x, a)] = S.g[a][x];
+  if (!mat3inv(G, Ginv)) return "singular reciprocal lattice";
+  std::vector<std::array<double, 9>> rk(T.npg);  // reduced-frame rational action
+  for (int o = 0; o < T.npg; ++o) {
+    double t1[9], t2[9];
+    mat3mul(T.opk[o], G, t1);
+    mat3mul(Ginv, t1, t2);
+    for (int i = 0; i < 9; ++i) rk[o][i] = t2[i];
+  }
+  // map reduced coordinates (h_a / 2N_a) of a rotated point back to a mesh
+  // index; returns -1 when the point is not on the mesh, and reports
+  // whether it lies inside the cell the mesh spans (exact match) or only a
+  // reciprocal-lattice vector away (folded)
+  auto locate = [&](const double* f, bool& in_cell) -> int {
+    int m[3];
+    in_cell = true;
+    for (int a = 0; a < 3; ++a) {
+      double x = f[a] * S.nc[a] + (T.shifted ? 0.5 * S.nc[a] : 0.0);
+      double r = std::nearbyint(x);
+      // x is in units of one mesh step; FP32 mesh fractions leave ~1e-6 noise
+      if (std::fabs(r - x) > 1e-3) return -1;
+      long ir = (long)r;
+      if (ir < 0 || ir >= S.nc[a]) in_cell = false;
+      m[a] = wrap((int)(ir % S.nc[a]), S.nc[a]);
+    }
+    return mesh_index(m[0], m[1], m[2]);
+  };
+  // getstar: arms of the star of a Cartesian k (duplicates removed with the
+  // reference's test on v.primitivelattice differences)
+  auto star = [&](const double* kc, std::vector<std::array<double, 3>>& arms, std::vector<int>& armop) {
+    arms.clear();
+    armop.clear();
+    std::vector<std::array<double, 3>> key;
+    for (int o = 0; o < T.npg; ++o) {
+      double v[3], v2[3];
+      for (int a = 0; a < 3; ++a) {
+        double s = 0;
+        for (int b = 0; b < 3; ++b) s = s + T.opk[o][cm(a, b)] * kc[b];
+        v[a] = s;
+      }
+      for (int a = 0; a < 3; ++a) {
+        double s = 0;
+        for (int k = 0; k < 3; ++k) s = s + v[k] * S.primlatt[cm(k, a)];
+        v2[a] = s;
+      }
+      bool dup = false;
+      for (auto& kk : key) {
+        int c;
+        for (c = 0; c < 3; ++c) {
+          double d = v2[c] - kk[c];
+          if (std::fabs(d - std::nearbyint(d)) > 1e-6) break;
+        }
+        if (c == 3) {
+          dup = true;
+          break;
+        }
+      }
+      if (dup) continue;
+      key.push_back({v2[0], v2[1], v2[2]});
+      arms.push_back({v[0], v[1], v[2]});
+      armop.push_back(o);
+    }
+  };
+  auto reduced = [&](const double* kc, double* f) {
+    for (int a = 0; a < 3; ++a) f[a] = Ginv[cm(a, 0)] * kc[0] + Ginv[cm(a, 1)] * kc[1] + Ginv[cm(a, 2)] * kc[2];
+  };
+  // ---- IBZ (get_weights): first mesh point of each exact (unfolded) orbit
+  T.mapibz.assign(T.nkc, 0);
+  T.mapinv.clear();
+  std::vector<double> w;
+  std::vector<std::array<double, 3>> arms;
+  std::vector<int> armop;
+  for (int n = 0; n < T.nkc; ++n) {
+    star(&T.kpc32[3 * (size_t)n], arms, armop);
+    int found = -1;
+    for (auto& a : arms) {
+      double f[3];
+      reduced(a.data(), f);
+      bool in_cell;
+      int idx = locate(f, in_cell);
+      if (idx >= 0 && in_cell && idx < n && T.mapibz[idx] > 0) {
+        found = T.mapibz[idx];
+        break;
+      }
+    }
+    if (found > 0) {
+      T.mapibz[n] = found;
+      w[found - 1] += 1.0;
+    } else {
+      T.mapinv.push_back(n + 1);
+      w.push_back(1.0);
+      T.mapibz[n] = (int)T.mapinv.size();
+    }
+  }
+  T.nibz = (int)T.mapinv.size();
+  double sw = 0;
+  for (double x : w) sw += x;
+  T.wibz.resize(T.nibz);
+  T.kibz.resize(3 * (size_t)T.nibz);
+  for (int i = 0; i < T.nibz; ++i) {
+    T.wibz[i] = w[i] / sw;
+    for (int x = 0; x < 3; ++x) T.kibz[3 * i + x] = T.kpc32[3 * (size_t)(T.mapinv[i] - 1) + x];
+  }
+  // ---- get_negatives + subst_eivecs: e(q_pos) := conj(e(q_neg))
+  for (int n = 0; n < T.nkc; ++n) {
+    int h[3], m[3];
+    h_of(n, h);
+    for (int a = 0; a < 3; ++a) {
+      int hm = -h[a] + (T.shifted ? S.nc[a] : 0);  // 2*m' for -q
+      m[a] = wrap(hm / 2, S.nc[a]);
+    }
+    int mk = mesh_index(m[0], m[1], m[2]);
+    if (mk < n) {  // n is in the negative list; its partner mk gets conj(e(n))
+      T.neg_src.push_back(n);
+      T.neg_dst.push_back(mk);
+    }
+  }
+  // ---- star arms per IBZ point: mesh arms (kstarsinfbz1) and folded arms
+  T.arm_off.assign(1, 0);
+  T.star_off.assign(1, 0);
+  for (int i = 0; i < T.nibz; ++i) {
+    star(&T.kibz[3 * (size_t)i], arms, armop);
+    for (size_t s = 0; s < arms.size(); ++s) {
+      double f[3];
+      reduced(arms[s].data(), f);
+      bool in_cell;
+      int idx = locate(f, in_cell);
+      if (idx < 0) return "star arm is not a kpoint";
+      if (in_cell) {
+        T.arm_q.push_back(idx);
+        T.arm_op.push_back(armop[s]);
+      }
+      T.star_q.push_back(idx);
+      T.star_op.push_back(armop[s]);
+    }
+    T.arm_off.push_back((int)T.arm_q.size());
+    T.star_off.push_back((int)T.star_q.size());
+  }
+  // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table
+  static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
+                                      {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
+  static const int off8[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
+                                  {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+  T.tet_corner.assign(24 * (size_t)T.nkc, 0);
+  std::vector<std::vector<int>> inc(T.nkc);
+  for (int n = 0; n < T.nkc; ++n) {
+    int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
+    int pt[8];
+    for (int c = 0; c < 8; ++c)
+      pt[c] = mesh_index(wrap(m[0] + off8[c][0], N0), wrap(m[1] + off8[c][1], N1), wrap(m[2] + off8[c][2], N2));
+    for (int l = 0; l < 6; ++l)
+      for (int k = 0; k < 4; ++k) {
+        int p = pt[corner_of[l][k]];
+        T.tet_corner[4 * (6 * (size_t)n + l) + k] = p;
+        inc[p].push_back((6 * n + l) * 4 + k);
+      }
+  }
+  T.tet_inc.assign(24 * (size_t)T.nkc, 0);
+  for (int p = 0; p < T.nkc; ++p) {
+    if (inc[p].size() != 24) return "tetrahedron incidence count";
+    std::sort(inc[p].begin(), inc[p].end());
+    std::copy(inc[p].begin(), inc[p].end(), T.tet_inc.begin() + 24 * (size_t)p);
+  }
+  // ---- exact phases: q(m).R_j = 2 pi sum_a (m_a/N_a - s/2) n_ja
+  long L = 1;
+  for (int a = 0; a < 3; ++a) L = std::lcm(L, (long)S.nc[a]);
+  if (T.shifted && L % 2) L *= 2;
+  if (L > (1 << 20)) return "mesh too large for the phase table";
+  T.L = (int)L;
+  T.phase_coef.assign(4 * (size_t)S.natoms, 0);
+  for (int j = 0; j < S.natoms; ++j) {
+    int j0 = S.cell0[j] - 1;
+    // check the lattice vector of lat_fc.dat against the positions
+    for (int x = 0; x < 3; ++x) {
+      double R = S.atompos[3 * j + x] - S.atompos[3 * j0 + x];
+      double Rn = S.cell[3 * j] * S.r[0][x] + S.cell[3 * j + 1] * S.r[1][x] + S.cell[3 * j + 2] * S.r[2][x];
+      if (std::fabs(R - Rn) > 1e-5 * (1 + std::fabs(R)))
+        return "lat_fc.dat: atom " + std::to_string(j + 1) + " position is not its cell vector n1 n2 n3";
+    }
+    long s = 0;
+    for (int a = 0; a < 3; ++a) {
+      long c = (long)S.cell[3 * j + a] * (L / S.nc[a]);
+      T.phase_coef[4 * j + a] = (int)(((c % L) + L) % L);
+      s += S.cell[3 * j + a];
+    }
+    T.phase_coef[4 * j + 3] = T.shifted ? (int)((((s * (L / 2)) % L) + L) % L) : 0;
+  }
+  return "";
+}
+
+// ======================================================================
+std::string build_fc3(const System& S, Fc3Blocks& F) {
+  int nb = S.nat0;
+  int nt = (int)S.f3.size();
+  struct Key {
+    int blk, j, k;
+  };
+  // map (i0, j, k) -> triple
+  std::unordered_map<long long, int> where;
+  std::vector<Key> keys;
+  std::vector<std::array<double, 27>> vals;
+  for (int t = 0; t < nt; ++t) {
+    const int* id = &S.t3[6 * t];
+    int i = id[0] - 1, j = id[2] - 1, k = id[4] - 1;
+    if (S.cell0[i] != i + 1) continue;  // first index must be in the primitive cell
+    int i0 = i, j0 = S.cell0[j] - 1, k0 = S.cell0[k] - 1;
+    long long key = ((long long)i0 * S.natoms + j) * S.natoms + k;
+    auto it = where.find(key);
+    int tr;
+    if (it == where.end()) {
+      tr = (int)keys.size();
+      where[key] = tr;
+      keys.push_back({(i0 * nb + j0) * nb + k0, j, k});
+      vals.push_back({});
+      vals.back().fill(0.0);
+    } else {
+      tr = it->second;
+    }
+    double mi = S.mass0[i0], mj = S.mass0[j0], mk = S.mass0[k0];
+    int comp = (id[1] - 1) * 9 + (id[3] - 1) * 3 + (id[5] - 1);
+    vals[tr][comp] += S.f3[t] / std::sqrt(mi * mj * mk);
+  }
+  int nblk = nb * nb * nb;
+  std::vector<int> order(keys.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return keys[a].blk < keys[b].blk; });
+  F.ntrip = (int)keys.size();
+  F.blk_off.assign(nblk + 1, 0);
+  F.trip_j.resize(F.ntrip);
+  F.trip_k.resize(F.ntrip);
+  F.w.resize(27 * (size_t)F.ntrip);
+  for (int n = 0; n < F.ntrip; ++n) {
+    const Key& kk = keys[order[n]];
+    F.blk_off[kk.blk + 1]++;
+    F.trip_j[n] = kk.j;
+    F.trip_k[n] = kk.k;
+    for (int c = 0; c < 27; ++c) F.w[27 * (size_t)n + c] = vals[order[n]][c];
+  }
+  for (int b = 0; b < nblk; ++b) F.blk_off[b + 1] += F.blk_off[b];
+  return "";
+}
+
+std::string build_fc2(const System& S, Fc2Csr& F) {
+  int b = 3 * S.nat0;
+  int nt = (int)S.f2.size();
+  std::vector<std::vector<int>> per(b * b);
+  for (int t = 0; t < nt; ++t) {
+    const int* id = &S.t2[4 * t];
+    int i = id[0], al = id[1], j = id[2], be = id[3];
+    if (i < 1 || i > S.nat0) continue;  // rows are primitive-cell atoms only
+    int j0 = S.cell0[j - 1];
+    int i3 = (al - 1) + 3 * (i - 1), j3 = (be - 1) + 3 * (j0 - 1);
+    per[i3 * b + j3].push_back(t);
+  }
+  F.off.assign(b * b + 1, 0);
+  for (int e = 0; e < b * b; ++e) F.off[e + 1] = F.off[e] + (int)per[e].size();
+  F.atom.resize(F.off[b * b]);
+  F.val.resize(F.off[b * b]);
+  F.sqm.resize(F.off[b * b]);
+  for (int e = 0; e < b * b; ++e) {
+    int i0 = e / b / 3;
+    for (size_t s = 0; s < per[e].size(); ++s) {
+      int t = per[e][s];
+      int j = S.t2[4 * t + 2] - 1;
+      int j0 = S.cell0[j] - 1;
+      F.atom[F.off[e] + s] = j;
+      F.val[F.off[e] + s] = S.f2[t];
+      F.sqm[F.off[e] + s] = std::sqrt(S.mass0[i0] * S.mass0[j0]);
+    }
+  }
+  return "";
+}
+
+}  // namespace ald

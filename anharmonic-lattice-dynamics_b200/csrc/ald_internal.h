@@ -1,0 +1,267 @@
+// Internal types of libald.  Host-side tables are built once per context
+// from the reference's input files; device buffers live in DevBuf.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/ald.h"
+
+#ifdef __CUDACC__
+#define ALD_HD __host__ __device__
+#else
+#define ALD_HD
+#endif
+
+namespace ald {
+
+// ------------------------------------------------------------ constants
+// THERMACOND/modules.f90:4-23 and kappa.f90:182.  `cnst` is a REAL(8)
+// initialised from a default-REAL literal, hence the float rounding.
+struct PhysConst {
+  static constexpr double pi = 3.14159265358979323846;
+  static constexpr double h_plank = 6.62606896e-34;
+  static constexpr double k_b = 1.3806504e-23;
+  static constexpr double c_light = 2.99792458e+8;
+  static constexpr double hbar = 1.054571628e-34;
+  static constexpr double ee = 1.60217653e-19;
+  static constexpr double uma = 1.66053878e-27;
+  static ALD_HD double cnst() { return (double)521.1098918f; }
+  static double const33();
+};
+
+// Everything the input files define (record layout: rest.f90:2-443).
+struct System {
+  // latdyn.params
+  int nc[3] = {0, 0, 0};
+  double shft[3] = {0, 0, 0};
+  double width = 0, etaz = 0, tmin = 0, tmax = 0;
+  int job = 0, iso = 0, classical = 0;
+  // structure.params
+  double latp[6] = {0};
+  double primlatt[9] = {0};  // column-major (3,3)
+  double scale = 0;
+  int include_fc[4] = {0};
+  std::vector<double> mas;
+  int nat0 = 0;
+  std::vector<int> atype;
+  std::vector<double> mass0;
+  // lat_fc.dat
+  double r[3][3] = {{0}};  // r[a] = primitive vector a (Cartesian, A)
+  double g[3][3] = {{0}};  // reciprocal vectors incl. 2*pi
+  double volume_r = 0, volume_g = 0;
+  int nterms[4] = {0};
+  int natoms = 0;
+  std::vector<double> atompos;  // 3*natoms
+  std::vector<int> cell0;       // natoms, 1-based primitive atom
+  std::vector<int> cell;        // 3*natoms, lattice-vector integers
+  // fc2 / fc3 (1-based atom and xyz indices as in the files)
+  std::vector<int> t2;          // 4*nt2: i, a, j, b
+  std::vector<double> f2;
+  std::vector<int> t3;          // 6*nt3: i, a, j, b, k, c
+  std::vector<double> f3;
+  // dielectric.params
+  int born_flag = 0;
+  double epsil[9] = {0};        // column-major (3,3)
+  std::vector<double> charge;   // 9*nat0 column-major charge(i,j) per atom
+  // b200.params (optional)
+  int delta = -1, precision = -1, cg_stop = -1;
+  double cg_tol = -1, width_cm = -1;
+};
+
+std::string read_system(const std::string& dir, System& S);
+
+// Mesh / IBZ / symmetry tables (host).
+struct Tables {
+  int nkc = 0, nibz = 0, b = 0, npg = 0;
+  bool shifted = false;            // all mesh divisions even: q = (m/N - 1/2) g
+  double opk[48][9];               // op_kmatrix, column-major
+  std::vector<double> kpc32;       // 3*nkc: mesh of make_kp_reg (FP32 fractions)
+  std::vector<int> mapibz;         // nkc, 1-based
+  std::vector<int> mapinv;         // nibz, 1-based
+  std::vector<double> kibz, wibz;  // 3*nibz, nibz
+  std::vector<int> neg_src, neg_dst;  // subst_eivecs copies (0-based)
+  // star arms that are mesh points (kstarsinfbz1): CSR over IBZ points
+  std::vector<int> arm_off, arm_q, arm_op;   // arm_op 0-based op index
+  // all star arms folded onto the mesh (getstar + get_k_info), for the
+  // star-averaged velocities of mode_kappa_d
+  std::vector<int> star_off, star_q, star_op;
+  // tetrahedra: corner mesh indices (6*nkc x 4) and per-point incidences
+  std::vector<int> tet_corner;     // 4 per tetrahedron, 0-based
+  std::vector<int> tet_inc;        // 24 per point: tet*4 + slot, ascending
+  // exact phases: q(m).R_j = 2*pi*t/L with t = sum_a m_a*pc[j][a] + ps[j] (mod L)
+  int L = 1;
+  std::vector<int> phase_coef;     // 4*natoms: L/N_a*n_a (a=0..2), shift term
+};
+
+std::string build_tables(const System& S, Tables& T);
+
+// FC3 regrouped by atom triple (i0, j, k): 27 mass-scaled components per
+// triple, triples grouped by the primitive-atom block (i0, j0, k0).
+struct Fc3Blocks {
+  int ntrip = 0;
+  std::vector<int> blk_off;        // nat0^3 + 1
+  std::vector<int> trip_j, trip_k; // supercell atom indices (0-based)
+  std::vector<double> w;           // 27 per triple: fcs/sqrt(mi*mj*mk), comp = a*9+b*3+c
+};
+std::string build_fc3(const System& S, Fc3Blocks& F);
+
+// FC2 grouped per dynamical-matrix element (i3, j3) in the file's term
+// order (the order set_dynamical_matrix sums them).
+struct Fc2Csr {
+  std::vector<int> off;            // b*b + 1, element = i3*b + j3 (0-based)
+  std::vector<int> atom;           // supercell atom j (0-based)
+  std::vector<double> val;         // fcs_2
+  std::vector<double> sqm;         // sqrt(mi*mj)
+};
+std::string build_fc2(const System& S, Fc2Csr& F);
+
+// ------------------------------------------------------------ device side
+template <class T>
+struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  cudaError_t alloc(size_t count) {
+    if (count == n && p) return cudaSuccess;
+    free();
+    n = count;
+    if (count == 0) return cudaSuccess;
+    return cudaMalloc((void**)&p, count * sizeof(T));
+  }
+  void free() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DevBuf() { free(); }
+};
+
+struct Geometry {  // passed by value to kernels
+  int nc[3];
+  int nkc;
+  int b;
+  int nat0;
+  int shifted;
+  int L;
+};
+
+// kernels (implemented in the .cu files)
+struct PhononArgs {
+  Geometry geo;
+  const double* kpc32;       // 3*nkc
+  const double* g;           // 9: g1,g2,g3 rows
+  const int* fc2_off;        // b*b+1
+  const int* fc2_atom;
+  const double* fc2_val;
+  const double* fc2_sqm;
+  const double* rr;          // 3*natoms: atompos(j) - atompos(j0)
+  int born_flag;
+  const double* born;        // epsil(9), charge(9*nat0), masses(nat0), scalars(4): eps_scale, rho2, om0, pad
+  double dq;
+  double* w2_all;            // nkc*7*b |lambda| in get_freq order
+  double* w2;                // nkc*b eigenval after get_frequencies' sort
+  double* evec;              // 2*b*b*nkc (complex) for the central point
+  int* err;
+};
+cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s);
+cudaError_t launch_phonon_post(const Geometry& geo, const double* w2_all, double dq, double cnst, double* vel,
+                               cudaStream_t s);
+cudaError_t launch_subst_eivecs(const Geometry& geo, const int* src, const int* dst, int n, double* evec,
+                                cudaStream_t s);
+cudaError_t launch_freq_dist(const Geometry& geo, const double* w2, double cnst, double temp, int classical,
+                             double* freq, double* dist, int* err, cudaStream_t s);
+
+struct V3Args {
+  Geometry geo;
+  int n1_first;              // first IBZ row of the chunk (0-based)
+  int nrows;                 // rows in the chunk
+  const int* mapinv;         // 0-based mesh index of IBZ rows
+  const double* evec;        // complex (b,b,nkc)
+  const double* w2;          // (b,nkc)
+  int ntrip;                 // FC3 atom triples
+  int natoms;                // supercell atoms (phase table rows)
+  const int* blk_off;
+  const int* trip_j;
+  const int* trip_k;
+  const double* fc3w;        // 27*ntrip
+  const int* phase_coef;     // 4*natoms
+  const double* roots;       // 2*L
+  double const33;
+  double* v3sq;              // [row][q2][l1][l2][l3]
+  int* err;
+};
+cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s);
+cudaError_t launch_v3_mixed(const V3Args& a, cudaStream_t s);
+
+struct CombineArgs {
+  Geometry geo;
+  int n1_first, nrows;
+  const int* mapinv;
+  const double* v3sq;        // [row][q2][l1][l2][l3]
+  const double* freq;        // [q][l]
+  const double* dist;        // [q][l]
+  const int* tet_corner;
+  const int* tet_inc;
+  int gauss;
+  double sigma;
+  double* R1;                // [row][q][l1][l2], row local to the chunk
+  double* R2;
+  double* P1s;               // optional [row][q][l1][l2][l3] (P1smpi)
+  double* P2s;
+  double* P1;                // optional Bose-weighted
+  double* P2;
+};
+// scratch: the corner energies of the chunk (combine_scratch_bytes)
+size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss);
+cudaError_t launch_combine(const CombineArgs& a, float* scratch, cudaStream_t s);
+// Q/QN/QU[(n1_first+row)*b + l1] from R1/R2 of rows [0, nrows)
+cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
+                            const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s);
+
+struct KappaArgs {
+  Geometry geo;
+  int nibz;
+  const int* mapinv;
+  const double* freq;
+  const double* dist;
+  const double* vel;         // (3,b,nkc)
+  const double* w2;
+  const int* arm_off;
+  const int* arm_q;
+  const int* arm_op;
+  const int* star_off;
+  const int* star_q;
+  const int* star_op;
+  const double* opk;         // 48*9
+  const double* opk_inv;     // 48*9
+  double tempk, temp, const1;
+  int classical;
+};
+cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaStream_t s);
+cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
+                         cudaStream_t s);
+cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s);
+cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
+                             const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
+                             const double* Q, const double* R1, const double* R2, double* CM, int ld,
+                             cudaStream_t s);
+
+// layout conversions and the stand-alone stage kernels (ald_util.cu)
+// internal 5-index arrays are [row][q][l1][l2][l3]; the reference's are
+// Fortran (row,q,l1,l2,l3) with the row index fastest
+cudaError_t launch_to_fortran5(const double* src, double* dst, int nr, int nkc, int b, cudaStream_t s);
+cudaError_t launch_from_fortran5(const double* src, double* dst, int nr, int nkc, int b, cudaStream_t s);
+cudaError_t launch_transpose(const double* src, double* dst, int rows, int cols, cudaStream_t s);
+// calculate_tauRTA_mpi2 from given P1smpi/P2smpi (internal layout)
+cudaError_t launch_tau(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* P1s,
+                       const double* P2s, const double* dist, double* Q, double* QN, double* QU, double* P1,
+                       double* P2, cudaStream_t s);
+// R1/R2 = sum_l3 P1/P2 and Qd = sum (P1 + P2/2) from Bose-weighted P (internal layout)
+cudaError_t launch_collapse(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1,
+                            double* R2, double* Qd, cudaStream_t s);
+int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,
+              double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, std::string& msg);
+
+}  // namespace ald

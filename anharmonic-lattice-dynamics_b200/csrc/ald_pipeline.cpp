@@ -1,0 +1,239 @@
+// ald_kappa_pipeline: the whole job=1 sequence of THERMACOND/kappa.f90:389-871
+// on the device, without materialising any (nibz, nkc, ndyn^3) array:
+//
+//   phonons (get_frequencies + subst_eivecs)      unless injected
+//   distribution                                   sub.f90:1955
+//   for each chunk of IBZ rows:
+//     |V3|^2                  calculate_w3_ibz_split_sq  sub.f90:1050
+//     delta, Bose, band sums  calculate_FGR_mpi2 + calculate_tauRTA_mpi2
+//   Q, Q_N, Q_U                                   (MPI_Allgatherv at kappa.f90:641 is a no-op here)
+//   F_RTA, kappa_RTA          sub.f90:1238, 1292
+//   collision matrix          CollisionMatrix_mpi sub.f90:3034 (kept row-major on the device)
+//   RHS, CG, kappa            sub.f90:2618, cg.f90:19, sub.f90:1407
+//
+// Every stage is bracketed by CUDA events on the context's stream; the
+// per-stage device times and kernel launch counts come back in the result.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "ald_ctx.h"
+
+using namespace ald;
+using namespace ald::capi;
+
+namespace {
+
+struct StageTimer {
+  cudaStream_t s;
+  std::vector<std::pair<int, std::pair<cudaEvent_t, cudaEvent_t>>> marks;
+  cudaEvent_t open_ev = nullptr;
+  int open_stage = -1;
+  cudaError_t begin(int stage) {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return r;
+    open_ev = e;
+    open_stage = stage;
+    return cudaEventRecord(e, s);
+  }
+  cudaError_t end() {
+    cudaEvent_t e;
+    cudaError_t r = cudaEventCreate(&e);
+    if (r != cudaSuccess) return r;
+    r = cudaEventRecord(e, s);
+    marks.push_back({open_stage, {open_ev, e}});
+    open_ev = nullptr;
+    return r;
+  }
+  void collect(double* ms) {
+    for (auto& m : marks) {
+      float t = 0;
+      cudaEventElapsedTime(&t, m.second.first, m.second.second);
+      ms[m.first] += t;
+    }
+  }
+  ~StageTimer() {
+    for (auto& m : marks) {
+      cudaEventDestroy(m.second.first);
+      cudaEventDestroy(m.second.second);
+    }
+    if (open_ev) cudaEventDestroy(open_ev);
+  }
+};
+
+}  // namespace
+
+extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo,
+                                  double* QUo, double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
+  if (!c || !res) return fail(ALD_ERR_ARG, "null argument");
+  if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
+  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 12 bands is not supported by this build");
+  ALD_CK(cudaSetDevice(c->device));
+  std::memset(res, 0, sizeof *res);
+  cudaStream_t s = c->stream;
+  StageTimer tm;
+  tm.s = s;
+  const int b = c->geo.b, nkc = c->T.nkc, nibz = c->T.nibz;
+  cudaEvent_t t0, t1;
+  ALD_CK(cudaEventCreate(&t0));
+  ALD_CK(cudaEventCreate(&t1));
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } evg{t0, t1};
+  ALD_CK(cudaEventRecord(t0, s));
+  // ---- 0: phonons and occupations
+  ALD_CK(tm.begin(0));
+  bool had = c->have_phonons;
+  int r = ensure_phonons(c);
+  if (r) return r;
+  if (!had) res->launches[0] += 3;
+  if (c->dist_tempk != tempk) res->launches[0] += 1;
+  r = ensure_dist(c, tempk);
+  if (r) return r;
+  ALD_CK(tm.end());
+  // ---- 1, 2: V3 and delta/Bose/band sums, chunk by chunk
+  const size_t rsz = (size_t)nibz * nkc * b * b;
+  DevBuf<double> R1, R2, Q, v3;
+  DevBuf<float> escratch;
+  ALD_CKA(R1.alloc(rsz));
+  ALD_CKA(R2.alloc(rsz));
+  ALD_CKA(Q.alloc((size_t)3 * nibz * b));
+  const int K = rows_per_chunk(c);
+  ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
+  const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
+  ALD_CKA(escratch.alloc(std::max<size_t>(1, combine_scratch_bytes(c->geo, K, gauss) / sizeof(float))));
+  for (int r0 = 0; r0 < nibz; r0 += K) {
+    int nr = std::min(K, nibz - r0);
+    ALD_CK(tm.begin(1));
+    r = run_v3(c, v3_args(c, r0, nr, v3.p));
+    if (r) return r;
+    res->launches[1] += 1;
+    ALD_CK(tm.end());
+    CombineArgs a;
+    a.geo = c->geo;
+    a.n1_first = r0;
+    a.nrows = nr;
+    a.mapinv = c->mapinv.p;
+    a.v3sq = v3.p;
+    a.freq = c->freq.p;
+    a.dist = c->dist.p;
+    a.tet_corner = c->tet_corner.p;
+    a.tet_inc = c->tet_inc.p;
+    a.gauss = gauss;
+    a.sigma = gauss_width(c);
+    a.R1 = R1.p + (size_t)r0 * nkc * b * b;
+    a.R2 = R2.p + (size_t)r0 * nkc * b * b;
+    a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
+    ALD_CK(tm.begin(2));
+    ALD_CK(launch_combine(a, escratch.p, s));
+    res->launches[2] += gauss ? 1 : 2;
+    ALD_CK(tm.end());
+  }
+  // ---- 3: Q, Q_N, Q_U from the band sums
+  double* dQ = Q.p;
+  double* dQN = Q.p + (size_t)nibz * b;
+  double* dQU = Q.p + (size_t)2 * nibz * b;
+  ALD_CK(tm.begin(3));
+  ALD_CK(launch_q_from_r(c->geo, 0, nibz, c->mapinv.p, R1.p, R2.p, dQ, dQN, dQU, nibz, s));
+  res->launches[3] += 1;
+  ALD_CK(tm.end());
+  // ---- 4: RTA
+  KappaArgs k = kappa_args(c, tempk);
+  const size_t N = (size_t)3 * b * nibz;
+  DevBuf<double> F, x, rhs, kr, kc, cm;
+  ALD_CKA(F.alloc(N));
+  ALD_CKA(x.alloc(N));
+  ALD_CKA(rhs.alloc(N));
+  ALD_CKA(kr.alloc((size_t)9 * b));
+  ALD_CKA(kc.alloc((size_t)9 * b));
+  ALD_CK(tm.begin(4));
+  ALD_CK(launch_rta_F(k, dQ, F.p, s));
+  ALD_CK(launch_kappa(k, F.p, 0, kr.p, c->err.p, s));
+  res->launches[4] += 2;
+  ALD_CK(tm.end());
+  // ---- 5: collision matrix (row-major, all IBZ rows)
+  ALD_CKA(cm.alloc(N * N));
+  ALD_CK(tm.begin(5));
+  ALD_CK(launch_collision(c->geo, nibz, 0, nibz, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, dQ,
+                          R1.p, R2.p, cm.p, (int)N, s));
+  res->launches[5] += 1;
+  ALD_CK(tm.end());
+  // ---- 6: RHS and the initial guess x0 = F_RTA (kappa.f90:835-843)
+  ALD_CK(tm.begin(6));
+  ALD_CK(launch_rhs(k, rhs.p, s));
+  ALD_CK(cudaMemcpyAsync(x.p, F.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  res->launches[6] += 1;
+  ALD_CK(tm.end());
+  // ---- 7: cg_quadratic(nibz*ndyn*3, CM, RHS, x, fm, 100, 2) (kappa.f90:846)
+  int iters = 0;
+  double cg_err = 0, fm = 0;
+  std::string msg;
+  double tol = c->opt.cg_stop == ALD_CG_REFERENCE ? 1.0 / std::pow(10.0, 2 * c->opt.cg_ndig) : c->opt.cg_tol;
+  ALD_CK(tm.begin(7));
+  int rc = cg_device((int)N, cm.p, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters, &cg_err, &fm, s,
+                     msg);
+  if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
+  res->launches[7] += 4 + 2 * c->opt.cg_max_iter;
+  ALD_CK(tm.end());
+  // ---- 8: mode_kappa_d
+  ALD_CK(tm.begin(8));
+  ALD_CK(launch_kappa(k, x.p, 1, kc.p, c->err.p, s));
+  res->launches[8] += 1;
+  ALD_CK(tm.end());
+  ALD_CK(cudaEventRecord(t1, s));
+  // ---- results to the host
+  std::vector<double> hkr((size_t)9 * b), hkc((size_t)9 * b);
+  ALD_CK(cudaMemcpyAsync(hkr.data(), kr.p, hkr.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  ALD_CK(cudaMemcpyAsync(hkc.data(), kc.p, hkc.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  double d2h = 2.0 * hkr.size() * sizeof(double);
+  std::vector<double> hq;
+  if (Qo || QNo || QUo) {
+    hq.resize((size_t)3 * nibz * b);
+    ALD_CK(cudaMemcpyAsync(hq.data(), Q.p, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    d2h += hq.size() * sizeof(double);
+  }
+  if (xo) {
+    ALD_CK(cudaMemcpyAsync(xo, x.p, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+    d2h += N * sizeof(double);
+  }
+  ALD_CK(cudaStreamSynchronize(s));
+  r = check_err_flags(c);
+  if (r) return r;
+  tm.collect(res->stage_ms);
+  float total = 0;
+  cudaEventElapsedTime(&total, t0, t1);
+  res->stage_ms[9] = total;
+  for (int i = 0; i < 9; ++i) res->launches[9] += res->launches[i];
+  for (int e = 0; e < 9; ++e) {
+    double sr = 0, sc = 0;
+    for (int l = 0; l < b; ++l) {
+      sr += hkr[l + (size_t)b * e];
+      sc += hkc[l + (size_t)b * e];
+    }
+    res->kappa_rta[e] = sr;
+    res->kappa_cg[e] = sc;
+  }
+  if (kappa_rta_modes) std::memcpy(kappa_rta_modes, hkr.data(), hkr.size() * sizeof(double));
+  if (kappa_cg_modes) std::memcpy(kappa_cg_modes, hkc.data(), hkc.size() * sizeof(double));
+  for (int i = 0; i < nibz; ++i)
+    for (int l = 0; l < b; ++l) {
+      if (Qo) Qo[i + (size_t)nibz * l] = hq[(size_t)i * b + l];
+      if (QNo) QNo[i + (size_t)nibz * l] = hq[(size_t)nibz * b + (size_t)i * b + l];
+      if (QUo) QUo[i + (size_t)nibz * l] = hq[(size_t)2 * nibz * b + (size_t)i * b + l];
+    }
+  res->cg_iters = iters;
+  res->status_cg = rc;
+  res->cg_err = cg_err;
+  res->triplet_bands = (double)nibz * nkc * (double)b * b * b;
+  res->d2h_bytes = d2h;
+  return ALD_OK;
+}

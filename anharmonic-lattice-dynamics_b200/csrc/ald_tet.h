@@ -1,0 +1,146 @@
+// Tetrahedron corner weights of THERMACOND's weight_tet
+// (THERMACOND/tetrahedron.f90:188-384), for host and device.
+//
+// weight_tet sorts the four corner energies (SSORT, descending, values as
+// default REAL), maps sorted positions back to corners with a tie rule, and
+// evaluates the linear-tetrahedron delta weights in mixed FP32/FP64: the
+// energies and their differences are REAL, every term that involves the
+// REAL(8) energy e is promoted to double, and the c/b temporaries of the
+// middle branch are REAL.  Callers compile this with FMA contraction off
+// (-fmad=false / -ffp-contract=off) so each operation rounds like the
+// reference's.
+//
+// Tie rule: among equal corner energies the corner with the smaller index
+// takes the earlier (higher) sorted position, which is what the uns
+// bookkeeping of tetrahedron.f90:227-290 produces; hence
+//   pos(corner) = #{m : E_m > E_corner} + #{m < corner : E_m == E_corner}
+// with pos 0 the highest and 3 the lowest energy.
+#pragma once
+
+#ifdef __CUDACC__
+#define ALD_TET_HD __host__ __device__ __forceinline__
+#else
+#define ALD_TET_HD inline
+#include <cmath>
+#endif
+
+namespace ald {
+
+struct TetSorted {
+  float e1, e2, e3, e4;              // ascending: e1 lowest
+  float e21, e31, e41, e32, e42, e43;
+};
+
+ALD_TET_HD void tet_fix_small(float& x) {
+  const double small1 = 1e-10, small2 = 1e-10;
+  if (fabs((double)x) < small1 && x > 0.0f) x = (float)small2;
+  if (fabs((double)x) < small1 && x < 0.0f) x = (float)(-small2);
+}
+
+ALD_TET_HD float fmax4(float a, float b) { return a > b ? a : b; }
+ALD_TET_HD float fmin4(float a, float b) { return a < b ? a : b; }
+
+// sorted energies of one tetrahedron (corner order irrelevant for the values)
+ALD_TET_HD TetSorted tet_sort(float a, float b, float c, float d) {
+  // sorting network, ascending
+  float t;
+  if (a > b) { t = a; a = b; b = t; }
+  if (c > d) { t = c; c = d; d = t; }
+  if (a > c) { t = a; a = c; c = t; }
+  if (b > d) { t = b; b = d; d = t; }
+  if (b > c) { t = b; b = c; c = t; }
+  TetSorted s;
+  s.e1 = a;
+  s.e2 = b;
+  s.e3 = c;
+  s.e4 = d;
+  s.e21 = s.e2 - s.e1;
+  s.e31 = s.e3 - s.e1;
+  s.e41 = s.e4 - s.e1;
+  s.e32 = s.e3 - s.e2;
+  s.e42 = s.e4 - s.e2;
+  s.e43 = s.e4 - s.e3;
+  tet_fix_small(s.e21);
+  tet_fix_small(s.e31);
+  tet_fix_small(s.e41);
+  tet_fix_small(s.e42);
+  tet_fix_small(s.e43);
+  return s;
+}
+
+// sorted position (0 highest ... 3 lowest) of corner `slot` among en[0..3]
+ALD_TET_HD int tet_pos(const float* en, int slot) {
+  float x = en[slot];
+  int p = 0;
+  for (int m = 0; m < 4; ++m) p += (en[m] > x) || (m < slot && en[m] == x);
+  return p;
+}
+
+// weight c of the corner at sorted position `pos` for energy e
+ALD_TET_HD double tet_weight(const TetSorted& t, int pos, double e) {
+  const double E1 = t.e1, E2 = t.e2, E3 = t.e3, E4 = t.e4;
+  if (e < E1 || e > E4) return 0.0;
+  const float e21 = t.e21, e31 = t.e31, e41 = t.e41, e32 = t.e32, e42 = t.e42, e43 = t.e43;
+  if (E1 <= e && e <= E2) {
+    double x = e - E1;
+    double x3 = x * (x * x);
+    switch (pos) {
+      case 3:
+        return ((E2 - e) / (double)e21 + (E3 - e) / (double)e31 + (E4 - e) / (double)e41) * (x * x) /
+               (double)((e41 * e31) * e21);
+      case 2: return x3 / (double)(((e21 * e21) * e31) * e41);
+      case 1: return x3 / (double)((e21 * (e31 * e31)) * e41);
+      default: return x3 / (double)((e21 * e31) * (e41 * e41));
+    }
+  }
+  if (E2 <= e && e <= E3) {
+    float ca, cb, ba, bb;
+    switch (pos) {
+      case 3:
+        ca = (float)((E3 - e) / (double)(e31 * e31));
+        cb = (float)((E4 - e) / (double)(e41 * e41));
+        ba = (float)((E3 - e) * (e - E2) / (double)(e42 * e32) + (E4 - e) * (e - E1) / (double)(e41 * e42) +
+                     (E3 - e) * (e - E1) / (double)(e32 * e41));
+        bb = (float)((E4 - e) * (e - E1) / (double)(e42 * e31) + (E4 - e) * (e - E2) / (double)(e42 * e32) +
+                     (E3 - e) * (e - E1) / (double)(e31 * e32));
+        break;
+      case 2:
+        ca = (float)((E3 - e) / (double)(e32 * e32));
+        cb = (float)((E4 - e) / (double)(e42 * e42));
+        ba = (float)((E3 - e) * (e - E2) / (double)(e42 * e31) + (E4 - e) * (e - E2) / (double)(e42 * e41) +
+                     (E3 - e) * (e - E1) / (double)(e31 * e41));
+        bb = (float)((E3 - e) * (e - E2) / (double)(e32 * e31) + (E4 - e) * (e - E1) / (double)(e41 * e31) +
+                     (E4 - e) * (e - E2) / (double)(e32 * e41));
+        break;
+      case 1:
+        ca = (float)((e - E2) / (double)(e32 * e32));
+        cb = (float)((e - E1) / (double)(e31 * e31));
+        ba = (float)((E3 - e) * (e - E2) / (double)(e42 * e31) + (E4 - e) * (e - E2) / (double)(e42 * e41) +
+                     (E3 - e) * (e - E1) / (double)(e31 * e41));
+        bb = (float)((E3 - e) * (e - E2) / (double)(e42 * e32) + (E4 - e) * (e - E1) / (double)(e41 * e42) +
+                     (E3 - e) * (e - E1) / (double)(e32 * e41));
+        break;
+      default:
+        ca = (float)((e - E2) / (double)(e42 * e42));
+        cb = (float)((e - E1) / (double)(e41 * e41));
+        ba = (float)((E3 - e) * (e - E2) / (double)(e32 * e31) + (E4 - e) * (e - E1) / (double)(e41 * e31) +
+                     (E4 - e) * (e - E2) / (double)(e32 * e41));
+        bb = (float)((E4 - e) * (e - E1) / (double)(e42 * e31) + (E4 - e) * (e - E2) / (double)(e42 * e32) +
+                     (E3 - e) * (e - E1) / (double)(e31 * e32));
+        break;
+    }
+    return (double)(0.5f * (ca * ba + cb * bb));
+  }
+  double x = E4 - e;
+  double x3 = x * (x * x);
+  switch (pos) {
+    case 3: return x3 / (double)(((e41 * e41) * e42) * e43);
+    case 2: return x3 / (double)((e41 * (e42 * e42)) * e43);
+    case 1: return x3 / (double)((e41 * e42) * (e43 * e43));
+    default:
+      return ((e - E3) / (double)e43 + (e - E2) / (double)e42 + (e - E1) / (double)e41) * (x * x) /
+             (double)((e41 * e42) * e43);
+  }
+}
+
+}  // namespace ald

@@ -1,0 +1,283 @@
+"""Python binding of libald (the C ABI declared in include/ald.h).
+
+Names follow the THERMACOND subroutines each call replaces
+(calculate_w3_ibz_split_sq, calculate_FGR_mpi2, calculate_tauRTA_mpi2,
+CollisionMatrix_mpi, cal_RHS_IBZ, cg_quadratic, mode_kappa_d ...).
+Arrays come back as numpy arrays in the reference's Fortran layout
+(order='F', 1-based index values), so indexing reads like the Fortran.
+
+All compute runs in the CUDA library; if libald.so is missing the import
+fails -- there is no CPU fallback.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from typing import Optional, Sequence, Tuple
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+LIB_PATH = os.path.join(_PKG, "lib", "libald.so")
+
+ALD_OK = 0
+ALD_WARN_CG_MAXITER = 100
+STATUS = {1: "ALD_ERR_ARG", 2: "ALD_ERR_IO", 3: "ALD_ERR_NOT_KPOINT", 4: "ALD_ERR_DEN_ZERO", 5: "ALD_ERR_NBE",
+          6: "ALD_ERR_INDEX", 7: "ALD_ERR_CUDA", 8: "ALD_ERR_UNSUPPORTED", 9: "ALD_ERR_NOMEM",
+          100: "ALD_WARN_CG_MAXITER"}
+DELTA_TETRA, DELTA_GAUSS = 0, 1
+FP64, MIXED = 0, 1
+CG_REFERENCE, CG_RESIDUAL = 0, 1
+
+
+class AldError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__("%s (%d): %s" % (STATUS.get(code, "?"), code, msg))
+        self.code = code
+
+
+class Options(C.Structure):
+    _fields_ = [("delta", C.c_int), ("precision", C.c_int), ("cg_stop", C.c_int), ("cg_max_iter", C.c_int),
+                ("cg_ndig", C.c_int), ("cg_tol", C.c_double), ("width_cm", C.c_double), ("device", C.c_int),
+                ("chunk_bytes", C.c_size_t)]
+
+
+class Info(C.Structure):
+    _fields_ = [("ndyn", C.c_int), ("natoms0", C.c_int), ("nc", C.c_int * 3), ("nkc", C.c_int), ("nibz", C.c_int),
+                ("nterms2", C.c_int), ("nterms3", C.c_int), ("natoms", C.c_int), ("lattpgcount", C.c_int),
+                ("born_flag", C.c_int), ("tempk", C.c_double), ("width_cm", C.c_double), ("volume_r", C.c_double)]
+
+
+class KappaResult(C.Structure):
+    _fields_ = [("kappa_rta", C.c_double * 9), ("kappa_cg", C.c_double * 9), ("cg_iters", C.c_int),
+                ("status_cg", C.c_int), ("cg_err", C.c_double), ("stage_ms", C.c_double * 10),
+                ("launches", C.c_int * 10), ("triplet_bands", C.c_double), ("d2h_bytes", C.c_double)]
+
+
+STAGES = ["phonons", "v3", "delta", "q_reduce", "rta", "collision", "rhs", "cg", "kappa_cg", "total"]
+
+
+_lib = None
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int)
+EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_destroy", "ald_get_info",
+           "ald_read_mesh", "ald_get_mesh", "ald_get_frequencies", "ald_set_phonons",
+           "ald_calculate_w3_ibz_split_sq", "ald_calculate_fgr", "ald_distribution", "ald_calculate_tau_rta",
+           "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
+           "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes"]
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libald.so not built (%s); run anharmonic-lattice-dynamics_b200/python/ald/build.py"
+                              % LIB_PATH)
+        L = C.CDLL(LIB_PATH)
+        L.ald_last_error.restype = C.c_char_p
+        L.ald_default_options.argtypes = [C.POINTER(Options)]
+        L.ald_create_from_dir.argtypes = [C.c_char_p, C.POINTER(Options), C.POINTER(C.c_void_p)]
+        L.ald_destroy.argtypes = [C.c_void_p]
+        L.ald_destroy.restype = None
+        L.ald_h2d_bytes.restype = C.c_double
+        L.ald_h2d_bytes.argtypes = [C.c_void_p]
+        L.ald_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        for n in EXPORTS[2:]:
+            if n not in ("ald_destroy", "ald_h2d_bytes"):
+                getattr(L, n).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(dp)
+
+
+def _check(r: int, allow=(ALD_OK,)) -> int:
+    if r not in allow:
+        raise AldError(r, lib().ald_last_error().decode())
+    return r
+
+
+def default_options(**kw) -> Options:
+    o = Options()
+    lib().ald_default_options(C.byref(o))
+    for k, v in kw.items():
+        setattr(o, k, v)
+    return o
+
+
+def read_mesh(d: str):
+    """Host-only mesh/IBZ tables of an input directory (no GPU needed)."""
+    info = Info()
+    _check(lib().ald_read_mesh(d.encode(), C.byref(info), None, None, None, None, None))
+    kpc = np.zeros((3, info.nkc), order="F")
+    mapibz = np.zeros(info.nkc, dtype=np.int32)
+    mapinv = np.zeros(info.nibz, dtype=np.int32)
+    kibz = np.zeros((3, info.nibz), order="F")
+    wibz = np.zeros(info.nibz)
+    _check(lib().ald_read_mesh(d.encode(), C.byref(info), _p(kpc), mapibz.ctypes.data_as(ip),
+                               mapinv.ctypes.data_as(ip), _p(kibz), _p(wibz)))
+    return info, {"kpc": kpc, "mapibz": mapibz, "mapinv": mapinv, "kibz": kibz, "wibz": wibz}
+
+
+class Context:
+    """One loaded system (lat_fc/fc2/fc3/params of a directory) on one GPU."""
+
+    def __init__(self, d: str, options: Optional[Options] = None):
+        h = C.c_void_p()
+        _check(lib().ald_create_from_dir(d.encode(), C.byref(options) if options is not None else None, C.byref(h)))
+        self.h = h
+        info = Info()
+        _check(lib().ald_get_info(h, C.byref(info)))
+        self.info = info
+        self.ndyn, self.nkc, self.nibz = info.ndyn, info.nkc, info.nibz
+        self.nc = tuple(info.nc)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().ald_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def set_stream(self, stream_handle: Optional[int]):
+        """Issue work on a caller's cudaStream_t (an int handle, e.g.
+        torch.cuda.current_stream().cuda_stream); None restores the own stream."""
+        _check(lib().ald_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None))
+
+    def h2d_bytes(self) -> float:
+        return lib().ald_h2d_bytes(self.h)
+
+    def invalidate_phonons(self):
+        """Make the next pipeline call recompute eigenpairs (get_frequencies)."""
+        _check(lib().ald_get_frequencies(self.h, None, None, None))
+
+    # ---------------------------------------------------------- tables
+    def get_mesh(self):
+        kpc = np.zeros((3, self.nkc), order="F")
+        mapibz = np.zeros(self.nkc, dtype=np.int32)
+        mapinv = np.zeros(self.nibz, dtype=np.int32)
+        kibz = np.zeros((3, self.nibz), order="F")
+        wibz = np.zeros(self.nibz)
+        _check(lib().ald_get_mesh(self.h, _p(kpc), mapibz.ctypes.data_as(ip), mapinv.ctypes.data_as(ip), _p(kibz),
+                                  _p(wibz)))
+        return {"kpc": kpc, "mapibz": mapibz, "mapinv": mapinv, "kibz": kibz, "wibz": wibz}
+
+    # ---------------------------------------------------------- stage 1
+    def get_frequencies(self):
+        """get_frequencies + subst_eivecs: eigenval(ndyn,nkc), eigenvec(ndyn,ndyn,nkc), veloc(3,ndyn,nkc)."""
+        n, nk = self.ndyn, self.nkc
+        ev = np.zeros((n, nk), order="F")
+        vec = np.zeros((n, n, nk), dtype=complex, order="F")
+        vel = np.zeros((3, n, nk), order="F")
+        _check(lib().ald_get_frequencies(self.h, _p(ev), vec.ctypes.data_as(dp), _p(vel)))
+        return ev, vec, vel
+
+    def set_phonons(self, eigenval, eigenvec, veloc):
+        ev = np.asfortranarray(eigenval, dtype=float)
+        vec = np.asfortranarray(eigenvec, dtype=complex)
+        vel = np.asfortranarray(veloc, dtype=float)
+        _check(lib().ald_set_phonons(self.h, _p(ev), vec.ctypes.data_as(dp), _p(vel)))
+
+    # ---------------------------------------------------------- stage 2-4
+    def calculate_w3_ibz_split_sq(self, ksubset: Sequence[int]):
+        k = (C.c_int * 2)(*ksubset)
+        n, nk = self.ndyn, self.nkc
+        out = np.zeros((ksubset[1] - ksubset[0] + 1, nk, n, n, n), order="F")
+        _check(lib().ald_calculate_w3_ibz_split_sq(self.h, k, _p(out)))
+        return out
+
+    def calculate_fgr(self, ksubset, v33s8):
+        k = (C.c_int * 2)(*ksubset)
+        v = np.asfortranarray(v33s8, dtype=float)
+        P1 = np.zeros_like(v, order="F")
+        P2 = np.zeros_like(v, order="F")
+        _check(lib().ald_calculate_fgr(self.h, k, _p(v), _p(P1), _p(P2)))
+        return P1, P2
+
+    def distribution(self, tempk: float):
+        f = np.zeros((self.nkc, self.ndyn), order="F")
+        d = np.zeros((self.nkc, self.ndyn), order="F")
+        _check(lib().ald_distribution(self.h, C.c_double(tempk), _p(f), _p(d)))
+        return f, d
+
+    def calculate_tau_rta(self, ksubset, tempk, P1smpi, P2smpi, want_p=True):
+        k = (C.c_int * 2)(*ksubset)
+        nr = ksubset[1] - ksubset[0] + 1
+        s1 = np.asfortranarray(P1smpi, dtype=float)
+        s2 = np.asfortranarray(P2smpi, dtype=float)
+        Q = np.zeros((nr, self.ndyn), order="F")
+        QN, QU = np.zeros_like(Q), np.zeros_like(Q)
+        P1 = np.zeros_like(s1, order="F") if want_p else None
+        P2 = np.zeros_like(s1, order="F") if want_p else None
+        _check(lib().ald_calculate_tau_rta(self.h, k, C.c_double(tempk), _p(s1), _p(s2), _p(Q), _p(QN), _p(QU),
+                                           _p(P1), _p(P2)))
+        return Q, QN, QU, P1, P2
+
+    def rta_kappa(self, tempk, Q):
+        q = np.asfortranarray(Q, dtype=float)
+        FFF = np.zeros((self.nibz, self.ndyn, 3), order="F")
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        _check(lib().ald_rta_kappa(self.h, C.c_double(tempk), _p(q), _p(FFF), _p(kap)))
+        return FFF, kap
+
+    def collision_matrix(self, ksubset, P1, P2):
+        k = (C.c_int * 2)(*ksubset)
+        nr = ksubset[1] - ksubset[0] + 1
+        CM = np.zeros((nr * self.ndyn * 3, self.nibz * self.ndyn * 3), order="F")
+        _check(lib().ald_collision_matrix(self.h, k, _p(np.asfortranarray(P1, dtype=float)),
+                                          _p(np.asfortranarray(P2, dtype=float)), _p(CM)))
+        return CM
+
+    def rhs(self, tempk):
+        r = np.zeros(self.nibz * self.ndyn * 3)
+        _check(lib().ald_rhs(self.h, C.c_double(tempk), _p(r)))
+        return r
+
+    def mode_kappa_d(self, tempk, x):
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        _check(lib().ald_mode_kappa_d(self.h, C.c_double(tempk), _p(np.ascontiguousarray(x, dtype=float)), _p(kap)))
+        return kap
+
+    def kappa_pipeline(self, tempk: Optional[float] = None, want_modes=True):
+        if tempk is None:
+            tempk = self.info.tempk
+        res = KappaResult()
+        n, ni = self.ndyn, self.nibz
+        Q = np.zeros((ni, n), order="F") if want_modes else None
+        QN = np.zeros((ni, n), order="F") if want_modes else None
+        QU = np.zeros((ni, n), order="F") if want_modes else None
+        kr = np.zeros((n, 3, 3), order="F") if want_modes else None
+        kc = np.zeros((n, 3, 3), order="F") if want_modes else None
+        x = np.zeros(ni * n * 3) if want_modes else None
+        _check(lib().ald_kappa_pipeline(self.h, C.c_double(tempk), C.byref(res), _p(Q), _p(QN), _p(QU), _p(kr),
+                                        _p(kc), _p(x)))
+        out = {"kappa_rta": np.array(res.kappa_rta).reshape(3, 3, order="F"),
+               "kappa_cg": np.array(res.kappa_cg).reshape(3, 3, order="F"), "cg_iters": res.cg_iters,
+               "status_cg": res.status_cg, "cg_err": res.cg_err,
+               "stage_ms": dict(zip(STAGES, list(res.stage_ms))),
+               "launches": dict(zip(STAGES, list(res.launches))),
+               "triplet_bands": res.triplet_bands, "d2h_bytes": res.d2h_bytes}
+        if want_modes:
+            out.update({"Q": Q, "QN": QN, "QU": QU, "kappa_rta_modes": kr, "kappa_cg_modes": kc, "x": x})
+        return out
+
+
+def cg_quadratic(a, b, vmin, max_iter=100, n_dig_accur=2):
+    """cg_quadratic (cg.f90:19) on the GPU; returns (vmin, funcmin, iters, status)."""
+    A = np.asfortranarray(a, dtype=float)
+    n = A.shape[0]
+    x = np.array(vmin, dtype=float)
+    fm = C.c_double(0)
+    it = C.c_int(0)
+    r = _check(lib().ald_cg_quadratic(n, _p(A), _p(np.ascontiguousarray(b, dtype=float)), _p(x), C.byref(fm),
+                                      max_iter, n_dig_accur, C.byref(it)), allow=(ALD_OK, ALD_WARN_CG_MAXITER))
+    return x, fm.value, it.value, r

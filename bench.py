@@ -1,0 +1,313 @@
+"""Benchmark: THERMACOND's three-phonon kappa path on B200.
+
+Workload (one step): the full job=1 sequence -- phonons on the mesh, |V3|^2
+for every IBZ q1 against every mesh q2, tetrahedron delta + Bose weights,
+linewidths Q, RTA kappa, collision matrix, RHS, CG solve, kappa -- for the
+rock-salt Morse crystal of the benchmark suite (2 atoms, 6 bands, 16x16x16
+mesh, 276 IBZ points, T = 300 K).  Inputs are synthetic: analytic Morse
+force constants written in the reference's file formats.
+
+metric: triplet-bands per second over the whole time-to-kappa step
+(triplet-bands = nibz * nkc * ndyn^3 = 2.44e8 per step), higher is better.
+
+  value  device time of K steps with the context's tables already in HBM
+         (CUDA events on the stream the library runs on; max over ranks)
+  e2e    the same metric through the C ABI from the input files: file
+         reading, table build and host->device upload, the pipeline and the
+         device->host copy of the results, per step (wall clock)
+
+--impl reference times the reference algorithm's CPU implementation (the
+oracle restatement, all host threads) on a bounded sample of IBZ rows of
+the same workload and prints the same JSON line with "impl": "reference".
+With torchrun (N>1) every rank runs its own copy of the workload (weak
+scaling, no data-path collective); the reference arm runs on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "anharmonic-lattice-dynamics_b200", "python"))
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "V3 triplet-bands/s & time-to-κ: mixed vs FP64 GPU path, 1 B200, κ err≤1e-4"
+UNIT = "triplet-bands/s"
+WORKLOAD = "rocksalt-Morse NaCl-type, 2 atoms (6 bands), 16x16x16 q-mesh, tetrahedron delta, T=300 K, FP64"
+
+
+def _peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
+    return {"hbm_gbs": 6650.0, "src": "fallback"}
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clocks and throttle reasons during the timed region."""
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "--query-gpu=" + q, "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except OSError:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9 or f[0] != str(self.index):
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"], f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(name)
+        sm.sort()
+        return {"sm_mhz": sm[len(sm) // 2] if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def make_workload(d: str, mesh=(16, 16, 16)):
+    from ald import inputs as I
+    st, rp = I.config(1, mesh=mesh)
+    I.write_inputs(st, rp, d)
+    return rp
+
+
+def cpu_baseline(d: str, rows: int = 0):
+    """The oracle (literal CPU restatement of the reference) on a bounded sample of IBZ rows:
+    V3 + tetrahedron FGR + tauRTA for `rows` rows, all host threads."""
+    import oracle_py
+    oracle_py.build()
+    nthreads = os.cpu_count() or 1
+    O = oracle_py.Oracle(d, nthreads)
+    t0 = time.time()
+    O.mesh()
+    O.phonons()
+    O.tet()
+    t_setup = time.time() - t0
+    rows = rows or min(O.nibz, nthreads)
+    t0 = time.time()
+    v33 = O.v3(1, rows)
+    P1, P2 = O.fgr(1, rows, v33)
+    O.distribution(300.0)
+    O.tau(1, rows, 300.0, P1, P2, want_p=False)
+    dt = time.time() - t0
+    tb = rows * O.nkc * O.ndyn ** 3
+    return {"value": tb / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
+            "sample": "%d of %d IBZ rows of the same workload: V3 + tetrahedron FGR + tauRTA (%.1f s); "
+                      "mesh/IBZ/phonon setup %.1f s not counted" % (rows, O.nibz, dt, t_setup),
+            "seconds": dt}
+
+
+def roofline(stage_ms, launches, nibz, nkc, b, peaks):
+    """Dominant device stage and its achieved HBM bandwidth from algorithmic bytes."""
+    stages = {k: v for k, v in stage_ms.items() if k != "total"}
+    dom = max(stages, key=stages.get)
+    n = launches.get(dom, 1) or 1
+    ms = stages[dom] / n
+    N = 3 * b * nibz
+    b3 = b ** 3
+    # algorithmic bytes per launch ("Rooflines")
+    per = {
+        "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n,            # |V3|^2 out + e(q2), e(q3) in
+        "delta": nibz * nkc * (b3 * 8 + 2 * b * b * 8 * 2) / n,      # |V3|^2 in + R1/R2 out (read+write)
+        "collision": N * N * 8 / n,                                  # CM written once
+        "cg": None,
+    }
+    bytes_ = per.get(dom)
+    if dom == "cg":
+        bytes_ = N * N * 8  # one matrix-vector product streams the matrix
+        ms = stages[dom] / max(1, (launches.get("cg", 2) - 4) // 2)
+    if bytes_ is None or ms <= 0:
+        return {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
+                "traffic": None, "kernel": dom}
+    ach = bytes_ / (ms * 1e-3) / 1e9
+    return {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+            "frac": ach / peaks["hbm_gbs"], "traffic": None, "kernel": dom, "ms_per_launch": ms,
+            "algorithmic_bytes": bytes_, "peak_source": peaks["src"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ald", choices=["ald", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--mesh", type=int, default=16)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    mesh = (args.mesh,) * 3
+
+    if args.impl == "reference":
+        if rank != 0:
+            return
+        with tempfile.TemporaryDirectory() as d:
+            make_workload(d, mesh)
+            vals = []
+            cb = None
+            for _ in range(args.warmup + args.steps):
+                cb = cpu_baseline(d)
+                vals.append(cb["value"])
+            v = sorted(vals[args.warmup:])[len(vals[args.warmup:]) // 2] if args.steps else vals[-1]
+        line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Morse FC2/FC3, reference file formats)",
+                "config": {"workload": WORKLOAD, "mesh": list(mesh)},
+                "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
+                "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+        print(json.dumps(line))
+        return
+
+    import numpy as np
+    import torch
+
+    import ald
+
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    dev = local
+    torch.cuda.set_device(dev)
+    opts = ald.default_options(device=dev, precision=ald.MIXED if args.precision == "mixed" else ald.FP64)
+    tmp = tempfile.TemporaryDirectory()
+    d = tmp.name
+    make_workload(d, mesh)
+    ctx = ald.Context(d, opts)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    tempk = ctx.info.tempk
+    nibz, nkc, b = ctx.nibz, ctx.nkc, ctx.ndyn
+
+    def step():
+        ctx.invalidate_phonons()
+        return ctx.kappa_pipeline(tempk, want_modes=False)
+
+    for _ in range(args.warmup):
+        out = step()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    stage_sum = {k: 0.0 for k in ald.STAGES}
+    launches = 0
+    with ClockSampler(dev) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            out = step()
+            for k, v in out["stage_ms"].items():
+                stage_sum[k] += v
+            launches += out["launches"]["total"] + 3  # + the eigensolver launches of get_frequencies
+        e1.record(stream)
+        torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms_max = float(t.item())
+    tb = out["triplet_bands"]
+    value = world * tb * args.steps / (ms_max * 1e-3)
+    per_step = {k: v / args.steps for k, v in stage_sum.items()}
+    per_launch_counts = dict(out["launches"])
+
+    # ---- end to end through the C ABI from the input files
+    e2e_times, h2d, d2h = [], 0.0, 0.0
+    for i in range(max(2, min(args.steps, 5)) + 1):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        c2 = ald.Context(d, opts)
+        o2 = c2.kappa_pipeline(tempk, want_modes=True)
+        torch.cuda.synchronize()
+        dt = time.perf_counter() - t0
+        h2d, d2h = c2.h2d_bytes(), o2["d2h_bytes"] + 9 * 2 * 8
+        c2.close()
+        if i > 0:
+            e2e_times.append(dt)
+    e2e = world * tb / (sorted(e2e_times)[len(e2e_times) // 2])
+    if world > 1:
+        te = torch.tensor([e2e / world], dtype=torch.float64, device="cuda")
+        torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MIN)
+        e2e = float(te.item()) * world
+
+    line = None
+    if rank == 0:
+        peaks = _peaks()
+        rf = roofline(per_step, per_launch_counts, nibz, nkc, b, peaks)
+        cb = None
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                cb = cpu_baseline(d)
+                cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+            except Exception as ex:  # the baseline is reported, never required
+                cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % ex}
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "mixed",
+                "data": "synthetic (analytic Morse FC2/FC3 written in the reference's file formats)",
+                "config": {"workload": WORKLOAD, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
+                           "triplet_bands_per_step": tb, "precision": args.precision,
+                           "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
+                               2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * 8 / 1e6),
+                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                "time_to_kappa_ms": ms_max / args.steps,
+                "stage_ms_per_step": {k: round(v, 4) for k, v in per_step.items()},
+                "kappa_cg_trace_over_3": float(np.trace(out["kappa_cg"]) / 3),
+                "cg_iters": out["cg_iters"],
+                "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                        "seconds_per_step": sorted(e2e_times)[len(e2e_times) // 2]},
+                "gpu_launches": launches, "roofline": rf, "cpu_baseline": cb, "clocks": clk.summary()}
+        print(json.dumps(line))
+    ctx.close()
+    tmp.cleanup()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

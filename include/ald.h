@@ -1,0 +1,196 @@
+/*
+ * ald.h -- C ABI of libald, the B200 (sm_100a) implementation of THERMACOND's
+ * three-phonon hot path (KeivanS/Anharmonic-lattice-dynamics).
+ *
+ * Each entry point replaces one Fortran subroutine of the job=1 sequence in
+ * THERMACOND/kappa.f90:389-871 and keeps its argument meaning:
+ *   - arrays are HOST pointers in the reference's Fortran layout
+ *     (column-major, first index fastest) with 1-based index *values*;
+ *   - complex arrays are interleaved (re, im) doubles, i.e. complex(8);
+ *   - the caller owns every host buffer; the context owns device memory and
+ *     never keeps a host pointer past the call;
+ *   - every call returns an int status, 0 = success.  The nonzero codes map
+ *     the reference's `stop` sites (a Fortran shim turns them into `stop`).
+ *
+ * Calls on one context are blocking and not thread-safe (the reference runs
+ * one thread per MPI rank); separate contexts may run concurrently.
+ */
+#ifndef ALD_H
+#define ALD_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum ald_status {
+  ALD_OK = 0,
+  ALD_ERR_ARG = 1,          /* bad argument, sizes or ksubset                        */
+  ALD_ERR_IO = 2,           /* input file missing/malformed: read_params, read_input_fit,
+                               read_lattice, read_fc234, read_born stops (rest.f90:2-443,3580) */
+  ALD_ERR_NOT_KPOINT = 3,   /* get_k_info: "vector is not a kpoint" (rest.f90:3052-3055)  */
+  ALD_ERR_DEN_ZERO = 4,     /* matrix_elt_simplified: den=0 (sub.f90:6002-6004)          */
+  ALD_ERR_NBE = 5,          /* nbe: w<=0 or t<=0 (extratools.f90:263-270)                */
+  ALD_ERR_INDEX = 6,        /* k-index round trip mismatch (sub.f90:1127-1133,8022-8025) */
+  ALD_ERR_CUDA = 7,         /* CUDA runtime or kernel error                              */
+  ALD_ERR_UNSUPPORTED = 8,  /* input outside what this build implements (message says)   */
+  ALD_ERR_NOMEM = 9,        /* device allocation failed                                  */
+  ALD_WARN_CG_MAXITER = 100 /* cg_quadratic reached max_iter; results are still returned */
+};
+
+enum ald_delta { ALD_DELTA_TETRA = 0, ALD_DELTA_GAUSS = 1 };
+enum ald_precision { ALD_FP64 = 0, ALD_MIXED = 1 };
+enum ald_cg_stop { ALD_CG_REFERENCE = 0, ALD_CG_RESIDUAL = 1 };
+
+typedef struct ald_options {
+  int delta;         /* ALD_DELTA_TETRA (reference, calculate_FGR_mpi2) or ALD_DELTA_GAUSS
+                        (extension: delta_g of width `width_cm`, extratools.f90:239)    */
+  int precision;     /* ALD_FP64 or ALD_MIXED (V3 contraction on tensor cores)          */
+  int cg_stop;       /* ALD_CG_REFERENCE: (dv/v)^2 < 10^(-2*cg_ndig) (cg.f90:30,47);
+                        ALD_CG_RESIDUAL: |Ax-b|/|b| < cg_tol                            */
+  int cg_max_iter;   /* 100 at kappa.f90:846                                            */
+  int cg_ndig;       /* 2 at kappa.f90:846                                              */
+  double cg_tol;     /* for ALD_CG_RESIDUAL                                             */
+  double width_cm;   /* Gaussian width in cm^-1 for ALD_DELTA_GAUSS (<=0: latdyn width) */
+  int device;        /* CUDA device ordinal                                             */
+  size_t chunk_bytes;/* device bytes for one chunk of |V3|^2 rows (0 = automatic)      */
+} ald_options;
+
+typedef struct ald_ctx ald_ctx;
+
+/* sizes of a loaded system */
+typedef struct ald_info {
+  int ndyn;          /* 3*natoms0 (bands)             */
+  int natoms0;       /* atoms in the primitive cell   */
+  int nc[3];         /* q-mesh                        */
+  int nkc;           /* nc(1)*nc(2)*nc(3)             */
+  int nibz;          /* IBZ size (get_weights rule)   */
+  int nterms2, nterms3;
+  int natoms;        /* supercell atoms in lat_fc.dat */
+  int lattpgcount;   /* lattice point-group order     */
+  int born_flag;
+  double tempk;      /* tmin of latdyn.params         */
+  double width_cm;   /* width of latdyn.params        */
+  double volume_r;   /* primitive-cell volume (A^3)   */
+} ald_info;
+
+void ald_default_options(ald_options* opt);
+
+/* Message of the last failing call on this thread. */
+const char* ald_last_error(void);
+
+/* Reads latdyn.params, structure.params, lat_fc.dat, fc2.dat, fc3.dat and
+ * dielectric.params from `dir` with the reference readers' record rules
+ * (read_params rest.f90:2, read_input_fit :78, read_lattice :152,
+ * read_fc234 :303, read_born :3580), builds the lattice point group
+ * (force_constants_init force_constants.f90:3-186), the q-mesh
+ * (make_kp_reg modules.f90:1721), e(-q) pairs (get_negatives rest.f90:3208),
+ * the IBZ (get_weights modules.f90:2006) and the tetrahedra
+ * (make_kp_reg_tet tetrahedron.f90:2), and uploads the tables. */
+int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out);
+void ald_destroy(ald_ctx* ctx);
+int ald_get_info(ald_ctx* ctx, ald_info* info);
+
+/* Host-only: read the input files of `dir` and build the mesh/IBZ tables
+ * without touching a GPU (no context).  `info` is filled; any array pointer
+ * may be NULL (call once with NULLs to learn nkc and nibz).  Layouts as in
+ * ald_get_mesh.  Mirrors the setup part of kappa.f90:185-337. */
+int ald_read_mesh(const char* dir, ald_info* info, double* kpc, int* mapibz, int* mapinv, double* kibz,
+                  double* wibz);
+
+/* Mesh and IBZ tables (modules.f90:1721-1784, 2006-2160):
+ * kpc(3,nkc) Cartesian 1/A including 2*pi (the FP32-fraction mesh that
+ * get_frequencies diagonalises on), mapibz(nkc), mapinv(nibz) 1-based,
+ * kibz(3,nibz), wibz(nibz).  Any pointer may be NULL. */
+int ald_get_mesh(ald_ctx* ctx, double* kpc, int* mapibz, int* mapinv, double* kibz, double* wibz);
+
+/* get_frequencies (rest.f90:2230) on the full mesh followed by subst_eivecs
+ * (rest.f90:3262): eigenval(ndyn,nkc) = |omega^2| (eV/A^2/amu),
+ * eigenvec(ndyn,ndyn,nkc) complex, veloc(3,ndyn,nkc) in units of c.
+ * Outputs may be NULL (then they are only kept on the device). */
+int ald_get_frequencies(ald_ctx* ctx, double* eigenval, double* eigenvec, double* veloc);
+
+/* Load eigenpairs and velocities from the host instead of computing them
+ * (the module arrays `eigenval`, `eigenvec`, `veloc` the reference passes
+ * between stages).  Same layouts as ald_get_frequencies. */
+int ald_set_phonons(ald_ctx* ctx, const double* eigenval, const double* eigenvec, const double* veloc);
+
+/* calculate_w3_ibz_split_sq (sub.f90:1050): |V3|^2 in cm^-2 for IBZ rows
+ * ksubset(1)..ksubset(2) (1-based, inclusive) against every mesh q2, with
+ * q3 = -q1-q2 folded on the mesh.  v33s8(nk1,nkc,ndyn,ndyn,ndyn),
+ * nk1 = ksubset(2)-ksubset(1)+1. */
+int ald_calculate_w3_ibz_split_sq(ald_ctx* ctx, const int ksubset[2], double* v33s8);
+
+/* calculate_FGR_mpi2 (sub.f90:7199): tetrahedron (or Gaussian) weighted
+ * |V3|^2: P1smpi, P2smpi(nk1,nkc,ndyn,ndyn,ndyn).  v33s8 as returned by
+ * ald_calculate_w3_ibz_split_sq for the same ksubset. */
+int ald_calculate_fgr(ald_ctx* ctx, const int ksubset[2], const double* v33s8, double* P1smpi, double* P2smpi);
+
+/* distribution (sub.f90:1955): frequency(nkc,ndyn) cm^-1, dist(nkc,ndyn). */
+int ald_distribution(ald_ctx* ctx, double tempk, double* frequency, double* dist);
+
+/* calculate_tauRTA_mpi2 (sub.f90:7953): Q, Q_N, Q_U(nk1,ndyn) and the
+ * Bose-weighted P1, P2(nk1,nkc,ndyn,ndyn,ndyn) (P1/P2 may be NULL). */
+int ald_calculate_tau_rta(ald_ctx* ctx, const int ksubset[2], double tempk, const double* P1smpi,
+                          const double* P2smpi, double* Q, double* QN, double* QU, double* P1, double* P2);
+
+/* calculate_RTA_distributionfunction (sub.f90:1238) + mode_kappa
+ * (sub.f90:1292): FFF(nibz,ndyn,3) and kappa(ndyn,3,3) in W/m/K from
+ * Q(nibz,ndyn). */
+int ald_rta_kappa(ald_ctx* ctx, double tempk, const double* Q, double* FFF, double* kappa);
+
+/* CollisionMatrix_mpi (sub.f90:3034): Collision_Matrix(nk1*ndyn*3,
+ * nibz*ndyn*3) from the Bose-weighted P1, P2 of the same ksubset. */
+int ald_collision_matrix(ald_ctx* ctx, const int ksubset[2], const double* P1, const double* P2, double* CM);
+
+/* cal_RHS_IBZ (sub.f90:2618): RHS(nibz*ndyn*3). */
+int ald_rhs(ald_ctx* ctx, double tempk, double* RHS);
+
+/* cg_quadratic (cg.f90:19): minimises 1/2 v.a.v - b.v from the initial
+ * guess vmin (overwritten), a(n,n) column-major.  Returns ALD_OK or
+ * ALD_WARN_CG_MAXITER; *iters receives the iteration count. */
+int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
+                     int n_dig_accur, int* iters);
+
+/* mode_kappa_d (sub.f90:1407): kappa(ndyn,3,3) from the CG solution
+ * Fi_x(nibz*ndyn*3) with star-averaged velocities
+ * (veloc_avergeIBZ_invsyFBZ sub.f90:5479). */
+int ald_mode_kappa_d(ald_ctx* ctx, double tempk, const double* Fi_x, double* kappa);
+
+/* The whole job=1 sequence (kappa.f90:389-871) on the device without
+ * materialising any (nibz,nkc,ndyn^3) array: phonons (unless injected),
+ * V3, delta, Q, RTA kappa, collision matrix, RHS, CG, kappa.  Only the
+ * per-mode results come back. */
+typedef struct ald_kappa_result {
+  double kappa_rta[9];     /* sum over bands, (3,3) column-major, W/m/K  */
+  double kappa_cg[9];
+  int cg_iters;
+  int status_cg;           /* ALD_OK or ALD_WARN_CG_MAXITER              */
+  double cg_err;           /* last error measure of the stop rule        */
+  /* device time per stage (CUDA events on the context's stream), ms:
+     0 phonons+occupations, 1 V3, 2 delta+Bose+band sums, 3 Q reduce,
+     4 RTA kappa, 5 collision matrix, 6 RHS, 7 CG, 8 CG kappa, 9 total   */
+  double stage_ms[10];
+  int launches[10];        /* kernel launches per stage (same indices)   */
+  double triplet_bands;    /* nibz*nkc*ndyn^3                            */
+  double d2h_bytes;        /* bytes copied back to the host by the call  */
+} ald_kappa_result;
+
+/* Run the context's work on a caller-provided cudaStream_t (e.g. one a
+ * framework already uses) instead of the context's own stream.  The
+ * stream must belong to the context's device; NULL restores the own one. */
+int ald_set_stream(ald_ctx* ctx, void* stream);
+
+/* Bytes uploaded to the device when the context was created. */
+double ald_h2d_bytes(ald_ctx* ctx);
+
+/* Q, QN, QU (nibz,ndyn), kappa_rta_modes / kappa_cg_modes (ndyn,3,3),
+ * x (nibz*ndyn*3, the CG solution) may be NULL. */
+int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double* Q, double* QN, double* QU,
+                       double* kappa_rta_modes, double* kappa_cg_modes, double* x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* ALD_H */

@@ -1,0 +1,92 @@
+"""The C ABI library on the CPU: symbols, host-side tables, error codes."""
+import os
+import re
+import shutil
+
+import numpy as np
+import pytest
+
+import example_inputs as E
+from conftest import ROOT, make_case
+
+
+def _declared_symbols():
+    txt = open(os.path.join(ROOT, "include", "ald.h")).read()
+    return sorted(set(re.findall(r"\b(ald_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(ald_lib):
+    import ctypes
+    L = ctypes.CDLL(ald_lib.LIB_PATH)
+    missing = [s for s in _declared_symbols() if not hasattr(L, s)]
+    assert not missing, missing
+    assert set(ald_lib.EXPORTS) <= set(_declared_symbols())
+
+
+@pytest.mark.parametrize("cfg,mesh", [(0, (10, 10, 10)), (1, (16, 16, 16)), (1, (6, 6, 6)), (2, (8, 8, 8))])
+def test_host_tables_equal_oracle(ald_lib, oracle_lib, workdir, cfg, mesh):
+    d = make_case(workdir, cfg, mesh)
+    info, M = ald_lib.read_mesh(d)
+    O = oracle_lib.Oracle(d)
+    O.mesh()
+    R = O.ibz()
+    assert info.nibz == O.nibz and info.lattpgcount == O.npg
+    assert np.array_equal(M["kpc"], O.kpc())
+    assert np.array_equal(M["mapinv"], R["mapinv"])
+    assert np.array_equal(M["mapibz"], R["mapibz"])
+    assert np.array_equal(M["kibz"], R["kibz"])
+    assert np.allclose(M["wibz"], R["wibz"], rtol=0, atol=1e-15)
+
+
+@pytest.mark.parametrize("name", ["ge_example", "gese_example"])
+def test_host_tables_equal_reference_ibz(ald_lib, workdir, name):
+    d = os.path.join(str(workdir), "abi_" + name)
+    z = E.materialize(name, d)
+    info, M = ald_lib.read_mesh(d)
+    assert info.nibz == len(z["out_ibz_w"])
+    assert np.abs(M["kibz"].T - z["out_ibz_kcart"]).max() < 6e-5
+    assert np.abs(M["wibz"] - z["out_ibz_w"]).max() < 1e-8
+
+
+def test_missing_file_is_an_io_error(ald_lib, workdir):
+    d = make_case(workdir, 1, (4, 4, 4))
+    bad = os.path.join(str(workdir), "bad_missing")
+    shutil.copytree(d, bad, dirs_exist_ok=True)
+    os.remove(os.path.join(bad, "fc2.dat"))
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.read_mesh(bad)
+    assert e.value.code == 2
+
+
+def test_fc3_term_count_mismatch_is_an_io_error(ald_lib, workdir):
+    d = make_case(workdir, 1, (4, 4, 4))
+    bad = os.path.join(str(workdir), "bad_count")
+    shutil.copytree(d, bad, dirs_exist_ok=True)
+    lines = open(os.path.join(bad, "fc3.dat")).read().splitlines()
+    open(os.path.join(bad, "fc3.dat"), "w").write("\n".join(lines[:-1]) + "\n")
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.read_mesh(bad)
+    assert e.value.code == 2
+    assert "READ_FC3" in str(e.value)
+
+
+def test_incompatible_masses_are_rejected(ald_lib, workdir):
+    d = make_case(workdir, 1, (4, 4, 4))
+    bad = os.path.join(str(workdir), "bad_mass")
+    shutil.copytree(d, bad, dirs_exist_ok=True)
+    p = os.path.join(bad, "lat_fc.dat")
+    txt = open(p).read().replace(" 22.99\n", " 23.0\n", 1)
+    open(p, "w").write(txt)
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.read_mesh(bad)
+    assert "not compatible" in str(e.value)
+
+
+def test_create_without_device_fails_cleanly(ald_lib, workdir):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    d = make_case(workdir, 1, (4, 4, 4))
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.Context(d)
+    assert e.value.code == 7

@@ -1,0 +1,101 @@
+"""Known-answer and property checks of the oracle and the input generators (CPU)."""
+import numpy as np
+import pytest
+
+from conftest import make_case
+
+
+@pytest.mark.parametrize("cfg,mesh,nibz", [(0, (10, 10, 10), 85), (1, (16, 16, 16), 276), (2, (32, 32, 32), 1768)])
+def test_ibz_sizes_of_the_workloads(oracle_lib, workdir, cfg, mesh, nibz):
+    d = make_case(workdir, cfg, mesh)
+    O = oracle_lib.Oracle(d)
+    assert O.mesh() == nibz
+    assert O.npg == 48
+
+
+@pytest.mark.parametrize("cfg", [0, 1])
+def test_acoustic_sum_rule_gamma(oracle_lib, workdir, cfg):
+    d = make_case(workdir, cfg, (4, 4, 4))
+    O = oracle_lib.Oracle(d)
+    ev, _ = O.get_freq(np.zeros(3))
+    assert np.all(np.abs(ev[:3]) < 1e-12 * np.abs(ev).max() + 1e-14)
+    assert np.all(ev[3:] > 1e-3 * np.abs(ev).max()) if O.ndyn > 3 else True
+
+
+def test_jacobi_matches_lapack_zheev(oracle_lib, workdir):
+    from scipy.linalg import lapack
+    d = make_case(workdir, 1, (4, 4, 4))
+    O = oracle_lib.Oracle(d)
+    O.mesh()
+    rng = np.random.default_rng(7)
+    kpc = O.kpc()
+    for n in rng.choice(O.nkc, 12, replace=False):
+        q = kpc[:, n] + rng.normal(scale=1e-2, size=3)
+        D = O.dynmat(q)
+        H = np.triu(D) + np.triu(D, 1).conj().T
+        H[np.diag_indices_from(H)] = D.diagonal().real
+        w, v, info = lapack.zheev(H)
+        assert info == 0
+        ev, vec = O.get_freq(q)
+        assert np.allclose(np.sort(np.abs(w)), ev, rtol=1e-12, atol=1e-14 * np.abs(w).max())
+
+
+def test_weight_tet_corner_map_is_a_permutation(oracle_lib):
+    """Every tie pattern of four corner energies assigns all four corners."""
+    import itertools
+    vals = [1.0, 2.0, 3.0, 4.0]
+    before = oracle_lib.weight_tet_nonperm()
+    for pat in itertools.product(range(4), repeat=4):
+        w = np.array([vals[p] for p in pat])
+        for e in (0.5, 1.0, 1.5, 2.5, 3.5, 4.0, 5.0):
+            c = oracle_lib.weight_tet(w, e)
+            assert not np.any(c == -12345.0)
+    assert oracle_lib.weight_tet_nonperm() == before
+
+
+def test_weight_tet_sum_is_tetrahedron_dos(oracle_lib):
+    """sum_k c_k equals the linear-tetrahedron density of states g(e)."""
+    rng = np.random.default_rng(3)
+    for _ in range(300):
+        w = rng.uniform(-5, 5, size=4)
+        e1, e2, e3, e4 = np.sort(np.float32(w)).astype(float)
+        e = rng.uniform(e1 - 0.2, e4 + 0.2)
+        c = oracle_lib.weight_tet(w, e)
+        if e < e1 or e > e4:
+            g = 0.0
+        elif e <= e2:
+            g = 3 * (e - e1) ** 2 / ((e2 - e1) * (e3 - e1) * (e4 - e1))
+        elif e <= e3:
+            g = 3 * ((e2 - e1) + 2 * (e - e2) - (e3 - e1 + e4 - e2) * (e - e2) ** 2 / ((e3 - e2) * (e4 - e2))) / \
+                ((e3 - e1) * (e4 - e1))
+        else:
+            g = 3 * (e4 - e) ** 2 / ((e4 - e1) * (e4 - e2) * (e4 - e3))
+        assert abs(c.sum() - g) <= 1e-4 * max(abs(g), 1e-3)
+
+
+def test_cg_quadratic_solves_spd(oracle_lib):
+    rng = np.random.default_rng(1)
+    n = 40
+    A = rng.normal(size=(n, n))
+    A = A @ A.T + n * np.eye(n)
+    b = rng.normal(size=n)
+    x, fm, it = oracle_lib.Oracle.cg(None, A, b, np.zeros(n), max_iter=200, ndig=6) if False else (None, None, None)
+    O = oracle_lib.lib()
+    import ctypes as C
+    xx = np.zeros(n)
+    fmin = C.c_double(0)
+    Af = np.asfortranarray(A)
+    it = O.orc_cg(n, Af.ctypes.data_as(oracle_lib.dp), np.ascontiguousarray(b).ctypes.data_as(oracle_lib.dp),
+                  xx.ctypes.data_as(oracle_lib.dp), C.byref(fmin), 200, 6, 2)
+    assert it < 200
+    assert np.allclose(A @ xx, b, rtol=1e-5, atol=1e-6)
+
+
+def test_small_case_end_to_end_is_finite(oracle_lib, workdir):
+    d = make_case(workdir, 1, (4, 4, 4))
+    r = oracle_lib.run_job1(d)
+    assert np.all(np.isfinite(r["kappa_cg"]))
+    kd = np.diag(r["kappa_cg"].sum(0))
+    assert np.all(kd > 0)
+    # cubic crystal: kappa isotropic within the CG tolerance
+    assert np.ptp(kd) < 0.05 * kd.mean()
