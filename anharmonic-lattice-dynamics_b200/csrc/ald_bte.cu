@@ -350,40 +350,54 @@ cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nr
 // iterations are captured once into a CUDA graph; a device flag turns the
 // remaining launches into no-ops after the stop rule fires.
 int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
-              double* err_out, double* funcmin, cudaStream_t s, std::string& msg) {
-  int nblk = (n + kGemvWarps - 1) / kGemvWarps;
-  DevBuf<double> grad, conj, aux, v0, partial, fmin;
-  DevBuf<CgDev> st;
-  if (grad.alloc(n) || conj.alloc(n) || aux.alloc(n) || v0.alloc(n) || partial.alloc(nblk) || fmin.alloc(1) ||
-      st.alloc(1)) {
+              double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
+  const int nblk = (n + kGemvWarps - 1) / kGemvWarps;
+  if (w.grad.alloc(n) || w.conj.alloc(n) || w.aux.alloc(n) || w.v0.alloc(n) || w.partial.alloc(nblk) ||
+      w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev))) {
     msg = "cg: device allocation failed";
     return ALD_ERR_NOMEM;
   }
-  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, aux.p, nullptr, nullptr);
-  cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, aux.p, db, grad.p, conj.p, st.p);
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-  if (e == cudaSuccess) {
-    for (int it = 0; it < max_iter; ++it) {
-      gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, conj.p, aux.p, partial.p, st.p);
-      cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, aux.p, partial.p, nblk, grad.p, conj.p, v0.p, dx, st.p, mode, tol);
+  CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
+  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, w.aux.p, nullptr, nullptr);
+  cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, db, w.grad.p, w.conj.p, st);
+  cudaError_t e = cudaSuccess;
+  const bool same = w.exec && w.n == n && w.max_iter == max_iter && w.mode == mode && w.tol == tol && w.A == dA &&
+                    w.b == db && w.x == dx;
+  if (!same) {
+    if (w.exec) cudaGraphExecDestroy(w.exec);
+    w.exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      for (int it = 0; it < max_iter; ++it) {
+        gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, w.conj.p, w.aux.p, w.partial.p, st);
+        cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, w.partial.p, nblk, w.grad.p, w.conj.p, w.v0.p, dx, st,
+                                                 mode, tol);
+      }
+      e = cudaStreamEndCapture(s, &graph);
     }
-    e = cudaStreamEndCapture(s, &graph);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&w.exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (e == cudaSuccess) {
+      w.n = n;
+      w.max_iter = max_iter;
+      w.mode = mode;
+      w.tol = tol;
+      w.A = dA;
+      w.b = db;
+      w.x = dx;
+    }
   }
-  if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
-  if (e == cudaSuccess) e = cudaGraphLaunch(exec, s);
-  if (exec) cudaGraphExecDestroy(exec);
-  if (graph) cudaGraphDestroy(graph);
+  if (e == cudaSuccess) e = cudaGraphLaunch(w.exec, s);
   if (e != cudaSuccess) {
     msg = std::string("cg: ") + cudaGetErrorString(e);
     return ALD_ERR_CUDA;
   }
-  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, aux.p, nullptr, nullptr);
-  cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, aux.p, db, fmin.p);
+  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, w.aux.p, nullptr, nullptr);
+  cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, w.aux.p, db, w.fmin.p);
   CgDev h;
-  e = cudaMemcpyAsync(&h, st.p, sizeof h, cudaMemcpyDeviceToHost, s);
-  if (e == cudaSuccess) e = cudaMemcpyAsync(funcmin, fmin.p, sizeof(double), cudaMemcpyDeviceToHost, s);
+  e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(funcmin, w.fmin.p, sizeof(double), cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) {
     msg = std::string("cg: ") + cudaGetErrorString(e);

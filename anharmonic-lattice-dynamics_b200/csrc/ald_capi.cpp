@@ -475,14 +475,14 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc;
   const size_t n = (size_t)nr * nkc * b * b * b;
   DevBuf<double> vf, v, p1, p2, R1, R2;
-  DevBuf<float> scratch;
+  DevBuf<char> scratch;
   CKA(vf.alloc(n));
   CKA(v.alloc(n));
   CKA(p1.alloc(n));
   CKA(p2.alloc(n));
   CKA(R1.alloc((size_t)nr * nkc * b * b));
   CKA(R2.alloc((size_t)nr * nkc * b * b));
-  CKA(scratch.alloc(std::max<size_t>(1, combine_scratch_bytes(c->geo, nr, 0) / sizeof(float))));
+  CKA(scratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, nr, 0))));
   CK(cudaMemcpyAsync(vf.p, v33s8, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(launch_from_fortran5(vf.p, v.p, nr, nkc, b, c->stream));
   CombineArgs a;
@@ -677,7 +677,8 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
   double err = 0, fm = 0;
   std::string msg;
   double tol = 1.0 / std::pow(10.0, 2 * n_dig_accur);
-  int r = cg_device(n, At.p, db.p, dx.p, max_iter, ALD_CG_REFERENCE, tol, &it, &err, &fm, s, msg);
+  CgWork work;
+  int r = cg_device(n, At.p, db.p, dx.p, max_iter, ALD_CG_REFERENCE, tol, &it, &err, &fm, s, work, msg);
   if (r != ALD_OK && r != ALD_WARN_CG_MAXITER) return fail(r, msg);
   CK(cudaMemcpyAsync(vmin, dx.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));

@@ -24,6 +24,10 @@ struct ald_ctx {
       arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
+  // pipeline workspaces, kept across calls (allocation outside the timed work)
+  DevBuf<double> w_R1, w_R2, w_Q, w_v3, w_F, w_x, w_rhs, w_kr, w_kc, w_cm;
+  DevBuf<char> w_scratch;
+  CgWork cg;
   bool have_phonons = false;
   double dist_tempk = -1;
 };

@@ -215,7 +215,7 @@ struct CombineArgs {
 };
 // scratch: the corner energies of the chunk (combine_scratch_bytes)
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss);
-cudaError_t launch_combine(const CombineArgs& a, float* scratch, cudaStream_t s);
+cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s);
 // Q/QN/QU[(n1_first+row)*b + l1] from R1/R2 of rows [0, nrows)
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s);
@@ -261,7 +261,23 @@ cudaError_t launch_tau(const Geometry& geo, int n1_first, int nrows, const int* 
 // R1/R2 = sum_l3 P1/P2 and Qd = sum (P1 + P2/2) from Bose-weighted P (internal layout)
 cudaError_t launch_collapse(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1,
                             double* R2, double* Qd, cudaStream_t s);
+// CG workspace: vectors, scalars and the captured CUDA graph of the
+// iteration loop, kept across calls and re-captured only when the problem
+// (size, pointers, stop rule) changes
+struct CgWork {
+  DevBuf<double> grad, conj, aux, v0, partial, fmin;
+  DevBuf<char> st;
+  cudaGraphExec_t exec = nullptr;
+  int n = -1, max_iter = -1, mode = -1;
+  double tol = 0;
+  const double* A = nullptr;
+  const double* b = nullptr;
+  double* x = nullptr;
+  ~CgWork() {
+    if (exec) cudaGraphExecDestroy(exec);
+  }
+};
 int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,
-              double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, std::string& msg);
+              double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg);
 
 }  // namespace ald

@@ -102,15 +102,18 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   ALD_CK(tm.end());
   // ---- 1, 2: V3 and delta/Bose/band sums, chunk by chunk
   const size_t rsz = (size_t)nibz * nkc * b * b;
-  DevBuf<double> R1, R2, Q, v3;
-  DevBuf<float> escratch;
+  DevBuf<double>& R1 = c->w_R1;
+  DevBuf<double>& R2 = c->w_R2;
+  DevBuf<double>& Q = c->w_Q;
+  DevBuf<double>& v3 = c->w_v3;
+  DevBuf<char>& escratch = c->w_scratch;
   ALD_CKA(R1.alloc(rsz));
   ALD_CKA(R2.alloc(rsz));
   ALD_CKA(Q.alloc((size_t)3 * nibz * b));
   const int K = rows_per_chunk(c);
   ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
-  ALD_CKA(escratch.alloc(std::max<size_t>(1, combine_scratch_bytes(c->geo, K, gauss) / sizeof(float))));
+  ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   for (int r0 = 0; r0 < nibz; r0 += K) {
     int nr = std::min(K, nibz - r0);
     ALD_CK(tm.begin(1));
@@ -135,7 +138,7 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
     ALD_CK(tm.begin(2));
     ALD_CK(launch_combine(a, escratch.p, s));
-    res->launches[2] += gauss ? 1 : 2;
+    res->launches[2] += gauss ? 1 : 3;
     ALD_CK(tm.end());
   }
   // ---- 3: Q, Q_N, Q_U from the band sums
@@ -149,7 +152,12 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   // ---- 4: RTA
   KappaArgs k = kappa_args(c, tempk);
   const size_t N = (size_t)3 * b * nibz;
-  DevBuf<double> F, x, rhs, kr, kc, cm;
+  DevBuf<double>& F = c->w_F;
+  DevBuf<double>& x = c->w_x;
+  DevBuf<double>& rhs = c->w_rhs;
+  DevBuf<double>& kr = c->w_kr;
+  DevBuf<double>& kc = c->w_kc;
+  DevBuf<double>& cm = c->w_cm;
   ALD_CKA(F.alloc(N));
   ALD_CKA(x.alloc(N));
   ALD_CKA(rhs.alloc(N));
@@ -180,7 +188,7 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   double tol = c->opt.cg_stop == ALD_CG_REFERENCE ? 1.0 / std::pow(10.0, 2 * c->opt.cg_ndig) : c->opt.cg_tol;
   ALD_CK(tm.begin(7));
   int rc = cg_device((int)N, cm.p, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters, &cg_err, &fm, s,
-                     msg);
+                     c->cg, msg);
   if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
   res->launches[7] += 4 + 2 * c->opt.cg_max_iter;
   ALD_CK(tm.end());

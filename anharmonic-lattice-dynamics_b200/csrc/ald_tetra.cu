@@ -8,21 +8,29 @@
 // that CollisionMatrix_mpi (sub.f90:3034) reads, so the (nibz,nkc,b^3)
 // arrays of the reference are never stored.
 //
-// Structure.  For one IBZ row q1 and bands (l2, l3) the reference gives
-// every mesh point w the corner energies
+// For one IBZ row q1 and bands (l2, l3) -- a "slice" -- the reference gives
+// every mesh point w the corner energy
 //   process 1: E(w) = -omega(w,l2) + omega(q1+w,l3)   (coalescence)
 //   process 2: E(w) =  omega(w,l2) + omega(q1-w,l3)   (decay)
-// evaluates weight_tet(omega1) on the 6*nkc tetrahedra and adds c/6 * F(w)
-// into P(w) for each of the four corners.  Here each thread owns one mesh
-// point w and gathers the 24 (tetrahedron, corner) incidences of w; all
-// their corners lie in the 3x3x3 neighbourhood of w, whose 27 energies the
-// thread holds in registers (the incidence table is a compile-time
-// constant).  P = F * sum(c/6) is formed only where a weight is nonzero,
-// then Bose-weighted and summed over l3 in registers.
-//
-// The corner weights reproduce weight_tet's mixed FP32/FP64 arithmetic
-// (ald_tet.h); this file is compiled with -fmad=false.
+// runs weight_tet(omega1(l1)) over the 6*nkc tetrahedra and adds c/6 * F(w)
+// into P(w) at the four corners.  Only tetrahedra whose energy range
+// contains omega1 carry weight.  Since omega1(l1) is ascending in l1, the
+// bands with weight on a tetrahedron form one contiguous range.  So:
+//   1. tet_energy_kernel   E(w) for every slice, as default REAL;
+//   2. delta_tet_kernel    a CTA sorts a block of tetrahedra once, queues
+//                          the (tetrahedron, l1) pairs with weight in shared
+//                          memory, then processes the queue densely: four
+//                          corner weights per pair, accumulated into
+//                          W(slice, w, l1) with FP64 atomics;
+//   3. delta_point_kernel  per mesh point: P = W * |V3|^2 * (2pi)^2/nkc,
+//                          Bose factors, sum over l3 in registers -> R1, R2.
+// The corner weights reproduce weight_tet's mixed FP32/FP64 arithmetic bit
+// for bit (ald_tet.h; this file is compiled with -fmad=false).  The sum of
+// the corner contributions into W(w, l1) runs in atomic order, so P1smpi
+// agrees with the reference to FP64 rounding, not bitwise.
 #include <cuda_runtime.h>
+
+#include <algorithm>
 
 #include "ald_internal.h"
 #include "ald_tet.h"
@@ -31,7 +39,10 @@ namespace ald {
 
 namespace {
 
-constexpr int kBlock = 128;
+constexpr int kTets = 1024;     // tetrahedra per CTA of delta_tet_kernel
+constexpr int kTetThreads = 256;
+constexpr int kPointBlock = 128;
+constexpr int kMaxBandsTet = 16;  // queue entries pack l1 into 4 bits
 
 __device__ __forceinline__ int wrapm(int v, int n) {
   v %= n;
@@ -67,46 +78,31 @@ __device__ __forceinline__ double delta_g(double x, double w) {  // extratools.f
   return exp(-x * x / 2.0 / w / w) / sqrt(2 * PhysConst::pi) / w;
 }
 
-// ---------------------------------------------------------------------------
-// The 24 incidences of a mesh point.  Cube corners (make_kp_reg_tet):
-// pt1..pt8 at offsets (0,0,0) (1,0,0) (0,1,0) (1,1,0) (0,0,1) (1,0,1) (0,1,1)
-// (1,1,1); tetrahedra l=1..6 use corners (1,2,3,6) (2,3,4,6) (1,3,5,6)
-// (3,4,6,8) (3,5,6,7) (3,6,7,8).  A point w is corner p of the cube based at
-// w - off(p).  Each incidence stores its four corners as indices of the
-// 3x3x3 neighbourhood of w (nb = (dx+1)*9 + (dy+1)*3 + (dz+1)) in the
-// tetrahedron's corner order, and which of the four is w.
-struct Incidence {
-  int nb[4];
-  int slot;
-};
+// make_kp_reg_tet (tetrahedron.f90:2-142): tetrahedron t = 6*cube + l; cube
+// corners pt1..pt8 at offsets (0,0,0) (1,0,0) (0,1,0) (1,1,0) (0,0,1) (1,0,1)
+// (0,1,1) (1,1,1); tetrahedra use (1,2,3,6) (2,3,4,6) (1,3,5,6) (3,4,6,8)
+// (3,5,6,7) (3,6,7,8)
+__constant__ int c_off[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
+                                {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+__constant__ int c_tet[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
 
-struct IncTable {
-  Incidence inc[24];
-};
-
-constexpr int kOff[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0}, {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-constexpr int kTet[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
-
-__host__ __device__ constexpr IncTable make_table() {
-  IncTable t{};
-  int n = 0;
-  for (int p = 0; p < 8; ++p)
-    for (int l = 0; l < 6; ++l)
-      for (int k = 0; k < 4; ++k)
-        if (kTet[l][k] == p) {
-          for (int c = 0; c < 4; ++c) {
-            int q = kTet[l][c];
-            int dx = kOff[q][0] - kOff[p][0], dy = kOff[q][1] - kOff[p][1], dz = kOff[q][2] - kOff[p][2];
-            t.inc[n].nb[c] = (dx + 1) * 9 + (dy + 1) * 3 + (dz + 1);
-          }
-          t.inc[n].slot = k;
-          ++n;
-        }
-  return t;
+__device__ __forceinline__ void tet_corners(const Geometry& g, int t, int* c) {
+  int m[3];
+  decompose(g, t / 6, m);
+  const int l = t % 6;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const int* o = c_off[c_tet[l][k]];
+    int mm[3] = {m[0] + o[0], m[1] + o[1], m[2] + o[2]};
+    if (mm[0] == g.nc[0]) mm[0] = 0;
+    if (mm[1] == g.nc[1]) mm[1] = 0;
+    if (mm[2] == g.nc[2]) mm[2] = 0;
+    c[k] = compose(g, mm);
+  }
 }
 
 // ---------------------------------------------------------------------------
-// corner energies E[row][l2][l3][proc][w] as default REAL (weight_tet's en)
+// E[slice][w], slice = ((row*b + l2)*b + l3)*2 + process
 __global__ void tet_energy_kernel(Geometry g, int n1_first, int nrows, const int* mapinv, const double* freq,
                                   float* E) {
   const int b = g.b, nkc = g.nkc;
@@ -131,19 +127,81 @@ __global__ void tet_energy_kernel(Geometry g, int n1_first, int nrows, const int
   }
 }
 
-__constant__ int c_inc[24][5];  // four neighbourhood indices + the slot of w
+// weight_tet over a block of tetrahedra of one slice; W[slice][w][l1] += c/6
+__global__ void __launch_bounds__(kTetThreads) delta_tet_kernel(Geometry g, int n1_first, const int* mapinv,
+                                                                const double* freq, const float* __restrict__ E,
+                                                                double* W) {
+  __shared__ double s_om[kMaxBandsTet];
+  __shared__ unsigned short s_queue[kTets * kMaxBandsTet];
+  __shared__ int s_qn;
+  const int b = g.b, nkc = g.nkc, tid = threadIdx.x, lane = tid & 31;
+  const int slice = blockIdx.y;
+  const int row = slice / (2 * b * b);
+  const int q1 = mapinv[n1_first + row];
+  if (tid < b) s_om[tid] = freq[(size_t)q1 * b + tid];
+  if (tid == 0) s_qn = 0;
+  __syncthreads();
+  const float* Es = E + (size_t)slice * nkc;
+  double* Ws = W + (size_t)slice * nkc * b;
+  const int ntet = 6 * nkc, t0 = blockIdx.x * kTets;
+  // phase 1: sort every tetrahedron once and queue (tetrahedron, l1) pairs with weight
+  for (int k = 0; k < kTets / kTetThreads; ++k) {
+    const int tl = k * kTetThreads + tid, t = t0 + tl;
+    int lo = 0, hi = 0;
+    if (t < ntet) {
+      int c[4];
+      tet_corners(g, t, c);
+      TetSorted ts = tet_sort(__ldg(Es + c[0]), __ldg(Es + c[1]), __ldg(Es + c[2]), __ldg(Es + c[3]));
+      const double E1 = ts.e1, E4 = ts.e4;
+      lo = b;
+      for (int l = 0; l < b; ++l) {
+        double e = s_om[l];
+        if (!(e < E1 || e > E4)) {
+          lo = min(lo, l);
+          hi = l + 1;
+        }
+      }
+    }
+    int cnt = hi > lo ? hi - lo : 0;
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      int v = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += v;
+    }
+    int base = 0;
+    if (lane == 31) base = atomicAdd(&s_qn, incl);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    int pos = base + incl - cnt;
+    for (int l = lo; l < hi; ++l) s_queue[pos++] = (unsigned short)((tl << 4) | l);
+  }
+  __syncthreads();
+  // phase 2: the queued pairs, four corner weights each
+  const int n = s_qn;
+  for (int i = tid; i < n; i += kTetThreads) {
+    const unsigned v = s_queue[i];
+    const int t = t0 + (int)(v >> 4), l = (int)(v & 15u);
+    int c[4];
+    tet_corners(g, t, c);
+    float en[4] = {__ldg(Es + c[0]), __ldg(Es + c[1]), __ldg(Es + c[2]), __ldg(Es + c[3])};
+    TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+    double cp[4];
+    if (!tet_weights4(ts, s_om[l], cp)) continue;
+    for (int k = 0; k < 4; ++k) {
+      const double cw = cp[tet_pos(en, k)];
+      if (cw != 0.0) atomicAdd(Ws + (size_t)c[k] * b + l, cw / 6.0);
+    }
+  }
+}
 
+// per mesh point: P = F * W, Bose factors, sums over l3
 template <int B>
-__global__ void __launch_bounds__(kBlock) delta_gather_kernel(CombineArgs a, const float* __restrict__ E) {
+__global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a, const double* __restrict__ W) {
   __shared__ double s_om1[B], s_nb1[B];
-  __shared__ float s_en[27 * kBlock];  // s_en[k * kBlock + tid]: energies of the 3x3x3 neighbourhood
-  __shared__ int s_nbr[27 * kBlock];
-  __shared__ double s_W[B * kBlock];   // per-thread sum_inc c/6 for each lambda1
   const Geometry& g = a.geo;
   const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
   const int row = blockIdx.z, l2 = blockIdx.y, tid = threadIdx.x;
-  const int n1 = a.n1_first + row;
-  const int q1 = a.mapinv[n1];
+  const int q1 = a.mapinv[a.n1_first + row];
   if (tid < B) {
     s_om1[tid] = tid < b ? a.freq[(size_t)q1 * b + tid] : 0.0;
     s_nb1[tid] = tid < b ? a.dist[(size_t)q1 * b + tid] : 0.0;
@@ -154,16 +212,6 @@ __global__ void __launch_bounds__(kBlock) delta_gather_kernel(CombineArgs a, con
   int m1[3], mw[3];
   decompose(g, q1, m1);
   decompose(g, w, mw);
-  double emin = 1e300, emax = -1e300;
-  for (int l = 0; l < b; ++l) {
-    emin = fmin(emin, s_om1[l]);
-    emax = fmax(emax, s_om1[l]);
-  }
-  for (int k = 0; k < 27; ++k) {
-    int dx = k / 9 - 1, dy = (k / 3) % 3 - 1, dz = k % 3 - 1;
-    int m[3] = {wrapm(mw[0] + dx, g.nc[0]), wrapm(mw[1] + dy, g.nc[1]), wrapm(mw[2] + dz, g.nc[2])};
-    s_nbr[k * kBlock + tid] = compose(g, m);
-  }
   int ins1, ins2;
   const int q3p = pm_index(g, m1, mw, 1, ins1);   // q1 + w
   const int q3m = pm_index(g, m1, mw, -1, ins2);  // q1 - w
@@ -176,51 +224,31 @@ __global__ void __launch_bounds__(kBlock) delta_gather_kernel(CombineArgs a, con
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   const double n2 = a.dist[(size_t)w * b + l2];
   const double* v3 = a.v3sq + (size_t)row * nkc * b3;
-
   double R1[B], R2[B];
 #pragma unroll
   for (int l = 0; l < B; ++l) R1[l] = R2[l] = 0.0;
-
   for (int l3 = 0; l3 < b; ++l3) {
-    for (int proc = 0; proc < 2; ++proc) {
-      double* W = s_W + tid;  // W[l * kBlock]
-      for (int l = 0; l < b; ++l) W[l * kBlock] = 0.0;
-      const int q3 = proc == 0 ? q3p : q3m;
-      if (!a.gauss) {
-        const float* Ep = E + ((((size_t)row * b + l2) * b + l3) * 2 + proc) * nkc;
-        for (int k = 0; k < 27; ++k) s_en[k * kBlock + tid] = __ldg(Ep + s_nbr[k * kBlock + tid]);
-        for (int i = 0; i < 24; ++i) {
-          float c4[4];
 #pragma unroll
-          for (int c = 0; c < 4; ++c) c4[c] = s_en[c_inc[i][c] * kBlock + tid];
-          TetSorted ts = tet_sort(c4[0], c4[1], c4[2], c4[3]);
-          if (emax < (double)ts.e1 || emin > (double)ts.e4) continue;
-          int pos = tet_pos(c4, c_inc[i][4]);
-#pragma unroll 1
-          for (int l = 0; l < b; ++l) {
-            double c = tet_weight(ts, pos, s_om1[l]);
-            if (c != 0.0) W[l * kBlock] += c / 6.0;
-          }
-        }
-      } else {
-        double w2 = a.freq[(size_t)w * b + l2], w3 = a.freq[(size_t)q3 * b + l3];
-        for (int l = 0; l < b; ++l)
-          W[l * kBlock] = delta_g(proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3, a.sigma);
-      }
+    for (int proc = 0; proc < 2; ++proc) {
+      const int q3 = proc == 0 ? q3p : q3m;
+      const size_t slice = (((size_t)row * b + l2) * b + l3) * 2 + proc;
       const bool zero = (l2 < 3 && w_gamma) || (l3 < 3 && (proc == 0 ? p_gamma : m_gamma));
       const int src = proc == 0 ? w : wneg;
       const double n3 = a.dist[(size_t)q3 * b + l3];
+      const double w2 = a.freq[(size_t)w * b + l2], w3 = a.freq[(size_t)q3 * b + l3];
       double* Ps = proc == 0 ? a.P1s : a.P2s;
       double* Pb = proc == 0 ? a.P1 : a.P2;
 #pragma unroll
       for (int l = 0; l < B; ++l) {
         if (l >= b) continue;
+        double wl;
+        if (a.gauss) wl = delta_g(proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3, a.sigma);
+        else wl = W[(slice * nkc + w) * b + l];
         double ps = 0.0;
-        const double wl = W[l * kBlock];
         if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * b3 + (l * b + l2) * b + l3] * fnorm);
-        double nb1 = s_nb1[l];
-        double Fb = proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1);
-        double p = ps * Fb;
+        const double nb1 = s_nb1[l];
+        const double Fb = proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1);
+        const double p = ps * Fb;
         if (proc == 0) R1[l] += p;
         else R2[l] += p;
         if (Ps || Pb) {
@@ -243,7 +271,7 @@ __global__ void __launch_bounds__(kBlock) delta_gather_kernel(CombineArgs a, con
 // Q, Q_N, Q_U from the band sums: Q = sum_{w,l2} R1 + R2/2, split by the
 // normal/umklapp flag of q1+w (process 1) and q1-w (process 2)
 __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, const double* R1, const double* R2,
-                                double* Q, double* QN, double* QU, int nibz) {
+                                double* Q, double* QN, double* QU) {
   __shared__ double red[3][32];
   const int b = g.b, nkc = g.nkc;
   const int row = blockIdx.x, l1 = blockIdx.y;
@@ -263,8 +291,7 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
       r2 += R2[base + l2];
     }
     s += r1 + 0.5 * r2;
-    double n = (i1 ? r1 : 0.0) + (i2 ? 0.5 * r2 : 0.0);
-    sn += n;
+    sn += (i1 ? r1 : 0.0) + (i2 ? 0.5 * r2 : 0.0);
     su += (i1 ? 0.0 : r1) + (i2 ? 0.0 : 0.5 * r2);
   }
   double v[3] = {s, sn, su};
@@ -285,35 +312,39 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
 }  // namespace
 
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss) {
-  return gauss ? 0 : (size_t)nrows * geo.b * geo.b * 2 * geo.nkc * sizeof(float);
+  if (gauss) return 0;
+  size_t nslice = (size_t)nrows * geo.b * geo.b * 2;
+  size_t ebytes = (nslice * geo.nkc * sizeof(float) + 255) / 256 * 256;
+  return ebytes + nslice * geo.nkc * geo.b * sizeof(double);
 }
 
-cudaError_t launch_combine(const CombineArgs& a, float* scratch, cudaStream_t s) {
+cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) {
   const Geometry& g = a.geo;
-  static bool table_set = false;
-  if (!table_set) {
-    constexpr IncTable T = make_table();
-    int h[24][5];
-    for (int i = 0; i < 24; ++i) {
-      for (int c = 0; c < 4; ++c) h[i][c] = T.inc[i].nb[c];
-      h[i][4] = T.inc[i].slot;
-    }
-    cudaError_t e = cudaMemcpyToSymbol(c_inc, h, sizeof h);
-    if (e != cudaSuccess) return e;
-    table_set = true;
-  }
+  if (g.b > kMaxBandsTet) return cudaErrorInvalidValue;
+  const double* W = nullptr;
   if (!a.gauss) {
-    size_t total = (size_t)a.nrows * g.b * g.b * 2 * g.nkc;
+    size_t nslice = (size_t)a.nrows * g.b * g.b * 2;
+    float* E = static_cast<float*>(scratch);
+    size_t ebytes = (nslice * g.nkc * sizeof(float) + 255) / 256 * 256;
+    double* Wd = reinterpret_cast<double*>(static_cast<char*>(scratch) + ebytes);
+    size_t total = nslice * g.nkc;
     int blocks = (int)std::min<size_t>((total + 255) / 256, 148 * 64);
-    tet_energy_kernel<<<blocks, 256, 0, s>>>(g, a.n1_first, a.nrows, a.mapinv, a.freq, scratch);
+    tet_energy_kernel<<<blocks, 256, 0, s>>>(g, a.n1_first, a.nrows, a.mapinv, a.freq, E);
+    cudaError_t e = cudaMemsetAsync(Wd, 0, nslice * g.nkc * g.b * sizeof(double), s);
+    if (e != cudaSuccess) return e;
+    dim3 tg((6 * g.nkc + kTets - 1) / kTets, (unsigned)nslice);
+    delta_tet_kernel<<<tg, kTetThreads, 0, s>>>(g, a.n1_first, a.mapinv, a.freq, E, Wd);
+    W = Wd;
   }
-  dim3 grid((g.nkc + kBlock - 1) / kBlock, g.b, a.nrows);
+  dim3 grid((g.nkc + kPointBlock - 1) / kPointBlock, g.b, a.nrows);
   if (g.b <= 3)
-    delta_gather_kernel<3><<<grid, kBlock, 0, s>>>(a, scratch);
+    delta_point_kernel<3><<<grid, kPointBlock, 0, s>>>(a, W);
   else if (g.b <= 6)
-    delta_gather_kernel<6><<<grid, kBlock, 0, s>>>(a, scratch);
+    delta_point_kernel<6><<<grid, kPointBlock, 0, s>>>(a, W);
   else if (g.b <= 12)
-    delta_gather_kernel<12><<<grid, kBlock, 0, s>>>(a, scratch);
+    delta_point_kernel<12><<<grid, kPointBlock, 0, s>>>(a, W);
+  else if (g.b <= 16)
+    delta_point_kernel<16><<<grid, kPointBlock, 0, s>>>(a, W);
   else
     return cudaErrorInvalidValue;
   return cudaGetLastError();
@@ -321,8 +352,9 @@ cudaError_t launch_combine(const CombineArgs& a, float* scratch, cudaStream_t s)
 
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s) {
+  (void)nibz;
   dim3 grid(nrows, geo.b);
-  q_from_r_kernel<<<grid, 256, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU, nibz);
+  q_from_r_kernel<<<grid, 256, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU);
   return cudaGetLastError();
 }
 

@@ -10,6 +10,10 @@ int main() {
     float en[4] = {(float)w[0], (float)w[1], (float)w[2], (float)w[3]};
     ald::TetSorted ts = ald::tet_sort(en[0], en[1], en[2], en[3]);
     for (int k = 0; k < 4; ++k) std::printf("%.17g ", ald::tet_weight(ts, ald::tet_pos(en, k), e));
+    // the four-at-once form used by the delta kernel
+    double cp[4] = {0, 0, 0, 0};
+    if (!ald::tet_weights4(ts, e, cp)) cp[0] = cp[1] = cp[2] = cp[3] = 0.0;
+    for (int k = 0; k < 4; ++k) std::printf("%.17g ", cp[ald::tet_pos(en, k)]);
     std::printf("\n");
   }
   return 0;
