@@ -109,6 +109,9 @@ struct State {
   std::vector<double> mass0;    // atom0(i)%mass
   // ---- lat_fc.dat (rest.f90:164-289)
   double r1[3], r2[3], r3[3], g1[3], g2[3], g3[3];
+  // make_reciprocal_lattice of g1..g3 (no 2*pi): the dual basis get_k_info
+  // projects on (extratools.f90:188-207); set by set_k_dual once g is known
+  double gd1[3], gd2[3], gd3[3];
   double volume_r = 0, volume_g = 0;
   int nterms[4] = {0};
   int natoms = 0;
@@ -159,6 +162,7 @@ void make_kp_reg(State& S);
 void get_negatives(State& S);
 void getstar(const State& S, const double kvec[3], int& narms, double kvecstar[][3], int kvecop[]);
 void get_weights(State& S);
+void set_k_dual(State& S);
 void get_k_info(const State& S, const double q[3], int& nk, int& i, int& j, int& k, int& inside);
 void set_dynamical_matrix(const State& S, const double kpt[3], cplx* dynmat);
 void hermitian_eigen(int n, const cplx* upper, double* eival, cplx* eivec);

@@ -451,6 +451,7 @@ std::string read_inputs(State& S, const std::string& dir) {
       S.g2[i] = 2 * S.K.pi * c31[i] / om;
       S.g3[i] = 2 * S.K.pi * c12[i] / om;
     }
+    set_k_dual(S);
     // calculate_volume (extratools.f90:177-186)
     S.volume_r = std::fabs(dot(S.r3, c12));
     double gc[3];

@@ -71,13 +71,16 @@ void fsort(int n, const double* r, int* mcor) {
 }
 }  // namespace
 
-void get_k_info(const State& S, const double q[3], int& nk, int& i, int& j, int& k, int& inside) {
-  static thread_local const State* cached = nullptr;
-  static thread_local RecipNo2pi rr;
-  if (cached != &S) {
-    rr = make_reciprocal_lattice(S.g1, S.g2, S.g3);
-    cached = &S;
+void set_k_dual(State& S) {
+  RecipNo2pi r = make_reciprocal_lattice(S.g1, S.g2, S.g3);
+  for (int c = 0; c < 3; ++c) {
+    S.gd1[c] = r.rr1[c];
+    S.gd2[c] = r.rr2[c];
+    S.gd3[c] = r.rr3[c];
   }
+}
+
+void get_k_info(const State& S, const double q[3], int& nk, int& i, int& j, int& k, int& inside) {
   const int* N = S.nc;
   double w[3];
   if (N[0] % 2 == 0 && N[1] % 2 == 0 && N[2] % 2 == 0) {
@@ -87,9 +90,9 @@ void get_k_info(const State& S, const double q[3], int& nk, int& i, int& j, int&
     for (int c = 0; c < 3; ++c) w[c] = q[c];
   }
   inside = 1;
-  comp1(w, rr.rr1, N[0], i, inside);
-  comp1(w, rr.rr2, N[1], j, inside);
-  comp1(w, rr.rr3, N[2], k, inside);
+  comp1(w, S.gd1, N[0], i, inside);
+  comp1(w, S.gd2, N[1], j, inside);
+  comp1(w, S.gd3, N[2], k, inside);
   nk = k + (j - 1) * N[2] + (i - 1) * N[1] * N[2];  // indexg(i,j,k,1,N1,1,N2,1,N3)
 }
 

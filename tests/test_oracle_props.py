@@ -99,3 +99,24 @@ def test_small_case_end_to_end_is_finite(oracle_lib, workdir):
     assert np.all(kd > 0)
     # cubic crystal: kappa isotropic within the CG tolerance
     assert np.ptp(kd) < 0.05 * kd.mean()
+
+
+def test_get_k_info_has_no_state_across_oracles(oracle_lib, workdir):
+    """get_k_info folds with the dual basis of the State it is given: oracles of
+    crystals with different lattice constants, created and freed one after the
+    other (so a new State may reuse a freed one's address), keep exact mesh
+    index round trips."""
+    dirs = [make_case(workdir, 1, (8, 8, 8)), make_case(workdir, 0, (8, 8, 8))]
+    kpcs = {}
+    for d in dirs:
+        O = oracle_lib.Oracle(d)
+        O.mesh()
+        kpcs[d] = O.kpc()
+        del O
+    for rep in range(16):
+        d = dirs[rep % 2]
+        O = oracle_lib.Oracle(d)
+        kpc = kpcs[d]
+        idx = [O.get_k_info(kpc[:, n])[0] for n in range(kpc.shape[1])]
+        assert idx == list(range(1, kpc.shape[1] + 1))
+        del O
