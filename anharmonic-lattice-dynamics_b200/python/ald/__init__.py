@@ -64,7 +64,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_read_mesh", "ald_get_mesh", "ald_get_frequencies", "ald_set_phonons",
            "ald_calculate_w3_ibz_split_sq", "ald_calculate_fgr", "ald_distribution", "ald_calculate_tau_rta",
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
-           "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes"]
+           "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static"]
+CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
 def lib():
@@ -82,6 +83,8 @@ def lib():
         L.ald_h2d_bytes.restype = C.c_double
         L.ald_h2d_bytes.argtypes = [C.c_void_p]
         L.ald_set_stream.argtypes = [C.c_void_p, C.c_void_p]
+        L.ald_cg_quadratic_static.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
+                                              C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p]
         for n in EXPORTS[2:]:
             if n not in ("ald_destroy", "ald_h2d_bytes"):
                 getattr(L, n).restype = C.c_int
@@ -281,3 +284,18 @@ def cg_quadratic(a, b, vmin, max_iter=100, n_dig_accur=2):
     r = _check(lib().ald_cg_quadratic(n, _p(A), _p(np.ascontiguousarray(b, dtype=float)), _p(x), C.byref(fm),
                                       max_iter, n_dig_accur, C.byref(it)), allow=(ALD_OK, ALD_WARN_CG_MAXITER))
     return x, fm.value, it.value, r
+
+
+def cg_quadratic_static(n: int, a_ptr: int, b_ptr: int, x_ptr: int, max_iter=100, n_dig_accur=2, stream: int = 0):
+    """cg_quadratic on caller-owned DEVICE buffers without any device
+    allocation (ald_cg_quadratic_static).  a_ptr, b_ptr, x_ptr are device
+    addresses of a(n,n) column-major, b(n) and the initial guess, which is
+    overwritten by the solution; `stream` is a cudaStream_t handle (0 = the
+    default stream).  Returns (funcmin, iters, status)."""
+    fm = C.c_double(0)
+    it = C.c_int(0)
+    r = _check(lib().ald_cg_quadratic_static(n, C.c_void_p(a_ptr), C.c_void_p(b_ptr), C.c_void_p(x_ptr),
+                                             C.byref(fm), max_iter, n_dig_accur, C.byref(it),
+                                             C.c_void_p(stream) if stream else None),
+               allow=(ALD_OK, ALD_WARN_CG_MAXITER))
+    return fm.value, it.value, r

@@ -31,6 +31,7 @@ SOURCES = {
     "ald_tetra.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
     "ald_bte.cu": [],
     "ald_util.cu": [],
+    "ald_cg_static.cu": [],
 }
 
 

@@ -153,6 +153,23 @@ int ald_rhs(ald_ctx* ctx, double tempk, double* RHS);
 int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
                      int n_dig_accur, int* iters);
 
+/* No counterpart in the reference: cg_quadratic (cg.f90:19) for callers that
+ * cannot allocate device memory -- codes whose device memory all comes from
+ * their own pool or from another framework's allocator, where a cudaMalloc
+ * inside the library breaks the pool's accounting and a cudaFree stalls the
+ * whole device.  a(n,n) (column-major), b(n) and vmin(n) are DEVICE pointers
+ * on the current device; vmin holds the initial guess and receives the
+ * solution.  The work runs on `stream` (a cudaStream_t, NULL = the default
+ * stream) and the call returns after it finished.  Nothing is allocated: the
+ * CG work vectors live in a fixed __device__ array of the library, so
+ * n <= ALD_CG_STATIC_MAX_N (ALD_ERR_ARG otherwise).  The first call on a
+ * device looks that array's address up; make it before any stream capture.
+ * Calls share the array: calls that overlap on one device race.  Returns
+ * ALD_OK or ALD_WARN_CG_MAXITER like ald_cg_quadratic. */
+#define ALD_CG_STATIC_MAX_N 32768
+int ald_cg_quadratic_static(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
+                            int n_dig_accur, int* iters, void* stream);
+
 /* mode_kappa_d (sub.f90:1407): kappa(ndyn,3,3) from the CG solution
  * Fi_x(nibz*ndyn*3) with star-averaged velocities
  * (veloc_avergeIBZ_invsyFBZ sub.f90:5479). */
