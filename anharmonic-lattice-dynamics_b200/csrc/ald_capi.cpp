@@ -134,13 +134,33 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
   a.const33 = PhysConst::const33();
   a.v3sq = out;
   a.err = c->err.p;
+  a.ncls = c->VC.ncls;
+  a.cls_grp_off = c->cls_grp_off.p;
+  a.cls_pc = c->cls_pc.p;
+  a.cls_trip_off = c->cls_trip_off.p;
+  a.cls_trip = c->cls_trip.p;
+  a.cls_trip_i0 = c->cls_trip_i0.p;
+  a.cls_trip_k = c->cls_trip_k.p;
+  a.hbuf = nullptr;
   return a;
 }
 
-int run_v3(ald_ctx* c, const V3Args& a) {
+int run_v3(ald_ctx* c, const V3Args& a0) {
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
   if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "V3: more than 12 bands is not supported by this build");
-  cudaError_t e = (c->opt.precision == ALD_MIXED) ? launch_v3_mixed(a, c->stream) : launch_v3_fp64(a, c->stream);
+  const int prec = c->opt.precision;
+  V3Args a = a0;
+  cudaError_t e;
+  if (v3_pair_supported(c->geo.b, prec)) {
+    const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
+    if (c->w_h.n < need) CKA(c->w_h.alloc(need));
+    a.hbuf = c->w_h.p;
+    e = launch_v3_pair(a, prec, c->stream);
+  } else if (prec == ALD_FP64) {
+    e = launch_v3_fp64(a, c->stream);
+  } else {
+    return fail(ALD_ERR_UNSUPPORTED, "V3: the mixed-precision path supports 3 or 6 bands in this build");
+  }
   if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 launch: ") + cudaGetErrorString(e));
   return ALD_OK;
 }
@@ -211,7 +231,7 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   else ald_default_options(&c->opt);
   std::string e = read_system(dir, c->S);
   if (!e.empty()) return fail(ALD_ERR_IO, e);
-  // b200.params knobs apply where the caller left the defaults
+  // b200.params knobs apply when the caller passes no options
   if (!opt) {
     if (c->S.delta >= 0) c->opt.delta = c->S.delta;
     if (c->S.precision >= 0) c->opt.precision = c->S.precision;
@@ -223,6 +243,8 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   if (!e.empty()) return fail(e.find("not a kpoint") != std::string::npos ? ALD_ERR_NOT_KPOINT : ALD_ERR_IO, e);
   if (c->S.include_fc[2] == 1) {
     e = build_fc3(c->S, c->F3);
+    if (!e.empty()) return fail(ALD_ERR_IO, e);
+    e = build_v3_classes(c->S, c->T, c->F3, c->VC);
     if (!e.empty()) return fail(ALD_ERR_IO, e);
   }
   e = build_fc2(c->S, c->F2);
@@ -274,6 +296,12 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
     CKA(upload(c->trip_j, c->F3.trip_j, s));
     CKA(upload(c->trip_k, c->F3.trip_k, s));
     CKA(upload(c->fc3w, c->F3.w, s));
+    CKA(upload(c->cls_grp_off, c->VC.grp_off, s));
+    CKA(upload(c->cls_pc, c->VC.pc, s));
+    CKA(upload(c->cls_trip_off, c->VC.trip_off, s));
+    CKA(upload(c->cls_trip, c->VC.trip, s));
+    CKA(upload(c->cls_trip_i0, c->VC.trip_i0, s));
+    CKA(upload(c->cls_trip_k, c->VC.trip_k, s));
   }
   {
     std::vector<double> rt(2 * (size_t)c->T.L);

@@ -11,6 +11,7 @@ struct ald_ctx {
   System S;
   Tables T;
   Fc3Blocks F3;
+  V3Classes VC;
   Fc2Csr F2;
   ald_options opt;
   int device = 0;
@@ -22,6 +23,8 @@ struct ald_ctx {
   DevBuf<double> kpc32, rr, fc2_val, fc2_sqm, born, fc3w, roots, opk, opk_inv;
   DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,
       arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
+  DevBuf<int> cls_grp_off, cls_pc, cls_trip_off, cls_trip, cls_trip_i0, cls_trip_k;
+  DevBuf<char> w_h;                   // per-row phase-class sums of the pair kernel
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
   // pipeline workspaces, kept across calls (allocation outside the timed work)

@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <numeric>
 #include <unordered_map>
 
@@ -746,6 +747,64 @@ std::string build_fc3(const System& S, Fc3Blocks& F) {
     for (int c = 0; c < 27; ++c) F.w[27 * (size_t)n + c] = vals[order[n]][c];
   }
   for (int b = 0; b < nblk; ++b) F.blk_off[b + 1] += F.blk_off[b];
+  return "";
+}
+
+std::string build_v3_classes(const System& S, const Tables& T, const Fc3Blocks& F, V3Classes& C) {
+  const int nb = S.nat0, L = T.L;
+  struct Cls {
+    int g, d[3];
+    std::vector<int> members;
+  };
+  std::map<std::array<int, 4>, int> where;  // (g, d) -> class
+  std::vector<Cls> cls;
+  std::vector<int> owner_i0(F.ntrip);
+  for (int blk = 0; blk < nb * nb * nb; ++blk)
+    for (int t = F.blk_off[blk]; t < F.blk_off[blk + 1]; ++t) owner_i0[t] = blk / (nb * nb);
+  for (int t = 0; t < F.ntrip; ++t) {
+    const int j = F.trip_j[t], k = F.trip_k[t];
+    const int j0 = S.cell0[j] - 1, k0 = S.cell0[k] - 1;
+    std::array<int, 4> key = {j0 * nb + k0, S.cell[3 * j] - S.cell[3 * k], S.cell[3 * j + 1] - S.cell[3 * k + 1],
+                              S.cell[3 * j + 2] - S.cell[3 * k + 2]};
+    auto it = where.find(key);
+    int c;
+    if (it == where.end()) {
+      c = (int)cls.size();
+      where[key] = c;
+      cls.push_back({key[0], {key[1], key[2], key[3]}, {}});
+    } else {
+      c = it->second;
+    }
+    cls[c].members.push_back(t);
+  }
+  // group order; within a group, first appearance order
+  std::vector<int> order(cls.size());
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cls[a].g < cls[b].g; });
+  C.ncls = (int)cls.size();
+  C.grp_off.assign(nb * nb + 1, 0);
+  C.pc.assign(4 * (size_t)C.ncls, 0);
+  C.trip_off.assign(1, 0);
+  C.trip.clear();
+  C.trip_i0.clear();
+  C.trip_k.clear();
+  for (int n = 0; n < C.ncls; ++n) {
+    const Cls& c = cls[order[n]];
+    C.grp_off[c.g + 1]++;
+    // phase of q(m).(R_j - R_k): the difference of the two atoms' coefficients
+    const int j = F.trip_j[c.members[0]], k = F.trip_k[c.members[0]];
+    for (int a = 0; a < 4; ++a) {
+      long v = (long)T.phase_coef[4 * j + a] - (long)T.phase_coef[4 * k + a];
+      C.pc[4 * (size_t)n + a] = (int)(((v % L) + L) % L);
+    }
+    for (int t : c.members) {
+      C.trip.push_back(t);
+      C.trip_i0.push_back(owner_i0[t]);
+      C.trip_k.push_back(F.trip_k[t]);
+    }
+    C.trip_off.push_back((int)C.trip.size());
+  }
+  for (int g = 0; g < nb * nb; ++g) C.grp_off[g + 1] += C.grp_off[g];
   return "";
 }
 

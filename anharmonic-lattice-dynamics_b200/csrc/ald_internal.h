@@ -108,6 +108,21 @@ struct Fc3Blocks {
 };
 std::string build_fc3(const System& S, Fc3Blocks& F);
 
+// The FC3 triples regrouped for the pair kernel.  With q3 = -q1-q2 on the
+// mesh, the phase of triple (i0, j, k) is exp(i q2.(R_j - R_k)) exp(-i q1.R_k),
+// so triples that share (j0, k0, R_j - R_k) -- a "class" -- share their
+// q2-dependent phase.  Classes are grouped by g = j0*nat0 + k0.
+struct V3Classes {
+  int ncls = 0;
+  std::vector<int> grp_off;   // nat0^2 + 1
+  std::vector<int> pc;        // 4 per class: phase coefficients of R_j - R_k (mod L)
+  std::vector<int> trip_off;  // ncls + 1: member triples of each class
+  std::vector<int> trip;      // member triple (index into Fc3Blocks)
+  std::vector<int> trip_i0;   // its primitive atom i0
+  std::vector<int> trip_k;    // its supercell atom k (row phase exp(-i q1.R_k))
+};
+std::string build_v3_classes(const System& S, const Tables& T, const Fc3Blocks& F, V3Classes& C);
+
 // FC2 grouped per dynamical-matrix element (i3, j3) in the file's term
 // order (the order set_dynamical_matrix sums them).
 struct Fc2Csr {
@@ -191,9 +206,21 @@ struct V3Args {
   double const33;
   double* v3sq;              // [row][q2][l1][l2][l3]
   int* err;
+  // phase classes (pair kernel)
+  int ncls;
+  const int* cls_grp_off;
+  const int* cls_pc;
+  const int* cls_trip_off;
+  const int* cls_trip;
+  const int* cls_trip_i0;
+  const int* cls_trip_k;
+  void* hbuf;                // row workspace: nrows*ncls*9*b complex (v3_hbuf_bytes)
 };
 cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s);
-cudaError_t launch_v3_mixed(const V3Args& a, cudaStream_t s);
+// pair kernel: bands it handles and the row workspace it needs (0 = not handled)
+bool v3_pair_supported(int b, int precision);
+size_t v3_hbuf_bytes(int b, int ncls, int nrows, int precision);
+cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s);
 
 struct CombineArgs {
   Geometry geo;

@@ -180,6 +180,5 @@ cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-cudaError_t launch_v3_mixed(const V3Args&, cudaStream_t) { return cudaErrorNotSupported; }
 
 }  // namespace ald

@@ -412,4 +412,11 @@ def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0) -
         return lj_argon(), RunParams(mesh=tuple(mesh or (32, 32, 32)), tempk=tempk,
                                      width_cm=0.05 * THZ_TO_CM, delta="gauss", cg_stop="residual",
                                      cg_tol=1e-8)
+    if n == 3:
+        # one structure of the batched suite: superlattice p (default 1: the
+        # 4-atom conventional cell, 12 bands), mesh (ceil(12/p) >= 2) x 12 x 12
+        p = 1
+        m = mesh or (max(2, -(-12 // p)), 12, 12)
+        return lj_superlattice(p, seed=20261203), RunParams(mesh=tuple(m), tempk=tempk, width_cm=0.1 * THZ_TO_CM,
+                                                              delta="gauss")
     raise ValueError("unknown configuration %r" % n)
