@@ -243,6 +243,10 @@ struct CombineArgs {
 // scratch: the corner energies of the chunk (combine_scratch_bytes)
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss);
 cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s);
+// tetrahedron delta fused into R1/R2 (pipeline; P1s/P2s/P1/P2 not produced);
+// R1/R2 of the chunk must be zero on entry
+bool delta_fused_supported(const Geometry& g);
+cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s);
 // Q/QN/QU[(n1_first+row)*b + l1] from R1/R2 of rows [0, nrows)
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s);

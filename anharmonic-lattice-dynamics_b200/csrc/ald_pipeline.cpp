@@ -113,7 +113,9 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   const int K = rows_per_chunk(c);
   ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
-  ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
+  // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
+  const bool fused = !gauss && delta_fused_supported(c->geo);
+  if (!fused) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   for (int r0 = 0; r0 < nibz; r0 += K) {
     int nr = std::min(K, nibz - r0);
     ALD_CK(tm.begin(1));
@@ -137,8 +139,16 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
     a.R2 = R2.p + (size_t)r0 * nkc * b * b;
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
     ALD_CK(tm.begin(2));
-    ALD_CK(launch_combine(a, escratch.p, s));
-    res->launches[2] += gauss ? 1 : 3;
+    if (fused) {
+      const size_t n = (size_t)nr * nkc * b * b * sizeof(double);
+      ALD_CK(cudaMemsetAsync(a.R1, 0, n, s));
+      ALD_CK(cudaMemsetAsync(a.R2, 0, n, s));
+      ALD_CK(launch_delta_fused(a, s));
+      res->launches[2] += 1;
+    } else {
+      ALD_CK(launch_combine(a, escratch.p, s));
+      res->launches[2] += gauss ? 1 : 3;
+    }
     ALD_CK(tm.end());
   }
   // ---- 3: Q, Q_N, Q_U from the band sums

@@ -309,6 +309,174 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
   }
 }
 
+// ---------------------------------------------------------------------------
+// Fused tetrahedron delta for the pipeline: the weights of every
+// (tetrahedron, l1) pair go straight into R1/R2 -- no corner-energy or weight
+// array in HBM.  A CTA owns one IBZ row, one process and one band l2, and a
+// block of mesh cells: plane i, rows j0 .. j0+R-1, all k (thread = cell).  The
+// corners of those cells form a window of 2 x (R+1) x N2 mesh points, whose
+// energies, Bose factors and indices are staged in shared memory once per l3.
+// Per l3 (one slice of the reference's loops):
+//   1. per window point: E = -+omega(w,l2) + omega(q1+-w,l3) as default REAL,
+//      G = n2 (n3+1) [process 1] or (n2+1)(n3+1) [process 2], G = 0 where the
+//      reference zeroes acoustic modes at Gamma (sub.f90:7351-7356, 7412-7417);
+//   2. per cell: its 8 corner energies, its 6 tetrahedra sorted once; each
+//      tetrahedron whose range may contain a band energy omega1(l1) is stored
+//      as a record (sorted energies + corner of each sorted position) and its
+//      (record, l1) pairs queued;
+//   3. per queued pair: weight_tet's four corner weights c (bitwise, ald_tet.h)
+//      and R(row, w, l1, l2) += c/6 (2pi)^2/nkc |V3|^2 n1 G for each corner.
+// The sums run in atomic order (FP64 rounding, not bitwise, against the
+// reference's P1/P2 summed over l3).
+constexpr int kFusedThreads = 128;
+
+template <int B>
+__global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs a, int R, int nbj) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  __shared__ double s_om[B], s_nb1[B];
+  __shared__ float s_omlo[B], s_omhi[B];
+  __shared__ int s_nrec, s_nq;
+  const Geometry& g = a.geo;
+  const int N0 = g.nc[0], N1 = g.nc[1], N2 = g.nc[2], nkc = g.nkc, b = g.b, b2 = b * b, b3 = b2 * b;
+  const int NW = 2 * (R + 1) * N2, ncell = R * N2, maxrec = 6 * ncell;
+  const int tid = threadIdx.x, lane = tid & 31;
+  const int row = blockIdx.y, proc = blockIdx.z % 2, l2 = blockIdx.z / 2;
+  const int pi = blockIdx.x / nbj, j0 = (blockIdx.x % nbj) * R;
+  // shared layout
+  double* s_G = reinterpret_cast<double*>(smraw);
+  float4* s_rece = reinterpret_cast<float4*>(s_G + NW + (NW & 1));
+  ushort4* s_recp = reinterpret_cast<ushort4*>(s_rece + maxrec);
+  int* s_w = reinterpret_cast<int*>(s_recp + maxrec);
+  int* s_q3 = s_w + NW;
+  int* s_src = s_q3 + NW;
+  float* s_E = reinterpret_cast<float*>(s_src + NW);
+  unsigned char* s_fl = reinterpret_cast<unsigned char*>(s_E + NW);
+  unsigned short* s_queue = reinterpret_cast<unsigned short*>(s_fl + ((NW + 3) & ~3));
+
+  const int q1 = a.mapinv[a.n1_first + row];
+  int m1[3];
+  decompose(g, q1, m1);
+  if (tid < b) {
+    const double om = a.freq[(size_t)q1 * b + tid];
+    s_om[tid] = om;
+    s_omlo[tid] = __double2float_rd(om);
+    s_omhi[tid] = __double2float_ru(om);
+    s_nb1[tid] = a.dist[(size_t)q1 * b + tid];
+  }
+  // window points: global index, q3 = q1 +- w, source row of |V3|^2, Gamma flags
+  for (int p = tid; p < NW; p += blockDim.x) {
+    const int k = p % N2, t = p / N2, dj = t % (R + 1), di = t / (R + 1);
+    int mw[3] = {(pi + di) % N0, (j0 + dj) % N1, k};
+    const int w = compose(g, mw);
+    int ins;
+    const int q3 = pm_index(g, m1, mw, proc == 0 ? 1 : -1, ins);
+    int m3[3];
+    decompose(g, q3, m3);
+    s_w[p] = w;
+    s_q3[p] = q3;
+    s_src[p] = proc == 0 ? w : neg_index(g, mw);
+    s_fl[p] = (unsigned char)((at_gamma_index(g, mw) ? 1 : 0) | (at_gamma_index(g, m3) ? 2 : 0));
+  }
+  const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
+  double* Rp = proc == 0 ? a.R1 : a.R2;
+  const double* v3row = a.v3sq + (size_t)row * nkc * b3;
+  // this thread's cell
+  const int cdj = tid / N2, ck = tid % N2;
+  const bool cell_ok = tid < ncell && j0 + cdj < N1;
+  int lp[8];
+#pragma unroll
+  for (int c = 0; c < 8; ++c) {
+    const int o0 = c_off[c][0], o1 = c_off[c][1], o2 = c_off[c][2];
+    const int kk = ck + o2 == N2 ? 0 : ck + o2;
+    lp[c] = cell_ok ? (o0 * (R + 1) + cdj + o1) * N2 + kk : 0;
+  }
+  for (int l3 = 0; l3 < b; ++l3) {
+    __syncthreads();  // previous slice done with the window and the queue
+    if (tid == 0) {
+      s_nrec = 0;
+      s_nq = 0;
+    }
+    for (int p = tid; p < NW; p += blockDim.x) {
+      const int w = s_w[p], q3 = s_q3[p];
+      const double fw = a.freq[(size_t)w * b + l2], f3 = a.freq[(size_t)q3 * b + l3];
+      s_E[p] = (float)(proc == 0 ? -fw + f3 : fw + f3);
+      const double n2 = a.dist[(size_t)w * b + l2], n3 = a.dist[(size_t)q3 * b + l3];
+      const bool zero = (l2 < 3 && (s_fl[p] & 1)) || (l3 < 3 && (s_fl[p] & 2));
+      s_G[p] = zero ? 0.0 : (proc == 0 ? n2 * (n3 + 1) : (n2 + 1) * (n3 + 1));
+    }
+    __syncthreads();
+    // phase 1: sort the 6 tetrahedra of this cell, queue (record, l1) pairs
+    constexpr int kTet[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
+    float ec[8];
+#pragma unroll
+    for (int c = 0; c < 8; ++c) ec[c] = s_E[lp[c]];
+#pragma unroll
+    for (int l = 0; l < 6; ++l) {
+      float en[4];
+#pragma unroll
+      for (int k = 0; k < 4; ++k) en[k] = ec[kTet[l][k]];
+      const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+      int lo = b, hi = 0;
+      if (cell_ok) {
+        for (int l1 = 0; l1 < b; ++l1)
+          if (s_omhi[l1] >= ts.e1 && s_omlo[l1] <= ts.e4) {
+            lo = min(lo, l1);
+            hi = l1 + 1;
+          }
+      }
+      const int cnt = hi > lo ? hi - lo : 0;
+      const unsigned mask = __ballot_sync(0xffffffffu, cnt > 0);
+      if (mask == 0u) continue;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int rbase = 0, qbase = 0;
+      if (lane == 31) {
+        rbase = atomicAdd(&s_nrec, __popc(mask));
+        qbase = atomicAdd(&s_nq, incl);
+      }
+      rbase = __shfl_sync(0xffffffffu, rbase, 31);
+      qbase = __shfl_sync(0xffffffffu, qbase, 31);
+      if (cnt > 0) {
+        const int rec = rbase + __popc(mask & ((1u << lane) - 1u));
+        s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
+        // corner at each sorted position (tet_pos is a permutation of 0..3)
+        const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2), ps3 = tet_pos(en, 3);
+        const int c0 = lp[kTet[l][0]], c1 = lp[kTet[l][1]], c2 = lp[kTet[l][2]], c3 = lp[kTet[l][3]];
+        auto at = [&](int p) { return (unsigned short)(ps0 == p ? c0 : ps1 == p ? c1 : ps2 == p ? c2 : c3); };
+        s_recp[rec] = make_ushort4(at(0), at(1), at(2), at(3));
+        int q = qbase + incl - cnt;
+        for (int l1 = lo; l1 < hi; ++l1) s_queue[q++] = (unsigned short)((rec << 4) | l1);
+      }
+    }
+    __syncthreads();
+    // phase 2: corner weights of the queued pairs into R
+    const int nq = s_nq;
+    for (int i = tid; i < nq; i += blockDim.x) {
+      const unsigned v = s_queue[i];
+      const int rec = (int)(v >> 4), l1 = (int)(v & 15u);
+      const float4 e = s_rece[rec];
+      const TetSorted ts = tet_sort(e.x, e.y, e.z, e.w);
+      double cp[4];
+      if (!tet_weights4(ts, s_om[l1], cp)) continue;
+      const ushort4 pp = s_recp[rec];
+      const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int p = pos_pt[k];
+        const double G = s_G[p];
+        if (cp[k] == 0.0 || G == 0.0) continue;
+        const double v3 = v3row[(size_t)s_src[p] * b3 + (l1 * b + l2) * b + l3];
+        const double val = (cp[k] / 6.0) * (v3 * fnorm) * (s_nb1[l1] * G);
+        atomicAdd(Rp + (((size_t)row * nkc + s_w[p]) * b + l1) * b + l2, val);
+      }
+    }
+  }
+}
+
 }  // namespace
 
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss) {
@@ -347,6 +515,44 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) 
     delta_point_kernel<16><<<grid, kPointBlock, 0, s>>>(a, W);
   else
     return cudaErrorInvalidValue;
+  return cudaGetLastError();
+}
+
+// rows of cells per CTA of the fused kernel and its shared memory
+static void fused_shape(const Geometry& g, int& R, int& nbj, size_t& smem) {
+  const int N1 = g.nc[1], N2 = g.nc[2];
+  R = std::max(1, std::min(N1, kFusedThreads / N2));
+  nbj = (N1 + R - 1) / R;
+  const int NW = 2 * (R + 1) * N2, maxrec = 6 * R * N2;
+  smem = (size_t)(NW + (NW & 1)) * 8 + (size_t)maxrec * 16 + (size_t)maxrec * 8 + (size_t)NW * 3 * 4 +
+         (size_t)NW * 4 + (size_t)((NW + 3) & ~3) + (size_t)maxrec * g.b * 2;
+}
+
+bool delta_fused_supported(const Geometry& g) { return g.b <= kMaxBandsTet && g.nc[2] <= kFusedThreads; }
+
+cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
+  const Geometry& g = a.geo;
+  if (!delta_fused_supported(g)) return cudaErrorInvalidValue;
+  int R, nbj;
+  size_t smem;
+  fused_shape(g, R, nbj, smem);
+  if (smem > 200 * 1024) return cudaErrorInvalidValue;
+  dim3 grid(g.nc[0] * nbj, a.nrows, 2 * g.b);
+  cudaError_t e;
+#define ALD_FUSED(BB)                                                                                   \
+  e = cudaFuncSetAttribute(delta_fused_kernel<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+  if (e != cudaSuccess) return e;                                                                       \
+  delta_fused_kernel<BB><<<grid, kFusedThreads, smem, s>>>(a, R, nbj);
+  if (g.b <= 3) {
+    ALD_FUSED(3)
+  } else if (g.b <= 6) {
+    ALD_FUSED(6)
+  } else if (g.b <= 12) {
+    ALD_FUSED(12)
+  } else {
+    ALD_FUSED(16)
+  }
+#undef ALD_FUSED
   return cudaGetLastError();
 }
 

@@ -402,7 +402,8 @@ def lj_superlattice(p: int, seed: int, a: float = 5.26, eps: float = 0.0104,
 
 
 # configurations of the benchmark suite (seeded synthetic stand-ins)
-def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0) -> Tuple[Structure, RunParams]:
+def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0,
+           rc_sigma: float = 2.5) -> Tuple[Structure, RunParams]:
     if n == 0:
         return lj_argon(), RunParams(mesh=tuple(mesh or (10, 10, 10)), tempk=tempk,
                                      width_cm=0.1 * THZ_TO_CM, delta="gauss")
@@ -417,6 +418,6 @@ def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0) -
         # 4-atom conventional cell, 12 bands), mesh (ceil(12/p) >= 2) x 12 x 12
         p = 1
         m = mesh or (max(2, -(-12 // p)), 12, 12)
-        return lj_superlattice(p, seed=20261203), RunParams(mesh=tuple(m), tempk=tempk, width_cm=0.1 * THZ_TO_CM,
-                                                              delta="gauss")
+        return (lj_superlattice(p, seed=20261203, rc_sigma=rc_sigma),
+                RunParams(mesh=tuple(m), tempk=tempk, width_cm=0.1 * THZ_TO_CM, delta="gauss"))
     raise ValueError("unknown configuration %r" % n)

@@ -38,8 +38,12 @@ def workdir(tmp_path_factory):
 def make_case(workdir, cfg, mesh, **kw):
     """Write one synthetic configuration into workdir and return its path."""
     from ald import inputs as I
-    st, rp = I.config(cfg, mesh=mesh)
+    skw = {"rc_sigma": kw.pop("rc_sigma")} if "rc_sigma" in kw else {}
+    st, rp = I.config(cfg, mesh=mesh, **skw)
+    kw.update({"_" + k: v for k, v in skw.items()})  # part of the directory tag only
     for k, v in kw.items():
+        if k.startswith("_"):
+            continue
         setattr(rp, k, v)
     tag = "c%d_%s_%s" % (cfg, "x".join(map(str, mesh)), "_".join("%s%s" % kv for kv in sorted(kw.items())))
     d = os.path.join(str(workdir), tag)

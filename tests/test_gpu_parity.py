@@ -30,9 +30,10 @@ def close(g, r, rtol=RTOL, atol=ATOL):
 
 
 # rock-salt Morse (6 bands), LJ argon (3 bands) and the 4-atom LJ superlattice
-# cell (12 bands, broad Gaussian so that the small mesh scatters at all)
+# cell (12 bands; nearest-neighbour cutoff 1.2 sigma so that the oracle stays
+# fast, broad Gaussian so that the small mesh scatters at all)
 CASES = [(1, (4, 4, 4), {}), (1, (6, 6, 6), {}), (0, (6, 6, 6), {"delta": "gauss"}), (0, (4, 4, 4), {"delta": "tetra"}),
-         (3, (4, 2, 2), {"delta": "gauss", "width_cm": 5.0})]
+         (3, (4, 4, 4), {"delta": "gauss", "width_cm": 5.0, "rc_sigma": 1.2})]
 
 
 @pytest.fixture(scope="module", params=CASES, ids=lambda c: "cfg%d_%s_%s" % (c[0], c[1][0], c[2].get("delta", "")))
