@@ -133,6 +133,7 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
   a.roots = c->roots.p;
   a.const33 = PhysConst::const33();
   a.v3sq = out;
+  a.v3_layout = 0;
   a.err = c->err.p;
   a.ncls = c->VC.ncls;
   a.cls_grp_off = c->cls_grp_off.p;
@@ -156,10 +157,10 @@ int run_v3(ald_ctx* c, const V3Args& a0) {
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
     e = launch_v3_pair(a, prec, c->stream);
-  } else if (prec == ALD_FP64) {
+  } else if (prec == ALD_FP64 && a.v3_layout == 0) {
     e = launch_v3_fp64(a, c->stream);
   } else {
-    return fail(ALD_ERR_UNSUPPORTED, "V3: the mixed-precision path supports 3 or 6 bands in this build");
+    return fail(ALD_ERR_UNSUPPORTED, "V3: the mixed-precision path and the slice-major layout support 3 or 6 bands");
   }
   if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 launch: ") + cudaGetErrorString(e));
   return ALD_OK;

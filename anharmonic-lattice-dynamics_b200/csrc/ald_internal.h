@@ -204,7 +204,8 @@ struct V3Args {
   const int* phase_coef;     // 4*natoms
   const double* roots;       // 2*L
   double const33;
-  double* v3sq;              // [row][q2][l1][l2][l3]
+  double* v3sq;              // v3_layout 0: [row][q2][l1][l2][l3] (the reference's order, per row)
+  int v3_layout;             //           1: [row][l2][l3][l1][q2] (slices of the delta, q2 fastest)
   int* err;
   // phase classes (pair kernel)
   int ncls;
@@ -226,7 +227,8 @@ struct CombineArgs {
   Geometry geo;
   int n1_first, nrows;
   const int* mapinv;
-  const double* v3sq;        // [row][q2][l1][l2][l3]
+  const double* v3sq;        // v3_layout 0: [row][q2][l1][l2][l3]; 1: [row][l2][l3][l1][q2]
+  int v3_layout;
   const double* freq;        // [q][l]
   const double* dist;        // [q][l]
   const int* tet_corner;

@@ -116,10 +116,14 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
   const bool fused = !gauss && delta_fused_supported(c->geo);
   if (!fused) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
+  // the fused delta reads |V3|^2 slice by slice: the pair kernel writes that layout
+  const int v3_layout = fused && v3_pair_supported(b, c->opt.precision) ? 1 : 0;
   for (int r0 = 0; r0 < nibz; r0 += K) {
     int nr = std::min(K, nibz - r0);
     ALD_CK(tm.begin(1));
-    r = run_v3(c, v3_args(c, r0, nr, v3.p));
+    V3Args va = v3_args(c, r0, nr, v3.p);
+    va.v3_layout = v3_layout;
+    r = run_v3(c, va);
     if (r) return r;
     res->launches[1] += 1;
     ALD_CK(tm.end());
@@ -129,6 +133,7 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
     a.nrows = nr;
     a.mapinv = c->mapinv.p;
     a.v3sq = v3.p;
+    a.v3_layout = v3_layout;
     a.freq = c->freq.p;
     a.dist = c->dist.p;
     a.tet_corner = c->tet_corner.p;

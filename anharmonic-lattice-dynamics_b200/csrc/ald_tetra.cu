@@ -314,42 +314,72 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
 // (tetrahedron, l1) pair go straight into R1/R2 -- no corner-energy or weight
 // array in HBM.  A CTA owns one IBZ row, one process and one band l2, and a
 // block of mesh cells: plane i, rows j0 .. j0+R-1, all k (thread = cell).  The
-// corners of those cells form a window of 2 x (R+1) x N2 mesh points, whose
-// energies, Bose factors and indices are staged in shared memory once per l3.
-// Per l3 (one slice of the reference's loops):
+// corners of those cells form a window of 2 x (R+1) x N2 mesh points.
+// Once per CTA the window's indices, omega(w,l2), n(w,l2) and flags are staged
+// in shared memory; then per l3 (one slice of the reference's loops):
 //   1. per window point: E = -+omega(w,l2) + omega(q1+-w,l3) as default REAL,
 //      G = n2 (n3+1) [process 1] or (n2+1)(n3+1) [process 2], G = 0 where the
 //      reference zeroes acoustic modes at Gamma (sub.f90:7351-7356, 7412-7417);
-//   2. per cell: its 8 corner energies, its 6 tetrahedra sorted once; each
-//      tetrahedron whose range may contain a band energy omega1(l1) is stored
-//      as a record (sorted energies + corner of each sorted position) and its
-//      (record, l1) pairs queued;
+//   2. per cell: min/max of its 8 corner energies; cells whose range holds
+//      no band energy omega1(l1) are skipped, else its 6 tetrahedra are
+//      sorted once and each one whose range may hold an omega1(l1) is stored
+//      as a record (sorted energies + corner at each sorted position) with
+//      its (record, l1) pairs queued;
 //   3. per queued pair: weight_tet's four corner weights c (bitwise, ald_tet.h)
-//      and R(row, w, l1, l2) += c/6 (2pi)^2/nkc |V3|^2 n1 G for each corner.
+//      and R(row, w, l1, l2) += c/6 (2pi)^2/nkc |V3|^2 n1 G for each corner
+//      (FP64 atomics in L2; FP64 atomics on shared memory would be CAS loops).
+//      |V3|^2(src(w), l1, l2, l3) is gathered where needed; in the slice-major
+//      layout the corners of one tetrahedron share sectors.
 // The sums run in atomic order (FP64 rounding, not bitwise, against the
 // reference's P1/P2 summed over l3).
 constexpr int kFusedThreads = 128;
 
+struct FusedShape {
+  int R, nbj, NW, maxrec;
+  size_t smem;
+};
+
+__host__ __device__ inline FusedShape fused_shape(const Geometry& g) {
+  FusedShape f;
+  const int N1 = g.nc[1], N2 = g.nc[2];
+  f.R = kFusedThreads / N2;
+  if (f.R < 1) f.R = 1;
+  if (f.R > N1) f.R = N1;
+  f.nbj = (N1 + f.R - 1) / f.R;
+  f.NW = 2 * (f.R + 1) * N2;
+  f.maxrec = 6 * f.R * N2;
+  const size_t nw2 = (size_t)(f.NW + (f.NW & 1));
+  // doubles: G, fw, n2; float4 records; ushort4 records;
+  // ints: w, src, q3; floats: E; bytes: flags; ushorts: queue
+  f.smem = nw2 * 8 * 3 + (size_t)f.maxrec * 16 + (size_t)f.maxrec * 8 + (size_t)f.NW * 3 * 4 +
+           (size_t)f.NW * 4 + (size_t)((f.NW + 3) & ~3) + (size_t)f.maxrec * g.b * 2;
+  return f;
+}
+
 template <int B>
-__global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs a, int R, int nbj) {
+__global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double s_om[B], s_nb1[B];
   __shared__ float s_omlo[B], s_omhi[B];
   __shared__ int s_nrec, s_nq;
   const Geometry& g = a.geo;
-  const int N0 = g.nc[0], N1 = g.nc[1], N2 = g.nc[2], nkc = g.nkc, b = g.b, b2 = b * b, b3 = b2 * b;
-  const int NW = 2 * (R + 1) * N2, ncell = R * N2, maxrec = 6 * ncell;
+  const FusedShape F = fused_shape(g);
+  const int R = F.R, NW = F.NW, maxrec = F.maxrec;
+  const int N0 = g.nc[0], N1 = g.nc[1], N2 = g.nc[2], nkc = g.nkc, b = g.b;
   const int tid = threadIdx.x, lane = tid & 31;
   const int row = blockIdx.y, proc = blockIdx.z % 2, l2 = blockIdx.z / 2;
-  const int pi = blockIdx.x / nbj, j0 = (blockIdx.x % nbj) * R;
+  const int pi = blockIdx.x / F.nbj, j0 = (blockIdx.x % F.nbj) * R;
   // shared layout
+  const int nw2 = NW + (NW & 1);
   double* s_G = reinterpret_cast<double*>(smraw);
-  float4* s_rece = reinterpret_cast<float4*>(s_G + NW + (NW & 1));
+  double* s_fw = s_G + nw2;
+  double* s_n2 = s_fw + nw2;
+  float4* s_rece = reinterpret_cast<float4*>(s_n2 + nw2);
   ushort4* s_recp = reinterpret_cast<ushort4*>(s_rece + maxrec);
   int* s_w = reinterpret_cast<int*>(s_recp + maxrec);
-  int* s_q3 = s_w + NW;
-  int* s_src = s_q3 + NW;
-  float* s_E = reinterpret_cast<float*>(s_src + NW);
+  int* s_src = s_w + NW;
+  int* s_q3 = s_src + NW;
+  float* s_E = reinterpret_cast<float*>(s_q3 + NW);
   unsigned char* s_fl = reinterpret_cast<unsigned char*>(s_E + NW);
   unsigned short* s_queue = reinterpret_cast<unsigned short*>(s_fl + ((NW + 3) & ~3));
 
@@ -363,7 +393,8 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     s_omhi[tid] = __double2float_ru(om);
     s_nb1[tid] = a.dist[(size_t)q1 * b + tid];
   }
-  // window points: global index, q3 = q1 +- w, source row of |V3|^2, Gamma flags
+  // window points: global index, q3 = q1 +- w, source of |V3|^2, Gamma flags,
+  // omega and n of band l2
   for (int p = tid; p < NW; p += blockDim.x) {
     const int k = p % N2, t = p / N2, dj = t % (R + 1), di = t / (R + 1);
     int mw[3] = {(pi + di) % N0, (j0 + dj) % N1, k};
@@ -376,84 +407,110 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     s_q3[p] = q3;
     s_src[p] = proc == 0 ? w : neg_index(g, mw);
     s_fl[p] = (unsigned char)((at_gamma_index(g, mw) ? 1 : 0) | (at_gamma_index(g, m3) ? 2 : 0));
+    s_fw[p] = a.freq[(size_t)w * b + l2];
+    s_n2[p] = a.dist[(size_t)w * b + l2];
   }
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   double* Rp = proc == 0 ? a.R1 : a.R2;
-  const double* v3row = a.v3sq + (size_t)row * nkc * b3;
-  // this thread's cell
+  // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
+  size_t sq, s1, s2, s3;
+  if (a.v3_layout == 1) {
+    sq = 1;
+    s1 = nkc;
+    s3 = (size_t)b * nkc;
+    s2 = (size_t)b * b * nkc;
+  } else {
+    s3 = 1;
+    s2 = b;
+    s1 = (size_t)b * b;
+    sq = (size_t)b * b * b;
+  }
+  const double* v3row = a.v3sq + (size_t)row * nkc * b * b * b;
+  // this thread's cell and its corners in the window
   const int cdj = tid / N2, ck = tid % N2;
-  const bool cell_ok = tid < ncell && j0 + cdj < N1;
+  const bool cell_ok = tid < R * N2 && j0 + cdj < N1;
   int lp[8];
 #pragma unroll
   for (int c = 0; c < 8; ++c) {
-    const int o0 = c_off[c][0], o1 = c_off[c][1], o2 = c_off[c][2];
+    const int o0 = c & 1, o1 = (c >> 1) & 1, o2 = (c >> 2) & 1;  // c_off order
     const int kk = ck + o2 == N2 ? 0 : ck + o2;
     lp[c] = cell_ok ? (o0 * (R + 1) + cdj + o1) * N2 + kk : 0;
   }
   for (int l3 = 0; l3 < b; ++l3) {
-    __syncthreads();  // previous slice done with the window and the queue
+    __syncthreads();  // window staged / previous slice done
     if (tid == 0) {
       s_nrec = 0;
       s_nq = 0;
     }
     for (int p = tid; p < NW; p += blockDim.x) {
-      const int w = s_w[p], q3 = s_q3[p];
-      const double fw = a.freq[(size_t)w * b + l2], f3 = a.freq[(size_t)q3 * b + l3];
+      const int q3 = s_q3[p];
+      const double fw = s_fw[p], f3 = a.freq[(size_t)q3 * b + l3];
       s_E[p] = (float)(proc == 0 ? -fw + f3 : fw + f3);
-      const double n2 = a.dist[(size_t)w * b + l2], n3 = a.dist[(size_t)q3 * b + l3];
+      const double n2 = s_n2[p], n3 = a.dist[(size_t)q3 * b + l3];
       const bool zero = (l2 < 3 && (s_fl[p] & 1)) || (l3 < 3 && (s_fl[p] & 2));
       s_G[p] = zero ? 0.0 : (proc == 0 ? n2 * (n3 + 1) : (n2 + 1) * (n3 + 1));
     }
     __syncthreads();
-    // phase 1: sort the 6 tetrahedra of this cell, queue (record, l1) pairs
-    constexpr int kTet[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
+    // phase 1: cells -> tetrahedron records and (record, l1) pairs
+    // (make_kp_reg_tet's six tetrahedra of a cell, as corner numbers)
+    constexpr int kTetOf[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
     float ec[8];
+    float emin = 3.4e38f, emax = -3.4e38f;
 #pragma unroll
-    for (int c = 0; c < 8; ++c) ec[c] = s_E[lp[c]];
+    for (int c = 0; c < 8; ++c) {
+      ec[c] = s_E[lp[c]];
+      emin = fminf(emin, ec[c]);
+      emax = fmaxf(emax, ec[c]);
+    }
+    bool any = false;
+    if (cell_ok)
+      for (int l1 = 0; l1 < b; ++l1) any |= (s_omhi[l1] >= emin && s_omlo[l1] <= emax);
+    if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
-    for (int l = 0; l < 6; ++l) {
-      float en[4];
+      for (int l = 0; l < 6; ++l) {
+        float en[4];
 #pragma unroll
-      for (int k = 0; k < 4; ++k) en[k] = ec[kTet[l][k]];
-      const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
-      int lo = b, hi = 0;
-      if (cell_ok) {
-        for (int l1 = 0; l1 < b; ++l1)
-          if (s_omhi[l1] >= ts.e1 && s_omlo[l1] <= ts.e4) {
-            lo = min(lo, l1);
-            hi = l1 + 1;
-          }
-      }
-      const int cnt = hi > lo ? hi - lo : 0;
-      const unsigned mask = __ballot_sync(0xffffffffu, cnt > 0);
-      if (mask == 0u) continue;
-      int incl = cnt;
+        for (int k = 0; k < 4; ++k) en[k] = ec[kTetOf[l][k]];
+        const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+        int lo = b, hi = 0;
+        if (any) {
+          for (int l1 = 0; l1 < b; ++l1)
+            if (s_omhi[l1] >= ts.e1 && s_omlo[l1] <= ts.e4) {
+              lo = min(lo, l1);
+              hi = l1 + 1;
+            }
+        }
+        const int cnt = hi > lo ? hi - lo : 0;
+        const unsigned mask = __ballot_sync(0xffffffffu, cnt > 0);
+        if (mask == 0u) continue;
+        int incl = cnt;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      int rbase = 0, qbase = 0;
-      if (lane == 31) {
-        rbase = atomicAdd(&s_nrec, __popc(mask));
-        qbase = atomicAdd(&s_nq, incl);
-      }
-      rbase = __shfl_sync(0xffffffffu, rbase, 31);
-      qbase = __shfl_sync(0xffffffffu, qbase, 31);
-      if (cnt > 0) {
-        const int rec = rbase + __popc(mask & ((1u << lane) - 1u));
-        s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
-        // corner at each sorted position (tet_pos is a permutation of 0..3)
-        const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2), ps3 = tet_pos(en, 3);
-        const int c0 = lp[kTet[l][0]], c1 = lp[kTet[l][1]], c2 = lp[kTet[l][2]], c3 = lp[kTet[l][3]];
-        auto at = [&](int p) { return (unsigned short)(ps0 == p ? c0 : ps1 == p ? c1 : ps2 == p ? c2 : c3); };
-        s_recp[rec] = make_ushort4(at(0), at(1), at(2), at(3));
-        int q = qbase + incl - cnt;
-        for (int l1 = lo; l1 < hi; ++l1) s_queue[q++] = (unsigned short)((rec << 4) | l1);
+        for (int o = 1; o < 32; o <<= 1) {
+          const int v = __shfl_up_sync(0xffffffffu, incl, o);
+          if (lane >= o) incl += v;
+        }
+        int rbase = 0, qbase = 0;
+        if (lane == 31) {
+          rbase = atomicAdd(&s_nrec, __popc(mask));
+          qbase = atomicAdd(&s_nq, incl);
+        }
+        rbase = __shfl_sync(0xffffffffu, rbase, 31);
+        qbase = __shfl_sync(0xffffffffu, qbase, 31);
+        if (cnt > 0) {
+          const int rec = rbase + __popc(mask & ((1u << lane) - 1u));
+          s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
+          // corner at each sorted position (tet_pos is a permutation of 0..3)
+          const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2);
+          const int c0 = lp[kTetOf[l][0]], c1 = lp[kTetOf[l][1]], c2 = lp[kTetOf[l][2]], c3 = lp[kTetOf[l][3]];
+          auto at = [&](int p) { return (unsigned short)(ps0 == p ? c0 : ps1 == p ? c1 : ps2 == p ? c2 : c3); };
+          s_recp[rec] = make_ushort4(at(0), at(1), at(2), at(3));
+          int q = qbase + incl - cnt;
+          for (int l1 = lo; l1 < hi; ++l1) s_queue[q++] = (unsigned short)((rec << 4) | l1);
+        }
       }
     }
     __syncthreads();
-    // phase 2: corner weights of the queued pairs into R
+    // phase 2: corner weights of the queued pairs into Rs
     const int nq = s_nq;
     for (int i = tid; i < nq; i += blockDim.x) {
       const unsigned v = s_queue[i];
@@ -464,14 +521,16 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       if (!tet_weights4(ts, s_om[l1], cp)) continue;
       const ushort4 pp = s_recp[rec];
       const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
+      const double nb1 = s_nb1[l1];
+      double* Rrow = Rp + (size_t)row * nkc * b * b + l1 * b + l2;
+      const double* vs = v3row + l2 * s2 + l3 * s3 + l1 * s1;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
         const int p = pos_pt[k];
         const double G = s_G[p];
         if (cp[k] == 0.0 || G == 0.0) continue;
-        const double v3 = v3row[(size_t)s_src[p] * b3 + (l1 * b + l2) * b + l3];
-        const double val = (cp[k] / 6.0) * (v3 * fnorm) * (s_nb1[l1] * G);
-        atomicAdd(Rp + (((size_t)row * nkc + s_w[p]) * b + l1) * b + l2, val);
+        const double val = (cp[k] / 6.0) * (__ldg(vs + (size_t)s_src[p] * sq) * fnorm) * (nb1 * G);
+        atomicAdd(Rrow + (size_t)s_w[p] * b * b, val);
       }
     }
   }
@@ -518,31 +577,20 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) 
   return cudaGetLastError();
 }
 
-// rows of cells per CTA of the fused kernel and its shared memory
-static void fused_shape(const Geometry& g, int& R, int& nbj, size_t& smem) {
-  const int N1 = g.nc[1], N2 = g.nc[2];
-  R = std::max(1, std::min(N1, kFusedThreads / N2));
-  nbj = (N1 + R - 1) / R;
-  const int NW = 2 * (R + 1) * N2, maxrec = 6 * R * N2;
-  smem = (size_t)(NW + (NW & 1)) * 8 + (size_t)maxrec * 16 + (size_t)maxrec * 8 + (size_t)NW * 3 * 4 +
-         (size_t)NW * 4 + (size_t)((NW + 3) & ~3) + (size_t)maxrec * g.b * 2;
+bool delta_fused_supported(const Geometry& g) {
+  return g.b <= kMaxBandsTet && g.nc[2] <= kFusedThreads && fused_shape(g).smem <= 200 * 1024;
 }
-
-bool delta_fused_supported(const Geometry& g) { return g.b <= kMaxBandsTet && g.nc[2] <= kFusedThreads; }
 
 cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
   const Geometry& g = a.geo;
   if (!delta_fused_supported(g)) return cudaErrorInvalidValue;
-  int R, nbj;
-  size_t smem;
-  fused_shape(g, R, nbj, smem);
-  if (smem > 200 * 1024) return cudaErrorInvalidValue;
-  dim3 grid(g.nc[0] * nbj, a.nrows, 2 * g.b);
+  const FusedShape f = fused_shape(g);
+  dim3 grid(g.nc[0] * f.nbj, a.nrows, 2 * g.b);
   cudaError_t e;
-#define ALD_FUSED(BB)                                                                                   \
-  e = cudaFuncSetAttribute(delta_fused_kernel<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
-  if (e != cudaSuccess) return e;                                                                       \
-  delta_fused_kernel<BB><<<grid, kFusedThreads, smem, s>>>(a, R, nbj);
+#define ALD_FUSED(BB)                                                                                       \
+  e = cudaFuncSetAttribute(delta_fused_kernel<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem); \
+  if (e != cudaSuccess) return e;                                                                           \
+  delta_fused_kernel<BB><<<grid, kFusedThreads, f.smem, s>>>(a);
   if (g.b <= 3) {
     ALD_FUSED(3)
   } else if (g.b <= 6) {

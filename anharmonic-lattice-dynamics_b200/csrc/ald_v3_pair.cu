@@ -244,7 +244,11 @@ __global__ void __launch_bounds__(NT) v3_pair_kernel(V3Args a) {
     if (q2 < g.nkc) {
       const int q3 = s_q3[q];
       const double wq1 = w2[(size_t)q1 * B + l1];
-      double* out = a.v3sq + ((size_t)row * g.nkc + q2) * B3 + l1 * B2 + l2b * B;
+      // layout 0: [row][q2][l1][l2][l3]; layout 1: [row][l2][l3][l1][q2]
+      const size_t nk = g.nkc;
+      double* out = a.v3_layout == 1 ? a.v3sq + ((size_t)row * B3 + l2b * B2 + l1) * nk + q2
+                                     : a.v3sq + ((size_t)row * nk + q2) * B3 + l1 * B2 + l2b * B;
+      const size_t st_l2 = a.v3_layout == 1 ? (size_t)B2 * nk : B, st_l3 = a.v3_layout == 1 ? (size_t)B * nk : 1;
 #pragma unroll
       for (int i = 0; i < BS; ++i) {
         const double w12 = wq1 * w2[(size_t)q2 * B + l2b + i];
@@ -258,7 +262,7 @@ __global__ void __launch_bounds__(NT) v3_pair_kernel(V3Args a) {
           } else {
             atomicOr(a.err, 2);
           }
-          out[i * B + l] = v;
+          out[i * st_l2 + l * st_l3] = v;
         }
       }
     }
