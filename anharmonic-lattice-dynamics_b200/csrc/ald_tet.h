@@ -143,47 +143,60 @@ ALD_TET_HD double tet_weight(const TetSorted& t, int pos, double e) {
   }
 }
 
-// all four weights at once: c[pos] for sorted positions 0 (highest) .. 3
-// (lowest); the same expressions as tet_weight, evaluated in one branch.
-// Returns false when e lies outside [E1, E4] (all four weights zero).
-ALD_TET_HD bool tet_weights4(const TetSorted& t, double e, double* c) {
+// The energy regime of e for a sorted tetrahedron, in weight_tet's test
+// order: 0 outside [E1, E4] (all weights zero), 1 E1 <= e <= E2, 2 E2 <= e <= E3,
+// 3 E3 < e <= E4.
+ALD_TET_HD int tet_regime(const TetSorted& t, double e) {
   const double E1 = t.e1, E2 = t.e2, E3 = t.e3, E4 = t.e4;
-  if (e < E1 || e > E4) return false;
-  const float e21 = t.e21, e31 = t.e31, e41 = t.e41, e32 = t.e32, e42 = t.e42, e43 = t.e43;
-  if (E1 <= e && e <= E2) {
-    double x = e - E1;
-    double x3 = x * (x * x);
-    c[3] = ((E2 - e) / (double)e21 + (E3 - e) / (double)e31 + (E4 - e) / (double)e41) * (x * x) /
-           (double)((e41 * e31) * e21);
-    c[2] = x3 / (double)(((e21 * e21) * e31) * e41);
-    c[1] = x3 / (double)((e21 * (e31 * e31)) * e41);
-    c[0] = x3 / (double)((e21 * e31) * (e41 * e41));
-    return true;
-  }
-  if (E2 <= e && e <= E3) {
-    const double a3 = E3 - e, a4 = E4 - e, b1 = e - E1, b2 = e - E2;
-    float c11 = (float)(a3 / (double)(e31 * e31));
-    float c12 = (float)(a4 / (double)(e41 * e41));
-    float c21 = (float)(a3 / (double)(e32 * e32));
-    float c22 = (float)(a4 / (double)(e42 * e42));
-    float c31 = (float)(b2 / (double)(e32 * e32));
-    float c32 = (float)(b1 / (double)(e31 * e31));
-    float c41 = (float)(b2 / (double)(e42 * e42));
-    float c42 = (float)(b1 / (double)(e41 * e41));
-    float b11 = (float)(a3 * b2 / (double)(e42 * e32) + a4 * b1 / (double)(e41 * e42) + a3 * b1 / (double)(e32 * e41));
-    float b12 = (float)(a4 * b1 / (double)(e42 * e31) + a4 * b2 / (double)(e42 * e32) + a3 * b1 / (double)(e31 * e32));
-    float b21 = (float)(a3 * b2 / (double)(e42 * e31) + a4 * b2 / (double)(e42 * e41) + a3 * b1 / (double)(e31 * e41));
-    float b22 = (float)(a3 * b2 / (double)(e32 * e31) + a4 * b1 / (double)(e41 * e31) + a4 * b2 / (double)(e32 * e41));
-    float b31 = b21;  // identical expressions in the reference
-    float b32 = b11;
-    float b41 = b22;
-    float b42 = b12;
-    c[3] = (double)(0.5f * (c11 * b11 + c12 * b12));
-    c[2] = (double)(0.5f * (c21 * b21 + c22 * b22));
-    c[1] = (double)(0.5f * (c31 * b31 + c32 * b32));
-    c[0] = (double)(0.5f * (c41 * b41 + c42 * b42));
-    return true;
-  }
+  if (e < E1 || e > E4) return 0;
+  if (E1 <= e && e <= E2) return 1;
+  if (E2 <= e && e <= E3) return 2;
+  return 3;
+}
+
+// all four weights of one regime: c[pos] for sorted positions 0 (highest) ..
+// 3 (lowest); the same expressions as tet_weight.
+ALD_TET_HD void tet_weights_low(const TetSorted& t, double e, double* c) {
+  const double E1 = t.e1, E2 = t.e2, E3 = t.e3, E4 = t.e4;
+  const float e21 = t.e21, e31 = t.e31, e41 = t.e41;
+  double x = e - E1;
+  double x3 = x * (x * x);
+  c[3] = ((E2 - e) / (double)e21 + (E3 - e) / (double)e31 + (E4 - e) / (double)e41) * (x * x) /
+         (double)((e41 * e31) * e21);
+  c[2] = x3 / (double)(((e21 * e21) * e31) * e41);
+  c[1] = x3 / (double)((e21 * (e31 * e31)) * e41);
+  c[0] = x3 / (double)((e21 * e31) * (e41 * e41));
+}
+
+ALD_TET_HD void tet_weights_mid(const TetSorted& t, double e, double* c) {
+  const double E1 = t.e1, E2 = t.e2, E3 = t.e3, E4 = t.e4;
+  const float e31 = t.e31, e41 = t.e41, e32 = t.e32, e42 = t.e42;
+  const double a3 = E3 - e, a4 = E4 - e, b1 = e - E1, b2 = e - E2;
+  float c11 = (float)(a3 / (double)(e31 * e31));
+  float c12 = (float)(a4 / (double)(e41 * e41));
+  float c21 = (float)(a3 / (double)(e32 * e32));
+  float c22 = (float)(a4 / (double)(e42 * e42));
+  float c31 = (float)(b2 / (double)(e32 * e32));
+  float c32 = (float)(b1 / (double)(e31 * e31));
+  float c41 = (float)(b2 / (double)(e42 * e42));
+  float c42 = (float)(b1 / (double)(e41 * e41));
+  float b11 = (float)(a3 * b2 / (double)(e42 * e32) + a4 * b1 / (double)(e41 * e42) + a3 * b1 / (double)(e32 * e41));
+  float b12 = (float)(a4 * b1 / (double)(e42 * e31) + a4 * b2 / (double)(e42 * e32) + a3 * b1 / (double)(e31 * e32));
+  float b21 = (float)(a3 * b2 / (double)(e42 * e31) + a4 * b2 / (double)(e42 * e41) + a3 * b1 / (double)(e31 * e41));
+  float b22 = (float)(a3 * b2 / (double)(e32 * e31) + a4 * b1 / (double)(e41 * e31) + a4 * b2 / (double)(e32 * e41));
+  float b31 = b21;  // identical expressions in the reference
+  float b32 = b11;
+  float b41 = b22;
+  float b42 = b12;
+  c[3] = (double)(0.5f * (c11 * b11 + c12 * b12));
+  c[2] = (double)(0.5f * (c21 * b21 + c22 * b22));
+  c[1] = (double)(0.5f * (c31 * b31 + c32 * b32));
+  c[0] = (double)(0.5f * (c41 * b41 + c42 * b42));
+}
+
+ALD_TET_HD void tet_weights_high(const TetSorted& t, double e, double* c) {
+  const double E1 = t.e1, E2 = t.e2, E3 = t.e3, E4 = t.e4;
+  const float e41 = t.e41, e42 = t.e42, e43 = t.e43;
   double x = E4 - e;
   double x3 = x * (x * x);
   c[3] = x3 / (double)(((e41 * e41) * e42) * e43);
@@ -191,6 +204,19 @@ ALD_TET_HD bool tet_weights4(const TetSorted& t, double e, double* c) {
   c[1] = x3 / (double)((e41 * e42) * (e43 * e43));
   c[0] = ((e - E3) / (double)e43 + (e - E2) / (double)e42 + (e - E1) / (double)e41) * (x * x) /
          (double)((e41 * e42) * e43);
+}
+
+ALD_TET_HD void tet_weights_in(const TetSorted& t, int regime, double e, double* c) {
+  if (regime == 1) tet_weights_low(t, e, c);
+  else if (regime == 2) tet_weights_mid(t, e, c);
+  else tet_weights_high(t, e, c);
+}
+
+// all four weights at once; false when e lies outside [E1, E4] (all zero)
+ALD_TET_HD bool tet_weights4(const TetSorted& t, double e, double* c) {
+  const int r = tet_regime(t, e);
+  if (r == 0) return false;
+  tet_weights_in(t, r, e, c);
   return true;
 }
 

@@ -360,7 +360,6 @@ template <int B>
 __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double s_om[B], s_nb1[B];
-  __shared__ float s_omlo[B], s_omhi[B];
   __shared__ int s_nrec, s_nq;
   const Geometry& g = a.geo;
   const FusedShape F = fused_shape(g);
@@ -387,11 +386,16 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
   int m1[3];
   decompose(g, q1, m1);
   if (tid < b) {
-    const double om = a.freq[(size_t)q1 * b + tid];
-    s_om[tid] = om;
-    s_omlo[tid] = __double2float_rd(om);
-    s_omhi[tid] = __double2float_ru(om);
+    s_om[tid] = a.freq[(size_t)q1 * b + tid];
     s_nb1[tid] = a.dist[(size_t)q1 * b + tid];
+  }
+  // conservative FP32 bounds of omega1 for the range tests (unused bands never count)
+  float omlo[B], omhi[B];
+#pragma unroll
+  for (int l1 = 0; l1 < B; ++l1) {
+    const double om = l1 < b ? a.freq[(size_t)q1 * b + l1] : 0.0;
+    omlo[l1] = l1 < b ? __double2float_rd(om) : 3.4e38f;
+    omhi[l1] = l1 < b ? __double2float_ru(om) : 3.4e38f;
   }
   // window points: global index, q3 = q1 +- w, source of |V3|^2, Gamma flags,
   // omega and n of band l2
@@ -452,7 +456,10 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     }
     __syncthreads();
     // phase 1: cells -> tetrahedron records and (record, l1) pairs
-    // (make_kp_reg_tet's six tetrahedra of a cell, as corner numbers)
+    // (make_kp_reg_tet's six tetrahedra of a cell, as corner numbers).  Bands
+    // lo .. hi-1 may carry weight on a tetrahedron with energies in [mn, mx]:
+    // omega1 is ascending, so lo and hi are counts; the exact test is
+    // tet_weights4's in phase 2.
     constexpr int kTetOf[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
     float ec[8];
     float emin = 3.4e38f, emax = -3.4e38f;
@@ -462,25 +469,28 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       emin = fminf(emin, ec[c]);
       emax = fmaxf(emax, ec[c]);
     }
-    bool any = false;
-    if (cell_ok)
-      for (int l1 = 0; l1 < b; ++l1) any |= (s_omhi[l1] >= emin && s_omlo[l1] <= emax);
+    int clo = 0, chi = 0;
+#pragma unroll
+    for (int l1 = 0; l1 < B; ++l1) {
+      clo += omhi[l1] < emin;
+      chi += omlo[l1] <= emax;
+    }
+    const bool any = cell_ok && chi > clo;
     if (__any_sync(0xffffffffu, any)) {
 #pragma unroll
       for (int l = 0; l < 6; ++l) {
         float en[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) en[k] = ec[kTetOf[l][k]];
-        const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
-        int lo = b, hi = 0;
-        if (any) {
-          for (int l1 = 0; l1 < b; ++l1)
-            if (s_omhi[l1] >= ts.e1 && s_omlo[l1] <= ts.e4) {
-              lo = min(lo, l1);
-              hi = l1 + 1;
-            }
+        const float mn = fminf(fminf(en[0], en[1]), fminf(en[2], en[3]));
+        const float mx = fmaxf(fmaxf(en[0], en[1]), fmaxf(en[2], en[3]));
+        int lo = 0, hi = 0;
+#pragma unroll
+        for (int l1 = 0; l1 < B; ++l1) {
+          lo += omhi[l1] < mn;
+          hi += omlo[l1] <= mx;
         }
-        const int cnt = hi > lo ? hi - lo : 0;
+        const int cnt = any && hi > lo ? hi - lo : 0;
         const unsigned mask = __ballot_sync(0xffffffffu, cnt > 0);
         if (mask == 0u) continue;
         int incl = cnt;
@@ -498,6 +508,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
         qbase = __shfl_sync(0xffffffffu, qbase, 31);
         if (cnt > 0) {
           const int rec = rbase + __popc(mask & ((1u << lane) - 1u));
+          const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
           s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
           // corner at each sorted position (tet_pos is a permutation of 0..3)
           const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2);
@@ -510,7 +521,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       }
     }
     __syncthreads();
-    // phase 2: corner weights of the queued pairs into Rs
+    // phase 2: corner weights of the queued pairs into R
     const int nq = s_nq;
     for (int i = tid; i < nq; i += blockDim.x) {
       const unsigned v = s_queue[i];
