@@ -140,26 +140,29 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
   }
 }
 
-// collision matrix: thread per (row group (n1,l1), column group (n2,l2))
+// collision matrix: thread per (n1, n2, l1, l2), l2 fastest, so that the b*b
+// band block of R(q1, arm, ., .) read for one arm is contiguous across the
+// threads of a warp (one IBZ row n1 per blockIdx.y)
 __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* mapinv, const int* arm_off,
                                  const int* arm_q, const int* arm_op, const double* opk, const double* Q,
                                  const double* R1, const double* R2, double* CM, int ld) {
-  const int b = g.b, nkc = g.nkc;
-  int col = blockIdx.x * blockDim.x + threadIdx.x;  // n2*b + l2
-  if (col >= nibz * b) return;
-  int rowg = blockIdx.y;                             // local row group: nl*b + l1
-  int n1 = n1_first + rowg / b, l1 = rowg % b;
-  int n2 = col / b, l2 = col % b;
-  int q1 = mapinv[n1];
+  const int b = g.b, b2 = b * b, nkc = g.nkc;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= nibz * b2) return;
+  const int n2 = t / b2, l1 = (t / b) % b, l2 = t % b;
+  const int nl = blockIdx.y;  // IBZ row local to the range
+  const int n1 = n1_first + nl;
+  const int q1 = mapinv[n1];
   int m1[3];
   decompose(g, q1, m1);
+  const size_t base = (size_t)nl * nkc;  // R arrays are local to the row range
   double blk[9];
   for (int k = 0; k < 9; ++k) blk[k] = 0.0;
   for (int s = arm_off[n2]; s < arm_off[n2 + 1]; ++s) {
     int n0 = arm_q[s];
     double C;
     if (n0 == q1 && l1 == l2) {
-      C = -Q[(size_t)(rowg / b) * b + l1];
+      C = -Q[(size_t)nl * b + l1];
     } else {
       int m0[3], mp1[3], mp2[3];
       decompose(g, n0, m0);
@@ -169,17 +172,17 @@ __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* 
         mp2[a] = wrapm(m0[a] - m1[a] + sh, g.nc[a]);  // arm - q1
       }
       int nk3_p1 = compose(g, mp1), nk3_p2 = compose(g, mp2);
-      size_t base = (size_t)(rowg / b) * nkc;  // R arrays are local to the row range
-      C = -R1[((base + n0) * b + l1) * b + l2] + R1[((base + nk3_p2) * b + l1) * b + l2] +
-          0.5 * R2[((base + n0) * b + l1) * b + l2] + 0.5 * R2[((base + nk3_p1) * b + l1) * b + l2];
+      const int bl = l1 * b + l2;
+      C = -R1[(base + n0) * b2 + bl] + R1[(base + nk3_p2) * b2 + bl] + 0.5 * R2[(base + n0) * b2 + bl] +
+          0.5 * R2[(base + nk3_p1) * b2 + bl];
     }
     const double* op = opk + 9 * arm_op[s];
     for (int i = 0; i < 3; ++i)
       for (int j = 0; j < 3; ++j) blk[i + 3 * j] = blk[i + 3 * j] + (C * op[i + 3 * j]);
   }
-  size_t r0 = 3 * ((size_t)rowg);
+  const size_t r0 = 3 * ((size_t)nl * b + l1), c0 = 3 * ((size_t)n2 * b + l2);
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + 3 * (size_t)col + j] = blk[i + 3 * j];
+    for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + c0 + j] = blk[i + 3 * j];
 }
 
 // ---------------------------------------------------------------- CG
@@ -339,22 +342,43 @@ cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nr
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
                              const double* Q, const double* R1, const double* R2, double* CM, int ld,
                              cudaStream_t s) {
-  int ncolg = nibz * geo.b;
-  dim3 grid((ncolg + 127) / 128, nrows * geo.b);
+  const int nt = nibz * geo.b * geo.b;
+  dim3 grid((nt + 127) / 128, nrows);
   collision_kernel<<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2, CM,
                                          ld);
   return cudaGetLastError();
 }
 
-// Conjugate gradients of cg_quadratic on a device matrix.  The max_iter
-// iterations are captured once into a CUDA graph; a device flag turns the
-// remaining launches into no-ops after the stop rule fires.
+// Conjugate gradients of cg_quadratic on a device matrix.  The iterations
+// run as CUDA graphs of kCgChunk iterations each (captured once per problem);
+// a device flag turns the rest of a chunk into no-ops once the stop rule
+// fires, and the host reads that flag between chunks, so a solve that stops
+// after k iterations launches at most k + kCgChunk - 1 of them.
+constexpr int kCgChunk = 8;
+
+static cudaError_t capture_cg(int iters, int n, int nblk, const double* dA, double* dx, CgWork& w, CgDev* st,
+                              int mode, double tol, cudaStream_t s, cudaGraphExec_t* out) {
+  cudaGraph_t graph = nullptr;
+  cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return e;
+  for (int it = 0; it < iters; ++it) {
+    gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, w.conj.p, w.aux.p, w.partial.p, st);
+    cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, w.partial.p, nblk, w.grad.p, w.conj.p, w.v0.p, dx, st, mode,
+                                             tol);
+  }
+  e = cudaStreamEndCapture(s, &graph);
+  if (e == cudaSuccess) e = cudaGraphInstantiate(out, graph, 0);
+  if (graph) cudaGraphDestroy(graph);
+  return e;
+}
+
 int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
               double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
   const int nblk = (n + kGemvWarps - 1) / kGemvWarps;
   if (w.grad.alloc(n) || w.conj.alloc(n) || w.aux.alloc(n) || w.v0.alloc(n) || w.partial.alloc(nblk) ||
-      w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev))) {
-    msg = "cg: device allocation failed";
+      w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev)) ||
+      (!w.h_done && cudaHostAlloc((void**)&w.h_done, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
+    msg = "cg: allocation failed";
     return ALD_ERR_NOMEM;
   }
   CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
@@ -363,21 +387,14 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
   cudaError_t e = cudaSuccess;
   const bool same = w.exec && w.n == n && w.max_iter == max_iter && w.mode == mode && w.tol == tol && w.A == dA &&
                     w.b == db && w.x == dx;
-  if (!same) {
+  const int chunk = max_iter <= 0 ? 1 : (max_iter < kCgChunk ? max_iter : kCgChunk);
+  const int tail = max_iter > 0 ? max_iter % chunk : 0;
+  if (!same && max_iter > 0) {
     if (w.exec) cudaGraphExecDestroy(w.exec);
-    w.exec = nullptr;
-    cudaGraph_t graph = nullptr;
-    e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
-    if (e == cudaSuccess) {
-      for (int it = 0; it < max_iter; ++it) {
-        gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, w.conj.p, w.aux.p, w.partial.p, st);
-        cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, w.partial.p, nblk, w.grad.p, w.conj.p, w.v0.p, dx, st,
-                                                 mode, tol);
-      }
-      e = cudaStreamEndCapture(s, &graph);
-    }
-    if (e == cudaSuccess) e = cudaGraphInstantiate(&w.exec, graph, 0);
-    if (graph) cudaGraphDestroy(graph);
+    if (w.exec_tail) cudaGraphExecDestroy(w.exec_tail);
+    w.exec = w.exec_tail = nullptr;
+    e = capture_cg(chunk, n, nblk, dA, dx, w, st, mode, tol, s, &w.exec);
+    if (e == cudaSuccess && tail) e = capture_cg(tail, n, nblk, dA, dx, w, st, mode, tol, s, &w.exec_tail);
     if (e == cudaSuccess) {
       w.n = n;
       w.max_iter = max_iter;
@@ -388,7 +405,16 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
       w.x = dx;
     }
   }
-  if (e == cudaSuccess) e = cudaGraphLaunch(w.exec, s);
+  for (int done = 0; e == cudaSuccess && done < max_iter;) {
+    const bool full = max_iter - done >= chunk;
+    e = cudaGraphLaunch(full ? w.exec : w.exec_tail, s);
+    done += full ? chunk : tail;
+    if (e == cudaSuccess && done < max_iter) {
+      e = cudaMemcpyAsync(w.h_done, &st->done, sizeof(int), cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e == cudaSuccess && *w.h_done) break;
+    }
+  }
   if (e != cudaSuccess) {
     msg = std::string("cg: ") + cudaGetErrorString(e);
     return ALD_ERR_CUDA;

@@ -300,7 +300,9 @@ cudaError_t launch_collapse(const Geometry& geo, int nrows, const double* P1, co
 struct CgWork {
   DevBuf<double> grad, conj, aux, v0, partial, fmin;
   DevBuf<char> st;
-  cudaGraphExec_t exec = nullptr;
+  cudaGraphExec_t exec = nullptr;       // kCgChunk iterations
+  cudaGraphExec_t exec_tail = nullptr;  // max_iter % kCgChunk iterations
+  int* h_done = nullptr;                // pinned copy of the stop flag
   int n = -1, max_iter = -1, mode = -1;
   double tol = 0;
   const double* A = nullptr;
@@ -308,6 +310,8 @@ struct CgWork {
   double* x = nullptr;
   ~CgWork() {
     if (exec) cudaGraphExecDestroy(exec);
+    if (exec_tail) cudaGraphExecDestroy(exec_tail);
+    if (h_done) cudaFreeHost(h_done);
   }
 };
 int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,

@@ -122,7 +122,7 @@ __global__ void v3_row_kernel(V3Args a) {
 // mode product 2 (q, c', l1 block) -> (B/S) x B accumulators;
 // mode product 3 (q, l1, l2 block) -> (B/S) x B accumulators and |V|^2.
 template <class T, int B, int QT, int S, int NT>
-__global__ void __launch_bounds__(NT) v3_pair_kernel(V3Args a) {
+__global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
   using C = typename Cx<T>::t;
   constexpr int NAT = B / 3, B2 = B * B, B3 = B2 * B, NG = NAT * NAT;
   constexpr int AP = B3 | 1, EP = B2 | 1, BS = B / S;
@@ -308,10 +308,10 @@ cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s) {
   const int b = a.geo.b;
   if (precision == ALD_MIXED) {
     if (b == 3) return launch_pair_t<float, 3, 32, 3, 288>(a, s);
-    if (b == 6) return launch_pair_t<float, 6, 16, 2, 192>(a, s);
+    if (b == 6) return launch_pair_t<float, 6, 16, 3, 288>(a, s);
   } else {
     if (b == 3) return launch_pair_t<double, 3, 32, 3, 288>(a, s);
-    if (b == 6) return launch_pair_t<double, 6, 16, 2, 192>(a, s);
+    if (b == 6) return launch_pair_t<double, 6, 16, 3, 288>(a, s);
   }
   return cudaErrorInvalidValue;
 }

@@ -9,6 +9,10 @@ force constants written in the reference's file formats.
 
 metric: triplet-bands per second over the whole time-to-kappa step
 (triplet-bands = nibz * nkc * ndyn^3 = 2.44e8 per step), higher is better.
+Both precision paths run: FP64 (every stage double) and mixed (the V3
+contraction in FP32, everything else double); the line's value is the mixed
+path's, the FP64 path's numbers, the speed-up and the kappa difference
+between the two sit beside it.
 
   value  device time of K steps with the context's tables already in HBM
          (CUDA events on the stream the library runs on; max over ranks)
@@ -39,7 +43,7 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "V3 triplet-bands/s & time-to-κ: mixed vs FP64 GPU path, 1 B200, κ err≤1e-4"
 UNIT = "triplet-bands/s"
-WORKLOAD = "rocksalt-Morse NaCl-type, 2 atoms (6 bands), 16x16x16 q-mesh, tetrahedron delta, T=300 K, FP64"
+WORKLOAD = "rocksalt-Morse NaCl-type, 2 atoms (6 bands), 16x16x16 q-mesh, tetrahedron delta, T=300 K"
 
 
 def _peaks():
@@ -169,7 +173,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ald", choices=["ald", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
+                    help="both: time the FP64 and the mixed path; the line's value is the mixed path's")
     ap.add_argument("--mesh", type=int, default=16)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -212,50 +217,68 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     dev = local
     torch.cuda.set_device(dev)
-    opts = ald.default_options(device=dev, precision=ald.MIXED if args.precision == "mixed" else ald.FP64)
     tmp = tempfile.TemporaryDirectory()
     d = tmp.name
     make_workload(d, mesh)
-    ctx = ald.Context(d, opts)
     stream = torch.cuda.Stream(device=dev)
-    ctx.set_stream(stream.cuda_stream)
-    tempk = ctx.info.tempk
-    nibz, nkc, b = ctx.nibz, ctx.nkc, ctx.ndyn
 
-    def step():
-        ctx.invalidate_phonons()
-        return ctx.kappa_pipeline(tempk, want_modes=False)
+    def timed_path(precision):
+        """K timed steps of one precision path on a context whose tables are in HBM."""
+        opts = ald.default_options(device=dev, precision=precision)
+        ctx = ald.Context(d, opts)
+        ctx.set_stream(stream.cuda_stream)
+        tempk = ctx.info.tempk
 
-    for _ in range(args.warmup):
-        out = step()
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
-    stage_sum = {k: 0.0 for k in ald.STAGES}
-    launches = 0
-    with ClockSampler(dev) as clk:
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record(stream)
-        for _ in range(args.steps):
+        def step():
+            ctx.invalidate_phonons()
+            return ctx.kappa_pipeline(tempk, want_modes=False)
+
+        for _ in range(args.warmup):
             out = step()
-            for k, v in out["stage_ms"].items():
-                stage_sum[k] += v
-            launches += out["launches"]["total"] + 3  # + the eigensolver launches of get_frequencies
-        e1.record(stream)
+        if world > 1:
+            torch.distributed.barrier()
         torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
-    ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    ms_max = float(t.item())
-    tb = out["triplet_bands"]
-    value = world * tb * args.steps / (ms_max * 1e-3)
-    per_step = {k: v / args.steps for k, v in stage_sum.items()}
-    per_launch_counts = dict(out["launches"])
+        stage_sum = {k: 0.0 for k in ald.STAGES}
+        launches = 0
+        with ClockSampler(dev) as clk:
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(args.steps):
+                out = step()
+                for k, v in out["stage_ms"].items():
+                    stage_sum[k] += v
+                launches += out["launches"]["total"] + 3  # + the eigensolver launches of get_frequencies
+            e1.record(stream)
+            torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        ms = e0.elapsed_time(e1)
+        t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        ms_max = float(t.item())
+        res = {"ms": ms_max, "stage": {k: v / args.steps for k, v in stage_sum.items()},
+               "launch_counts": dict(out["launches"]), "launches": launches, "out": out, "clocks": clk.summary(),
+               "tempk": tempk, "nibz": ctx.nibz, "nkc": ctx.nkc, "b": ctx.ndyn, "opts": opts}
+        ctx.close()
+        return res
 
-    # ---- end to end through the C ABI from the input files
+    precisions = {"fp64": [ald.FP64], "mixed": [ald.MIXED], "both": [ald.FP64, ald.MIXED]}[args.precision]
+    runs = {p: timed_path(p) for p in precisions}
+    head = runs[precisions[-1]]  # the mixed path when both run
+    nibz, nkc, b = head["nibz"], head["nkc"], head["b"]
+    out = head["out"]
+    tb = out["triplet_bands"]
+    ms_max = head["ms"]
+    value = world * tb * args.steps / (ms_max * 1e-3)
+    per_step = head["stage"]
+    per_launch_counts = head["launch_counts"]
+    launches = head["launches"]
+    clk_summary = head["clocks"]
+    opts = head["opts"]
+    tempk = head["tempk"]
+
+    # ---- end to end through the C ABI from the input files (headline path)
     e2e_times, h2d, d2h = [], 0.0, 0.0
     for i in range(max(2, min(args.steps, 5)) + 1):
         torch.cuda.synchronize()
@@ -285,12 +308,14 @@ def main():
                 cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             except Exception as ex:  # the baseline is reported, never required
                 cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % ex}
+        mixed_head = precisions[-1] == ald.MIXED
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "mixed",
+                "scaling": "weak", "vs_baseline": None,
+                "dtype": "mixed: f32 V3 contraction, f64 elsewhere" if mixed_head else "f64",
                 "data": "synthetic (analytic Morse FC2/FC3 written in the reference's file formats)",
                 "config": {"workload": WORKLOAD, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
-                           "triplet_bands_per_step": tb, "precision": args.precision,
+                           "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
                            "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
                                2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * 8 / 1e6),
                            "parallelism": "replicas" if world > 1 else "single GPU"},
@@ -300,9 +325,21 @@ def main():
                 "cg_iters": out["cg_iters"],
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "seconds_per_step": sorted(e2e_times)[len(e2e_times) // 2]},
-                "gpu_launches": launches, "roofline": rf, "cpu_baseline": cb, "clocks": clk.summary()}
+                "gpu_launches": launches, "roofline": rf, "cpu_baseline": cb, "clocks": clk_summary}
+        if ald.FP64 in runs and ald.MIXED in runs:
+            f, m = runs[ald.FP64], runs[ald.MIXED]
+            kf, km = np.asarray(f["out"]["kappa_cg"]), np.asarray(m["out"]["kappa_cg"])
+            krf, krm = np.asarray(f["out"]["kappa_rta"]), np.asarray(m["out"]["kappa_rta"])
+            line["fp64"] = {"value": world * tb * args.steps / (f["ms"] * 1e-3), "unit": UNIT,
+                            "ms_per_step": f["ms"] / args.steps,
+                            "stage_ms_per_step": {k: round(v, 4) for k, v in f["stage"].items()},
+                            "clocks": f["clocks"]}
+            line["mixed_speedup_vs_fp64"] = f["ms"] / m["ms"]
+            line["mixed_v3_speedup_vs_fp64"] = f["stage"]["v3"] / m["stage"]["v3"]
+            line["kappa_rel_err_mixed_vs_fp64"] = {
+                "cg": float(np.abs(km - kf).max() / np.abs(kf).max()),
+                "rta": float(np.abs(krm - krf).max() / np.abs(krf).max())}
         print(json.dumps(line))
-    ctx.close()
     tmp.cleanup()
     if world > 1:
         torch.distributed.barrier()
