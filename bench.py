@@ -162,9 +162,16 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks):
         return {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
                 "traffic": None, "kernel": dom}
     ach = bytes_ / (ms * 1e-3) / 1e9
+    # DRAM bytes (read + write) per launch from one ncu capture of a 72-row chunk of this
+    # workload (profiles/kappa_pipeline_nacl_morse_mesh16.md), scaled to the rows of a launch
+    ncu_bytes_72rows = {("delta", 4096, 6): 444.64e6, ("v3", 4096, 6): 479.12e6}
+    traffic = None
+    if (dom, nkc, b) in ncu_bytes_72rows:
+        traffic = ncu_bytes_72rows[(dom, nkc, b)] * (nibz / n) / 72
     return {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": ach / peaks["hbm_gbs"], "traffic": None, "kernel": dom, "ms_per_launch": ms,
-            "algorithmic_bytes": bytes_, "peak_source": peaks["src"]}
+            "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom, "ms_per_launch": ms,
+            "algorithmic_bytes": bytes_, "peak_source": peaks["src"],
+            "note": "the delta and V3 kernels are FP64-ALU bound; ncu FP64-pipe utilisation is in profiles/"}
 
 
 def main():
