@@ -33,6 +33,17 @@ __device__ __forceinline__ void decompose(const Geometry& g, int n, int* m) {
   m[2] = n % g.nc[2];
 }
 __device__ __forceinline__ int compose(const Geometry& g, const int* m) { return m[2] + g.nc[2] * (m[1] + g.nc[1] * m[0]); }
+// mesh index of q1 + w (sign=+1) or q1 - w (sign=-1); `inside` is get_k_info's flag
+__device__ __forceinline__ int pm_index(const Geometry& g, const int* m1, const int* mw, int sign, int& inside) {
+  int m[3];
+  inside = 1;
+  for (int a = 0; a < 3; ++a) {
+    int v = m1[a] + sign * mw[a] + (g.shifted ? -sign * (g.nc[a] / 2) : 0);
+    if (v < 0 || v >= g.nc[a]) inside = 0;
+    m[a] = wrapm(v, g.nc[a]);
+  }
+  return compose(g, m);
+}
 
 __device__ __forceinline__ double nbe_dev(double w, double t, int m, int* err) {
   if (t <= 0 || w <= 0) {
@@ -185,6 +196,81 @@ __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* 
     for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + c0 + j] = blk[i + 3 * j];
 }
 
+// ------------------------------------------------- iterative BTE (job=3)
+// F over the whole mesh: Ff[q][l][:] = op_kmatrix(op(q)) F[ibz(q)][l][:]
+// (syop_f, sub.f90:2117), op(q) the op of q's arm in kstarsinfbz1 of its
+// IBZ point -- what update_mpi's kvecop and get_kvecopn2 pick
+__global__ void ffull_kernel(Geometry g, const int* mapibz, const int* full_op, const double* opk, const double* F,
+                             double* Ff) {
+  const int b = g.b;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= g.nkc * b) return;
+  const int q = e / b, l = e % b;
+  const double* f = F + ((size_t)mapibz[q] * b + l) * 3;
+  double in[3] = {f[0], f[1], f[2]}, out[3];
+  opmul(opk + 9 * full_op[q], in, out);
+  double* o = Ff + ((size_t)q * b + l) * 3;
+  o[0] = out[0];
+  o[1] = out[1];
+  o[2] = out[2];
+}
+
+// update_mpi for one IBZ row per CTA: threads walk q2, each accumulating
+// A[l1][xyz] for every l1; CTA sums in a fixed order
+template <int B>
+__global__ void __launch_bounds__(256) update_kernel(Geometry g, int n1_first, const int* mapinv, const double* R1,
+                                                     const double* R1p, const double* R2, const double* R2p,
+                                                     const double* Ff, const double* Q, const double* F_RTA,
+                                                     const double* F, double mix, double* Fout) {
+  __shared__ double red[8][3 * B];
+  const int b = g.b, nkc = g.nkc, nl = blockIdx.x, n1 = n1_first + nl;
+  const int q1 = mapinv[n1];
+  int m1[3];
+  decompose(g, q1, m1);
+  double acc[B][3];
+#pragma unroll
+  for (int l1 = 0; l1 < B; ++l1) acc[l1][0] = acc[l1][1] = acc[l1][2] = 0.0;
+  const size_t rb = (size_t)nl * nkc;
+  for (int q = threadIdx.x; q < nkc; q += blockDim.x) {
+    int mq[3], ins;
+    decompose(g, q, mq);
+    const int qp = pm_index(g, m1, mq, 1, ins), qm = pm_index(g, m1, mq, -1, ins);
+    const double* fq = Ff + (size_t)q * b * 3;
+    const double* fp = Ff + (size_t)qp * b * 3;
+    const double* fm = Ff + (size_t)qm * b * 3;
+    const size_t o = (rb + q) * b * b;
+#pragma unroll
+    for (int l1 = 0; l1 < B; ++l1) {
+      if (l1 >= b) break;
+      for (int l = 0; l < b; ++l) {
+        const size_t i = o + l1 * b + l;
+        const double c1 = R1[i], c1p = R1p[i], c2 = R2[i], c2p = R2p[i];
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+          acc[l1][x] += c1p * fp[l * 3 + x] - c1 * fq[l * 3 + x] + 0.5 * (c2 * fq[l * 3 + x] + c2p * fm[l * 3 + x]);
+      }
+    }
+  }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+#pragma unroll
+  for (int l1 = 0; l1 < B; ++l1)
+#pragma unroll
+    for (int x = 0; x < 3; ++x) {
+      double v = acc[l1][x];
+      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
+      if (lane == 0) red[warp][l1 * 3 + x] = v;
+    }
+  __syncthreads();
+  if (threadIdx.x < 3 * b) {
+    const int l1 = threadIdx.x / 3, x = threadIdx.x % 3;
+    double A = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) A += red[w][threadIdx.x];
+    const size_t fi = ((size_t)n1 * b + l1) * 3 + x;
+    const double f2 = F_RTA[fi] + A / Q[(size_t)n1 * b + l1];
+    Fout[((size_t)nl * b + l1) * 3 + x] = mix > 0 ? F[fi] + mix * (f2 - F[fi]) : f2;
+  }
+}
+
 // ---------------------------------------------------------------- CG
 constexpr int kGemvWarps = 8;
 constexpr int kVecThreads = 1024;
@@ -329,6 +415,27 @@ cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaS
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s) {
   kappa_kernel<<<a.geo.b, 256, 0, s>>>(a, F, averaged, kappa_modes, err);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_ffull(const Geometry& geo, const int* mapibz, const int* full_op, const double* opk,
+                         const double* F, double* Ff, cudaStream_t s) {
+  const int n = geo.nkc * geo.b;
+  ffull_kernel<<<(n + 255) / 256, 256, 0, s>>>(geo, mapibz, full_op, opk, F, Ff);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
+                          const double* R1p, const double* R2, const double* R2p, const double* Ff, const double* Q,
+                          const double* F_RTA, const double* F, double mix, double* Fout, cudaStream_t s) {
+  if (geo.b <= 3)
+    update_kernel<3><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
+  else if (geo.b <= 6)
+    update_kernel<6><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
+  else if (geo.b <= 12)
+    update_kernel<12><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
+  else
+    return cudaErrorInvalidValue;
   return cudaGetLastError();
 }
 

@@ -336,6 +336,20 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   CKA(upload(c->tet_corner, c->T.tet_corner, s));
   CKA(upload(c->tet_inc, c->T.tet_inc, s));
   {
+    // update_mpi's rotation of F to every mesh point: the op of the point's
+    // arm in kstarsinfbz1 of its IBZ point (every mesh point is such an arm
+    // exactly once on the meshes the reference accepts)
+    std::vector<int> m0(c->T.nkc), fop(c->T.nkc, -1);
+    for (int q = 0; q < c->T.nkc; ++q) m0[q] = c->T.mapibz[q] - 1;
+    for (int i = 0; i < c->T.nibz; ++i)
+      for (int a = c->T.arm_off[i]; a < c->T.arm_off[i + 1]; ++a)
+        if (fop[c->T.arm_q[a]] < 0 && m0[c->T.arm_q[a]] == i) fop[c->T.arm_q[a]] = c->T.arm_op[a];
+    c->full_op_ok = std::all_of(fop.begin(), fop.end(), [](int v) { return v >= 0; });
+    for (int& v : fop) v = std::max(v, 0);
+    CKA(upload(c->mapibz0, m0, s));
+    CKA(upload(c->full_op, fop, s));
+  }
+  {
     std::vector<double> op(48 * 9, 0.0), opi(48 * 9, 0.0);
     for (int o = 0; o < c->T.npg; ++o) {
       const double* m = c->T.opk[o];
@@ -532,6 +546,8 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   a.P2s = p2.p;
   a.P1 = nullptr;
   a.P2 = nullptr;
+  a.R1p = a.R2p = nullptr;
+  a.v3_layout = 0;
   CK(launch_combine(a, scratch.p, c->stream));
   CK(launch_to_fortran5(p1.p, vf.p, nr, nkc, b, c->stream));
   CK(cudaMemcpyAsync(P1smpi, vf.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -714,6 +730,61 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
   if (funcmin) *funcmin = fm;
   if (iters) *iters = it;
   return r;
+}
+
+int ald_update_mpi(ald_ctx* c, const int ksubset[2], const double* P1, const double* P2, const double* Qv,
+                   const double* F_RTA, const double* FFF, double* F2mpi) {
+  if (!c || !P1 || !P2 || !Qv || !F_RTA || !FFF || !F2mpi) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  if (!c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
+  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: more than 12 bands is not supported");
+  CK(cudaSetDevice(c->device));
+  const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc, nibz = c->T.nibz;
+  const size_t n = (size_t)nr * nkc * b * b * b, nm = (size_t)nr * nkc * b * b, nf = (size_t)nibz * b * 3;
+  DevBuf<double> tmp, s1, s2, R1, R2, R1p, R2p, Qd, q, frta, f, ff, out;
+  CKA(tmp.alloc(n));
+  CKA(s1.alloc(n));
+  CKA(s2.alloc(n));
+  CKA(R1.alloc(nm));
+  CKA(R2.alloc(nm));
+  CKA(R1p.alloc(nm));
+  CKA(R2p.alloc(nm));
+  CKA(Qd.alloc((size_t)nr * b));
+  CKA(q.alloc((size_t)nibz * b));
+  CKA(frta.alloc(nf));
+  CKA(f.alloc(nf));
+  CKA(ff.alloc((size_t)nkc * b * 3));
+  CKA(out.alloc((size_t)nr * b * 3));
+  cudaStream_t s = c->stream;
+  CK(cudaMemcpyAsync(tmp.p, P1, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(launch_from_fortran5(tmp.p, s1.p, nr, nkc, b, s));
+  CK(cudaMemcpyAsync(tmp.p, P2, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(launch_from_fortran5(tmp.p, s2.p, nr, nkc, b, s));
+  CK(launch_collapse(c->geo, nr, s1.p, s2.p, R1.p, R2.p, Qd.p, s));
+  CK(launch_marginal_l2(c->geo, nr, s1.p, s2.p, R1p.p, R2p.p, s));
+  // Q(nibz,ndyn), F_RTA and FFF (nibz,ndyn,3) to [n][l] and [n][l][xyz]
+  std::vector<double> hq((size_t)nibz * b), hr(nf), hf(nf);
+  for (int i = 0; i < nibz; ++i)
+    for (int l = 0; l < b; ++l) {
+      hq[(size_t)i * b + l] = Qv[i + (size_t)nibz * l];
+      for (int x = 0; x < 3; ++x) {
+        hr[((size_t)i * b + l) * 3 + x] = F_RTA[i + (size_t)nibz * (l + (size_t)b * x)];
+        hf[((size_t)i * b + l) * 3 + x] = FFF[i + (size_t)nibz * (l + (size_t)b * x)];
+      }
+    }
+  CK(cudaMemcpyAsync(q.p, hq.data(), hq.size() * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(frta.p, hr.data(), nf * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(cudaMemcpyAsync(f.p, hf.data(), nf * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(launch_ffull(c->geo, c->mapibz0.p, c->full_op.p, c->opk.p, f.p, ff.p, s));
+  CK(launch_update(c->geo, ksubset[0] - 1, nr, c->mapinv.p, R1.p, R1p.p, R2.p, R2p.p, ff.p, q.p, frta.p, f.p, 0.0,
+                   out.p, s));
+  std::vector<double> ho((size_t)nr * b * 3);
+  CK(cudaMemcpyAsync(ho.data(), out.p, ho.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  for (int i = 0; i < nr; ++i)
+    for (int l = 0; l < b; ++l)
+      for (int x = 0; x < 3; ++x) F2mpi[i + (size_t)nr * (l + (size_t)b * x)] = ho[((size_t)i * b + l) * 3 + x];
+  return ALD_OK;
 }
 
 int ald_mode_kappa_d(ald_ctx* c, double tempk, const double* Fi_x, double* kappa) {

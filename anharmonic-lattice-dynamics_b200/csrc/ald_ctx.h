@@ -24,11 +24,14 @@ struct ald_ctx {
   DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,
       arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
   DevBuf<int> cls_grp_off, cls_pc, cls_trip_off, cls_trip, cls_trip_i0, cls_trip_k;
+  DevBuf<int> mapibz0, full_op;       // per mesh point: IBZ point and the op of its star arm (job=3)
+  bool full_op_ok = false;
   DevBuf<char> w_h;                   // per-row phase-class sums of the pair kernel
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
   // pipeline workspaces, kept across calls (allocation outside the timed work)
   DevBuf<double> w_R1, w_R2, w_Q, w_v3, w_F, w_x, w_rhs, w_kr, w_kc, w_cm;
+  DevBuf<double> w_R1p, w_R2p, w_Ff, w_Frta;  // iterative solution: band marginals, F on the mesh
   DevBuf<char> w_scratch;
   CgWork cg;
   bool have_phonons = false;

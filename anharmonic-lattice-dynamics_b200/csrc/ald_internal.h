@@ -237,6 +237,8 @@ struct CombineArgs {
   double sigma;
   double* R1;                // [row][q][l1][l2], row local to the chunk
   double* R2;
+  double* R1p;               // optional [row][q][l1][l3] = sum_l2 P1 (update_mpi); nullptr = skip
+  double* R2p;
   double* P1s;               // optional [row][q][l1][l2][l3] (P1smpi)
   double* P2s;
   double* P1;                // optional Bose-weighted
@@ -294,6 +296,22 @@ cudaError_t launch_tau(const Geometry& geo, int n1_first, int nrows, const int* 
 // R1/R2 = sum_l3 P1/P2 and Qd = sum (P1 + P2/2) from Bose-weighted P (internal layout)
 cudaError_t launch_collapse(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1,
                             double* R2, double* Qd, cudaStream_t s);
+// Rp = sum_l2 P (internal layout), the band marginal update_mpi needs besides R
+cudaError_t launch_marginal_l2(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1p,
+                               double* R2p, cudaStream_t s);
+// update_mpi (sub.f90:2295-2449) on band marginals:
+//   Ff[q][l][:] = S_op(q) F[ibz(q)][l][:] over the whole mesh (F [n][l][xyz]);
+//   F2[n1][l1] = F_RTA[n1][l1] + A/Q[n1][l1],
+//   A = sum_q sum_l R1p[q][l1][l] Ff[q1+q][l] - R1[q][l1][l] Ff[q][l]
+//             + (R2[q][l1][l] Ff[q][l] + R2p[q][l1][l] Ff[q1-q][l]) / 2;
+// with mix > 0 the output is Fout = F + mix (F2 - F) (in place allowed).
+// R arrays are local to rows [n1_first, n1_first + nrows); Q, F_RTA, F over
+// all IBZ points; Fout local to the rows.
+cudaError_t launch_ffull(const Geometry& geo, const int* mapibz, const int* full_op, const double* opk,
+                         const double* F, double* Ff, cudaStream_t s);
+cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
+                          const double* R1p, const double* R2, const double* R2p, const double* Ff, const double* Q,
+                          const double* F_RTA, const double* F, double mix, double* Fout, cudaStream_t s);
 // CG workspace: vectors, scalars and the captured CUDA graph of the
 // iteration loop, kept across calls and re-captured only when the problem
 // (size, pointers, stop rule) changes

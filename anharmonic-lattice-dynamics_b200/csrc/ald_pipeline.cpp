@@ -68,9 +68,17 @@ struct StageTimer {
 
 }  // namespace
 
-extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo,
-                                  double* QUo, double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
+// the job=3 iteration of kappa.f90:1390-1487 in place of the CG solve
+struct IterSpec {
+  int max_iter;
+  double mix;
+  double* F;  // optional out: FFF(nibz, ndyn, 3)
+};
+
+static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo, double* QUo,
+                        double* kappa_rta_modes, double* kappa_cg_modes, double* xo, const IterSpec* it) {
   if (!c || !res) return fail(ALD_ERR_ARG, "null argument");
+  if (it && !c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
   if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 12 bands is not supported by this build");
   ALD_CK(cudaSetDevice(c->device));
@@ -109,6 +117,10 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   DevBuf<char>& escratch = c->w_scratch;
   ALD_CKA(R1.alloc(rsz));
   ALD_CKA(R2.alloc(rsz));
+  if (it) {  // update_mpi also needs the band marginals over l2
+    ALD_CKA(c->w_R1p.alloc(rsz));
+    ALD_CKA(c->w_R2p.alloc(rsz));
+  }
   ALD_CKA(Q.alloc((size_t)3 * nibz * b));
   const int K = rows_per_chunk(c);
   ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
@@ -143,9 +155,16 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
     a.R1 = R1.p + (size_t)r0 * nkc * b * b;
     a.R2 = R2.p + (size_t)r0 * nkc * b * b;
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
+    a.R1p = it ? c->w_R1p.p + (size_t)r0 * nkc * b * b : nullptr;
+    a.R2p = it ? c->w_R2p.p + (size_t)r0 * nkc * b * b : nullptr;
     ALD_CK(tm.begin(2));
+    const size_t rbytes = (size_t)nr * nkc * b * b * sizeof(double);
+    if (it) {
+      ALD_CK(cudaMemsetAsync(a.R1p, 0, rbytes, s));
+      ALD_CK(cudaMemsetAsync(a.R2p, 0, rbytes, s));
+    }
     if (fused) {
-      const size_t n = (size_t)nr * nkc * b * b * sizeof(double);
+      const size_t n = rbytes;
       ALD_CK(cudaMemsetAsync(a.R1, 0, n, s));
       ALD_CK(cudaMemsetAsync(a.R2, 0, n, s));
       ALD_CK(launch_delta_fused(a, s));
@@ -183,6 +202,89 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   ALD_CK(launch_kappa(k, F.p, 0, kr.p, c->err.p, s));
   res->launches[4] += 2;
   ALD_CK(tm.end());
+  if (it) {
+    // ---- 7: FFF += mix (update_mpi(FFF) - FFF), kappa = mode_kappa(FFF), until
+    // sqrt(sum((kappa_new - kappa_old)^2) / (ndyn*9)) < 1e-4 (kappa.f90:1390-1487)
+    DevBuf<double>& Ff = c->w_Ff;
+    DevBuf<double>& Frta = c->w_Frta;
+    ALD_CKA(Ff.alloc((size_t)nkc * b * 3));
+    ALD_CKA(Frta.alloc(N));
+    ALD_CK(cudaMemcpyAsync(Frta.p, F.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    ALD_CK(tm.begin(7));
+    std::vector<double> kold((size_t)9 * b), knew((size_t)9 * b);
+    ALD_CK(cudaMemcpyAsync(kold.data(), kr.p, kold.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    ALD_CK(cudaStreamSynchronize(s));
+    int iters = 0;
+    double normk = 0;
+    bool conv = false;
+    for (int i = 1; i <= it->max_iter; ++i) {
+      ALD_CK(launch_ffull(c->geo, c->mapibz0.p, c->full_op.p, c->opk.p, F.p, Ff.p, s));
+      ALD_CK(launch_update(c->geo, 0, nibz, c->mapinv.p, R1.p, c->w_R1p.p, R2.p, c->w_R2p.p, Ff.p, dQ, Frta.p, F.p,
+                           it->mix, F.p, s));
+      ALD_CK(launch_kappa(k, F.p, 0, kc.p, c->err.p, s));
+      res->launches[7] += 3;
+      ALD_CK(cudaMemcpyAsync(knew.data(), kc.p, knew.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      ALD_CK(cudaStreamSynchronize(s));
+      double e = 0;
+      for (int j = 0; j < 9 * b; ++j) e = e + (knew[j] - kold[j]) * (knew[j] - kold[j]) / (b * 3 * 3);
+      iters = i;
+      normk = std::sqrt(e);
+      if (normk < 0.0001) {
+        conv = true;
+        break;
+      }
+      kold = knew;
+    }
+    ALD_CK(tm.end());
+    ALD_CK(cudaEventRecord(t1, s));
+    std::vector<double> hkr((size_t)9 * b), hF;
+    ALD_CK(cudaMemcpyAsync(hkr.data(), kr.p, hkr.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+    double d2h = 2.0 * hkr.size() * sizeof(double) * (1 + iters);
+    std::vector<double> hq;
+    if (Qo || QNo || QUo) {
+      hq.resize((size_t)3 * nibz * b);
+      ALD_CK(cudaMemcpyAsync(hq.data(), Q.p, hq.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      d2h += hq.size() * sizeof(double);
+    }
+    if (it->F) {
+      hF.resize(N);
+      ALD_CK(cudaMemcpyAsync(hF.data(), F.p, N * sizeof(double), cudaMemcpyDeviceToHost, s));
+      d2h += N * sizeof(double);
+    }
+    ALD_CK(cudaStreamSynchronize(s));
+    r = check_err_flags(c);
+    if (r) return r;
+    tm.collect(res->stage_ms);
+    float total = 0;
+    cudaEventElapsedTime(&total, t0, t1);
+    res->stage_ms[9] = total;
+    for (int i = 0; i < 9; ++i) res->launches[9] += res->launches[i];
+    for (int e = 0; e < 9; ++e) {
+      double sr = 0, sc = 0;
+      for (int l = 0; l < b; ++l) {
+        sr += hkr[l + (size_t)b * e];
+        sc += knew[l + (size_t)b * e];
+      }
+      res->kappa_rta[e] = sr;
+      res->kappa_cg[e] = sc;
+    }
+    if (kappa_rta_modes) std::memcpy(kappa_rta_modes, hkr.data(), hkr.size() * sizeof(double));
+    if (kappa_cg_modes) std::memcpy(kappa_cg_modes, knew.data(), knew.size() * sizeof(double));
+    for (int i = 0; i < nibz; ++i)
+      for (int l = 0; l < b; ++l) {
+        if (Qo) Qo[i + (size_t)nibz * l] = hq[(size_t)i * b + l];
+        if (QNo) QNo[i + (size_t)nibz * l] = hq[(size_t)nibz * b + (size_t)i * b + l];
+        if (QUo) QUo[i + (size_t)nibz * l] = hq[(size_t)2 * nibz * b + (size_t)i * b + l];
+        if (it->F)
+          for (int x = 0; x < 3; ++x) it->F[i + (size_t)nibz * (l + (size_t)b * x)] = hF[((size_t)i * b + l) * 3 + x];
+      }
+    res->cg_iters = iters;
+    res->status_cg = conv ? ALD_OK : ALD_WARN_CG_MAXITER;
+    res->cg_err = normk;
+    res->triplet_bands = (double)nibz * nkc * (double)b * b * b;
+    res->d2h_bytes = d2h;
+    return ALD_OK;
+  }
   // ---- 5: collision matrix (row-major, all IBZ rows)
   ALD_CKA(cm.alloc(N * N));
   ALD_CK(tm.begin(5));
@@ -259,4 +361,16 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   res->triplet_bands = (double)nibz * nkc * (double)b * b * b;
   res->d2h_bytes = d2h;
   return ALD_OK;
+}
+
+extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo,
+                                  double* QUo, double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
+  return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr);
+}
+
+extern "C" int ald_kappa_iterative(ald_ctx* c, double tempk, int max_iter, double update_mix, ald_kappa_result* res,
+                                   double* Qo, double* kappa_rta_modes, double* kappa_iter_modes, double* FFF) {
+  if (max_iter < 0 || !(update_mix > 0)) return fail(ALD_ERR_ARG, "max_iter < 0 or update_mix <= 0");
+  IterSpec it{max_iter, update_mix, FFF};
+  return run_pipeline(c, tempk, res, Qo, nullptr, nullptr, kappa_rta_modes, kappa_iter_modes, nullptr, &it);
 }

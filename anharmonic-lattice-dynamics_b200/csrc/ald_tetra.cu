@@ -251,6 +251,8 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
         const double p = ps * Fb;
         if (proc == 0) R1[l] += p;
         else R2[l] += p;
+        double* Rpm = proc == 0 ? a.R1p : a.R2p;
+        if (Rpm && p != 0.0) atomicAdd(Rpm + (((size_t)row * nkc + w) * b + l) * b + l3, p);
         if (Ps || Pb) {
           size_t o5 = (((size_t)row * nkc + w) * b + l) * b2 + l2 * b + l3;
           if (Ps) Ps[o5] = ps;
@@ -416,6 +418,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
   }
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   double* Rp = proc == 0 ? a.R1 : a.R2;
+  double* Rpp = proc == 0 ? a.R1p : a.R2p;  // band marginal over l2 (optional)
   // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
   size_t sq, s1, s2, s3;
   if (a.v3_layout == 1) {
@@ -534,6 +537,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
       const double nb1 = s_nb1[l1];
       double* Rrow = Rp + (size_t)row * nkc * b * b + l1 * b + l2;
+      double* Rrowp = Rpp ? Rpp + (size_t)row * nkc * b * b + l1 * b + l3 : nullptr;
       const double* vs = v3row + l2 * s2 + l3 * s3 + l1 * s1;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -542,6 +546,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
         if (cp[k] == 0.0 || G == 0.0) continue;
         const double val = (cp[k] / 6.0) * (__ldg(vs + (size_t)s_src[p] * sq) * fnorm) * (nb1 * G);
         atomicAdd(Rrow + (size_t)s_w[p] * b * b, val);
+        if (Rrowp) atomicAdd(Rrowp + (size_t)s_w[p] * b * b, val);
       }
     }
   }

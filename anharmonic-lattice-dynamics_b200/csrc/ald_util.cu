@@ -149,7 +149,32 @@ __global__ void qdiag_kernel(int nkc, int b, const double* R1, const double* R2,
 
 int grid_for(size_t total) { return (int)std::min<size_t>((total + 255) / 256, 148 * 32); }
 
+// Rp[row][q][l1][l3] = sum_l2 P[row][q][l1][l2][l3] (the other band marginal)
+__global__ void marginal_l2_kernel(int nrows, int nkc, int b, const double* P1, const double* P2, double* R1p,
+                                   double* R2p) {
+  const size_t total = (size_t)nrows * nkc * b * b;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t rq = e / ((size_t)b * b);
+    const int l1 = (int)((e / b) % b), l3 = (int)(e % b);
+    double s1 = 0, s2 = 0;
+    for (int l2 = 0; l2 < b; ++l2) {
+      const size_t o = ((rq * b + l1) * b + l2) * b + l3;
+      s1 += P1[o];
+      s2 += P2[o];
+    }
+    R1p[e] = s1;
+    R2p[e] = s2;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_marginal_l2(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1p,
+                               double* R2p, cudaStream_t s) {
+  const size_t total = (size_t)nrows * geo.nkc * geo.b * geo.b;
+  marginal_l2_kernel<<<grid_for(total), 256, 0, s>>>(nrows, geo.nkc, geo.b, P1, P2, R1p, R2p);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_to_fortran5(const double* src, double* dst, int nr, int nkc, int b, cudaStream_t s) {
   size_t total = (size_t)nr * nkc * b * b * b;

@@ -64,7 +64,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_read_mesh", "ald_get_mesh", "ald_get_frequencies", "ald_set_phonons",
            "ald_calculate_w3_ibz_split_sq", "ald_calculate_fgr", "ald_distribution", "ald_calculate_tau_rta",
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
-           "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static"]
+           "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
+           "ald_kappa_iterative"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -244,6 +245,34 @@ class Context:
         r = np.zeros(self.nibz * self.ndyn * 3)
         _check(lib().ald_rhs(self.h, C.c_double(tempk), _p(r)))
         return r
+
+    def update_mpi(self, ksubset, P1, P2, Q, F_RTA, FFF):
+        """update_mpi (sub.f90:2295): F2mpi(nk1, ndyn, 3) for IBZ rows ksubset."""
+        k = (C.c_int * 2)(*ksubset)
+        nr = ksubset[1] - ksubset[0] + 1
+        F2 = np.zeros((nr, self.ndyn, 3), order="F")
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        _check(lib().ald_update_mpi(self.h, k, f(P1), f(P2), f(Q), f(F_RTA), f(FFF), _p(F2)))
+        return F2
+
+    def kappa_iterative(self, tempk=None, max_iter=150, update_mix=0.4):
+        """The job=3 sequence (kappa.f90:1046-1487) on the device."""
+        if tempk is None:
+            tempk = self.info.tempk
+        res = KappaResult()
+        n, ni = self.ndyn, self.nibz
+        Q = np.zeros((ni, n), order="F")
+        kr = np.zeros((n, 3, 3), order="F")
+        ki = np.zeros((n, 3, 3), order="F")
+        F = np.zeros((ni, n, 3), order="F")
+        r = _check(lib().ald_kappa_iterative(self.h, C.c_double(tempk), max_iter, C.c_double(update_mix),
+                                             C.byref(res), _p(Q), _p(kr), _p(ki), _p(F)),
+                   allow=(ALD_OK,))
+        return {"kappa_rta": np.array(res.kappa_rta).reshape(3, 3, order="F"),
+                "kappa_iter": np.array(res.kappa_cg).reshape(3, 3, order="F"), "iters": res.cg_iters,
+                "normk": res.cg_err, "status": res.status_cg, "Q": Q, "kappa_rta_modes": kr,
+                "kappa_iter_modes": ki, "F": F, "stage_ms": dict(zip(STAGES, res.stage_ms)),
+                "launches": dict(zip(STAGES, res.launches)), "triplet_bands": res.triplet_bands}
 
     def mode_kappa_d(self, tempk, x):
         kap = np.zeros((self.ndyn, 3, 3), order="F")

@@ -175,6 +175,16 @@ int ald_cg_quadratic_static(int n, const double* a, const double* b, double* vmi
  * (veloc_avergeIBZ_invsyFBZ sub.f90:5479). */
 int ald_mode_kappa_d(ald_ctx* ctx, double tempk, const double* Fi_x, double* kappa);
 
+/* update_mpi (sub.f90:2295-2449), one step of the iterative BTE of job=3:
+ * F2mpi(nk1,ndyn,3) = F_RTA + A/Qvalue for IBZ rows ksubset, with A the sum
+ * over IBZ q2, its star arms (kstarsinfbz1) and l2, l3 of
+ *   P1 (S F(q1+q2,l3) - S F(q2,l2)) + P2/2 (S F(q2,l2) + S F(q1-q2,l3)),
+ * S the op that maps the IBZ point onto the arm (syop_f, get_kvecopn2).
+ * P1, P2(nk1,nkc,ndyn,ndyn,ndyn) Bose-weighted as ald_calculate_tau_rta
+ * returns them; Qvalue(nibz,ndyn); F_RTA, FFF(nibz,ndyn,3). */
+int ald_update_mpi(ald_ctx* ctx, const int ksubset[2], const double* P1, const double* P2, const double* Qvalue,
+                   const double* F_RTA, const double* FFF, double* F2mpi);
+
 /* The whole job=1 sequence (kappa.f90:389-871) on the device without
  * materialising any (nibz,nkc,ndyn^3) array: phonons (unless injected),
  * V3, delta, Q, RTA kappa, collision matrix, RHS, CG, kappa.  Only the
@@ -206,6 +216,17 @@ double ald_h2d_bytes(ald_ctx* ctx);
  * x (nibz*ndyn*3, the CG solution) may be NULL. */
 int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double* Q, double* QN, double* QU,
                        double* kappa_rta_modes, double* kappa_cg_modes, double* x);
+
+/* The job=3 sequence (kappa.f90:1046-1487): as ald_kappa_pipeline up to the
+ * RTA kappa, then from FFF = F_RTA repeat FFF += update_mix (update_mpi(FFF)
+ * - FFF) and kappa = mode_kappa(FFF) until sqrt(sum((kappa_new -
+ * kappa_old)^2)/(ndyn*9)) < 1e-4 or max_iter iterations (150 and 0.4 in
+ * read_params, rest.f90:36-44).  In `res`, kappa_cg holds the iterative kappa,
+ * cg_iters the iterations, cg_err the last change and status_cg ALD_OK or
+ * ALD_WARN_CG_MAXITER; stage 7 times the iterations, stages 5, 6, 8 are 0.
+ * Q(nibz,ndyn), the mode tensors (ndyn,3,3) and FFF(nibz,ndyn,3) may be NULL. */
+int ald_kappa_iterative(ald_ctx* ctx, double tempk, int max_iter, double update_mix, ald_kappa_result* res,
+                        double* Q, double* kappa_rta_modes, double* kappa_iter_modes, double* FFF);
 
 #ifdef __cplusplus
 }

@@ -17,7 +17,10 @@
 //   CollisionMatrix_mpi           THERMACOND/sub.f90:3034-3210
 //   cal_RHS_IBZ                   THERMACOND/sub.f90:2618-2691
 //   cg_quadratic                  THERMACOND/cg.f90:19-61
+//   get_kvecopn2, update_mpi      THERMACOND/sub.f90:2045-2111, 2295-2449
+//   the job=3 mixing loop         THERMACOND/kappa.f90:1390-1487
 #include <algorithm>
+#include <array>
 #include <atomic>
 #include <cstring>
 
@@ -714,4 +717,134 @@ int cg_quadratic(int n, const double* a, const double* b, double* vmin, double* 
   return iter;
 }
 
+// ------------------------------------------------- iterative BTE (job=3)
+// kstarsinfbz1 of every IBZ point, computed once (kstarsinfbz1 is a pure
+// function of the IBZ vector; update_mpi and get_kvecopn2 call it per arm)
+struct IbzArms {
+  std::vector<int> narms;
+  std::vector<std::array<std::array<double, 3>, 48>> star;
+  std::vector<std::array<int, 48>> op;
+  std::vector<std::array<int, 48>> idx;  // get_k_info index of each arm
+};
+
+static void ibz_arms(const State& S, IbzArms& A) {
+  A.narms.assign(S.nibz, 0);
+  A.star.resize(S.nibz);
+  A.op.resize(S.nibz);
+  A.idx.resize(S.nibz);
+  for (int n = 1; n <= S.nibz; ++n) {
+    double q[3] = {S.kibz[F2(1, n, 3)], S.kibz[F2(2, n, 3)], S.kibz[F2(3, n, 3)]};
+    int narms, ops[48];
+    double st[48][3];
+    kstarsinfbz1(S, q, narms, st, ops);
+    A.narms[n - 1] = narms;
+    for (int s = 0; s < narms; ++s) {
+      for (int c = 0; c < 3; ++c) A.star[n - 1][s][c] = st[s][c];
+      A.op[n - 1][s] = ops[s];
+      int i3, j3, k3, inside;
+      get_k_info(S, st[s], A.idx[n - 1][s], i3, j3, k3, inside);
+    }
+  }
+}
+
+// get_kvecopn2 (sub.f90:2045-2111): the op of the first arm of
+// kstarsinfbz1(kibz(n)) whose mesh index equals that of k.  Like the
+// reference, spf keeps its previous value when no arm matches.
+static void get_kvecopn2(const State& S, const IbzArms& A, int n, const double k[3], int& spf) {
+  int sk, i3, j3, k3, inside;
+  get_k_info(S, k, sk, i3, j3, k3, inside);
+  for (int s = 0; s < A.narms[n - 1]; ++s)
+    if (A.idx[n - 1][s] == sk) {
+      spf = A.op[n - 1][s];
+      return;
+    }
+}
+
+// update_mpi (sub.f90:2295-2449): F2(n1,l1,:) = F_RTA(n1,l1,:) + A(n1,l1,:)/Q(n1,l1)
+// with A = sum over IBZ q2, its arms s and l2, l3 of
+//   P1(n1,s,l1,l2,l3) (S_sp1 F(q1+s,l3) - S_sq2 F(q2,l2))
+//   + 0.5 P2(n1,s,l1,l2,l3) (S_sq2 F(q2,l2) + S_sp2 F(q1-s,l3)).
+// P1, P2: (nk1,nkc,ndn,ndn,ndn) Bose-weighted; Q, F_RTA, FFF over all IBZ
+// points; F2mpi(nk1,ndn,3).  The arm data, which do not depend on l1 and
+// xyz, are evaluated once per (q1, q2, arm) instead of inside those loops.
+void update_mpi(State& S, int k1, int k2, const double* P1, const double* P2, const double* Q,
+                const double* F_RTA, const double* FFF, double* F2mpi, int nthreads) {
+  const int ndn = S.ndyn, nkc = S.nkc, nibz = S.nibz, nsub = k2 - k1 + 1;
+  IbzArms A;
+  ibz_arms(S, A);
+  parfor(1, nsub, nthreads, [&](int ibz) {
+    const int n1 = ibz + k1 - 1;
+    const double q1[3] = {S.kibz[F2(1, n1, 3)], S.kibz[F2(2, n1, 3)], S.kibz[F2(3, n1, 3)]};
+    struct Arm {
+      int n2, ns, sq2, i1, i2, sp1f, sp2f;
+    };
+    std::vector<Arm> arms;
+    int sp1f = 1, sp2f = 1;
+    for (int n2 = 1; n2 <= nibz; ++n2)
+      for (int s = 0; s < A.narms[n2 - 1]; ++s) {
+        const double* ks = A.star[n2 - 1][s].data();
+        double q3p1[3], q3p2[3];
+        for (int c = 0; c < 3; ++c) {
+          q3p1[c] = q1[c] + ks[c];
+          q3p2[c] = q1[c] - ks[c];
+        }
+        int i3, j3, k3, inside, nk3p1, nk3p2;
+        get_k_info(S, q3p1, nk3p1, i3, j3, k3, inside);
+        get_k_info(S, q3p2, nk3p2, i3, j3, k3, inside);
+        const int i1 = S.mapibz[nk3p1 - 1], i2 = S.mapibz[nk3p2 - 1];
+        get_kvecopn2(S, A, i1, q3p1, sp1f);
+        get_kvecopn2(S, A, i2, q3p2, sp2f);
+        arms.push_back({n2, A.idx[n2 - 1][s], A.op[n2 - 1][s], i1, i2, sp1f, sp2f});
+      }
+    for (int l1 = 1; l1 <= ndn; ++l1)
+      for (int xyz = 1; xyz <= 3; ++xyz) {
+        double Av = 0;
+        for (const Arm& a : arms)
+          for (int l2 = 1; l2 <= ndn; ++l2)
+            for (int l3 = 1; l3 <= ndn; ++l3) {
+              double f[3], Fsq2[3], Fsp1[3], Fsp2[3];
+              for (int c = 1; c <= 3; ++c) f[c - 1] = FFF[F3(a.n2, l2, c, nibz, ndn)];
+              syop_f(S, a.sq2, f, Fsq2);
+              for (int c = 1; c <= 3; ++c) f[c - 1] = FFF[F3(a.i1, l3, c, nibz, ndn)];
+              syop_f(S, a.sp1f, f, Fsp1);
+              for (int c = 1; c <= 3; ++c) f[c - 1] = FFF[F3(a.i2, l3, c, nibz, ndn)];
+              syop_f(S, a.sp2f, f, Fsp2);
+              const size_t pi = F5(ibz, a.ns, l1, l2, l3, nsub, nkc, ndn, ndn);
+              Av = Av + P1[pi] * (Fsp1[xyz - 1] - Fsq2[xyz - 1]) + 0.5 * P2[pi] * (Fsq2[xyz - 1] + Fsp2[xyz - 1]);
+            }
+        F2mpi[F3(ibz, l1, xyz, nsub, ndn)] = F_RTA[F3(n1, l1, xyz, nibz, ndn)] + Av / Q[F2(n1, l1, nibz)];
+      }
+  });
+}
+
+// The job=3 iteration (kappa.f90:1390-1487): starting from F = F_RTA and the
+// RTA kappa, repeat update_mpi over all IBZ rows, F += update_mix (F2 - F),
+// kappa = mode_kappa(F), until sqrt(sum((kappa_new - kappa_old)^2)/(ndn*9)) <
+// 1e-4 or max_iter iterations.  Returns the nbe error flag; *iters and
+// *normk receive the iteration count and the last change.
+int iterative_bte(State& S, double tempk, const double* P1, const double* P2, const double* Q,
+                  const double* F_RTA, int max_iter, double update_mix, double* FFF, double* kappa, int* iters,
+                  double* normk, int nthreads) {
+  const int ndn = S.ndyn, nibz = S.nibz;
+  const size_t nf = (size_t)nibz * ndn * 3;
+  std::copy(F_RTA, F_RTA + nf, FFF);
+  int err = mode_kappa(S, tempk, FFF, kappa);
+  std::vector<double> F2(nf), kold(9 * (size_t)ndn);
+  *iters = 0;
+  *normk = 0;
+  for (int i = 1; i <= max_iter; ++i) {
+    std::copy(kappa, kappa + 9 * ndn, kold.begin());
+    update_mpi(S, 1, nibz, P1, P2, Q, F_RTA, FFF, F2.data(), nthreads);
+    for (size_t j = 0; j < nf; ++j) FFF[j] = FFF[j] + update_mix * (F2[j] - FFF[j]);
+    err |= mode_kappa(S, tempk, FFF, kappa);
+    double e = 0;
+    for (int j = 0; j < 9 * ndn; ++j) e = e + (kappa[j] - kold[j]) * (kappa[j] - kold[j]) / (ndn * 3 * 3);
+    *iters = i;
+    *normk = std::sqrt(e);
+    if (*normk < 0.0001) break;
+  }
+  return err;
+}
+
 }  // namespace orc
+

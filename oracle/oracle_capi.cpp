@@ -238,4 +238,17 @@ int orc_kappa_d(void* p, double tempk, const double* x, double* kappa) {
   return mode_kappa_d(S, tempk, x, kappa);
 }
 
+int orc_update_mpi(void* p, int k1, int k2, const double* P1, const double* P2, const double* Q,
+                   const double* F_RTA, const double* FFF, double* F2, int nthreads) {
+  State& S = *(State*)p;
+  update_mpi(S, k1, k2, P1, P2, Q, F_RTA, FFF, F2, nthreads);
+  return 0;
+}
+
+int orc_iterative(void* p, double tempk, const double* P1, const double* P2, const double* Q, const double* F_RTA,
+                  int max_iter, double mix, double* FFF, double* kappa, int* iters, double* normk, int nthreads) {
+  State& S = *(State*)p;
+  return iterative_bte(S, tempk, P1, P2, Q, F_RTA, max_iter, mix, FFF, kappa, iters, normk, nthreads);
+}
+
 }  // extern "C"

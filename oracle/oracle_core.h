@@ -191,5 +191,10 @@ void cal_RHS_IBZ(State& S, double tempk, double* RHS);
 int cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
                  int n_dig_accur, int nthreads);
 int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa);
+void update_mpi(State& S, int k1, int k2, const double* P1, const double* P2, const double* Q,
+                const double* F_RTA, const double* FFF, double* F2mpi, int nthreads);
+int iterative_bte(State& S, double tempk, const double* P1, const double* P2, const double* Q,
+                  const double* F_RTA, int max_iter, double update_mix, double* FFF, double* kappa, int* iters,
+                  double* normk, int nthreads);
 
 }  // namespace orc

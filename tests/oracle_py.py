@@ -37,7 +37,8 @@ def lib():
         for name in ["orc_sizes", "orc_lattice", "orc_op_kmatrix", "orc_mesh", "orc_get_kpc", "orc_get_ibz",
                      "orc_get_k_info", "orc_getstar", "orc_kstars", "orc_dynmat", "orc_get_freq", "orc_phonons",
                      "orc_get_phonons", "orc_set_phonons", "orc_tet", "orc_v3", "orc_fgr", "orc_distribution",
-                     "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d"]:
+                     "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d", "orc_update_mpi",
+                     "orc_iterative"]:
             getattr(L, name).restype = C.c_int
         L.orc_weight_tet_nonperm.restype = C.c_long
         _lib = L
@@ -215,6 +216,27 @@ class Oracle:
         it = lib().orc_cg(A.shape[0], _p(A), _p(np.ascontiguousarray(b, dtype=float)), _p(x), C.byref(fmin),
                           max_iter, ndig, self.nthreads)
         return x, fmin.value, it
+
+    def update_mpi(self, k1, k2, P1, P2, Q, F_RTA, FFF):
+        """update_mpi (sub.f90:2295): F2(nk1, ndyn, 3) from Bose-weighted P1/P2 of rows k1..k2."""
+        nr = k2 - k1 + 1
+        F2 = np.zeros((nr, self.ndyn, 3), order="F")
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        lib().orc_update_mpi(self.h, k1, k2, f(P1), f(P2), f(Q), f(F_RTA), f(FFF), _p(F2), self.nthreads)
+        return F2
+
+    def iterative(self, tempk, P1, P2, Q, F_RTA, max_iter=150, mix=0.4):
+        """The job=3 iteration (kappa.f90:1390-1487); returns (F, kappa(ndyn,3,3), iters, normk)."""
+        F = np.zeros((self.nibz, self.ndyn, 3), order="F")
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        it = C.c_int(0)
+        nk = C.c_double(0)
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        e = lib().orc_iterative(self.h, C.c_double(tempk), f(P1), f(P2), f(Q), f(F_RTA), max_iter, C.c_double(mix),
+                                _p(F), _p(kap), C.byref(it), C.byref(nk), self.nthreads)
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return F, kap, it.value, nk.value
 
     def kappa_d(self, tempk, x):
         kap = np.zeros((self.ndyn, 3, 3), order="F")

@@ -159,6 +159,41 @@ def test_pipeline_injected_phonons(case):
     assert ok, worst
 
 
+def test_update_mpi(case):
+    """update_mpi (sub.f90:2295) given the oracle's P1, P2, Q and F_RTA, for a
+    perturbed F, over all rows and over a ksubset."""
+    d, ref, ctx, _ = case
+    O = ref["O"]
+    rng = np.random.default_rng(3)
+    F = ref["FFF"] * (1 + 0.1 * rng.standard_normal(ref["FFF"].shape))
+    want = O.update_mpi(1, O.nibz, ref["P1"], ref["P2"], ref["Q"], ref["FFF"], F)
+    got = ctx.update_mpi([1, O.nibz], ref["P1"], ref["P2"], ref["Q"], ref["FFF"], F)
+    ok, worst = close(got, want)
+    assert ok, worst
+    n = O.nibz
+    k = [max(1, n // 3), max(1, n // 3) + min(3, n - n // 3) - 1]
+    P1s, P2s = ref["P1"][k[0] - 1:k[1]], ref["P2"][k[0] - 1:k[1]]
+    want = O.update_mpi(k[0], k[1], P1s, P2s, ref["Q"], ref["FFF"], F)
+    got = ctx.update_mpi(k, P1s, P2s, ref["Q"], ref["FFF"], F)
+    ok, worst = close(got, want)
+    assert ok, worst
+
+
+def test_pipeline_iterative(case):
+    """The job=3 sequence on the device against the oracle's mixing loop
+    (kappa.f90:1390-1487) on the oracle's P1/P2: same iteration count, kappa
+    per mode to 1e-8 (the loop reuses its result 10-20 times)."""
+    d, ref, ctx, _ = case
+    O = ref["O"]
+    out = ctx.kappa_iterative(ref["tempk"])
+    F, kap, iters, normk = O.iterative(ref["tempk"], ref["P1"], ref["P2"], ref["Q"], ref["FFF"])
+    assert out["iters"] == iters
+    ok, worst = close(out["kappa_iter_modes"], kap, rtol=1e-8, atol=1e-10)
+    assert ok, worst
+    ok, worst = close(out["F"], F, rtol=1e-8, atol=1e-10)
+    assert ok, worst
+
+
 # ----------------------------------------------------------------- phonons
 @pytest.fixture(scope="module", params=[(1, (6, 6, 6)), (0, (6, 6, 6))], ids=["nacl6", "lj6"])
 def phon(request, oracle_lib, ald_lib, workdir):
