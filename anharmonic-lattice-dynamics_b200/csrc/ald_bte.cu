@@ -215,60 +215,63 @@ __global__ void ffull_kernel(Geometry g, const int* mapibz, const int* full_op, 
   o[2] = out[2];
 }
 
-// update_mpi for one IBZ row per CTA: threads walk q2, each accumulating
-// A[l1][xyz] for every l1; CTA sums in a fixed order
-template <int B>
-__global__ void __launch_bounds__(256) update_kernel(Geometry g, int n1_first, const int* mapinv, const double* R1,
-                                                     const double* R1p, const double* R2, const double* R2p,
-                                                     const double* Ff, const double* Q, const double* F_RTA,
-                                                     const double* F, double mix, double* Fout) {
-  __shared__ double red[8][3 * B];
-  const int b = g.b, nkc = g.nkc, nl = blockIdx.x, n1 = n1_first + nl;
-  const int q1 = mapinv[n1];
+// update_mpi, pass 1: a CTA covers one IBZ row and one of kUpdSlices ranges
+// of q2.  Its threads walk the row's R1/R1p/R2/R2p blocks element by element
+// (coalesced); the block size is a multiple of b*b, so each thread keeps one
+// (l1, l) pair and three accumulators.  Per-CTA sums in a fixed order go to
+// part[row][slice][l1][xyz].
+constexpr int kUpdSlices = 8;
+
+__global__ void update_partial_kernel(Geometry g, int n1_first, const int* mapinv, const double* R1, const double* R1p,
+                                      const double* R2, const double* R2p, const double* Ff, double* part) {
+  __shared__ double red[256][3];
+  const int b = g.b, b2 = b * b, nkc = g.nkc;
+  const int nl = blockIdx.y, sl = blockIdx.x;
+  const int q1 = mapinv[n1_first + nl];
   int m1[3];
   decompose(g, q1, m1);
-  double acc[B][3];
-#pragma unroll
-  for (int l1 = 0; l1 < B; ++l1) acc[l1][0] = acc[l1][1] = acc[l1][2] = 0.0;
-  const size_t rb = (size_t)nl * nkc;
-  for (int q = threadIdx.x; q < nkc; q += blockDim.x) {
+  const int t = threadIdx.x, l = t % b;  // l1 = (t / b) % b
+  const size_t e0 = (size_t)(sl * nkc / kUpdSlices) * b2, e1 = (size_t)((sl + 1) * nkc / kUpdSlices) * b2;
+  const size_t rb = (size_t)nl * nkc * b2;
+  double a0 = 0, a1 = 0, a2 = 0;
+  for (size_t e = e0 + t; e < e1; e += blockDim.x) {
+    const int q = (int)(e / b2);
     int mq[3], ins;
     decompose(g, q, mq);
     const int qp = pm_index(g, m1, mq, 1, ins), qm = pm_index(g, m1, mq, -1, ins);
-    const double* fq = Ff + (size_t)q * b * 3;
-    const double* fp = Ff + (size_t)qp * b * 3;
-    const double* fm = Ff + (size_t)qm * b * 3;
-    const size_t o = (rb + q) * b * b;
-#pragma unroll
-    for (int l1 = 0; l1 < B; ++l1) {
-      if (l1 >= b) break;
-      for (int l = 0; l < b; ++l) {
-        const size_t i = o + l1 * b + l;
-        const double c1 = R1[i], c1p = R1p[i], c2 = R2[i], c2p = R2p[i];
-#pragma unroll
-        for (int x = 0; x < 3; ++x)
-          acc[l1][x] += c1p * fp[l * 3 + x] - c1 * fq[l * 3 + x] + 0.5 * (c2 * fq[l * 3 + x] + c2p * fm[l * 3 + x]);
-      }
-    }
+    const double c1 = R1[rb + e], c1p = R1p[rb + e], c2 = R2[rb + e], c2p = R2p[rb + e];
+    const double* fq = Ff + ((size_t)q * b + l) * 3;
+    const double* fp = Ff + ((size_t)qp * b + l) * 3;
+    const double* fm = Ff + ((size_t)qm * b + l) * 3;
+    a0 += c1p * fp[0] - c1 * fq[0] + 0.5 * (c2 * fq[0] + c2p * fm[0]);
+    a1 += c1p * fp[1] - c1 * fq[1] + 0.5 * (c2 * fq[1] + c2p * fm[1]);
+    a2 += c1p * fp[2] - c1 * fq[2] + 0.5 * (c2 * fq[2] + c2p * fm[2]);
   }
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-#pragma unroll
-  for (int l1 = 0; l1 < B; ++l1)
-#pragma unroll
-    for (int x = 0; x < 3; ++x) {
-      double v = acc[l1][x];
-      for (int off = 16; off > 0; off >>= 1) v += __shfl_down_sync(0xffffffffu, v, off);
-      if (lane == 0) red[warp][l1 * 3 + x] = v;
-    }
+  red[t][0] = a0;
+  red[t][1] = a1;
+  red[t][2] = a2;
   __syncthreads();
-  if (threadIdx.x < 3 * b) {
-    const int l1 = threadIdx.x / 3, x = threadIdx.x % 3;
+  if (t < 3 * b) {
+    const int L1 = t / 3, x = t % 3;
     double A = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) A += red[w][threadIdx.x];
-    const size_t fi = ((size_t)n1 * b + l1) * 3 + x;
-    const double f2 = F_RTA[fi] + A / Q[(size_t)n1 * b + l1];
-    Fout[((size_t)nl * b + l1) * 3 + x] = mix > 0 ? F[fi] + mix * (f2 - F[fi]) : f2;
+    for (int u = 0; u < (int)blockDim.x; ++u)
+      if ((u / b) % b == L1) A += red[u][x];
+    part[(((size_t)nl * kUpdSlices + sl) * b + L1) * 3 + x] = A;
   }
+}
+
+// update_mpi, pass 2: F2 = F_RTA + A/Q, optionally mixed into F
+__global__ void update_final_kernel(Geometry g, int n1_first, int nrows, const double* part, const double* Q,
+                                    const double* F_RTA, const double* F, double mix, double* Fout) {
+  const int b = g.b;
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= nrows * b * 3) return;
+  const int nl = e / (3 * b), l1 = (e / 3) % b, x = e % 3, n1 = n1_first + nl;
+  double A = 0;
+  for (int sl = 0; sl < kUpdSlices; ++sl) A += part[(((size_t)nl * kUpdSlices + sl) * b + l1) * 3 + x];
+  const size_t fi = ((size_t)n1 * b + l1) * 3 + x;
+  const double f2 = F_RTA[fi] + A / Q[(size_t)n1 * b + l1];
+  Fout[((size_t)nl * b + l1) * 3 + x] = mix > 0 ? F[fi] + mix * (f2 - F[fi]) : f2;
 }
 
 // ---------------------------------------------------------------- CG
@@ -425,17 +428,19 @@ cudaError_t launch_ffull(const Geometry& geo, const int* mapibz, const int* full
   return cudaGetLastError();
 }
 
+size_t update_part_doubles(const Geometry& geo, int nrows) { return (size_t)nrows * kUpdSlices * geo.b * 3; }
+
 cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                           const double* R1p, const double* R2, const double* R2p, const double* Ff, const double* Q,
-                          const double* F_RTA, const double* F, double mix, double* Fout, cudaStream_t s) {
-  if (geo.b <= 3)
-    update_kernel<3><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
-  else if (geo.b <= 6)
-    update_kernel<6><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
-  else if (geo.b <= 12)
-    update_kernel<12><<<nrows, 256, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, Q, F_RTA, F, mix, Fout);
-  else
-    return cudaErrorInvalidValue;
+                          const double* F_RTA, const double* F, double mix, double* Fout, double* part,
+                          cudaStream_t s) {
+  const int b2 = geo.b * geo.b;
+  if (b2 > 256) return cudaErrorInvalidValue;
+  const int threads = b2 * (256 / b2);
+  dim3 grid(kUpdSlices, nrows);
+  update_partial_kernel<<<grid, threads, 0, s>>>(geo, n1_first, mapinv, R1, R1p, R2, R2p, Ff, part);
+  const int n = nrows * geo.b * 3;
+  update_final_kernel<<<(n + 255) / 256, 256, 0, s>>>(geo, n1_first, nrows, part, Q, F_RTA, F, mix, Fout);
   return cudaGetLastError();
 }
 

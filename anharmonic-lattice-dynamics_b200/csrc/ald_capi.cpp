@@ -737,7 +737,7 @@ int ald_update_mpi(ald_ctx* c, const int ksubset[2], const double* P1, const dou
   if (!c || !P1 || !P2 || !Qv || !F_RTA || !FFF || !F2mpi) return fail(ALD_ERR_ARG, "null argument");
   if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
   if (!c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
-  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: more than 12 bands is not supported");
+  if (c->geo.b > 16) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: more than 16 bands is not supported");
   CK(cudaSetDevice(c->device));
   const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b, nkc = c->T.nkc, nibz = c->T.nibz;
   const size_t n = (size_t)nr * nkc * b * b * b, nm = (size_t)nr * nkc * b * b, nf = (size_t)nibz * b * 3;
@@ -755,6 +755,8 @@ int ald_update_mpi(ald_ctx* c, const int ksubset[2], const double* P1, const dou
   CKA(f.alloc(nf));
   CKA(ff.alloc((size_t)nkc * b * 3));
   CKA(out.alloc((size_t)nr * b * 3));
+  DevBuf<double> part;
+  CKA(part.alloc(update_part_doubles(c->geo, nr)));
   cudaStream_t s = c->stream;
   CK(cudaMemcpyAsync(tmp.p, P1, n * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(launch_from_fortran5(tmp.p, s1.p, nr, nkc, b, s));
@@ -777,7 +779,7 @@ int ald_update_mpi(ald_ctx* c, const int ksubset[2], const double* P1, const dou
   CK(cudaMemcpyAsync(f.p, hf.data(), nf * sizeof(double), cudaMemcpyHostToDevice, s));
   CK(launch_ffull(c->geo, c->mapibz0.p, c->full_op.p, c->opk.p, f.p, ff.p, s));
   CK(launch_update(c->geo, ksubset[0] - 1, nr, c->mapinv.p, R1.p, R1p.p, R2.p, R2p.p, ff.p, q.p, frta.p, f.p, 0.0,
-                   out.p, s));
+                   out.p, part.p, s));
   std::vector<double> ho((size_t)nr * b * 3);
   CK(cudaMemcpyAsync(ho.data(), out.p, ho.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
   CK(cudaStreamSynchronize(s));

@@ -31,7 +31,7 @@ struct ald_ctx {
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
   // pipeline workspaces, kept across calls (allocation outside the timed work)
   DevBuf<double> w_R1, w_R2, w_Q, w_v3, w_F, w_x, w_rhs, w_kr, w_kc, w_cm;
-  DevBuf<double> w_R1p, w_R2p, w_Ff, w_Frta;  // iterative solution: band marginals, F on the mesh
+  DevBuf<double> w_R1p, w_R2p, w_Ff, w_Frta, w_part;  // iterative solution: band marginals, F on the mesh
   DevBuf<char> w_scratch;
   CgWork cg;
   bool have_phonons = false;

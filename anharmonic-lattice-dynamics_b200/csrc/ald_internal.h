@@ -309,9 +309,12 @@ cudaError_t launch_marginal_l2(const Geometry& geo, int nrows, const double* P1,
 // all IBZ points; Fout local to the rows.
 cudaError_t launch_ffull(const Geometry& geo, const int* mapibz, const int* full_op, const double* opk,
                          const double* F, double* Ff, cudaStream_t s);
+// part: scratch of update_part_doubles(geo, nrows) doubles
+size_t update_part_doubles(const Geometry& geo, int nrows);
 cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                           const double* R1p, const double* R2, const double* R2p, const double* Ff, const double* Q,
-                          const double* F_RTA, const double* F, double mix, double* Fout, cudaStream_t s);
+                          const double* F_RTA, const double* F, double mix, double* Fout, double* part,
+                          cudaStream_t s);
 // CG workspace: vectors, scalars and the captured CUDA graph of the
 // iteration loop, kept across calls and re-captured only when the problem
 // (size, pointers, stop rule) changes

@@ -209,6 +209,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     DevBuf<double>& Frta = c->w_Frta;
     ALD_CKA(Ff.alloc((size_t)nkc * b * 3));
     ALD_CKA(Frta.alloc(N));
+    ALD_CKA(c->w_part.alloc(update_part_doubles(c->geo, nibz)));
     ALD_CK(cudaMemcpyAsync(Frta.p, F.p, N * sizeof(double), cudaMemcpyDeviceToDevice, s));
     ALD_CK(tm.begin(7));
     std::vector<double> kold((size_t)9 * b), knew((size_t)9 * b);
@@ -220,7 +221,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     for (int i = 1; i <= it->max_iter; ++i) {
       ALD_CK(launch_ffull(c->geo, c->mapibz0.p, c->full_op.p, c->opk.p, F.p, Ff.p, s));
       ALD_CK(launch_update(c->geo, 0, nibz, c->mapinv.p, R1.p, c->w_R1p.p, R2.p, c->w_R2p.p, Ff.p, dQ, Frta.p, F.p,
-                           it->mix, F.p, s));
+                           it->mix, F.p, c->w_part.p, s));
       ALD_CK(launch_kappa(k, F.p, 0, kc.p, c->err.p, s));
       res->launches[7] += 3;
       ALD_CK(cudaMemcpyAsync(knew.data(), kc.p, knew.size() * sizeof(double), cudaMemcpyDeviceToHost, s));

@@ -190,7 +190,11 @@ def test_pipeline_iterative(case):
     assert out["iters"] == iters
     ok, worst = close(out["kappa_iter_modes"], kap, rtol=1e-8, atol=1e-10)
     assert ok, worst
-    ok, worst = close(out["F"], F, rtol=1e-8, atol=1e-10)
+    # F of the acoustic modes at Gamma divides by a noise-level Q and carries no
+    # weight in kappa (omega v = 0 there): compared elsewhere
+    I = O.ibz()
+    live = (ref["freq"][I["mapinv"] - 1] > 1e-6 * ref["freq"].max())[:, :, None] & np.ones(3, bool)
+    ok, worst = close(out["F"][live], F[live], rtol=1e-8, atol=1e-10)
     assert ok, worst
 
 
