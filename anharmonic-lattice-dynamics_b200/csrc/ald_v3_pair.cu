@@ -15,7 +15,8 @@
 //               with P_c(q2) = exp(i q2.(R_j - R_k)), a tile of q2 per CTA;
 //               T[l1][l2][c']   = sum_b' A[l1][b'][c'] e2[b'][l2]   (e(q2))
 //               V[l1][l2][l3]   = sum_c' T[l1][l2][c'] e3[c'][l3]   (e(q3))
-//               |V|^2 (const33 / sqrt(8 sqrt|l1 l2 l3|))^2.
+//               |V|^2 (const33 / sqrt(8 sqrt|l1 l2 l3|))^2, the scale formed from
+//               per-mode factors 1/sqrt|l| (reordered against the reference).
 // Eigenvectors are not conjugated, as in the reference.  The sums are
 // reordered against the reference, so results agree to FP64 rounding.
 //
@@ -136,6 +137,9 @@ __global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
   C* E3 = E2 + QT * EP;
   C* P = E3 + QT * EP;
   __shared__ int s_q2[QT], s_q3[QT];
+  // 1/sqrt|lambda| of the tile's q2 and q3 modes: (const33/den)^2 with
+  // den = sqrt(8 sqrt|l1 l2 l3|) is const33^2/8 * t1 t2 t3
+  __shared__ double s_t2[QT * B], s_t3[QT * B];
 
   const int q1 = a.mapinv[a.n1_first + row];
   int m1[3];
@@ -149,6 +153,11 @@ __global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
     s_q3[tid] = idx_q3(g, m1, m2);
   }
   __syncthreads();
+  for (int i = tid; i < QT * B; i += NT) {
+    const int q = i / B, l = i % B;
+    s_t2[i] = 1.0 / sqrt(fabs(a.w2[(size_t)s_q2[q] * B + l]));
+    s_t3[i] = 1.0 / sqrt(fabs(a.w2[(size_t)s_q3[q] * B + l]));
+  }
   const double2* ev = reinterpret_cast<const double2*>(a.evec);
   for (int i = tid; i < QT * B2; i += NT) {
     const int q = i / B2, e = i % B2;
@@ -242,8 +251,7 @@ __global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
         for (int l = 0; l < B; ++l) cmac(acc[i][l], tv[i], evv[l]);
     }
     if (q2 < g.nkc) {
-      const int q3 = s_q3[q];
-      const double wq1 = w2[(size_t)q1 * B + l1];
+      const double c1 = a.const33 * a.const33 / 8 / sqrt(fabs(w2[(size_t)q1 * B + l1]));
       // layout 0: [row][q2][l1][l2][l3]; layout 1: [row][l2][l3][l1][q2]
       const size_t nk = g.nkc;
       double* out = a.v3_layout == 1 ? a.v3sq + ((size_t)row * B3 + l2b * B2 + l1) * nk + q2
@@ -251,16 +259,16 @@ __global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
       const size_t st_l2 = a.v3_layout == 1 ? (size_t)B2 * nk : B, st_l3 = a.v3_layout == 1 ? (size_t)B * nk : 1;
 #pragma unroll
       for (int i = 0; i < BS; ++i) {
-        const double w12 = wq1 * w2[(size_t)q2 * B + l2b + i];
+        const double c12 = c1 * s_t2[q * B + l2b + i];
 #pragma unroll
         for (int l = 0; l < B; ++l) {
-          const double den = sqrt(8 * sqrt(fabs(w12 * w2[(size_t)q3 * B + l])));
+          const double sc = c12 * s_t3[q * B + l];  // (const33/den)^2; inf where den = 0
+          const double re = (double)acc[i][l].x, im = (double)acc[i][l].y;
           double v = 0.0;
-          if (den != 0.0) {
-            const double re = (double)acc[i][l].x / den * a.const33, im = (double)acc[i][l].y / den * a.const33;
-            v = re * re + im * im;
+          if (sc < 1.0 / 0.0) {
+            v = (re * re + im * im) * sc;
           } else {
-            atomicOr(a.err, 2);
+            atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
           }
           out[i * st_l2 + l * st_l3] = v;
         }
