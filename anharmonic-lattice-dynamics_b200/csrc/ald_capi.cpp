@@ -152,7 +152,13 @@ int run_v3(ald_ctx* c, const V3Args& a0) {
   const int prec = c->opt.precision;
   V3Args a = a0;
   cudaError_t e;
-  if (v3_pair_supported(c->geo.b, prec)) {
+  if (prec == ALD_MIXED && v3_tc_supported(c->geo.b, c->VC.ncls)) {
+    const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
+    if (c->w_h.n < need) CKA(c->w_h.alloc(need));
+    a.hbuf = c->w_h.p;
+    e = launch_v3_rows_f32(a, c->stream);
+    if (e == cudaSuccess) e = launch_v3_tc(a, c->stream);
+  } else if (v3_pair_supported(c->geo.b, prec)) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;

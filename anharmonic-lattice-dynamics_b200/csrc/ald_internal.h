@@ -222,6 +222,11 @@ cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s);
 bool v3_pair_supported(int b, int precision);
 size_t v3_hbuf_bytes(int b, int ncls, int nrows, int precision);
 cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s);
+// row stage alone, H in FP32 (for the tensor-core class sums)
+cudaError_t launch_v3_rows_f32(const V3Args& a, cudaStream_t s);
+// 3 bands, ALD_MIXED: class sums on tcgen05 (ald_v3_tc.cu); hbuf from launch_v3_rows_f32
+bool v3_tc_supported(int b, int ncls);
+cudaError_t launch_v3_tc(const V3Args& a, cudaStream_t s);
 
 struct CombineArgs {
   Geometry geo;

@@ -302,19 +302,26 @@ cudaError_t launch_pair_t(const V3Args& a, cudaStream_t s) {
 
 }  // namespace
 
+cudaError_t launch_v3_rows_f32(const V3Args& a, cudaStream_t s) {
+  const int n = a.ncls * 9 * a.geo.b;
+  dim3 rg((n + 255) / 256, a.nrows);
+  v3_row_kernel<float2><<<rg, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 bool v3_pair_supported(int b, int precision) {
   (void)precision;
   return b == 3 || b == 6;
 }
 
 size_t v3_hbuf_bytes(int b, int ncls, int nrows, int precision) {
-  const size_t cplx = precision == ALD_MIXED ? sizeof(float2) : sizeof(double2);
+  const size_t cplx = precision != ALD_FP64 ? sizeof(float2) : sizeof(double2);
   return (size_t)nrows * ncls * 9 * b * cplx;
 }
 
 cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s) {
   const int b = a.geo.b;
-  if (precision == ALD_MIXED) {
+  if (precision != ALD_FP64) {
     if (b == 3) return launch_pair_t<float, 3, 32, 3, 288>(a, s);
     if (b == 6) return launch_pair_t<float, 6, 16, 3, 288>(a, s);
   } else {

@@ -26,7 +26,7 @@ STATUS = {1: "ALD_ERR_ARG", 2: "ALD_ERR_IO", 3: "ALD_ERR_NOT_KPOINT", 4: "ALD_ER
           6: "ALD_ERR_INDEX", 7: "ALD_ERR_CUDA", 8: "ALD_ERR_UNSUPPORTED", 9: "ALD_ERR_NOMEM",
           100: "ALD_WARN_CG_MAXITER"}
 DELTA_TETRA, DELTA_GAUSS = 0, 1
-FP64, MIXED = 0, 1
+FP64, MIXED, MIXED_FP32 = 0, 1, 2
 CG_REFERENCE, CG_RESIDUAL = 0, 1
 
 

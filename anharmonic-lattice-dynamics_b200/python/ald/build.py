@@ -27,6 +27,7 @@ SOURCES = {
     "ald_phonon.cu": [],
     "ald_v3.cu": [],
     "ald_v3_pair.cu": [],
+    "ald_v3_tc.cu": [],
     # weight_tet's FP32/FP64 arithmetic must not be contracted into FMAs
     "ald_tetra.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
     "ald_bte.cu": [],

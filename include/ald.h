@@ -40,13 +40,17 @@ enum ald_status {
 };
 
 enum ald_delta { ALD_DELTA_TETRA = 0, ALD_DELTA_GAUSS = 1 };
-enum ald_precision { ALD_FP64 = 0, ALD_MIXED = 1 };
+/* ALD_MIXED: the V3 contraction in reduced precision with FP32 accumulation --
+ * for 3 bands the phase-class sums run on the tensor cores (split-FP16
+ * tcgen05 MMAs), otherwise in FP32 on the CUDA cores; ALD_MIXED_FP32 always
+ * uses the FP32 CUDA-core form.  Everything outside V3 stays FP64. */
+enum ald_precision { ALD_FP64 = 0, ALD_MIXED = 1, ALD_MIXED_FP32 = 2 };
 enum ald_cg_stop { ALD_CG_REFERENCE = 0, ALD_CG_RESIDUAL = 1 };
 
 typedef struct ald_options {
   int delta;         /* ALD_DELTA_TETRA (reference, calculate_FGR_mpi2) or ALD_DELTA_GAUSS
                         (extension: delta_g of width `width_cm`, extratools.f90:239)    */
-  int precision;     /* ALD_FP64 or ALD_MIXED (V3 contraction on tensor cores)          */
+  int precision;     /* ALD_FP64, ALD_MIXED or ALD_MIXED_FP32 (enum ald_precision)      */
   int cg_stop;       /* ALD_CG_REFERENCE: (dv/v)^2 < 10^(-2*cg_ndig) (cg.f90:30,47);
                         ALD_CG_RESIDUAL: |Ax-b|/|b| < cg_tol                            */
   int cg_max_iter;   /* 100 at kappa.f90:846                                            */
