@@ -62,6 +62,7 @@ int check_err_flags(ald_ctx* c) {
   CK(cudaStreamSynchronize(c->stream));
   if (h) {
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
+    if (h & 16) return fail(ALD_ERR_CUDA, "V3: a tensor-core wait timed out (MMA completion not observed)");
     if (h & 2) return fail(ALD_ERR_DEN_ZERO, "MATRIX_ELT: den=0 (an eigenvalue is exactly zero)");
     if (h & 1) return fail(ALD_ERR_NBE, "ERROR in N_BE: w=<0 or t=<0");
   }
@@ -156,8 +157,16 @@ int run_v3(ald_ctx* c, const V3Args& a0) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
+    if (!c->ptiles_ok) {
+      CKA(c->w_ptiles.alloc(v3_tc_ptile_bytes(c->geo.nkc, c->VC.ncls)));
+      e = launch_v3_tc_ptiles(a, c->w_ptiles.p, c->stream);
+      if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 phase tiles: ") + cudaGetErrorString(e));
+      c->ptiles_ok = true;
+    }
+    const size_t bneed = v3_tc_btile_bytes(a.nrows, c->VC.ncls);
+    if (c->w_btiles.n < bneed) CKA(c->w_btiles.alloc(bneed));
     e = launch_v3_rows_f32(a, c->stream);
-    if (e == cudaSuccess) e = launch_v3_tc(a, c->stream);
+    if (e == cudaSuccess) e = launch_v3_tc(a, c->w_ptiles.p, c->w_btiles.p, c->stream);
   } else if (v3_pair_supported(c->geo.b, prec)) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));

@@ -27,6 +27,9 @@ struct ald_ctx {
   DevBuf<int> mapibz0, full_op;       // per mesh point: IBZ point and the op of its star arm (job=3)
   bool full_op_ok = false;
   DevBuf<char> w_h;                   // per-row phase-class sums of the pair kernel
+  DevBuf<char> w_ptiles;              // phase tiles of the tensor-core V3 (mesh-only, built once)
+  DevBuf<char> w_btiles;              // per-row B operands of the tensor-core V3
+  bool ptiles_ok = false;
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
   // pipeline workspaces, kept across calls (allocation outside the timed work)

@@ -226,7 +226,12 @@ cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s);
 cudaError_t launch_v3_rows_f32(const V3Args& a, cudaStream_t s);
 // 3 bands, ALD_MIXED: class sums on tcgen05 (ald_v3_tc.cu); hbuf from launch_v3_rows_f32
 bool v3_tc_supported(int b, int ncls);
-cudaError_t launch_v3_tc(const V3Args& a, cudaStream_t s);
+// the row-independent phase tiles (split FP16, canonical layout), built once per context
+size_t v3_tc_ptile_bytes(int nkc, int ncls);
+cudaError_t launch_v3_tc_ptiles(const V3Args& a, void* ptiles, cudaStream_t s);
+// btiles: scratch of v3_tc_btile_bytes(nrows, ncls) (B operands and scales of the chunk's rows)
+size_t v3_tc_btile_bytes(int nrows, int ncls);
+cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s);
 
 struct CombineArgs {
   Geometry geo;

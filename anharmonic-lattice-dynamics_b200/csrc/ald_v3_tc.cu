@@ -21,9 +21,14 @@
 // contiguous inside a core matrix (SBO = 128 bytes between 8-row groups) and
 // the two 8-element K halves of one MMA ROWS*16 bytes apart (LBO).
 //
-// The single wait of the CTA (the MMA-completion mbarrier) is bounded: on
-// timeout the CTA sets bit 4 of the error flag, waits (bounded) once more,
-// frees its TMEM and returns without storing.
+// The phase tiles (A) depend on q2 only and are built once per context; the
+// B operands (H of one row, split and scaled) once per row by
+// v3_btile_kernel.  Both reach shared memory by bulk copies; B streams
+// through two buffers so the next row's copy overlaps this row's MMAs.
+//
+// Every wait of the CTA (the bulk-copy and MMA-completion mbarriers) is
+// bounded: on timeout the CTA sets bit 16 of the error flag, waits (bounded)
+// for its copies and MMAs in flight, frees its TMEM and returns.
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -38,8 +43,7 @@ namespace {
 constexpr int kTM = 128;      // q2 per CTA = TMEM lanes = threads
 constexpr int kNC = 27;       // complex outputs (l1, be, ga) for 3 bands
 constexpr int kNP = 64;       // real outputs padded to a valid N
-constexpr int kTmemCols = 64; // FP32 accumulator columns
-constexpr int kMaxKp = 256;   // K' bound (ncls <= 128)
+constexpr int kMaxKp = 208;   // K' bound (ncls <= 104): A + 2 B buffers fit 227 KB
 constexpr unsigned kWaitLimit = 1u << 22;
 
 __device__ __forceinline__ int wrapm(int v, int n) {
@@ -111,42 +115,36 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
   return ok != 0;
 }
 
-__global__ void __launch_bounds__(kTM, 1) v3_tc3_kernel(V3Args a, int kp) {
-  extern __shared__ __align__(1024) unsigned char smraw[];
-  __shared__ uint32_t s_tmem;
-  __shared__ __align__(8) uint64_t s_bar;
-  __shared__ float s_scale[kNC];
-  __shared__ int s_ok;
-  const Geometry& g = a.geo;
-  const int tid = threadIdx.x, warp = tid >> 5, row = blockIdx.y;
-  const int ncls = a.ncls;
-  __half* Ahi = reinterpret_cast<__half*>(smraw);
-  __half* Alo = Ahi + kTM * kp;
-  __half* Bhi = Alo + kTM * kp;
-  __half* Blo = Bhi + kNP * kp;
-
-  // TMEM: 64 columns, allocated by warp 0
-  if (warp == 0) {
-    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTmemCols));
-    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
-  }
-  if (tid == 0) {
-    const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_bar);
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar));
-    asm volatile("fence.mbarrier_init.release.cluster;");
-    s_ok = 1;
-  }
-
-  const int q1 = a.mapinv[a.n1_first + row];
-  int m1[3];
-  decompose(g, q1, m1);
-  const int q2 = min((int)(blockIdx.x * kTM) + tid, g.nkc - 1);
+// The A operand (phases P_c(q2), split FP16 hi/lo in the canonical layout)
+// depends on q2 and the class only, not on the IBZ row: built once per
+// context for every 128-q2 tile, [tile][hi|lo][kmaj].
+__global__ void v3_ptile_kernel(Geometry g, int ncls, int kp, const int* cls_pc, const double* roots_d,
+                                __half* Pt) {
+  const int tile = blockIdx.x, r = threadIdx.x;
+  const int q2 = min(tile * kTM + r, g.nkc - 1);
   int m2[3];
   decompose(g, q2, m2);
-  const int q3 = idx_q3(g, m1, m2);
+  const double2* roots = reinterpret_cast<const double2*>(roots_d);
+  __half* hi = Pt + (size_t)tile * 2 * kTM * kp;
+  __half* lo = hi + (size_t)kTM * kp;
+  for (int k = 0; k < kp; ++k) {
+    float v = 0.f;
+    if (k < 2 * ncls) {
+      const int c = k < ncls ? k : k - ncls;
+      const double2 p = roots[phase_index(cls_pc + 4 * c, m2, g.L)];
+      v = (float)(k < ncls ? p.x : p.y);
+    }
+    split_store(hi, lo, kmaj(r, k, kTM), v);
+  }
+}
 
-  // H of this row: column scales (a power of two >= max |H| of the column)
+// The B operand of every IBZ row of the chunk (H in real form, split FP16,
+// canonical layout), built once per row: [row][hi|lo][kmaj], and the
+// inverses of the 27 column scales (powers of two with max |H| * scale in
+// [0.5, 1)).
+__global__ void v3_btile_kernel(V3Args a, int kp, __half* Bt, float* inv_scales) {
+  __shared__ float s_scale[kNC];
+  const int row = blockIdx.x, tid = threadIdx.x, ncls = a.ncls;
   const float2* H = static_cast<const float2*>(a.hbuf) + (size_t)row * ncls * 9 * 3;
   if (tid < kNC) {
     const int l1 = tid / 9, bg = tid % 9;
@@ -157,11 +155,13 @@ __global__ void __launch_bounds__(kTM, 1) v3_tc3_kernel(V3Args a, int kp) {
     }
     int e = 0;
     if (mx > 0.f) frexpf(mx, &e);
-    s_scale[tid] = ldexpf(1.f, -e);  // mx * scale in [0.5, 1)
+    s_scale[tid] = ldexpf(1.f, -e);
+    inv_scales[(size_t)row * kNC + tid] = ldexpf(1.f, e);
   }
   __syncthreads();
-  // B operand (N' x K'): n' = 2 col + {0: real, 1: imaginary}
-  for (int i = tid; i < kNP * kp; i += kTM) {
+  __half* hi = Bt + (size_t)row * 2 * kNP * kp;
+  __half* lo = hi + (size_t)kNP * kp;
+  for (int i = tid; i < kNP * kp; i += blockDim.x) {
     const int n = i / kp, k = i % kp;
     float v = 0.f;
     const int col = n >> 1;
@@ -172,148 +172,305 @@ __global__ void __launch_bounds__(kTM, 1) v3_tc3_kernel(V3Args a, int kp) {
       if ((n & 1) == 0) v = k < ncls ? h.x * sc : -h.y * sc;  // Ar = Pr Hr - Pi Hi
       else v = k < ncls ? h.y * sc : h.x * sc;                // Ai = Pr Hi + Pi Hr
     }
-    split_store(Bhi, Blo, kmaj(n, k, kNP), v);
+    split_store(hi, lo, kmaj(n, k, kNP), v);
   }
-  // A operand (M x K'): row = q2, [Pr | Pi] of every class
-  const double2* roots = reinterpret_cast<const double2*>(a.roots);
-  for (int k = 0; k < kp; ++k) {  // thread tid fills row tid (its own q2)
-    float v = 0.f;
-    if (k < 2 * ncls) {
-      const int c = k < ncls ? k : k - ncls;
-      const double2 p = roots[phase_index(a.cls_pc + 4 * c, m2, g.L)];
-      v = (float)(k < ncls ? p.x : p.y);
-    }
-    split_store(Ahi, Alo, kmaj(tid, k, kTM), v);
+}
+
+__device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+  for (unsigned it = 0; it < kWaitLimit; ++it)
+    if (mbar_try(bar, parity)) return true;
+  return false;
+}
+
+// bounded wait that also gives up once another warp has raised the CTA's
+// failure flag
+__device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity, const volatile int* fail) {
+  for (unsigned it = 0; it < kWaitLimit; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if ((it & 63u) == 63u && *fail) return false;
   }
-  // make the generic-proxy stores visible to the tensor core, then issue
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
+  const char* p = static_cast<const char*>(src);
+  for (uint32_t off = 0; off < bytes; off += 32768u) {
+    const uint32_t n = bytes - off < 32768u ? bytes - off : 32768u;
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     dst + off),
+                 "l"(p + off), "r"(n), "r"(bar)
+                 : "memory");
+  }
+}
+
+constexpr int kEpiWG = 2;                   // epilogue warpgroups = TMEM accumulators
+constexpr int kThreads = 128 * kEpiWG + 32;  // + one producer warp
+constexpr int kTmemAlloc = 128;              // kEpiWG x 64 columns
+
+// One CTA: one 128-q2 tile and up to `rpc` IBZ rows, warp-specialised.
+// * Producer warp (one lane): copies the phase tile once and the B tiles of
+//   the rows through two buffers, issues the 3 (kp/16) MMAs of a row into
+//   accumulator (row % 2) once that accumulator has been drained, commits.
+// * Epilogue warpgroup w takes the rows with (row - r0) % 2 == w: thread =
+//   TMEM lane = q2; it loads its 64 accumulator columns, releases the
+//   accumulator, then does the mode products with e(q2), e(q3), the scaling
+//   and the stores, while the producer already runs the next rows' MMAs.
+__global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, const __half* Pt, const __half* Bt,
+                                                             const float* inv_scales, int rpc) {
+  extern __shared__ __align__(1024) unsigned char smraw[];
+  __shared__ uint32_t s_tmem;
+  __shared__ __align__(8) uint64_t s_bar_a, s_bar_b[2], s_full[kEpiWG], s_empty[kEpiWG];
+  __shared__ volatile int s_fail;
+  const Geometry& g = a.geo;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
+  const int r0 = blockIdx.y * rpc, n = min(rpc, a.nrows - r0);
+  const uint32_t a_sh = (uint32_t)__cvta_generic_to_shared(smraw);
+  const uint32_t b_sh = a_sh + (uint32_t)(2 * kTM * kp * sizeof(__half));
+  const uint32_t bbytes = (uint32_t)(2 * kNP * kp * sizeof(__half));
+  const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&s_bar_a);
+  const uint32_t bar_b0 = (uint32_t)__cvta_generic_to_shared(&s_bar_b[0]);
+  const uint32_t bar_b1 = (uint32_t)__cvta_generic_to_shared(&s_bar_b[1]);
+  const uint32_t full0 = (uint32_t)__cvta_generic_to_shared(&s_full[0]);
+  const uint32_t full1 = (uint32_t)__cvta_generic_to_shared(&s_full[1]);
+  const uint32_t empty0 = (uint32_t)__cvta_generic_to_shared(&s_empty[0]);
+  const uint32_t empty1 = (uint32_t)__cvta_generic_to_shared(&s_empty[1]);
+
+  if (warp == 0) {
+    const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst), "r"(kTmemAlloc));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_b0));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_b1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full1));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0), "r"(kTM));
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty1), "r"(kTM));
+    asm volatile("fence.mbarrier_init.release.cluster;");
+    s_fail = 0;
+  }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
-  const uint32_t bar = (uint32_t)__cvta_generic_to_shared(&s_bar);
-  if (tid == 0) {
-    const uint32_t idesc = instr_desc(kTM, kNP);
-    const uint32_t aH = (uint32_t)__cvta_generic_to_shared(Ahi), aL = (uint32_t)__cvta_generic_to_shared(Alo);
-    const uint32_t bH = (uint32_t)__cvta_generic_to_shared(Bhi), bL = (uint32_t)__cvta_generic_to_shared(Blo);
-    for (int s = 0; s < kp / 16; ++s) {
-      // K step s covers K chunks 2s, 2s+1: start ROWS*16 bytes per chunk
-      const uint32_t oa = (uint32_t)(2 * s * kTM * 16), ob = (uint32_t)(2 * s * kNP * 16);
-      const uint64_t dAh = smem_desc(aH + oa, kTM * 16, 128), dAl = smem_desc(aL + oa, kTM * 16, 128);
-      const uint64_t dBh = smem_desc(bH + ob, kNP * 16, 128), dBl = smem_desc(bL + ob, kNP * 16, 128);
-      mma_f16(tmem, dAh, dBh, idesc, s > 0 ? 1u : 0u);
-      mma_f16(tmem, dAh, dBl, idesc, 1u);
-      mma_f16(tmem, dAl, dBh, idesc, 1u);
+
+  if (warp == 4 * kEpiWG) {
+    // ---------------- producer ----------------
+    if (lane == 0) {
+      int bq0 = -1, bq1 = -1, pend_acc = -1, pend_par = 0;  // copies and MMAs in flight
+      bulk_g2s(a_sh, Pt + (size_t)tile * 2 * kTM * kp, (uint32_t)(2 * kTM * kp * sizeof(__half)), bar_a);
+      bulk_g2s(b_sh, Bt + (size_t)r0 * 2 * kNP * kp, bbytes, bar_b0);
+      bq0 = 0;
+      if (n > 1) {
+        bulk_g2s(b_sh + bbytes, Bt + (size_t)(r0 + 1) * 2 * kNP * kp, bbytes, bar_b1);
+        bq1 = 0;
+      }
+      bool ok = mbar_wait_or_fail(bar_a, 0, &s_fail);
+      const uint32_t idesc = instr_desc(kTM, kNP);
+      const uint32_t aH = a_sh, aL = a_sh + (uint32_t)(kTM * kp * sizeof(__half));
+      for (int it = 0; ok && it < n; ++it) {
+        const int buf = it & 1;
+        ok = mbar_wait_or_fail(buf ? bar_b1 : bar_b0, (uint32_t)((it >> 1) & 1), &s_fail);
+        if (!ok) break;
+        if (buf) bq1 = -1;
+        else bq0 = -1;
+        if (it >= 2) {  // accumulator buf drained by the epilogue of row it - 2
+          ok = mbar_wait_or_fail(buf ? empty1 : empty0, (uint32_t)(((it >> 1) - 1) & 1), &s_fail);
+          if (!ok) break;
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        const uint32_t bH = b_sh + (uint32_t)buf * bbytes, bL = bH + (uint32_t)(kNP * kp * sizeof(__half));
+        const uint32_t dt = tmem + (uint32_t)(buf * kNP);
+        for (int st = 0; st < kp / 16; ++st) {
+          // K step st covers K chunks 2st, 2st+1: ROWS*16 bytes per chunk
+          const uint32_t oa = (uint32_t)(2 * st * kTM * 16), ob = (uint32_t)(2 * st * kNP * 16);
+          const uint64_t dAh = smem_desc(aH + oa, kTM * 16, 128), dAl = smem_desc(aL + oa, kTM * 16, 128);
+          const uint64_t dBh = smem_desc(bH + ob, kNP * 16, 128), dBl = smem_desc(bL + ob, kNP * 16, 128);
+          mma_f16(dt, dAh, dBh, idesc, st > 0 ? 1u : 0u);
+          mma_f16(dt, dAh, dBl, idesc, 1u);
+          mma_f16(dt, dAl, dBh, idesc, 1u);
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                         buf ? full1 : full0)
+                     : "memory");
+        pend_acc = buf;
+        pend_par = (it >> 1) & 1;
+        // B buffer of row it - 1 is free once that row's MMAs completed:
+        // refill it with row it + 1
+        if (it >= 1 && it + 1 < n) {
+          const int pb = buf ^ 1;
+          ok = mbar_wait_or_fail(pb ? full1 : full0, (uint32_t)(((it - 1) >> 1) & 1), &s_fail);
+          if (!ok) break;
+          bulk_g2s(b_sh + (uint32_t)pb * bbytes, Bt + (size_t)(r0 + it + 1) * 2 * kNP * kp, bbytes,
+                   pb ? bar_b1 : bar_b0);
+          if (pb) bq1 = ((it + 1) >> 1) & 1;
+          else bq0 = ((it + 1) >> 1) & 1;
+        }
+      }
+      if (!ok) s_fail = 1;
+      // wait (bounded) for whatever is still in flight before the TMEM and
+      // the CTA go; on the normal path these have completed already
+      mbar_wait_bounded(bar_a, 0);
+      if (bq0 >= 0) mbar_wait_bounded(bar_b0, (uint32_t)bq0);
+      if (bq1 >= 0) mbar_wait_bounded(bar_b1, (uint32_t)bq1);
+      if (pend_acc >= 0) mbar_wait_bounded(pend_acc ? full1 : full0, (uint32_t)pend_par);
     }
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
-                 : "memory");
-  }
-  // bounded wait for the MMAs
-  bool done = false;
-  for (unsigned it = 0; it < kWaitLimit && !done; ++it) done = mbar_try(bar, 0);
-  if (!done) s_ok = 0;  // benign race: every writer stores 0
-  __syncthreads();
-  const bool ok = s_ok != 0;
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (!ok) {
-    if (tid == 0) atomicOr(a.err, 16);
-    for (unsigned it = 0; it < kWaitLimit && !done; ++it) done = mbar_try(bar, 0);
   } else {
-    // this thread's accumulator row: TMEM lane 32*warp + lane
-    uint32_t d[kNP];
-    const uint32_t base = tmem + ((uint32_t)(32 * warp) << 16);
-#pragma unroll
-    for (int c8 = 0; c8 < kNP / 8; ++c8)
-      asm volatile(
-          "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-          : "=r"(d[8 * c8 + 0]), "=r"(d[8 * c8 + 1]), "=r"(d[8 * c8 + 2]), "=r"(d[8 * c8 + 3]), "=r"(d[8 * c8 + 4]),
-            "=r"(d[8 * c8 + 5]), "=r"(d[8 * c8 + 6]), "=r"(d[8 * c8 + 7])
-          : "r"(base + 8 * c8));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-    float2 A[kNC];
-#pragma unroll
-    for (int c = 0; c < kNC; ++c) {
-      const float inv = 1.f / s_scale[c];
-      A[c] = make_float2(__uint_as_float(d[2 * c]) * inv, __uint_as_float(d[2 * c + 1]) * inv);
-    }
-    // mode products with e(q2), e(q3): V[l1][l2][l3] = sum_{b,c} A[l1][b][c] e2[b][l2] e3[c][l3]
+    // ---------------- epilogue ----------------
+    const int wg = warp >> 2, lt = tid & (kTM - 1);
+    const int qg = tile * kTM + lt;
+    const int q2 = min(qg, g.nkc - 1);
+    int m2[3];
+    decompose(g, q2, m2);
     const double2* ev = reinterpret_cast<const double2*>(a.evec);
-    float2 e2[9], e3[9];
+    float2 e2[9];
 #pragma unroll
     for (int i = 0; i < 9; ++i) {
-      const double2 x = ev[(size_t)q2 * 9 + i], y = ev[(size_t)q3 * 9 + i];  // e[q][l][i]
+      const double2 x = ev[(size_t)q2 * 9 + i];  // e[q][l][i]
       e2[i] = make_float2((float)x.x, (float)x.y);
-      e3[i] = make_float2((float)y.x, (float)y.y);
     }
-    const int qg = blockIdx.x * kTM + tid;
-    if (qg < g.nkc) {
-      const double c33 = a.const33 * a.const33 / 8;
-      double t2[3], t3[3];
+    double t2[3];
+#pragma unroll
+    for (int l = 0; l < 3; ++l) t2[l] = 1.0 / sqrt(fabs(a.w2[(size_t)q2 * 3 + l]));
+    const size_t nk = g.nkc;
+    const double c33 = a.const33 * a.const33 / 8;
+    const uint32_t full = wg ? full1 : full0, empty = wg ? empty1 : empty0;
+    const uint32_t taddr = tmem + (uint32_t)(wg * kNP) + ((uint32_t)(32 * (warp & 3)) << 16);
+    for (int it = wg; it < n; it += kEpiWG) {
+      const int row = r0 + it;
+      // row-dependent data before the wait: q1, q3, e(q3), 1/sqrt|l|
+      const int q1 = a.mapinv[a.n1_first + row];
+      int m1[3];
+      decompose(g, q1, m1);
+      const int q3 = idx_q3(g, m1, m2);
+      float2 e3[9];
+#pragma unroll
+      for (int i = 0; i < 9; ++i) {
+        const double2 y = ev[(size_t)q3 * 9 + i];
+        e3[i] = make_float2((float)y.x, (float)y.y);
+      }
+      double t23[9], t1[3];
+#pragma unroll
+      for (int l = 0; l < 3; ++l) t1[l] = c33 / sqrt(fabs(a.w2[(size_t)q1 * 3 + l]));
 #pragma unroll
       for (int l = 0; l < 3; ++l) {
-        t2[l] = 1.0 / sqrt(fabs(a.w2[(size_t)q2 * 3 + l]));
-        t3[l] = 1.0 / sqrt(fabs(a.w2[(size_t)q3 * 3 + l]));
+        const double t3 = 1.0 / sqrt(fabs(a.w2[(size_t)q3 * 3 + l]));
+#pragma unroll
+        for (int l2 = 0; l2 < 3; ++l2) t23[l2 * 3 + l] = t2[l2] * t3;
       }
-      const size_t nk = g.nkc;
+      const float* isc = inv_scales + (size_t)row * kNC;
+      const bool w = mbar_wait_or_fail(full, (uint32_t)((it >> 1) & 1), &s_fail);
+      if (!__all_sync(0xffffffffu, w)) {  // warp-uniform exit
+        s_fail = 1;
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      uint32_t d[kNP];
 #pragma unroll
-      for (int l1 = 0; l1 < 3; ++l1) {
-        const double c1 = c33 / sqrt(fabs(a.w2[(size_t)q1 * 3 + l1]));
-        // T[l2][c] = sum_b A[l1][b][c] e2[b][l2]   (e2[b][l2] at e2[l2*3 + b])
-        float2 T[3][3];
+      for (int c8 = 0; c8 < kNP / 8; ++c8)
+        asm volatile(
+            "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+            : "=r"(d[8 * c8 + 0]), "=r"(d[8 * c8 + 1]), "=r"(d[8 * c8 + 2]), "=r"(d[8 * c8 + 3]), "=r"(d[8 * c8 + 4]),
+              "=r"(d[8 * c8 + 5]), "=r"(d[8 * c8 + 6]), "=r"(d[8 * c8 + 7])
+            : "r"(taddr + 8 * c8));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(empty) : "memory");
+      if (qg < g.nkc) {
 #pragma unroll
-        for (int l2 = 0; l2 < 3; ++l2)
+        for (int l1 = 0; l1 < 3; ++l1) {
+          // A[l1][b][c] and T[l2][c] = sum_b A[l1][b][c] e2[b][l2]   (e2[b][l2] at e2[l2*3 + b])
+          float2 A[9];
 #pragma unroll
-          for (int c = 0; c < 3; ++c) {
-            float2 s = make_float2(0.f, 0.f);
-#pragma unroll
-            for (int bb = 0; bb < 3; ++bb) {
-              const float2 x = A[l1 * 9 + bb * 3 + c], y = e2[l2 * 3 + bb];
-              s.x = fmaf(x.x, y.x, fmaf(-x.y, y.y, s.x));
-              s.y = fmaf(x.x, y.y, fmaf(x.y, y.x, s.y));
-            }
-            T[l2][c] = s;
+          for (int j = 0; j < 9; ++j) {
+            const float inv = __ldg(isc + l1 * 9 + j);
+            A[j] = make_float2(__uint_as_float(d[2 * (l1 * 9 + j)]) * inv,
+                               __uint_as_float(d[2 * (l1 * 9 + j) + 1]) * inv);
           }
+          float2 T[3][3];
 #pragma unroll
-        for (int l2 = 0; l2 < 3; ++l2)
-#pragma unroll
-          for (int l3 = 0; l3 < 3; ++l3) {
-            float2 s = make_float2(0.f, 0.f);
+          for (int l2 = 0; l2 < 3; ++l2)
 #pragma unroll
             for (int c = 0; c < 3; ++c) {
-              const float2 x = T[l2][c], y = e3[l3 * 3 + c];
-              s.x = fmaf(x.x, y.x, fmaf(-x.y, y.y, s.x));
-              s.y = fmaf(x.x, y.y, fmaf(x.y, y.x, s.y));
+              float2 sm = make_float2(0.f, 0.f);
+#pragma unroll
+              for (int bb = 0; bb < 3; ++bb) {
+                const float2 x = A[bb * 3 + c], y = e2[l2 * 3 + bb];
+                sm.x = fmaf(x.x, y.x, fmaf(-x.y, y.y, sm.x));
+                sm.y = fmaf(x.x, y.y, fmaf(x.y, y.x, sm.y));
+              }
+              T[l2][c] = sm;
             }
-            const double sc = c1 * t2[l2] * t3[l3];
-            double v = 0.0;
-            if (sc < 1.0 / 0.0) v = ((double)s.x * s.x + (double)s.y * s.y) * sc;
-            else atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
-            double* out = a.v3_layout == 1 ? a.v3sq + (((size_t)row * 27 + l2 * 9 + l3 * 3 + l1) * nk + qg)
-                                           : a.v3sq + ((size_t)row * nk + qg) * 27 + l1 * 9 + l2 * 3 + l3;
-            *out = v;
-          }
+#pragma unroll
+          for (int l2 = 0; l2 < 3; ++l2)
+#pragma unroll
+            for (int l3 = 0; l3 < 3; ++l3) {
+              float2 sm = make_float2(0.f, 0.f);
+#pragma unroll
+              for (int c = 0; c < 3; ++c) {
+                const float2 x = T[l2][c], y = e3[l3 * 3 + c];
+                sm.x = fmaf(x.x, y.x, fmaf(-x.y, y.y, sm.x));
+                sm.y = fmaf(x.x, y.y, fmaf(x.y, y.x, sm.y));
+              }
+              const double sc = t1[l1] * t23[l2 * 3 + l3];
+              double v = 0.0;
+              if (sc < 1.0 / 0.0) v = (double)fmaf(sm.x, sm.x, sm.y * sm.y) * sc;
+              else atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
+              double* out = a.v3_layout == 1 ? a.v3sq + (((size_t)row * 27 + l2 * 9 + l3 * 3 + l1) * nk + qg)
+                                             : a.v3sq + ((size_t)row * nk + qg) * 27 + l1 * 9 + l2 * 3 + l3;
+              *out = v;
+            }
+        }
       }
     }
   }
-  // free TMEM after every warp's loads
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+  if (tid == 0 && s_fail) atomicOr(a.err, 16);
+  if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemAlloc));
 }
 
 }  // namespace
 
 bool v3_tc_supported(int b, int ncls) { return b == 3 && ncls >= 1 && 2 * ncls <= kMaxKp; }
 
-cudaError_t launch_v3_tc(const V3Args& a, cudaStream_t s) {
+size_t v3_tc_ptile_bytes(int nkc, int ncls) {
+  const int kp = (2 * ncls + 15) / 16 * 16;
+  return (size_t)((nkc + kTM - 1) / kTM) * 2 * kTM * kp * sizeof(__half);
+}
+
+cudaError_t launch_v3_tc_ptiles(const V3Args& a, void* ptiles, cudaStream_t s) {
   if (!v3_tc_supported(a.geo.b, a.ncls)) return cudaErrorInvalidValue;
   const int kp = (2 * a.ncls + 15) / 16 * 16;
-  const size_t smem = (size_t)(kTM + kNP) * kp * 2 * sizeof(__half);
+  v3_ptile_kernel<<<(a.geo.nkc + kTM - 1) / kTM, kTM, 0, s>>>(a.geo, a.ncls, kp, a.cls_pc, a.roots,
+                                                              static_cast<__half*>(ptiles));
+  return cudaGetLastError();
+}
+
+size_t v3_tc_btile_bytes(int nrows, int ncls) {
+  const int kp = (2 * ncls + 15) / 16 * 16;
+  return (size_t)nrows * (2 * kNP * kp * sizeof(__half) + kNC * sizeof(float));
+}
+
+cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s) {
+  if (!v3_tc_supported(a.geo.b, a.ncls)) return cudaErrorInvalidValue;
+  const int kp = (2 * a.ncls + 15) / 16 * 16;
+  __half* bt = static_cast<__half*>(btiles);
+  float* sc = reinterpret_cast<float*>(bt + (size_t)a.nrows * 2 * kNP * kp);
+  v3_btile_kernel<<<a.nrows, 256, 0, s>>>(a, kp, bt, sc);
+  const size_t smem = (size_t)(2 * kTM + 4 * kNP) * kp * sizeof(__half);
   cudaError_t e = cudaFuncSetAttribute(v3_tc3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((a.geo.nkc + kTM - 1) / kTM, a.nrows);
-  v3_tc3_kernel<<<grid, kTM, smem, s>>>(a, kp);
+  const int ntiles = (a.geo.nkc + kTM - 1) / kTM;
+  // rows per CTA: reuse the phase tile over several rows while the grid still fills the GPU twice
+  int rpc = 16;
+  while (rpc > 1 && (long)ntiles * ((a.nrows + rpc - 1) / rpc) < 2 * 148) rpc /= 2;
+  dim3 grid(ntiles, (a.nrows + rpc - 1) / rpc);
+  v3_tc3_kernel<<<grid, kThreads, smem, s>>>(a, kp, static_cast<const __half*>(ptiles), bt, sc, rpc);
   return cudaGetLastError();
 }
 
