@@ -163,7 +163,7 @@ int run_v3(ald_ctx* c, const V3Args& a0) {
       if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 phase tiles: ") + cudaGetErrorString(e));
       c->ptiles_ok = true;
     }
-    const size_t bneed = v3_tc_btile_bytes(a.nrows, c->VC.ncls);
+    const size_t bneed = v3_tc_btile_bytes(a.nrows, c->VC.ncls, c->geo.nkc);
     if (c->w_btiles.n < bneed) CKA(c->w_btiles.alloc(bneed));
     e = launch_v3_rows_f32(a, c->stream);
     if (e == cudaSuccess) e = launch_v3_tc(a, c->w_ptiles.p, c->w_btiles.p, c->stream);
@@ -555,6 +555,7 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   a.tet_inc = c->tet_inc.p;
   a.gauss = delta_mode(c) == ALD_DELTA_GAUSS;
   a.sigma = gauss_width(c);
+  a.f32w = 0;  // the per-stage entry point keeps the reference's FP64 weights
   a.R1 = R1.p;
   a.R2 = R2.p;
   a.P1s = p1.p;

@@ -229,8 +229,9 @@ bool v3_tc_supported(int b, int ncls);
 // the row-independent phase tiles (split FP16, canonical layout), built once per context
 size_t v3_tc_ptile_bytes(int nkc, int ncls);
 cudaError_t launch_v3_tc_ptiles(const V3Args& a, void* ptiles, cudaStream_t s);
-// btiles: scratch of v3_tc_btile_bytes(nrows, ncls) (B operands and scales of the chunk's rows)
-size_t v3_tc_btile_bytes(int nrows, int ncls);
+// btiles: scratch of v3_tc_btile_bytes(nrows, ncls, nkc) (B operands and row data of the
+// chunk's rows, per-mode factors and FP32 eigenvectors of the mesh)
+size_t v3_tc_btile_bytes(int nrows, int ncls, int nkc);
 cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s);
 
 struct CombineArgs {
@@ -245,6 +246,7 @@ struct CombineArgs {
   const int* tet_inc;
   int gauss;
   double sigma;
+  int f32w;                  // 1: delta weights in FP32 (mixed-precision pipeline), 0: FP64 as the reference
   double* R1;                // [row][q][l1][l2], row local to the chunk
   double* R2;
   double* R1p;               // optional [row][q][l1][l3] = sum_l2 P1 (update_mpi); nullptr = skip

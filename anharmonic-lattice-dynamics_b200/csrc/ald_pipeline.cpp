@@ -128,8 +128,9 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
   const bool fused = !gauss && delta_fused_supported(c->geo);
   if (!fused) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
-  // the fused delta reads |V3|^2 slice by slice: the pair kernel writes that layout
-  const int v3_layout = fused && v3_pair_supported(b, c->opt.precision) ? 1 : 0;
+  // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
+  // class-form V3 kernels write that layout
+  const int v3_layout = v3_pair_supported(b, c->opt.precision) ? 1 : 0;
   for (int r0 = 0; r0 < nibz; r0 += K) {
     int nr = std::min(K, nibz - r0);
     ALD_CK(tm.begin(1));
@@ -152,6 +153,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     a.tet_inc = c->tet_inc.p;
     a.gauss = gauss;
     a.sigma = gauss_width(c);
+    a.f32w = c->opt.precision != ALD_FP64;  // mixed: FP32 delta weights
     a.R1 = R1.p + (size_t)r0 * nkc * b * b;
     a.R2 = R2.p + (size_t)r0 * nkc * b * b;
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;

@@ -220,4 +220,50 @@ ALD_TET_HD bool tet_weights4(const TetSorted& t, double e, double* c) {
   return true;
 }
 
+#ifdef __CUDACC__
+// The same four weights in FP32 for the mixed-precision pipeline: the regime
+// test and the four distances e - E_i are taken in double (e is the FP64
+// omega1, so the cancellation stays exact) and rounded once; every quotient
+// becomes a product with one reciprocal per sorted difference.  Not bitwise
+// against weight_tet: relative errors of a few FP32 ulps per weight.
+__device__ __forceinline__ float tet_rcp(float x) { return __fdividef(1.0f, x); }
+
+__device__ __forceinline__ bool tet_weights4_f32(const TetSorted& t, double e, float* c) {
+  const int r = tet_regime(t, e);
+  if (r == 0) return false;
+  const float d1 = (float)(e - (double)t.e1), d2 = (float)(e - (double)t.e2);
+  const float d3 = (float)(e - (double)t.e3), d4 = (float)(e - (double)t.e4);  // d4 <= 0
+  if (r == 1) {
+    const float r21 = tet_rcp(t.e21), r31 = tet_rcp(t.e31), r41 = tet_rcp(t.e41);
+    const float x = d1, base = x * x * (r21 * r31 * r41), xb = x * base;
+    c[3] = (-d2 * r21 - d3 * r31 - d4 * r41) * base;
+    c[2] = xb * r21;
+    c[1] = xb * r31;
+    c[0] = xb * r41;
+  } else if (r == 2) {
+    const float r31 = tet_rcp(t.e31), r41 = tet_rcp(t.e41), r32 = tet_rcp(t.e32), r42 = tet_rcp(t.e42);
+    const float a3 = -d3, a4 = -d4, b1 = d1, b2 = d2;
+    const float c11 = a3 * r31 * r31, c12 = a4 * r41 * r41, c21 = a3 * r32 * r32, c22 = a4 * r42 * r42;
+    const float c31 = b2 * r32 * r32, c32 = b1 * r31 * r31, c41 = b2 * r42 * r42, c42 = b1 * r41 * r41;
+    const float a3b2 = a3 * b2, a4b1 = a4 * b1, a3b1 = a3 * b1, a4b2 = a4 * b2;
+    const float b11 = a3b2 * (r42 * r32) + a4b1 * (r41 * r42) + a3b1 * (r32 * r41);
+    const float b12 = a4b1 * (r42 * r31) + a4b2 * (r42 * r32) + a3b1 * (r31 * r32);
+    const float b21 = a3b2 * (r42 * r31) + a4b2 * (r42 * r41) + a3b1 * (r31 * r41);
+    const float b22 = a3b2 * (r32 * r31) + a4b1 * (r41 * r31) + a4b2 * (r32 * r41);
+    c[3] = 0.5f * (c11 * b11 + c12 * b12);
+    c[2] = 0.5f * (c21 * b21 + c22 * b22);
+    c[1] = 0.5f * (c31 * b21 + c32 * b11);
+    c[0] = 0.5f * (c41 * b22 + c42 * b12);
+  } else {
+    const float r41 = tet_rcp(t.e41), r42 = tet_rcp(t.e42), r43 = tet_rcp(t.e43);
+    const float x = -d4, base = x * x * (r41 * r42 * r43), xb = x * base;
+    c[3] = xb * r41;
+    c[2] = xb * r42;
+    c[1] = xb * r43;
+    c[0] = (d3 * r43 + d2 * r42 + d1 * r41) * base;
+  }
+  return true;
+}
+#endif
+
 }  // namespace ald

@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(kTetThreads) delta_tet_kernel(Geometry g, int 
 }
 
 // per mesh point: P = F * W, Bose factors, sums over l3
-template <int B>
+template <int B, bool F32W>
 __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a, const double* __restrict__ W) {
   __shared__ double s_om1[B], s_nb1[B];
   const Geometry& g = a.geo;
@@ -224,6 +224,11 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   const double n2 = a.dist[(size_t)w * b + l2];
   const double* v3 = a.v3sq + (size_t)row * nkc * b3;
+  // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
+  const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
+  const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
+  // FP32 Gaussian (mixed-precision pipeline): exp(-(x/w)^2/2) / (sqrt(2 pi) w)
+  const float gi = (float)(1.0 / a.sigma), gn = (float)(1.0 / sqrt(2 * PhysConst::pi) / a.sigma);
   double R1[B], R2[B];
 #pragma unroll
   for (int l = 0; l < B; ++l) R1[l] = R2[l] = 0.0;
@@ -242,10 +247,19 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
       for (int l = 0; l < B; ++l) {
         if (l >= b) continue;
         double wl;
-        if (a.gauss) wl = delta_g(proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3, a.sigma);
-        else wl = W[(slice * nkc + w) * b + l];
+        if (a.gauss) {
+          const double x = proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3;
+          if constexpr (F32W) {
+            const float xs = (float)x * gi;
+            wl = (double)(expf(-0.5f * (xs * xs)) * gn);
+          } else {
+            wl = delta_g(x, a.sigma);
+          }
+        } else {
+          wl = W[(slice * nkc + w) * b + l];
+        }
         double ps = 0.0;
-        if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * b3 + (l * b + l2) * b + l3] * fnorm);
+        if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * sq + l * s1 + l2 * s2 + l3 * s3] * fnorm);
         const double nb1 = s_nb1[l];
         const double Fb = proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1);
         const double p = ps * Fb;
@@ -358,7 +372,7 @@ __host__ __device__ inline FusedShape fused_shape(const Geometry& g) {
   return f;
 }
 
-template <int B>
+template <int B, bool F32W>
 __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double s_om[B], s_nb1[B];
@@ -532,7 +546,14 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       const float4 e = s_rece[rec];
       const TetSorted ts = tet_sort(e.x, e.y, e.z, e.w);
       double cp[4];
-      if (!tet_weights4(ts, s_om[l1], cp)) continue;
+      if constexpr (F32W) {
+        float cf[4];
+        if (!tet_weights4_f32(ts, s_om[l1], cf)) continue;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) cp[k] = cf[k];
+      } else {
+        if (!tet_weights4(ts, s_om[l1], cp)) continue;
+      }
       const ushort4 pp = s_recp[rec];
       const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
       const double nb1 = s_nb1[l1];
@@ -580,16 +601,25 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) 
     W = Wd;
   }
   dim3 grid((g.nkc + kPointBlock - 1) / kPointBlock, g.b, a.nrows);
-  if (g.b <= 3)
-    delta_point_kernel<3><<<grid, kPointBlock, 0, s>>>(a, W);
-  else if (g.b <= 6)
-    delta_point_kernel<6><<<grid, kPointBlock, 0, s>>>(a, W);
-  else if (g.b <= 12)
-    delta_point_kernel<12><<<grid, kPointBlock, 0, s>>>(a, W);
-  else if (g.b <= 16)
-    delta_point_kernel<16><<<grid, kPointBlock, 0, s>>>(a, W);
-  else
+  // FP32 weights only for the Gaussian (the tetrahedron weights W are FP64 here)
+  const bool fw = a.f32w && a.gauss;
+#define ALD_POINT(BB)                                               \
+  if (fw)                                                           \
+    delta_point_kernel<BB, true><<<grid, kPointBlock, 0, s>>>(a, W); \
+  else                                                              \
+    delta_point_kernel<BB, false><<<grid, kPointBlock, 0, s>>>(a, W);
+  if (g.b <= 3) {
+    ALD_POINT(3)
+  } else if (g.b <= 6) {
+    ALD_POINT(6)
+  } else if (g.b <= 12) {
+    ALD_POINT(12)
+  } else if (g.b <= 16) {
+    ALD_POINT(16)
+  } else {
     return cudaErrorInvalidValue;
+  }
+#undef ALD_POINT
   return cudaGetLastError();
 }
 
@@ -603,10 +633,16 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
   const FusedShape f = fused_shape(g);
   dim3 grid(g.nc[0] * f.nbj, a.nrows, 2 * g.b);
   cudaError_t e;
-#define ALD_FUSED(BB)                                                                                       \
-  e = cudaFuncSetAttribute(delta_fused_kernel<BB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem); \
-  if (e != cudaSuccess) return e;                                                                           \
-  delta_fused_kernel<BB><<<grid, kFusedThreads, f.smem, s>>>(a);
+#define ALD_FUSED1(BB, FW)                                                                                       \
+  e = cudaFuncSetAttribute(delta_fused_kernel<BB, FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem); \
+  if (e != cudaSuccess) return e;                                                                                \
+  delta_fused_kernel<BB, FW><<<grid, kFusedThreads, f.smem, s>>>(a);
+#define ALD_FUSED(BB)     \
+  if (a.f32w) {           \
+    ALD_FUSED1(BB, true)  \
+  } else {                \
+    ALD_FUSED1(BB, false) \
+  }
   if (g.b <= 3) {
     ALD_FUSED(3)
   } else if (g.b <= 6) {
@@ -617,6 +653,7 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
     ALD_FUSED(16)
   }
 #undef ALD_FUSED
+#undef ALD_FUSED1
   return cudaGetLastError();
 }
 

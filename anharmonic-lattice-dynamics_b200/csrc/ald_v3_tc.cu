@@ -33,6 +33,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <cstdlib>
 
 #include "ald_internal.h"
 
@@ -46,18 +47,23 @@ constexpr int kNP = 64;       // real outputs padded to a valid N
 constexpr int kMaxKp = 208;   // K' bound (ncls <= 104): A + 2 B buffers fit 227 KB
 constexpr unsigned kWaitLimit = 1u << 22;
 
-__device__ __forceinline__ int wrapm(int v, int n) {
-  v %= n;
-  return v < 0 ? v + n : v;
-}
 __device__ __forceinline__ void decompose(const Geometry& g, int n, int* m) {
   m[0] = n / (g.nc[1] * g.nc[2]);
   m[1] = (n / g.nc[2]) % g.nc[1];
   m[2] = n % g.nc[2];
 }
-__device__ __forceinline__ int idx_q3(const Geometry& g, const int* m1, const int* m2) {
+// mesh index of q3 = -q1-q2 with the wrap done by compares (|m| < nc)
+__device__ __forceinline__ int idx_q3_fast(const Geometry& g, const int* m1, const int* m2) {
   int m3[3];
-  for (int a = 0; a < 3; ++a) m3[a] = wrapm(-m1[a] - m2[a] + (g.shifted ? g.nc[a] / 2 : 0), g.nc[a]);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const int n = g.nc[a];
+    int v = -m1[a] - m2[a] + (g.shifted ? n / 2 : 0);
+    v += v < 0 ? n : 0;
+    v += v < 0 ? n : 0;
+    v -= v >= n ? n : 0;
+    m3[a] = v;
+  }
   return m3[2] + g.nc[2] * (m3[1] + g.nc[1] * m3[0]);
 }
 __device__ __forceinline__ int phase_index(const int* pc, const int* m, int L) {
@@ -138,13 +144,74 @@ __global__ void v3_ptile_kernel(Geometry g, int ncls, int kp, const int* cls_pc,
   }
 }
 
+// Per-launch scratch of the tensor-core V3, carved from one buffer:
+//   bt     [row][hi|lo][kmaj]     B operands (2 kNP kp halves per row)
+//   isc    [row][32]              inverse column scales (27 used)
+//   rq     [row]                  int4 {q1, m1[0..2]}
+//   rt     [row][4]               const33^2/8 / sqrt|l(q1)| per band (3 used)
+//   tq     [q][3]                 1/sqrt|l(q)| of every mesh mode
+//   evf    [q][9]                 e(q) as float2, [l][i]
+struct TcScratch {
+  __half* bt;
+  float* isc;
+  int4* rq;
+  double* rt;
+  double* tq;
+  float2* evf;
+};
+__host__ __device__ inline size_t tc_align(size_t x) { return (x + 255) & ~(size_t)255; }
+inline TcScratch tc_carve(void* base, int nrows, int kp, int nkc, size_t* total) {
+  char* p = static_cast<char*>(base);
+  size_t o = 0;
+  TcScratch t;
+  t.bt = reinterpret_cast<__half*>(p + o);
+  o = tc_align(o + (size_t)nrows * 2 * kNP * kp * sizeof(__half));
+  t.isc = reinterpret_cast<float*>(p + o);
+  o = tc_align(o + (size_t)nrows * 32 * sizeof(float));
+  t.rq = reinterpret_cast<int4*>(p + o);
+  o = tc_align(o + (size_t)nrows * sizeof(int4));
+  t.rt = reinterpret_cast<double*>(p + o);
+  o = tc_align(o + (size_t)nrows * 4 * sizeof(double));
+  t.tq = reinterpret_cast<double*>(p + o);
+  o = tc_align(o + (size_t)nkc * 3 * sizeof(double));
+  t.evf = reinterpret_cast<float2*>(p + o);
+  o = tc_align(o + (size_t)nkc * 9 * sizeof(float2));
+  if (total) *total = o;
+  return t;
+}
+
+// per mesh mode: 1/sqrt|lambda| and the eigenvectors in FP32
+__global__ void v3_tc_modes_kernel(V3Args a, TcScratch t) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q >= a.geo.nkc) return;
+  const double2* ev = reinterpret_cast<const double2*>(a.evec);
+#pragma unroll
+  for (int l = 0; l < 3; ++l) t.tq[(size_t)q * 3 + l] = 1.0 / sqrt(fabs(a.w2[(size_t)q * 3 + l]));
+#pragma unroll
+  for (int i = 0; i < 9; ++i) {
+    const double2 x = ev[(size_t)q * 9 + i];
+    t.evf[(size_t)q * 9 + i] = make_float2((float)x.x, (float)x.y);
+  }
+}
+
 // The B operand of every IBZ row of the chunk (H in real form, split FP16,
 // canonical layout), built once per row: [row][hi|lo][kmaj], and the
 // inverses of the 27 column scales (powers of two with max |H| * scale in
 // [0.5, 1)).
-__global__ void v3_btile_kernel(V3Args a, int kp, __half* Bt, float* inv_scales) {
+__global__ void v3_btile_kernel(V3Args a, int kp, TcScratch t) {
   __shared__ float s_scale[kNC];
   const int row = blockIdx.x, tid = threadIdx.x, ncls = a.ncls;
+  __half* Bt = t.bt;
+  float* inv_scales = t.isc;
+  if (tid == 0) {
+    const int q1 = a.mapinv[a.n1_first + row];
+    int m1[3];
+    decompose(a.geo, q1, m1);
+    t.rq[row] = make_int4(q1, m1[0], m1[1], m1[2]);
+    const double c33 = a.const33 * a.const33 / 8;
+    for (int l = 0; l < 3; ++l) t.rt[(size_t)row * 4 + l] = c33 / sqrt(fabs(a.w2[(size_t)q1 * 3 + l]));
+    t.rt[(size_t)row * 4 + 3] = 0.0;
+  }
   const float2* H = static_cast<const float2*>(a.hbuf) + (size_t)row * ncls * 9 * 3;
   if (tid < kNC) {
     const int l1 = tid / 9, bg = tid % 9;
@@ -156,7 +223,7 @@ __global__ void v3_btile_kernel(V3Args a, int kp, __half* Bt, float* inv_scales)
     int e = 0;
     if (mx > 0.f) frexpf(mx, &e);
     s_scale[tid] = ldexpf(1.f, -e);
-    inv_scales[(size_t)row * kNC + tid] = ldexpf(1.f, e);
+    inv_scales[(size_t)row * 32 + tid] = ldexpf(1.f, e);
   }
   __syncthreads();
   __half* hi = Bt + (size_t)row * 2 * kNP * kp;
@@ -204,23 +271,29 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
   }
 }
 
-constexpr int kEpiWG = 2;                   // epilogue warpgroups = TMEM accumulators
-constexpr int kThreads = 128 * kEpiWG + 32;  // + one producer warp
-constexpr int kTmemAlloc = 128;              // kEpiWG x 64 columns
+// NE epilogue warpgroups = NE TMEM accumulators of 64 columns, + one producer warp
+template <int NE>
+struct TcShape {
+  static constexpr int threads = 128 * NE + 32;
+  static constexpr int tmem_cols = NE <= 2 ? 128 : 256;  // a power of two >= 64 NE
+};
 
 // One CTA: one 128-q2 tile and up to `rpc` IBZ rows, warp-specialised.
 // * Producer warp (one lane): copies the phase tile once and the B tiles of
 //   the rows through two buffers, issues the 3 (kp/16) MMAs of a row into
-//   accumulator (row % 2) once that accumulator has been drained, commits.
-// * Epilogue warpgroup w takes the rows with (row - r0) % 2 == w: thread =
+//   accumulator (row % NE) once that accumulator has been drained, commits.
+// * Epilogue warpgroup w takes the rows with (row - r0) % NE == w: thread =
 //   TMEM lane = q2; it loads its 64 accumulator columns, releases the
 //   accumulator, then does the mode products with e(q2), e(q3), the scaling
 //   and the stores, while the producer already runs the next rows' MMAs.
-__global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, const __half* Pt, const __half* Bt,
-                                                             const float* inv_scales, int rpc) {
+template <int NE>
+__global__ void __launch_bounds__(TcShape<NE>::threads, 1)
+    v3_tc3_kernel(V3Args a, int kp, const __half* Pt, TcScratch ts, int rpc) {
+  constexpr int kTmemAlloc = TcShape<NE>::tmem_cols;
+  const __half* Bt = ts.bt;
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ uint32_t s_tmem;
-  __shared__ __align__(8) uint64_t s_bar_a, s_bar_b[2], s_full[kEpiWG], s_empty[kEpiWG];
+  __shared__ __align__(8) uint64_t s_bar_a, s_bar_b[2], s_full[NE], s_empty[NE];
   __shared__ volatile int s_fail;
   const Geometry& g = a.geo;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, tile = blockIdx.x;
@@ -231,10 +304,9 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
   const uint32_t bar_a = (uint32_t)__cvta_generic_to_shared(&s_bar_a);
   const uint32_t bar_b0 = (uint32_t)__cvta_generic_to_shared(&s_bar_b[0]);
   const uint32_t bar_b1 = (uint32_t)__cvta_generic_to_shared(&s_bar_b[1]);
+  // accumulator k's barriers at full0 + 8k, empty0 + 8k
   const uint32_t full0 = (uint32_t)__cvta_generic_to_shared(&s_full[0]);
-  const uint32_t full1 = (uint32_t)__cvta_generic_to_shared(&s_full[1]);
   const uint32_t empty0 = (uint32_t)__cvta_generic_to_shared(&s_empty[0]);
-  const uint32_t empty1 = (uint32_t)__cvta_generic_to_shared(&s_empty[1]);
 
   if (warp == 0) {
     const uint32_t dst = (uint32_t)__cvta_generic_to_shared(&s_tmem);
@@ -245,10 +317,10 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_a));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_b0));
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar_b1));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full1));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0), "r"(kTM));
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty1), "r"(kTM));
+    for (int k = 0; k < NE; ++k) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(full0 + 8 * k));
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(empty0 + 8 * k), "r"(kTM));
+    }
     asm volatile("fence.mbarrier_init.release.cluster;");
     s_fail = 0;
   }
@@ -257,7 +329,7 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
 
-  if (warp == 4 * kEpiWG) {
+  if (warp == 4 * NE) {
     // ---------------- producer ----------------
     if (lane == 0) {
       int bq0 = -1, bq1 = -1, pend_acc = -1, pend_par = 0;  // copies and MMAs in flight
@@ -272,18 +344,18 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
       const uint32_t idesc = instr_desc(kTM, kNP);
       const uint32_t aH = a_sh, aL = a_sh + (uint32_t)(kTM * kp * sizeof(__half));
       for (int it = 0; ok && it < n; ++it) {
-        const int buf = it & 1;
+        const int buf = it & 1, acc = it % NE, use = it / NE;
         ok = mbar_wait_or_fail(buf ? bar_b1 : bar_b0, (uint32_t)((it >> 1) & 1), &s_fail);
         if (!ok) break;
         if (buf) bq1 = -1;
         else bq0 = -1;
-        if (it >= 2) {  // accumulator buf drained by the epilogue of row it - 2
-          ok = mbar_wait_or_fail(buf ? empty1 : empty0, (uint32_t)(((it >> 1) - 1) & 1), &s_fail);
+        if (use >= 1) {  // accumulator acc drained by the epilogue of row it - NE
+          ok = mbar_wait_or_fail(empty0 + 8 * acc, (uint32_t)((use - 1) & 1), &s_fail);
           if (!ok) break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t bH = b_sh + (uint32_t)buf * bbytes, bL = bH + (uint32_t)(kNP * kp * sizeof(__half));
-        const uint32_t dt = tmem + (uint32_t)(buf * kNP);
+        const uint32_t dt = tmem + (uint32_t)(acc * kNP);
         for (int st = 0; st < kp / 16; ++st) {
           // K step st covers K chunks 2st, 2st+1: ROWS*16 bytes per chunk
           const uint32_t oa = (uint32_t)(2 * st * kTM * 16), ob = (uint32_t)(2 * st * kNP * 16);
@@ -294,15 +366,15 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
           mma_f16(dt, dAl, dBh, idesc, 1u);
         }
         asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                         buf ? full1 : full0)
+                         full0 + 8 * acc)
                      : "memory");
-        pend_acc = buf;
-        pend_par = (it >> 1) & 1;
+        pend_acc = acc;
+        pend_par = use & 1;
         // B buffer of row it - 1 is free once that row's MMAs completed:
         // refill it with row it + 1
         if (it >= 1 && it + 1 < n) {
           const int pb = buf ^ 1;
-          ok = mbar_wait_or_fail(pb ? full1 : full0, (uint32_t)(((it - 1) >> 1) & 1), &s_fail);
+          ok = mbar_wait_or_fail(full0 + 8 * ((it - 1) % NE), (uint32_t)(((it - 1) / NE) & 1), &s_fail);
           if (!ok) break;
           bulk_g2s(b_sh + (uint32_t)pb * bbytes, Bt + (size_t)(r0 + it + 1) * 2 * kNP * kp, bbytes,
                    pb ? bar_b1 : bar_b0);
@@ -316,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
       mbar_wait_bounded(bar_a, 0);
       if (bq0 >= 0) mbar_wait_bounded(bar_b0, (uint32_t)bq0);
       if (bq1 >= 0) mbar_wait_bounded(bar_b1, (uint32_t)bq1);
-      if (pend_acc >= 0) mbar_wait_bounded(pend_acc ? full1 : full0, (uint32_t)pend_par);
+      if (pend_acc >= 0) mbar_wait_bounded(full0 + 8 * pend_acc, (uint32_t)pend_par);
     }
   } else {
     // ---------------- epilogue ----------------
@@ -325,44 +397,35 @@ __global__ void __launch_bounds__(kThreads, 1) v3_tc3_kernel(V3Args a, int kp, c
     const int q2 = min(qg, g.nkc - 1);
     int m2[3];
     decompose(g, q2, m2);
-    const double2* ev = reinterpret_cast<const double2*>(a.evec);
     float2 e2[9];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
-      const double2 x = ev[(size_t)q2 * 9 + i];  // e[q][l][i]
-      e2[i] = make_float2((float)x.x, (float)x.y);
-    }
+    for (int i = 0; i < 9; ++i) e2[i] = ts.evf[(size_t)q2 * 9 + i];  // e[q][l][i]
     double t2[3];
 #pragma unroll
-    for (int l = 0; l < 3; ++l) t2[l] = 1.0 / sqrt(fabs(a.w2[(size_t)q2 * 3 + l]));
+    for (int l = 0; l < 3; ++l) t2[l] = ts.tq[(size_t)q2 * 3 + l];
     const size_t nk = g.nkc;
-    const double c33 = a.const33 * a.const33 / 8;
-    const uint32_t full = wg ? full1 : full0, empty = wg ? empty1 : empty0;
+    const uint32_t full = full0 + 8 * wg, empty = empty0 + 8 * wg;
     const uint32_t taddr = tmem + (uint32_t)(wg * kNP) + ((uint32_t)(32 * (warp & 3)) << 16);
-    for (int it = wg; it < n; it += kEpiWG) {
+    for (int it = wg; it < n; it += NE) {
       const int row = r0 + it;
-      // row-dependent data before the wait: q1, q3, e(q3), 1/sqrt|l|
-      const int q1 = a.mapinv[a.n1_first + row];
-      int m1[3];
-      decompose(g, q1, m1);
-      const int q3 = idx_q3(g, m1, m2);
+      // row-dependent data before the wait: q3, e(q3), the mode factors
+      const int4 ri = ts.rq[row];
+      const int m1[3] = {ri.y, ri.z, ri.w};
+      const int q3 = idx_q3_fast(g, m1, m2);
       float2 e3[9];
 #pragma unroll
-      for (int i = 0; i < 9; ++i) {
-        const double2 y = ev[(size_t)q3 * 9 + i];
-        e3[i] = make_float2((float)y.x, (float)y.y);
-      }
+      for (int i = 0; i < 9; ++i) e3[i] = ts.evf[(size_t)q3 * 9 + i];
       double t23[9], t1[3];
 #pragma unroll
-      for (int l = 0; l < 3; ++l) t1[l] = c33 / sqrt(fabs(a.w2[(size_t)q1 * 3 + l]));
+      for (int l = 0; l < 3; ++l) t1[l] = ts.rt[(size_t)row * 4 + l];
 #pragma unroll
       for (int l = 0; l < 3; ++l) {
-        const double t3 = 1.0 / sqrt(fabs(a.w2[(size_t)q3 * 3 + l]));
+        const double t3 = ts.tq[(size_t)q3 * 3 + l];
 #pragma unroll
         for (int l2 = 0; l2 < 3; ++l2) t23[l2 * 3 + l] = t2[l2] * t3;
       }
-      const float* isc = inv_scales + (size_t)row * kNC;
-      const bool w = mbar_wait_or_fail(full, (uint32_t)((it >> 1) & 1), &s_fail);
+      const float* isc = ts.isc + (size_t)row * 32;
+      const bool w = mbar_wait_or_fail(full, (uint32_t)((it / NE) & 1), &s_fail);
       if (!__all_sync(0xffffffffu, w)) {  // warp-uniform exit
         s_fail = 1;
         break;
@@ -451,26 +514,37 @@ cudaError_t launch_v3_tc_ptiles(const V3Args& a, void* ptiles, cudaStream_t s) {
   return cudaGetLastError();
 }
 
-size_t v3_tc_btile_bytes(int nrows, int ncls) {
+size_t v3_tc_btile_bytes(int nrows, int ncls, int nkc) {
   const int kp = (2 * ncls + 15) / 16 * 16;
-  return (size_t)nrows * (2 * kNP * kp * sizeof(__half) + kNC * sizeof(float));
+  size_t total = 0;
+  tc_carve(nullptr, nrows, kp, nkc, &total);
+  return total;
 }
 
 cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s) {
   if (!v3_tc_supported(a.geo.b, a.ncls)) return cudaErrorInvalidValue;
   const int kp = (2 * a.ncls + 15) / 16 * 16;
-  __half* bt = static_cast<__half*>(btiles);
-  float* sc = reinterpret_cast<float*>(bt + (size_t)a.nrows * 2 * kNP * kp);
-  v3_btile_kernel<<<a.nrows, 256, 0, s>>>(a, kp, bt, sc);
+  const TcScratch ts = tc_carve(btiles, a.nrows, kp, a.geo.nkc, nullptr);
+  v3_tc_modes_kernel<<<(a.geo.nkc + 127) / 128, 128, 0, s>>>(a, ts);
+  v3_btile_kernel<<<a.nrows, 256, 0, s>>>(a, kp, ts);
   const size_t smem = (size_t)(2 * kTM + 4 * kNP) * kp * sizeof(__half);
-  cudaError_t e = cudaFuncSetAttribute(v3_tc3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // epilogue warpgroups: 2 by default; ALD_V3_TC_WG=3 selects three
+  static const int ne = [] {
+    const char* v = getenv("ALD_V3_TC_WG");
+    return v && atoi(v) == 3 ? 3 : 2;
+  }();
+  cudaError_t e = cudaFuncSetAttribute(ne == 3 ? v3_tc3_kernel<3> : v3_tc3_kernel<2>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) return e;
   const int ntiles = (a.geo.nkc + kTM - 1) / kTM;
   // rows per CTA: reuse the phase tile over several rows while the grid still fills the GPU twice
   int rpc = 16;
   while (rpc > 1 && (long)ntiles * ((a.nrows + rpc - 1) / rpc) < 2 * 148) rpc /= 2;
   dim3 grid(ntiles, (a.nrows + rpc - 1) / rpc);
-  v3_tc3_kernel<<<grid, kThreads, smem, s>>>(a, kp, static_cast<const __half*>(ptiles), bt, sc, rpc);
+  if (ne == 3)
+    v3_tc3_kernel<3><<<grid, TcShape<3>::threads, smem, s>>>(a, kp, static_cast<const __half*>(ptiles), ts, rpc);
+  else
+    v3_tc3_kernel<2><<<grid, TcShape<2>::threads, smem, s>>>(a, kp, static_cast<const __half*>(ptiles), ts, rpc);
   return cudaGetLastError();
 }
 

@@ -1,9 +1,11 @@
 """The mixed-precision V3 path (ALD_MIXED) against the FP64 oracle (GPU).
 
 ALD_MIXED runs the phase-class sums and the two eigenvector mode products of
-V3 in FP32 with FP32 accumulation; eigenvalues, den = sqrt(8 sqrt|l1 l2 l3|),
-the delta weights, Bose factors, Q, the collision matrix, CG and kappa stay
-FP64.  Tolerances (the targets of the mixed path):
+V3 in FP32 with FP32 accumulation (for 3-band cells the class sums as
+split-FP16 tensor-core MMAs); inside the pipeline the tetrahedron and
+Gaussian delta weights are FP32 as well.  Eigenvalues, den = sqrt(8
+sqrt|l1 l2 l3|), Bose factors, the sums into Q, the collision matrix, CG and
+kappa stay FP64.  Tolerances (the targets of the mixed path):
   |V3|^2      normwise relative error <= 1e-4 (Gamma-acoustic 0/0 entries excluded)
   linewidths  |Q - Q_ref| <= 1e-4 |Q_ref| + 1e-8 max|Q_ref| for every mode
   kappa       every component of the RTA and CG tensors within 1e-4 of max|kappa|
