@@ -153,10 +153,12 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
 
 // collision matrix: thread per (n1, n2, l1, l2), l2 fastest, so that the b*b
 // band block of R(q1, arm, ., .) read for one arm is contiguous across the
-// threads of a warp (one IBZ row n1 per blockIdx.y)
+// threads of a warp (one IBZ row n1 per blockIdx.y).  T = double, or float
+// for the mixed-precision pipeline (sums in double, stored rounded).
+template <class T>
 __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* mapinv, const int* arm_off,
                                  const int* arm_q, const int* arm_op, const double* opk, const double* Q,
-                                 const double* R1, const double* R2, double* CM, int ld) {
+                                 const double* R1, const double* R2, T* CM, size_t ld) {
   const int b = g.b, b2 = b * b, nkc = g.nkc;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nibz * b2) return;
@@ -193,7 +195,7 @@ __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* 
   }
   const size_t r0 = 3 * ((size_t)nl * b + l1), c0 = 3 * ((size_t)n2 * b + l2);
   for (int i = 0; i < 3; ++i)
-    for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + c0 + j] = blk[i + 3 * j];
+    for (int j = 0; j < 3; ++j) CM[(r0 + i) * ld + c0 + j] = (T)blk[i + 3 * j];
 }
 
 // ------------------------------------------------- iterative BTE (job=3)
@@ -284,31 +286,78 @@ struct CgDev {
   double bnorm;
 };
 
-// y = A x (row-major), partial[blk] = sum over the block's rows of y*x
-__global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, const double* __restrict__ A,
+// y = A x for a row-major A (leading dimension ld) of double or float, x
+// and y double; partial[blk] = the block's sum of y*x.  A warp takes
+// kGemvRows rows, so each x vector it loads serves all of them; with vec
+// (rows 16-byte aligned) A is read as 16-byte vectors, else element-wise.
+// The products are summed in double.
+constexpr int kGemvRows = 4;
+
+template <class T>
+struct Vec16;
+template <>
+struct Vec16<double> {
+  using t = double2;
+  static constexpr int w = 2;
+  __device__ static double at(const double2& v, int i) { return i == 0 ? v.x : v.y; }
+};
+template <>
+struct Vec16<float> {
+  using t = float4;
+  static constexpr int w = 4;
+  __device__ static double at(const float4& v, int i) {
+    return (double)(i == 0 ? v.x : i == 1 ? v.y : i == 2 ? v.z : v.w);
+  }
+};
+
+template <class T>
+__global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld, int vec, const T* __restrict__ A,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* partial, const CgDev* st) {
   if (st && st->done) return;
+  using V = typename Vec16<T>::t;
+  constexpr int W = Vec16<T>::w;
   __shared__ double wsum[kGemvWarps];
-  int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  int row = blockIdx.x * kGemvWarps + warp;
-  double dot = 0.0;
-  if (row < n) {
-    const double* Ar = A + (size_t)row * n;
-    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
-    int j = lane;
-    for (; j + 96 < n; j += 128) {
-      s0 += Ar[j] * x[j];
-      s1 += Ar[j + 32] * x[j + 32];
-      s2 += Ar[j + 64] * x[j + 64];
-      s3 += Ar[j + 96] * x[j + 96];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int row0 = (blockIdx.x * kGemvWarps + warp) * kGemvRows;
+  const T* Ar[kGemvRows];
+#pragma unroll
+  for (int r = 0; r < kGemvRows; ++r) Ar[r] = A + (size_t)min(row0 + r, n - 1) * ld;  // rows past n: discarded
+  double acc[kGemvRows];
+#pragma unroll
+  for (int r = 0; r < kGemvRows; ++r) acc[r] = 0.0;
+  const int nv = vec ? n / W : 0;
+  const double2* x2 = reinterpret_cast<const double2*>(x);
+#pragma unroll 2
+  for (int v = lane; v < nv; v += 32) {
+    double xv[W];
+#pragma unroll
+    for (int h = 0; h < W / 2; ++h) {
+      const double2 t2 = __ldg(x2 + (size_t)v * (W / 2) + h);
+      xv[2 * h] = t2.x;
+      xv[2 * h + 1] = t2.y;
     }
-    for (; j < n; j += 32) s0 += Ar[j] * x[j];
-    double s = (s0 + s1) + (s2 + s3);
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
-    if (lane == 0) {
-      y[row] = s;
-      dot = s * x[row];
+    V av[kGemvRows];
+#pragma unroll
+    for (int r = 0; r < kGemvRows; ++r) av[r] = __ldg(reinterpret_cast<const V*>(Ar[r]) + v);
+#pragma unroll
+    for (int r = 0; r < kGemvRows; ++r)
+#pragma unroll
+      for (int i = 0; i < W; ++i) acc[r] = fma(Vec16<T>::at(av[r], i), xv[i], acc[r]);
+  }
+  for (int j = nv * W + lane; j < n; j += 32) {
+    const double xj = x[j];
+#pragma unroll
+    for (int r = 0; r < kGemvRows; ++r) acc[r] = fma((double)Ar[r][j], xj, acc[r]);
+  }
+  double dot = 0.0;
+#pragma unroll
+  for (int r = 0; r < kGemvRows; ++r) {
+    double v = acc[r];
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (lane == 0 && row0 + r < n) {
+      y[row0 + r] = v;
+      dot += v * x[row0 + r];
     }
   }
   if (lane == 0) wsum[warp] = dot;
@@ -452,12 +501,16 @@ cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s) {
 
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
-                             const double* Q, const double* R1, const double* R2, double* CM, int ld,
+                             const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
                              cudaStream_t s) {
   const int nt = nibz * geo.b * geo.b;
   dim3 grid((nt + 127) / 128, nrows);
-  collision_kernel<<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2, CM,
-                                         ld);
+  if (cm_f32)
+    collision_kernel<float><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2,
+                                                 static_cast<float*>(CM), ld);
+  else
+    collision_kernel<double><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1,
+                                                  R2, static_cast<double*>(CM), ld);
   return cudaGetLastError();
 }
 
@@ -468,13 +521,14 @@ cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nr
 // after k iterations launches at most k + kCgChunk - 1 of them.
 constexpr int kCgChunk = 8;
 
-static cudaError_t capture_cg(int iters, int n, int nblk, const double* dA, double* dx, CgWork& w, CgDev* st,
+template <class T>
+static cudaError_t capture_cg(int iters, int n, size_t ld, int vec, int nblk, const T* dA, double* dx, CgWork& w, CgDev* st,
                               int mode, double tol, cudaStream_t s, cudaGraphExec_t* out) {
   cudaGraph_t graph = nullptr;
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
   for (int it = 0; it < iters; ++it) {
-    gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, w.conj.p, w.aux.p, w.partial.p, st);
+    gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, w.conj.p, w.aux.p, w.partial.p, st);
     cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, w.partial.p, nblk, w.grad.p, w.conj.p, w.v0.p, dx, st, mode,
                                              tol);
   }
@@ -484,9 +538,17 @@ static cudaError_t capture_cg(int iters, int n, int nblk, const double* dA, doub
   return e;
 }
 
-int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
-              double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
-  const int nblk = (n + kGemvWarps - 1) / kGemvWarps;
+template <class T>
+static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* dx, int max_iter, int mode,
+                       double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w,
+                       std::string& msg) {
+  const int rows_per_blk = kGemvWarps * kGemvRows;
+  const int nblk = (n + rows_per_blk - 1) / rows_per_blk;
+  if (ld < (size_t)n) {
+    msg = "cg: leading dimension below n";
+    return ALD_ERR_ARG;
+  }
+  const int vec = ((uintptr_t)dA & 15u) == 0 && (ld * sizeof(T)) % 16 == 0;  // rows 16-byte aligned
   if (w.grad.alloc(n) || w.conj.alloc(n) || w.aux.alloc(n) || w.v0.alloc(n) || w.partial.alloc(nblk) ||
       w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev)) ||
       (!w.h_done && cudaHostAlloc((void**)&w.h_done, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
@@ -494,10 +556,10 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
     return ALD_ERR_NOMEM;
   }
   CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
-  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, w.aux.p, nullptr, nullptr);
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr);
   cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, db, w.grad.p, w.conj.p, st);
   cudaError_t e = cudaSuccess;
-  const bool same = w.exec && w.n == n && w.max_iter == max_iter && w.mode == mode && w.tol == tol && w.A == dA &&
+  const bool same = w.exec && w.n == n && w.max_iter == max_iter && w.mode == mode && w.tol == tol && w.A == (const void*)dA && w.ld == ld &&
                     w.b == db && w.x == dx;
   const int chunk = max_iter <= 0 ? 1 : (max_iter < kCgChunk ? max_iter : kCgChunk);
   const int tail = max_iter > 0 ? max_iter % chunk : 0;
@@ -505,14 +567,16 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
     if (w.exec) cudaGraphExecDestroy(w.exec);
     if (w.exec_tail) cudaGraphExecDestroy(w.exec_tail);
     w.exec = w.exec_tail = nullptr;
-    e = capture_cg(chunk, n, nblk, dA, dx, w, st, mode, tol, s, &w.exec);
-    if (e == cudaSuccess && tail) e = capture_cg(tail, n, nblk, dA, dx, w, st, mode, tol, s, &w.exec_tail);
+    e = capture_cg<T>(chunk, n, ld, vec, nblk, dA, dx, w, st, mode, tol, s, &w.exec);
+    if (e == cudaSuccess && tail)
+      e = capture_cg<T>(tail, n, ld, vec, nblk, dA, dx, w, st, mode, tol, s, &w.exec_tail);
     if (e == cudaSuccess) {
       w.n = n;
       w.max_iter = max_iter;
       w.mode = mode;
       w.tol = tol;
       w.A = dA;
+      w.ld = ld;
       w.b = db;
       w.x = dx;
     }
@@ -531,7 +595,7 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
     msg = std::string("cg: ") + cudaGetErrorString(e);
     return ALD_ERR_CUDA;
   }
-  gemv_kernel<<<nblk, kGemvWarps * 32, 0, s>>>(n, dA, dx, w.aux.p, nullptr, nullptr);
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr);
   cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, w.aux.p, db, w.fmin.p);
   CgDev h;
   e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
@@ -544,6 +608,21 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
   *iters = h.iters;
   *err_out = h.err;
   return h.done ? ALD_OK : ALD_WARN_CG_MAXITER;
+}
+
+int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
+              double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
+  return cg_device_t<double>(n, (size_t)n, dA, db, dx, max_iter, mode, tol, iters, err_out, funcmin, s, w, msg);
+}
+
+int cg_device_ld(int n, size_t ld, const void* dA, int a_f32, const double* db, double* dx, int max_iter, int mode,
+                 double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w,
+                 std::string& msg) {
+  if (a_f32)
+    return cg_device_t<float>(n, ld, static_cast<const float*>(dA), db, dx, max_iter, mode, tol, iters, err_out,
+                              funcmin, s, w, msg);
+  return cg_device_t<double>(n, ld, static_cast<const double*>(dA), db, dx, max_iter, mode, tol, iters, err_out,
+                             funcmin, s, w, msg);
 }
 
 }  // namespace ald

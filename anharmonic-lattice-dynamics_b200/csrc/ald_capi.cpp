@@ -691,7 +691,7 @@ int ald_collision_matrix(ald_ctx* c, const int ksubset[2], const double* P1, con
   CK(launch_from_fortran5(tmp.p, p2.p, nr, nkc, b, c->stream));
   CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
   CK(launch_collision(c->geo, nibz, ksubset[0] - 1, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p,
-                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, cols, c->stream));
+                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, (size_t)cols, 0, c->stream));
   CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
   CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

@@ -290,9 +290,10 @@ cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaS
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s);
 cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s);
+// CM: double, or float when cm_f32 (mixed-precision pipeline); leading dimension ld
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
-                             const double* Q, const double* R1, const double* R2, double* CM, int ld,
+                             const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
                              cudaStream_t s);
 
 // layout conversions and the stand-alone stage kernels (ald_util.cu)
@@ -338,7 +339,8 @@ struct CgWork {
   int* h_done = nullptr;                // pinned copy of the stop flag
   int n = -1, max_iter = -1, mode = -1;
   double tol = 0;
-  const double* A = nullptr;
+  const void* A = nullptr;
+  size_t ld = 0;
   const double* b = nullptr;
   double* x = nullptr;
   ~CgWork() {
@@ -349,5 +351,10 @@ struct CgWork {
 };
 int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,
               double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg);
+// the same on a row-major A of double (a_f32 = 0) or float (a_f32 = 1) with
+// leading dimension ld (16-byte aligned rows are read as vectors)
+int cg_device_ld(int n, size_t ld, const void* dA, int a_f32, const double* db, double* dx, int max_iter, int mode,
+                 double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w,
+                 std::string& msg);
 
 }  // namespace ald

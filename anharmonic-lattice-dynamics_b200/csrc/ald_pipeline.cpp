@@ -288,11 +288,16 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     res->d2h_bytes = d2h;
     return ALD_OK;
   }
-  // ---- 5: collision matrix (row-major, all IBZ rows)
-  ALD_CKA(cm.alloc(N * N));
+  // ---- 5: collision matrix (row-major, all IBZ rows; rows padded to 16
+  // bytes).  The mixed-precision pipeline stores it in FP32: CG streams it
+  // once per iteration, and the products are still summed in FP64.
+  const int cm_f32 = c->opt.precision != ALD_FP64;
+  const size_t ld = cm_f32 ? (N + 3) / 4 * 4 : (N + 1) / 2 * 2;
+  const size_t cm_bytes = N * ld * (cm_f32 ? sizeof(float) : sizeof(double));
+  ALD_CKA(cm.alloc((cm_bytes + sizeof(double) - 1) / sizeof(double)));
   ALD_CK(tm.begin(5));
   ALD_CK(launch_collision(c->geo, nibz, 0, nibz, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, dQ,
-                          R1.p, R2.p, cm.p, (int)N, s));
+                          R1.p, R2.p, cm.p, ld, cm_f32, s));
   res->launches[5] += 1;
   ALD_CK(tm.end());
   // ---- 6: RHS and the initial guess x0 = F_RTA (kappa.f90:835-843)
@@ -307,8 +312,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   std::string msg;
   double tol = c->opt.cg_stop == ALD_CG_REFERENCE ? 1.0 / std::pow(10.0, 2 * c->opt.cg_ndig) : c->opt.cg_tol;
   ALD_CK(tm.begin(7));
-  int rc = cg_device((int)N, cm.p, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters, &cg_err, &fm, s,
-                     c->cg, msg);
+  int rc = cg_device_ld((int)N, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters,
+                        &cg_err, &fm, s, c->cg, msg);
   if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
   res->launches[7] += 4 + 2 * c->opt.cg_max_iter;
   ALD_CK(tm.end());
