@@ -287,10 +287,11 @@ struct CgDev {
 };
 
 // y = A x for a row-major A (leading dimension ld) of double or float, x
-// and y double; partial[blk] = the block's sum of y*x.  A warp takes
-// kGemvRows rows, so each x vector it loads serves all of them; with vec
-// (rows 16-byte aligned) A is read as 16-byte vectors, else element-wise.
-// The products are summed in double.
+// and y double; partial[blk] = the block's sum of y*x.  A block takes
+// kGemvRows rows; its warps split the columns, so each x vector a warp
+// loads serves all the rows, and small matrices still give n/kGemvRows
+// blocks.  With vec (rows 16-byte aligned) A is read as 16-byte vectors,
+// else element-wise.  The products are summed in double.
 constexpr int kGemvRows = 4;
 
 template <class T>
@@ -317,19 +318,22 @@ __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld,
   if (st && st->done) return;
   using V = typename Vec16<T>::t;
   constexpr int W = Vec16<T>::w;
-  __shared__ double wsum[kGemvWarps];
+  __shared__ double red[kGemvWarps][kGemvRows];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int row0 = (blockIdx.x * kGemvWarps + warp) * kGemvRows;
+  const int row0 = blockIdx.x * kGemvRows;
   const T* Ar[kGemvRows];
 #pragma unroll
   for (int r = 0; r < kGemvRows; ++r) Ar[r] = A + (size_t)min(row0 + r, n - 1) * ld;  // rows past n: discarded
   double acc[kGemvRows];
 #pragma unroll
   for (int r = 0; r < kGemvRows; ++r) acc[r] = 0.0;
+  // this warp's slice of the vectors [v0, v1), then of the scalar tail
   const int nv = vec ? n / W : 0;
+  const int per = (nv + kGemvWarps - 1) / kGemvWarps;
+  const int v0 = warp * per, v1 = min(nv, v0 + per);
   const double2* x2 = reinterpret_cast<const double2*>(x);
 #pragma unroll 2
-  for (int v = lane; v < nv; v += 32) {
+  for (int v = v0 + lane; v < v1; v += 32) {
     double xv[W];
 #pragma unroll
     for (int h = 0; h < W / 2; ++h) {
@@ -345,27 +349,27 @@ __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld,
 #pragma unroll
       for (int i = 0; i < W; ++i) acc[r] = fma(Vec16<T>::at(av[r], i), xv[i], acc[r]);
   }
-  for (int j = nv * W + lane; j < n; j += 32) {
+  for (int j = nv * W + warp * 32 + lane; j < n; j += 32 * kGemvWarps) {
     const double xj = x[j];
 #pragma unroll
     for (int r = 0; r < kGemvRows; ++r) acc[r] = fma((double)Ar[r][j], xj, acc[r]);
   }
-  double dot = 0.0;
 #pragma unroll
   for (int r = 0; r < kGemvRows; ++r) {
     double v = acc[r];
     for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    if (lane == 0 && row0 + r < n) {
-      y[row0 + r] = v;
-      dot += v * x[row0 + r];
-    }
+    if (lane == 0) red[warp][r] = v;
   }
-  if (lane == 0) wsum[warp] = dot;
   __syncthreads();
-  if (threadIdx.x == 0 && partial) {
-    double t = 0;
-    for (int w = 0; w < kGemvWarps; ++w) t += wsum[w];
-    partial[blockIdx.x] = t;
+  if (threadIdx.x == 0) {
+    double dot = 0.0;
+    for (int r = 0; r < kGemvRows && row0 + r < n; ++r) {
+      double t = 0.0;
+      for (int w = 0; w < kGemvWarps; ++w) t += red[w][r];
+      y[row0 + r] = t;
+      dot += t * x[row0 + r];
+    }
+    if (partial) partial[blockIdx.x] = dot;
   }
 }
 
@@ -542,8 +546,7 @@ template <class T>
 static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* dx, int max_iter, int mode,
                        double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w,
                        std::string& msg) {
-  const int rows_per_blk = kGemvWarps * kGemvRows;
-  const int nblk = (n + rows_per_blk - 1) / rows_per_blk;
+  const int nblk = (n + kGemvRows - 1) / kGemvRows;
   if (ld < (size_t)n) {
     msg = "cg: leading dimension below n";
     return ALD_ERR_ARG;
