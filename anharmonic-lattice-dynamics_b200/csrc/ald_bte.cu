@@ -618,6 +618,16 @@ int cg_device(int n, const double* dA, const double* db, double* dx, int max_ite
   return cg_device_t<double>(n, (size_t)n, dA, db, dx, max_iter, mode, tol, iters, err_out, funcmin, s, w, msg);
 }
 
+int cg_launched_iterations(int iters, int max_iter) {
+  if (max_iter <= 0) return 0;
+  const int chunk = max_iter < kCgChunk ? max_iter : kCgChunk;
+  const int full = max_iter / chunk, tail = max_iter % chunk;
+  const int nfull = std::min(full, (iters + chunk - 1) / chunk);
+  int n = nfull * chunk;
+  if (nfull == full && tail && iters > full * chunk) n += tail;
+  return std::max(n, std::min(iters, max_iter));
+}
+
 int cg_device_ld(int n, size_t ld, const void* dA, int a_f32, const double* db, double* dx, int max_iter, int mode,
                  double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w,
                  std::string& msg) {

@@ -85,6 +85,9 @@ int ensure_phonons(ald_ctx* c) {
   a.fc2_atom = c->fc2_atom.p;
   a.fc2_val = c->fc2_val.p;
   a.fc2_sqm = c->fc2_sqm.p;
+  a.fc2_uatom = c->fc2_uatom.p;
+  a.fc2_uidx = c->fc2_uidx.p;
+  a.nuniq = (int)c->F2.uatom.size();
   a.rr = c->rr.p;
   a.born_flag = c->S.born_flag;
   a.born = c->born.p;
@@ -147,7 +150,8 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
   return a;
 }
 
-int run_v3(ald_ctx* c, const V3Args& a0) {
+int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
+  int nl = 0;
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
   if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "V3: more than 12 bands is not supported by this build");
   const int prec = c->opt.precision;
@@ -162,22 +166,27 @@ int run_v3(ald_ctx* c, const V3Args& a0) {
       e = launch_v3_tc_ptiles(a, c->w_ptiles.p, c->stream);
       if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 phase tiles: ") + cudaGetErrorString(e));
       c->ptiles_ok = true;
+      nl += 1;
     }
     const size_t bneed = v3_tc_btile_bytes(a.nrows, c->VC.ncls, c->geo.nkc);
     if (c->w_btiles.n < bneed) CKA(c->w_btiles.alloc(bneed));
     e = launch_v3_rows_f32(a, c->stream);
     if (e == cudaSuccess) e = launch_v3_tc(a, c->w_ptiles.p, c->w_btiles.p, c->stream);
+    nl += 4;  // class sums H, mode factors, B tiles, the MMA kernel
   } else if (v3_pair_supported(c->geo.b, prec)) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
     e = launch_v3_pair(a, prec, c->stream);
+    nl += 2;
   } else if (prec == ALD_FP64 && a.v3_layout == 0) {
     e = launch_v3_fp64(a, c->stream);
+    nl += 1;
   } else {
     return fail(ALD_ERR_UNSUPPORTED, "V3: the mixed-precision path and the slice-major layout support 3 or 6 bands");
   }
   if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 launch: ") + cudaGetErrorString(e));
+  if (nlaunch) *nlaunch += nl;
   return ALD_OK;
 }
 
@@ -292,6 +301,8 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   CKA(upload(c->fc2_atom, c->F2.atom, s));
   CKA(upload(c->fc2_val, c->F2.val, s));
   CKA(upload(c->fc2_sqm, c->F2.sqm, s));
+  CKA(upload(c->fc2_uatom, c->F2.uatom, s));
+  CKA(upload(c->fc2_uidx, c->F2.uidx, s));
   {
     // epsil(9), charge(9*nat0), masses(nat0), eps_scale, rho2, om0
     std::vector<double> bo(9 + 10 * c->S.nat0 + 4, 0.0);
@@ -513,7 +524,7 @@ int ald_calculate_w3_ibz_split_sq(ald_ctx* c, const int ksubset[2], double* v33s
   DevBuf<double> v, f;
   CKA(v.alloc(n));
   CKA(f.alloc(n));
-  r = run_v3(c, v3_args(c, ksubset[0] - 1, nr, v.p));
+  r = run_v3(c, v3_args(c, ksubset[0] - 1, nr, v.p), nullptr);
   if (r) return r;
   CK(launch_to_fortran5(v.p, f.p, nr, c->T.nkc, c->geo.b, c->stream));
   CK(cudaMemcpyAsync(v33s8, f.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

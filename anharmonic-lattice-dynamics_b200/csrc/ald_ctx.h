@@ -21,6 +21,7 @@ struct ald_ctx {
   Geometry geo;
   // device tables
   DevBuf<double> kpc32, rr, fc2_val, fc2_sqm, born, fc3w, roots, opk, opk_inv;
+  DevBuf<int> fc2_uatom, fc2_uidx;
   DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,
       arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
   DevBuf<int> cls_grp_off, cls_pc, cls_trip_off, cls_trip, cls_trip_i0, cls_trip_k;
@@ -48,7 +49,8 @@ int check_err_flags(ald_ctx* c);
 int ensure_phonons(ald_ctx* c);
 int ensure_dist(ald_ctx* c, double tempk);
 V3Args v3_args(ald_ctx* c, int first, int nrows, double* out);
-int run_v3(ald_ctx* c, const V3Args& a);
+// nlaunch (optional) += the kernels launched
+int run_v3(ald_ctx* c, const V3Args& a, int* nlaunch);
 KappaArgs kappa_args(ald_ctx* c, double tempk);
 int delta_mode(ald_ctx* c);
 double gauss_width(ald_ctx* c);

@@ -836,6 +836,12 @@ std::string build_fc2(const System& S, Fc2Csr& F) {
       F.sqm[F.off[e] + s] = std::sqrt(S.mass0[i0] * S.mass0[j0]);
     }
   }
+  F.uatom = F.atom;
+  std::sort(F.uatom.begin(), F.uatom.end());
+  F.uatom.erase(std::unique(F.uatom.begin(), F.uatom.end()), F.uatom.end());
+  F.uidx.resize(F.atom.size());
+  for (size_t t = 0; t < F.atom.size(); ++t)
+    F.uidx[t] = (int)(std::lower_bound(F.uatom.begin(), F.uatom.end(), F.atom[t]) - F.uatom.begin());
   return "";
 }
 

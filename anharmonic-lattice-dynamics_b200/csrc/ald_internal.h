@@ -130,6 +130,8 @@ struct Fc2Csr {
   std::vector<int> atom;           // supercell atom j (0-based)
   std::vector<double> val;         // fcs_2
   std::vector<double> sqm;         // sqrt(mi*mj)
+  std::vector<int> uatom;          // the distinct atoms of `atom`, ascending (one phase each per q)
+  std::vector<int> uidx;           // per term: index of its atom in uatom
 };
 std::string build_fc2(const System& S, Fc2Csr& F);
 
@@ -171,6 +173,9 @@ struct PhononArgs {
   const int* fc2_atom;
   const double* fc2_val;
   const double* fc2_sqm;
+  const int* fc2_uatom;      // nuniq distinct atoms of fc2_atom
+  const int* fc2_uidx;       // per term: index into fc2_uatom
+  int nuniq;
   const double* rr;          // 3*natoms: atompos(j) - atompos(j0)
   int born_flag;
   const double* born;        // epsil(9), charge(9*nat0), masses(nat0), scalars(4): eps_scale, rho2, om0, pad
@@ -351,6 +356,9 @@ struct CgWork {
 };
 int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,
               double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg);
+// CG iterations whose kernels were launched for a solve that stopped after
+// iters (the captured chunks run to their end, as no-ops after the stop)
+int cg_launched_iterations(int iters, int max_iter);
 // the same on a row-major A of double (a_f32 = 0) or float (a_f32 = 1) with
 // leading dimension ld (16-byte aligned rows are read as vectors)
 int cg_device_ld(int n, size_t ld, const void* dA, int a_f32, const double* db, double* dx, int max_iter, int mode,

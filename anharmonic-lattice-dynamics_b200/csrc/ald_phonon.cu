@@ -297,6 +297,268 @@ __global__ void __launch_bounds__(kThreads) phonon_kernel(PhononArgs a) {
   }
 }
 
+// ------------------------------------------------------------------
+// Small cells (b <= 12): one warp per matrix, kPhWarps matrices per CTA,
+// synchronised with __syncwarp only.  The same arithmetic as phonon_kernel
+// element by element (FC2 sum in the file's term order, hermitisation,
+// dipole term, cyclic Jacobi rounds, sorts); the q.R phase of every distinct
+// FC2 atom is evaluated once per matrix instead of once per matrix element,
+// and the sweep's off-diagonal and diagonal norms are warp sums.  Each term
+// keeps the reference's (f cos)/sqrt(m m) rounding: the acoustic modes at
+// Gamma are rounding residues of these sums, and a sum rounded differently
+// can reach exactly zero.
+constexpr int kPhWarps = 4;
+constexpr int kPhBMax = 12;
+
+__device__ __forceinline__ double warp_sum(double v) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+__global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a, int nmat) {
+  extern __shared__ double2 smem[];
+  __shared__ double4 s_rot[kPhWarps][kPhBMax / 2];
+  __shared__ double2 s_nd[kPhWarps][kPhBMax / 2];
+  __shared__ int s_act[kPhWarps][kPhBMax / 2];
+  __shared__ int s_perm[kPhWarps][kPhBMax];
+  __shared__ double s_lam[kPhWarps][kPhBMax], s_lab[kPhWarps][kPhBMax];
+  __shared__ int s_ord[kPhWarps][kPhBMax], s_ord2[kPhWarps][kPhBMax];
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int m = blockIdx.x * kPhWarps + warp;
+  if (m >= nmat) return;  // whole warp; nothing below synchronises the CTA
+  const int b = a.geo.b, bb = b * b;
+  const int pt = m / 7, d = m % 7;
+  double2* A = smem + (size_t)warp * (2 * bb + a.nuniq);
+  double2* V = A + bb;
+  double2* ph = V + bb;
+  double4* rot = s_rot[warp];
+  double2* newdiag = s_nd[warp];
+  int* active = s_act[warp];
+  int* perm = s_perm[warp];
+
+  double q[3] = {a.kpc32[3 * pt], a.kpc32[3 * pt + 1], a.kpc32[3 * pt + 2]};
+  if (d > 0) {
+    int ax = (d - 1) / 2;
+    q[ax] = (d & 1) ? q[ax] + a.dq : q[ax] - a.dq;
+  }
+  // ------------------------------------------- phases, then the FC2 sum
+  for (int u = lane; u < a.nuniq; u += 32) {
+    const double* rr = a.rr + 3 * a.fc2_uatom[u];
+    double x = q[0] * rr[0] + q[1] * rr[1] + q[2] * rr[2];
+    double sn, cs;
+    sincos(x, &sn, &cs);
+    ph[u] = make_double2(cs, sn);
+  }
+  __syncwarp();
+  for (int e = lane; e < bb; e += 32) {
+    double2 acc = make_double2(0.0, 0.0);
+    for (int t = a.fc2_off[e]; t < a.fc2_off[e + 1]; ++t) {
+      const double2 p = ph[a.fc2_uidx[t]];
+      double f = a.fc2_val[t], sq = a.fc2_sqm[t];
+      acc.x += (f * p.x) / sq;
+      acc.y += (f * p.y) / sq;
+    }
+    A[e] = acc;
+  }
+  __syncwarp();
+  // ------------------------------------------ hermitisation (rest.f90:513-544)
+  for (int t = lane; t < b; t += 32) {
+    double2 v = A[t * b + t];
+    if (fabs(v.y) > 9e-4 * fabs(v.x)) A[t * b + t] = make_double2(v.x, 0.0);
+  }
+  __syncwarp();
+  for (int e = lane; e < bb; e += 32) {
+    int t = e / b, j = e % b;
+    if (j > t && j <= b - 2) {
+      double2 u = A[t * b + j], l = A[j * b + t];
+      double mi = (u.y - l.y) / 2, mj = (u.x + l.x) / 2;
+      A[t * b + j] = make_double2(mj, mi);
+      A[j * b + t] = make_double2(mj, -mi);
+    }
+  }
+  __syncwarp();
+  double sim = 0, sre = 0;
+  for (int e = lane; e < bb; e += 32) {
+    sim += fabs(A[e].y);
+    sre += fabs(A[e].x);
+  }
+  sim = warp_sum(sim) / bb;
+  sre = warp_sum(sre) / bb;
+  if (sim < sre * 1e-10)
+    for (int e = lane; e < bb; e += 32) A[e].y = 0.0;
+  __syncwarp();
+  // --------------------------------------------------- dipole term (nonanal)
+  if (a.born_flag != 0) {
+    int nat0 = a.geo.nat0;
+    const double* eps = a.born;
+    const double* chg = a.born + 9;
+    const double* mass = a.born + 9 + 9 * nat0;
+    const double* sc = a.born + 9 + 10 * nat0;  // eps_scale, rho2, om0
+    double kh[3] = {q[0], q[1], q[2]};
+    if (q[0] == 0.0 && q[1] == 0.0 && q[2] == 0.0) kh[0] = kh[1] = kh[2] = 1.0e-10;
+    double qeq = (kh[0] * (eps[0] * kh[0] + eps[3] * kh[1] + eps[6] * kh[2]) +
+                  kh[1] * (eps[1] * kh[0] + eps[4] * kh[1] + eps[7] * kh[2]) +
+                  kh[2] * (eps[2] * kh[0] + eps[5] * kh[1] + eps[8] * kh[2]));
+    double q2 = kh[0] * kh[0] + kh[1] * kh[1] + kh[2] * kh[2];
+    double ex = exp(-q2 / sc[1]);
+    for (int e = lane; e < bb; e += 32) {
+      int r = e / b, c = e % b;
+      int na = r / 3, i = r % 3, nb = c / 3, j = c % 3;
+      const double* za = chg + 9 * na;
+      const double* zb = chg + 9 * nb;
+      double zag = kh[0] * za[0 + 3 * i] + kh[1] * za[1 + 3 * i] + kh[2] * za[2 + 3 * i];
+      double zbg = kh[0] * zb[0 + 3 * j] + kh[1] * zb[1 + 3 * j] + kh[2] * zb[2 + 3 * j];
+      A[e].x += zag * zbg / (qeq * sc[0]) / sc[2] / sqrt(mass[na] * mass[nb]) * ex;
+    }
+    __syncwarp();
+  }
+  // --------------------- Hermitian matrix of the upper triangle (ZHEEV 'U')
+  for (int e = lane; e < bb; e += 32)
+    if (e / b == e % b) A[e].y = 0.0;
+  __syncwarp();
+  for (int e = lane; e < bb; e += 32) {
+    int i = e / b, j = e % b;
+    if (i > j) A[e] = cconj(A[j * b + i]);
+  }
+  if (d == 0)
+    for (int e = lane; e < bb; e += 32) V[e] = make_double2((e / b) == (e % b) ? 1.0 : 0.0, 0.0);
+  __syncwarp();
+  // ------------------------------------------------ parallel cyclic Jacobi
+  const int n2 = b + (b & 1);
+  const int npair = n2 / 2;
+  for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
+    double off = 0, dia = 0;
+    for (int e = lane; e < bb; e += 32) {
+      double m2 = A[e].x * A[e].x + A[e].y * A[e].y;
+      if (e / b == e % b) dia += m2;
+      else off += m2;
+    }
+    off = warp_sum(off);
+    dia = warp_sum(dia);
+    if (off == 0.0 || off <= 1e-32 * dia) break;  // warp-uniform
+    for (int r = 0; r < n2 - 1; ++r) {
+      if (lane < npair) {
+        const int k = lane;
+        int p, qq;
+        rr_pair(r, k, n2, p, qq);
+        int act = 0;
+        double4 R = make_double4(1, 0, 1, 0);
+        double2 nd = make_double2(0, 0);
+        if (qq < b) {
+          double app = A[p * b + p].x, aqq = A[qq * b + qq].x;
+          double2 apq = A[p * b + qq];
+          double mag = hypot(apq.x, apq.y);
+          if (mag > 0.0 && mag > 1e-300) {
+            double wx = apq.x / mag, wy = apq.y / mag;
+            double th = (aqq - app) / (2 * mag);
+            double t = (th >= 0 ? 1.0 : -1.0) / (fabs(th) + sqrt(th * th + 1));
+            double c = 1 / sqrt(t * t + 1), s = t * c;
+            R = make_double4(c, s, wx, wy);
+            nd = make_double2(app - t * mag, aqq + t * mag);
+            act = 1;
+          }
+        }
+        perm[2 * k] = p;
+        perm[2 * k + 1] = qq;
+        rot[k] = R;
+        newdiag[k] = nd;
+        active[k] = act;
+      }
+      __syncwarp();
+      // columns: A <- A J, V <- V J
+      for (int e = lane; e < npair * b; e += 32) {
+        int k = e / b, i = e % b;
+        if (!active[k]) continue;
+        int p = perm[2 * k], qq = perm[2 * k + 1];
+        double4 R = rot[k];
+        double2 wb = make_double2(R.z, -R.w);  // conj(w)
+        double2 aip = A[i * b + p], aiq = A[i * b + qq];
+        double2 t1 = cmul(wb, aiq);
+        A[i * b + p] = make_double2(R.x * aip.x - R.y * t1.x, R.x * aip.y - R.y * t1.y);
+        A[i * b + qq] = make_double2(R.y * aip.x + R.x * t1.x, R.y * aip.y + R.x * t1.y);
+        if (d == 0) {
+          double2 vip = V[i * b + p], viq = V[i * b + qq];
+          double2 t2 = cmul(wb, viq);
+          V[i * b + p] = make_double2(R.x * vip.x - R.y * t2.x, R.x * vip.y - R.y * t2.y);
+          V[i * b + qq] = make_double2(R.y * vip.x + R.x * t2.x, R.y * vip.y + R.x * t2.y);
+        }
+      }
+      __syncwarp();
+      // rows: A <- J^H A
+      for (int e = lane; e < npair * b; e += 32) {
+        int k = e / b, j = e % b;
+        if (!active[k]) continue;
+        int p = perm[2 * k], qq = perm[2 * k + 1];
+        double4 R = rot[k];
+        double2 w = make_double2(R.z, R.w);
+        double2 apj = A[p * b + j], aqj = A[qq * b + j];
+        double2 t1 = cmul(w, aqj);
+        A[p * b + j] = make_double2(R.x * apj.x - R.y * t1.x, R.x * apj.y - R.y * t1.y);
+        A[qq * b + j] = make_double2(R.y * apj.x + R.x * t1.x, R.y * apj.y + R.x * t1.y);
+      }
+      __syncwarp();
+      if (lane < npair && active[lane]) {
+        const int k = lane;
+        int p = perm[2 * k], qq = perm[2 * k + 1];
+        A[p * b + p] = make_double2(newdiag[k].x, 0.0);
+        A[qq * b + qq] = make_double2(newdiag[k].y, 0.0);
+        A[p * b + qq] = make_double2(0.0, 0.0);
+        A[qq * b + p] = make_double2(0.0, 0.0);
+      }
+      __syncwarp();
+    }
+  }
+  // ---------------------------------------------------------- ordering
+  double* lam = s_lam[warp];
+  double* lab = s_lab[warp];
+  int* ord = s_ord[warp];
+  int* ord2 = s_ord2[warp];
+  if (lane == 0) {
+    for (int i = 0; i < b; ++i) {
+      lam[i] = A[i * b + i].x;
+      ord[i] = i;
+    }
+    for (int i = 0; i < b; ++i)  // exchange sort of extratools.f90:154-175
+      for (int j = i + 1; j < b; ++j)
+        if (lam[ord[i]] > lam[ord[j]]) {
+          int t = ord[i];
+          ord[i] = ord[j];
+          ord[j] = t;
+        }
+    for (int i = 0; i < b; ++i) {
+      lab[i] = fabs(lam[ord[i]]);
+      ord2[i] = i;
+    }
+    for (int i = 0; i < b; ++i)
+      for (int j = i + 1; j < b; ++j)
+        if (lab[ord2[i]] > lab[ord2[j]]) {
+          int t = ord2[i];
+          ord2[i] = ord2[j];
+          ord2[j] = t;
+        }
+  }
+  __syncwarp();
+  for (int i = lane; i < b; i += 32) a.w2_all[((size_t)pt * 7 + d) * b + i] = lab[i];
+  if (d == 0) {
+    for (int l = 0; l < b; ++l) {
+      int col = ord[ord2[l]];
+      double sre2 = 0;
+      for (int c = lane; c < b; c += 32) sre2 += fabs(V[c * b + col].x);
+      sre2 = warp_sum(sre2);
+      bool rot90 = sre2 < 1e-3;
+      for (int c = lane; c < b; c += 32) {
+        double2 v = V[c * b + col];
+        if (rot90) v = make_double2(-v.y, v.x);
+        size_t o = (((size_t)pt * b + l) * b + c) * 2;
+        a.evec[o] = v.x;
+        a.evec[o + 1] = v.y;
+      }
+    }
+    for (int l = lane; l < b; l += 32) a.w2[(size_t)pt * b + l] = lab[ord2[l]];
+  }
+}
+
 // finite differences use the get_freq order (before the second sort)
 __global__ void phonon_post_kernel(Geometry geo, const double* w2_all, double dq, double cnst, double* vel) {
   int b = geo.b;
@@ -352,6 +614,16 @@ __global__ void freq_dist_kernel(Geometry geo, const double* w2, double cnst, do
 
 cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
   int b = a.geo.b;
+  const size_t smw = (size_t)kPhWarps * (2 * (size_t)b * b + a.nuniq) * sizeof(double2);
+  if (b <= kPhBMax && smw <= 160 * 1024) {
+    if (smw > 48 * 1024) {
+      cudaError_t e = cudaFuncSetAttribute(phonon_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
+      if (e != cudaSuccess) return e;
+    }
+    const int nmat = a.geo.nkc * 7;
+    phonon_warp_kernel<<<(nmat + kPhWarps - 1) / kPhWarps, kPhWarps * 32, smw, s>>>(a, nmat);
+    return cudaGetLastError();
+  }
   size_t sm = 2 * (size_t)b * b * sizeof(double2);
   if (b > 64) return cudaErrorInvalidValue;
   if (sm > 48 * 1024) {

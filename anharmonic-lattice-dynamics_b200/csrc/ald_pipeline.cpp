@@ -136,9 +136,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     ALD_CK(tm.begin(1));
     V3Args va = v3_args(c, r0, nr, v3.p);
     va.v3_layout = v3_layout;
-    r = run_v3(c, va);
+    r = run_v3(c, va, &res->launches[1]);
     if (r) return r;
-    res->launches[1] += 1;
     ALD_CK(tm.end());
     CombineArgs a;
     a.geo = c->geo;
@@ -315,7 +314,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   int rc = cg_device_ld((int)N, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters,
                         &cg_err, &fm, s, c->cg, msg);
   if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
-  res->launches[7] += 4 + 2 * c->opt.cg_max_iter;
+  res->launches[7] += 4 + 2 * cg_launched_iterations(iters, c->opt.cg_max_iter);
   ALD_CK(tm.end());
   // ---- 8: mode_kappa_d
   ALD_CK(tm.begin(8));

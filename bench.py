@@ -43,7 +43,13 @@ sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "V3 triplet-bands/s & time-to-κ: mixed vs FP64 GPU path, 1 B200, κ err≤1e-4"
 UNIT = "triplet-bands/s"
-WORKLOAD = "rocksalt-Morse NaCl-type, 2 atoms (6 bands), 16x16x16 q-mesh, tetrahedron delta, T=300 K"
+# --workload: the benchmark suite's configuration 1 (the metric's own) or
+# configuration 2 (the large single structure); mesh edge, description
+WORKLOADS = {
+    "rocksalt": (16, "rocksalt-Morse NaCl-type, 2 atoms (6 bands), %dx%dx%d q-mesh, tetrahedron delta, T=300 K"),
+    "lj-argon": (32, "fcc LJ argon, 1 atom (3 bands), %dx%dx%d q-mesh, Gaussian 0.05 THz, CG to residual 1e-8, "
+                     "T=300 K"),
+}
 
 
 def _peaks():
@@ -106,16 +112,25 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def make_workload(d: str, mesh=(16, 16, 16)):
+def make_workload(d: str, mesh=(16, 16, 16), workload: str = "rocksalt"):
     from ald import inputs as I
-    st, rp = I.config(1, mesh=mesh)
+    st, rp = I.config(1 if workload == "rocksalt" else 2, mesh=mesh)
     I.write_inputs(st, rp, d)
     return rp
 
 
-def cpu_baseline(d: str, rows: int = 0):
+def workload_options(ald, rp, workload: str, **kw):
+    """Library options of a workload: configuration 1 runs the defaults (tetrahedron delta, the
+    reference's CG stop rule); configuration 2 the Gaussian delta and CG to a residual."""
+    if workload == "rocksalt":
+        return ald.default_options(**kw)
+    return ald.default_options(delta=ald.DELTA_GAUSS, cg_stop=ald.CG_RESIDUAL, cg_tol=rp.cg_tol,
+                               width_cm=rp.width_cm, **kw)
+
+
+def cpu_baseline(d: str, rows: int = 0, gauss: bool = False):
     """The oracle (literal CPU restatement of the reference) on a bounded sample of IBZ rows:
-    V3 + tetrahedron FGR + tauRTA for `rows` rows, all host threads."""
+    V3 + tetrahedron (or Gaussian) FGR + tauRTA for `rows` rows, all host threads."""
     import oracle_py
     oracle_py.build()
     nthreads = os.cpu_count() or 1
@@ -128,18 +143,19 @@ def cpu_baseline(d: str, rows: int = 0):
     rows = rows or min(O.nibz, nthreads)
     t0 = time.time()
     v33 = O.v3(1, rows)
-    P1, P2 = O.fgr(1, rows, v33)
+    P1, P2 = O.fgr(1, rows, v33, gauss=gauss)
     O.distribution(300.0)
     O.tau(1, rows, 300.0, P1, P2, want_p=False)
     dt = time.time() - t0
     tb = rows * O.nkc * O.ndyn ** 3
     return {"value": tb / dt, "unit": UNIT, "cores": nthreads, "kind": "port",
-            "sample": "%d of %d IBZ rows of the same workload: V3 + tetrahedron FGR + tauRTA (%.1f s); "
-                      "mesh/IBZ/phonon setup %.1f s not counted" % (rows, O.nibz, dt, t_setup),
+            "sample": "%d of %d IBZ rows of the same workload: V3 + %s FGR + tauRTA (%.1f s); "
+                      "mesh/IBZ/phonon setup %.1f s not counted" % (rows, O.nibz, "Gaussian" if gauss else
+                                                                    "tetrahedron", dt, t_setup),
             "seconds": dt}
 
 
-def roofline(stage_ms, launches, nibz, nkc, b, peaks):
+def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8):
     """Dominant device stage and its achieved HBM bandwidth from algorithmic bytes."""
     stages = {k: v for k, v in stage_ms.items() if k != "total"}
     dom = max(stages, key=stages.get)
@@ -151,13 +167,13 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks):
     per = {
         "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n,            # |V3|^2 out + e(q2), e(q3) in
         "delta": nibz * nkc * (b3 * 8 + 2 * b * b * 8 * 2) / n,      # |V3|^2 in + R1/R2 out (read+write)
-        "collision": N * N * 8 / n,                                  # CM written once
+        "collision": N * N * cm_bytes / n,                           # CM written once
         "cg": None,
     }
     bytes_ = per.get(dom)
     if dom == "cg":
-        bytes_ = N * N * 8  # one matrix-vector product streams the matrix
-        ms = stages[dom] / max(1, (launches.get("cg", 2) - 4) // 2)
+        bytes_ = N * N * cm_bytes  # one matrix-vector product streams the matrix (per iteration)
+        ms = stages[dom] / max(1, cg_iters)
     if bytes_ is None or ms <= 0:
         return {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
                 "traffic": None, "kernel": dom}
@@ -182,30 +198,35 @@ def main():
     ap.add_argument("--impl", default="ald", choices=["ald", "reference"])
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: time the FP64 and the mixed path; the line's value is the mixed path's")
-    ap.add_argument("--mesh", type=int, default=16)
+    ap.add_argument("--workload", default="rocksalt", choices=sorted(WORKLOADS),
+                    help="rocksalt: the metric's configuration (default); lj-argon: the large single structure")
+    ap.add_argument("--mesh", type=int, default=0, help="mesh edge (default: the workload's own)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
-    mesh = (args.mesh,) * 3
+    mesh = (args.mesh or WORKLOADS[args.workload][0],) * 3
+    workload_desc = WORKLOADS[args.workload][1] % mesh
 
     if args.impl == "reference":
         if rank != 0:
             return
         with tempfile.TemporaryDirectory() as d:
-            make_workload(d, mesh)
+            make_workload(d, mesh, args.workload)
             vals = []
             cb = None
             for _ in range(args.warmup + args.steps):
-                cb = cpu_baseline(d)
+                cb = cpu_baseline(d, gauss=args.workload == "lj-argon")
                 vals.append(cb["value"])
             v = sorted(vals[args.warmup:])[len(vals[args.warmup:]) // 2] if args.steps else vals[-1]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic (analytic Morse FC2/FC3, reference file formats)",
-                "config": {"workload": WORKLOAD, "mesh": list(mesh)},
+                "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic (analytic %s FC2/FC3, reference file formats)" % (
+                    "Morse" if args.workload == "rocksalt" else "Lennard-Jones"),
+                "config": {"workload": workload_desc, "mesh": list(mesh)},
                 "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -226,12 +247,12 @@ def main():
     torch.cuda.set_device(dev)
     tmp = tempfile.TemporaryDirectory()
     d = tmp.name
-    make_workload(d, mesh)
+    rp = make_workload(d, mesh, args.workload)
     stream = torch.cuda.Stream(device=dev)
 
     def timed_path(precision):
         """K timed steps of one precision path on a context whose tables are in HBM."""
-        opts = ald.default_options(device=dev, precision=precision)
+        opts = workload_options(ald, rp, args.workload, device=dev, precision=precision)
         ctx = ald.Context(d, opts)
         ctx.set_stream(stream.cuda_stream)
         tempk = ctx.info.tempk
@@ -316,24 +337,28 @@ def main():
     line = None
     if rank == 0:
         peaks = _peaks()
-        rf = roofline(per_step, per_launch_counts, nibz, nkc, b, peaks)
+        mixed_head = precisions[-1] == ald.MIXED
+        rf = roofline(per_step, per_launch_counts, nibz, nkc, b, peaks, cg_iters=max(1, out["cg_iters"]),
+                      cm_bytes=4 if mixed_head else 8)
         cb = None
         if world == 1 and not args.no_cpu_baseline:
             try:
-                cb = cpu_baseline(d)
+                cb = cpu_baseline(d, gauss=args.workload == "lj-argon")
                 cb = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
             except Exception as ex:  # the baseline is reported, never required
                 cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % ex}
-        mixed_head = precisions[-1] == ald.MIXED
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
                 "scaling": "weak", "vs_baseline": None,
-                "dtype": "mixed: f32 V3 contraction, f64 elsewhere" if mixed_head else "f64",
-                "data": "synthetic (analytic Morse FC2/FC3 written in the reference's file formats)",
-                "config": {"workload": WORKLOAD, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
+                "dtype": ("mixed: V3 class sums split-f16 on tensor cores (3 bands) or f32, mode products, delta "
+                          "weights and CG matrix f32; eigensolve, sums, CG vectors and kappa f64")
+                if mixed_head else "f64",
+                "data": "synthetic (analytic %s FC2/FC3 written in the reference's file formats)" % (
+                    "Morse" if args.workload == "rocksalt" else "Lennard-Jones"),
+                "config": {"workload": workload_desc, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
                            "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
                            "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
-                               2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * 8 / 1e6),
+                               2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * (4 if mixed_head else 8) / 1e6),
                            "parallelism": "replicas" if world > 1 else "single GPU"},
                 "time_to_kappa_ms": ms_max / args.steps,
                 "stage_ms_per_step": {k: round(v, 4) for k, v in per_step.items()},
