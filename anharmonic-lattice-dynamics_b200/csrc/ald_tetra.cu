@@ -494,13 +494,16 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     }
     const bool any = cell_ok && chi > clo;
     if (__any_sync(0xffffffffu, any)) {
+      // band range of each tetrahedron, then one warp scan of the packed
+      // (queue entries << 16 | records) counts of the six, and one slot
+      // reservation per warp for both lists
+      int tlo[6], tcnt[6];
+      int nrec = 0, nq = 0;
 #pragma unroll
       for (int l = 0; l < 6; ++l) {
-        float en[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) en[k] = ec[kTetOf[l][k]];
-        const float mn = fminf(fminf(en[0], en[1]), fminf(en[2], en[3]));
-        const float mx = fmaxf(fmaxf(en[0], en[1]), fmaxf(en[2], en[3]));
+        const float e0 = ec[kTetOf[l][0]], e1 = ec[kTetOf[l][1]], e2 = ec[kTetOf[l][2]], e3 = ec[kTetOf[l][3]];
+        const float mn = fminf(fminf(e0, e1), fminf(e2, e3));
+        const float mx = fmaxf(fmaxf(e0, e1), fmaxf(e2, e3));
         int lo = 0, hi = 0;
 #pragma unroll
         for (int l1 = 0; l1 < B; ++l1) {
@@ -508,33 +511,42 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
           hi += omlo[l1] <= mx;
         }
         const int cnt = any && hi > lo ? hi - lo : 0;
-        const unsigned mask = __ballot_sync(0xffffffffu, cnt > 0);
-        if (mask == 0u) continue;
-        int incl = cnt;
+        tlo[l] = lo;
+        tcnt[l] = cnt;
+        nrec += cnt > 0;
+        nq += cnt;
+      }
+      const int packed = (nq << 16) | nrec;  // nrec <= 6 * 32 and nq <= 6 * 16 * 32 per warp
+      int incl = packed;
 #pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-          const int v = __shfl_up_sync(0xffffffffu, incl, o);
-          if (lane >= o) incl += v;
-        }
-        int rbase = 0, qbase = 0;
-        if (lane == 31) {
-          rbase = atomicAdd(&s_nrec, __popc(mask));
-          qbase = atomicAdd(&s_nq, incl);
-        }
-        rbase = __shfl_sync(0xffffffffu, rbase, 31);
-        qbase = __shfl_sync(0xffffffffu, qbase, 31);
-        if (cnt > 0) {
-          const int rec = rbase + __popc(mask & ((1u << lane) - 1u));
-          const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
-          s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
-          // corner at each sorted position (tet_pos is a permutation of 0..3)
-          const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2);
-          const int c0 = lp[kTetOf[l][0]], c1 = lp[kTetOf[l][1]], c2 = lp[kTetOf[l][2]], c3 = lp[kTetOf[l][3]];
-          auto at = [&](int p) { return (unsigned short)(ps0 == p ? c0 : ps1 == p ? c1 : ps2 == p ? c2 : c3); };
-          s_recp[rec] = make_ushort4(at(0), at(1), at(2), at(3));
-          int q = qbase + incl - cnt;
-          for (int l1 = lo; l1 < hi; ++l1) s_queue[q++] = (unsigned short)((rec << 4) | l1);
-        }
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      int rbase = 0, qbase = 0;
+      if (lane == 31 && incl != 0) {
+        rbase = atomicAdd(&s_nrec, incl & 0xffff);
+        qbase = atomicAdd(&s_nq, incl >> 16);
+      }
+      rbase = __shfl_sync(0xffffffffu, rbase, 31);
+      qbase = __shfl_sync(0xffffffffu, qbase, 31);
+      int rec = rbase + (incl & 0xffff) - nrec;
+      int q = qbase + (incl >> 16) - nq;
+#pragma unroll
+      for (int l = 0; l < 6; ++l) {
+        if (tcnt[l] == 0) continue;
+        float en[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) en[k] = ec[kTetOf[l][k]];
+        const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+        s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
+        // corner at each sorted position (tet_pos is a permutation of 0..3)
+        const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2);
+        const int c0 = lp[kTetOf[l][0]], c1 = lp[kTetOf[l][1]], c2 = lp[kTetOf[l][2]], c3 = lp[kTetOf[l][3]];
+        auto at = [&](int p) { return (unsigned short)(ps0 == p ? c0 : ps1 == p ? c1 : ps2 == p ? c2 : c3); };
+        s_recp[rec] = make_ushort4(at(0), at(1), at(2), at(3));
+        for (int l1 = tlo[l]; l1 < tlo[l] + tcnt[l]; ++l1) s_queue[q++] = (unsigned short)((rec << 4) | l1);
+        ++rec;
       }
     }
     __syncthreads();
