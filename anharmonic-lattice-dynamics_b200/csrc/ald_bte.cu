@@ -287,7 +287,8 @@ struct CgDev {
 };
 
 // y = A x for a row-major A (leading dimension ld) of double or float, x
-// and y double; partial[blk] = the block's sum of y*x.  A block takes
+// and y double; partial[blk] = the block's sum of y*x (and partial_g[blk]
+// that of g*x).  A block takes
 // kGemvRows rows; its warps split the columns, so each x vector a warp
 // loads serves all the rows, and small matrices still give n/kGemvRows
 // blocks.  With vec (rows 16-byte aligned) A is read as 16-byte vectors,
@@ -314,7 +315,8 @@ struct Vec16<float> {
 template <class T>
 __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld, int vec, const T* __restrict__ A,
                                                                const double* __restrict__ x, double* __restrict__ y,
-                                                               double* partial, const CgDev* st) {
+                                                               double* partial, const double* g, double* partial_g,
+                                                               const CgDev* st) {
   if (st && st->done) return;
   using V = typename Vec16<T>::t;
   constexpr int W = Vec16<T>::w;
@@ -362,14 +364,16 @@ __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld,
   }
   __syncthreads();
   if (threadIdx.x == 0) {
-    double dot = 0.0;
+    double dot = 0.0, gdot = 0.0;
     for (int r = 0; r < kGemvRows && row0 + r < n; ++r) {
       double t = 0.0;
       for (int w = 0; w < kGemvWarps; ++w) t += red[w][r];
       y[row0 + r] = t;
       dot += t * x[row0 + r];
+      if (g) gdot += g[row0 + r] * x[row0 + r];
     }
     if (partial) partial[blockIdx.x] = dot;
+    if (partial_g) partial_g[blockIdx.x] = gdot;
   }
 }
 
@@ -408,27 +412,38 @@ __global__ void cg_init_kernel(int n, const double* y, const double* b, double* 
   }
 }
 
-// one CG update after aux = A conj (cg.f90:37-55)
-__global__ void cg_step_kernel(int n, const double* aux, const double* partial, int nparts, double* grad,
-                               double* conj, double* v0, double* x, CgDev* st, int mode, double tol) {
+// One CG iteration after aux = A conj (cg.f90:37-55) in two grid-wide
+// kernels of kCgBlocks CTAs.  Every CTA reduces the same per-block partials
+// in the same order, so all of them hold the same alpha (and later beta).
+constexpr int kCgThreads = 256;
+constexpr int kCgBlocksMax = 64;
+
+// alpha = (grad . conj) / (conj . A conj); x -= alpha conj; grad -= alpha aux;
+// per-CTA partial sums of x.x, conj.conj, grad_new.grad_new, grad_old.grad_old
+__global__ void __launch_bounds__(kCgThreads) cg_update_kernel(int n, const double* aux, const double* pden,
+                                                              const double* pnum, int nparts, double* grad,
+                                                              const double* conj, double* v0, double* x,
+                                                              double* p4, CgDev* st) {
   if (st->done) return;
-  double num = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) num += grad[i] * conj[i];
+  double num = 0, den = 0;
+  for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+    num += pnum[i];
+    den += pden[i];
+  }
   num = vblock_sum(num);
-  double den = 0;
-  for (int i = threadIdx.x; i < nparts; i += blockDim.x) den += partial[i];
   den = vblock_sum(den);
-  double alpha = num / den;
+  const double alpha = num / den;
   double v2 = 0, cc = 0, gg = 0, g2 = 0;
-  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     double gi = grad[i];
     v0[i] = gi;
-    double xi = x[i] - alpha * conj[i];
+    double ci = conj[i];
+    double xi = x[i] - alpha * ci;
     x[i] = xi;
     double gn = gi - alpha * aux[i];
     grad[i] = gn;
     v2 += xi * xi;
-    cc += conj[i] * conj[i];
+    cc += ci * ci;
     gg += gn * gn;
     g2 += gi * gi;
   }
@@ -436,13 +451,39 @@ __global__ void cg_step_kernel(int n, const double* aux, const double* partial, 
   cc = vblock_sum(cc);
   gg = vblock_sum(gg);
   g2 = vblock_sum(g2);
+  if (threadIdx.x == 0) {
+    p4[0 * kCgBlocksMax + blockIdx.x] = v2;
+    p4[1 * kCgBlocksMax + blockIdx.x] = cc;
+    p4[2 * kCgBlocksMax + blockIdx.x] = gg;
+    p4[3 * kCgBlocksMax + blockIdx.x] = g2;
+    if (blockIdx.x == 0) {
+      st->num = num;
+      st->den = den;
+    }
+  }
+}
+
+// the stop rule; unless it fires, conj = -grad + beta conj with beta = gg/g2
+__global__ void __launch_bounds__(kCgThreads) cg_dir_kernel(int n, const double* p4, const double* grad,
+                                                           double* conj, CgDev* st, int mode, double tol) {
+  if (st->done) return;
+  __shared__ double s4[4];
+  if (threadIdx.x < 4) {
+    double t = 0;
+    for (int k = 0; k < (int)gridDim.x; ++k) t += p4[threadIdx.x * kCgBlocksMax + k];
+    s4[threadIdx.x] = t;
+  }
+  __syncthreads();
+  const double v2 = s4[0], cc = s4[1], gg = s4[2], g2 = s4[3];
+  const double num = st->num, den = st->den;
   double err = mode == ALD_CG_REFERENCE ? (num * num / den / den) * cc / v2 : sqrt(gg) / st->bnorm;
   bool stop = err < tol;
   if (!stop) {
     double beta = gg / g2;
-    for (int i = threadIdx.x; i < n; i += blockDim.x) conj[i] = -grad[i] + beta * conj[i];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+      conj[i] = -grad[i] + beta * conj[i];
   }
-  if (threadIdx.x == 0) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
     st->iters += 1;
     st->err = err;
     if (stop) st->done = 1;
@@ -529,12 +570,15 @@ template <class T>
 static cudaError_t capture_cg(int iters, int n, size_t ld, int vec, int nblk, const T* dA, double* dx, CgWork& w, CgDev* st,
                               int mode, double tol, cudaStream_t s, cudaGraphExec_t* out) {
   cudaGraph_t graph = nullptr;
+  const int nb = std::min(kCgBlocksMax, (n + kCgThreads - 1) / kCgThreads);
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
   for (int it = 0; it < iters; ++it) {
-    gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, w.conj.p, w.aux.p, w.partial.p, st);
-    cg_step_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, w.partial.p, nblk, w.grad.p, w.conj.p, w.v0.p, dx, st, mode,
-                                             tol);
+    gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, w.conj.p, w.aux.p, w.partial.p, w.grad.p,
+                                                     w.pnum.p, st);
+    cg_update_kernel<<<nb, kCgThreads, 0, s>>>(n, w.aux.p, w.partial.p, w.pnum.p, nblk, w.grad.p, w.conj.p, w.v0.p,
+                                               dx, w.p4.p, st);
+    cg_dir_kernel<<<nb, kCgThreads, 0, s>>>(n, w.p4.p, w.grad.p, w.conj.p, st, mode, tol);
   }
   e = cudaStreamEndCapture(s, &graph);
   if (e == cudaSuccess) e = cudaGraphInstantiate(out, graph, 0);
@@ -553,13 +597,15 @@ static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* 
   }
   const int vec = ((uintptr_t)dA & 15u) == 0 && (ld * sizeof(T)) % 16 == 0;  // rows 16-byte aligned
   if (w.grad.alloc(n) || w.conj.alloc(n) || w.aux.alloc(n) || w.v0.alloc(n) || w.partial.alloc(nblk) ||
+      w.pnum.alloc(nblk) || w.p4.alloc(4 * kCgBlocksMax) ||
       w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev)) ||
       (!w.h_done && cudaHostAlloc((void**)&w.h_done, sizeof(int), cudaHostAllocDefault) != cudaSuccess)) {
     msg = "cg: allocation failed";
     return ALD_ERR_NOMEM;
   }
   CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
-  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr);
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
+                                                   nullptr);
   cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, db, w.grad.p, w.conj.p, st);
   cudaError_t e = cudaSuccess;
   const bool same = w.exec && w.n == n && w.max_iter == max_iter && w.mode == mode && w.tol == tol && w.A == (const void*)dA && w.ld == ld &&
@@ -598,7 +644,8 @@ static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* 
     msg = std::string("cg: ") + cudaGetErrorString(e);
     return ALD_ERR_CUDA;
   }
-  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr);
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
+                                                   nullptr);
   cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, w.aux.p, db, w.fmin.p);
   CgDev h;
   e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);

@@ -337,7 +337,7 @@ cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const in
 // iteration loop, kept across calls and re-captured only when the problem
 // (size, pointers, stop rule) changes
 struct CgWork {
-  DevBuf<double> grad, conj, aux, v0, partial, fmin;
+  DevBuf<double> grad, conj, aux, v0, partial, pnum, p4, fmin;
   DevBuf<char> st;
   cudaGraphExec_t exec = nullptr;       // kCgChunk iterations
   cudaGraphExec_t exec_tail = nullptr;  // max_iter % kCgChunk iterations

@@ -314,7 +314,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   int rc = cg_device_ld((int)N, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters,
                         &cg_err, &fm, s, c->cg, msg);
   if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
-  res->launches[7] += 4 + 2 * cg_launched_iterations(iters, c->opt.cg_max_iter);
+  res->launches[7] += 4 + 3 * cg_launched_iterations(iters, c->opt.cg_max_iter);
   ALD_CK(tm.end());
   // ---- 8: mode_kappa_d
   ALD_CK(tm.begin(8));

@@ -331,16 +331,16 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
 // array in HBM.  A CTA owns one IBZ row, one process and one band l2, and a
 // block of mesh cells: plane i, rows j0 .. j0+R-1, all k (thread = cell).  The
 // corners of those cells form a window of 2 x (R+1) x N2 mesh points.
-// Once per CTA the window's indices, omega(w,l2), n(w,l2) and flags are staged
-// in shared memory; then per l3 (one slice of the reference's loops):
+// Once per CTA the window's indices and flags are staged in shared memory;
+// then per l3 (one slice of the reference's loops):
 //   1. per window point: E = -+omega(w,l2) + omega(q1+-w,l3) as default REAL,
 //      G = n2 (n3+1) [process 1] or (n2+1)(n3+1) [process 2], G = 0 where the
 //      reference zeroes acoustic modes at Gamma (sub.f90:7351-7356, 7412-7417);
 //   2. per cell: min/max of its 8 corner energies; cells whose range holds
 //      no band energy omega1(l1) are skipped, else its 6 tetrahedra are
 //      sorted once and each one whose range may hold an omega1(l1) is stored
-//      as a record (sorted energies + corner at each sorted position) with
-//      its (record, l1) pairs queued;
+//      as a record (the window point at each sorted position; the energies
+//      are read back from the window) with its (record, l1) pairs queued;
 //   3. per queued pair: weight_tet's four corner weights c (bitwise, ald_tet.h)
 //      and R(row, w, l1, l2) += c/6 (2pi)^2/nkc |V3|^2 n1 G for each corner
 //      (FP64 atomics in L2; FP64 atomics on shared memory would be CAS loops).
@@ -365,10 +365,9 @@ __host__ __device__ inline FusedShape fused_shape(const Geometry& g) {
   f.NW = 2 * (f.R + 1) * N2;
   f.maxrec = 6 * f.R * N2;
   const size_t nw2 = (size_t)(f.NW + (f.NW & 1));
-  // doubles: G, fw, n2; float4 records; ushort4 records;
-  // ints: w, src, q3; floats: E; bytes: flags; ushorts: queue
-  f.smem = nw2 * 8 * 3 + (size_t)f.maxrec * 16 + (size_t)f.maxrec * 8 + (size_t)f.NW * 3 * 4 +
-           (size_t)f.NW * 4 + (size_t)((f.NW + 3) & ~3) + (size_t)f.maxrec * g.b * 2;
+  // doubles: G; ushort4 records; ints: w, src, q3; floats: E; bytes: flags; ushorts: queue
+  f.smem = nw2 * 8 + (size_t)f.maxrec * 8 + (size_t)f.NW * 3 * 4 + (size_t)f.NW * 4 + (size_t)((f.NW + 3) & ~3) +
+           (size_t)f.maxrec * g.b * 2;
   return f;
 }
 
@@ -387,10 +386,7 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
   // shared layout
   const int nw2 = NW + (NW & 1);
   double* s_G = reinterpret_cast<double*>(smraw);
-  double* s_fw = s_G + nw2;
-  double* s_n2 = s_fw + nw2;
-  float4* s_rece = reinterpret_cast<float4*>(s_n2 + nw2);
-  ushort4* s_recp = reinterpret_cast<ushort4*>(s_rece + maxrec);
+  ushort4* s_recp = reinterpret_cast<ushort4*>(s_G + nw2);
   int* s_w = reinterpret_cast<int*>(s_recp + maxrec);
   int* s_src = s_w + NW;
   int* s_q3 = s_src + NW;
@@ -427,8 +423,6 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     s_q3[p] = q3;
     s_src[p] = proc == 0 ? w : neg_index(g, mw);
     s_fl[p] = (unsigned char)((at_gamma_index(g, mw) ? 1 : 0) | (at_gamma_index(g, m3) ? 2 : 0));
-    s_fw[p] = a.freq[(size_t)w * b + l2];
-    s_n2[p] = a.dist[(size_t)w * b + l2];
   }
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   double* Rp = proc == 0 ? a.R1 : a.R2;
@@ -465,9 +459,9 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     }
     for (int p = tid; p < NW; p += blockDim.x) {
       const int q3 = s_q3[p];
-      const double fw = s_fw[p], f3 = a.freq[(size_t)q3 * b + l3];
+      const double fw = a.freq[(size_t)s_w[p] * b + l2], f3 = a.freq[(size_t)q3 * b + l3];
       s_E[p] = (float)(proc == 0 ? -fw + f3 : fw + f3);
-      const double n2 = s_n2[p], n3 = a.dist[(size_t)q3 * b + l3];
+      const double n2 = a.dist[(size_t)s_w[p] * b + l2], n3 = a.dist[(size_t)q3 * b + l3];
       const bool zero = (l2 < 3 && (s_fl[p] & 1)) || (l3 < 3 && (s_fl[p] & 2));
       s_G[p] = zero ? 0.0 : (proc == 0 ? n2 * (n3 + 1) : (n2 + 1) * (n3 + 1));
     }
@@ -538,8 +532,6 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
         float en[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) en[k] = ec[kTetOf[l][k]];
-        const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
-        s_rece[rec] = make_float4(ts.e1, ts.e2, ts.e3, ts.e4);
         // corner at each sorted position (tet_pos is a permutation of 0..3)
         const int ps0 = tet_pos(en, 0), ps1 = tet_pos(en, 1), ps2 = tet_pos(en, 2);
         const int c0 = lp[kTetOf[l][0]], c1 = lp[kTetOf[l][1]], c2 = lp[kTetOf[l][2]], c3 = lp[kTetOf[l][3]];
@@ -555,8 +547,9 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     for (int i = tid; i < nq; i += blockDim.x) {
       const unsigned v = s_queue[i];
       const int rec = (int)(v >> 4), l1 = (int)(v & 15u);
-      const float4 e = s_rece[rec];
-      const TetSorted ts = tet_sort(e.x, e.y, e.z, e.w);
+      const ushort4 pp = s_recp[rec];
+      // sorted positions 0..3 hold the highest .. lowest corner
+      const TetSorted ts = tet_sort(s_E[pp.w], s_E[pp.z], s_E[pp.y], s_E[pp.x]);
       double cp[4];
       if constexpr (F32W) {
         float cf[4];
@@ -566,7 +559,6 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
       } else {
         if (!tet_weights4(ts, s_om[l1], cp)) continue;
       }
-      const ushort4 pp = s_recp[rec];
       const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
       const double nb1 = s_nb1[l1];
       double* Rrow = Rp + (size_t)row * nkc * b * b + l1 * b + l2;
