@@ -154,11 +154,13 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
 // collision matrix: thread per (n1, n2, l1, l2), l2 fastest, so that the b*b
 // band block of R(q1, arm, ., .) read for one arm is contiguous across the
 // threads of a warp (one IBZ row n1 per blockIdx.y).  T = double, or float
-// for the mixed-precision pipeline (sums in double, stored rounded).
+// for the mixed-precision pipeline (sums in double, stored rounded).  With
+// piso (iso=1) the arms off the diagonal take CollisionMatrix_iso's form
+// (sub.f90:3387-3570): C = -R1(arm) + R1(q1+arm) + R2(arm) + Piso(n1,l1).
 template <class T>
 __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* mapinv, const int* arm_off,
                                  const int* arm_q, const int* arm_op, const double* opk, const double* Q,
-                                 const double* R1, const double* R2, T* CM, size_t ld) {
+                                 const double* R1, const double* R2, T* CM, size_t ld, const double* piso) {
   const int b = g.b, b2 = b * b, nkc = g.nkc;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nibz * b2) return;
@@ -186,8 +188,15 @@ __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* 
       }
       int nk3_p1 = compose(g, mp1), nk3_p2 = compose(g, mp2);
       const int bl = l1 * b + l2;
-      C = -R1[(base + n0) * b2 + bl] + R1[(base + nk3_p2) * b2 + bl] + 0.5 * R2[(base + n0) * b2 + bl] +
-          0.5 * R2[(base + nk3_p1) * b2 + bl];
+      if (piso) {
+        int ins;
+        const int nqp = pm_index(g, m1, m0, 1, ins);  // q1 + arm
+        C = -R1[(base + n0) * b2 + bl] + R1[(base + nqp) * b2 + bl] + R2[(base + n0) * b2 + bl];
+        C = C + piso[(size_t)nl * b + l1];
+      } else {
+        C = -R1[(base + n0) * b2 + bl] + R1[(base + nk3_p2) * b2 + bl] + 0.5 * R2[(base + n0) * b2 + bl] +
+            0.5 * R2[(base + nk3_p1) * b2 + bl];
+      }
     }
     const double* op = opk + 9 * arm_op[s];
     for (int i = 0; i < 3; ++i)
@@ -547,15 +556,15 @@ cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s) {
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
                              const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
-                             cudaStream_t s) {
+                             const double* piso, cudaStream_t s) {
   const int nt = nibz * geo.b * geo.b;
   dim3 grid((nt + 127) / 128, nrows);
   if (cm_f32)
     collision_kernel<float><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2,
-                                                 static_cast<float*>(CM), ld);
+                                                 static_cast<float*>(CM), ld, piso);
   else
     collision_kernel<double><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1,
-                                                  R2, static_cast<double*>(CM), ld);
+                                                  R2, static_cast<double*>(CM), ld, piso);
   return cudaGetLastError();
 }
 

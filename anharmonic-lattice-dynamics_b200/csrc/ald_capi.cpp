@@ -190,6 +190,18 @@ int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
   return ALD_OK;
 }
 
+int ensure_giso(ald_ctx* c) {
+  if (!c->giso_ok) {
+    std::string e = isotope_g_atoms(c->S, c->giso);
+    if (!e.empty()) return fail(ALD_ERR_UNSUPPORTED, e);
+    c->giso_ok = true;
+  }
+  CKA(c->giso_d.alloc(c->giso.size()));
+  CK(cudaMemcpyAsync(c->giso_d.p, c->giso.data(), c->giso.size() * sizeof(double), cudaMemcpyHostToDevice,
+                     c->stream));
+  return ALD_OK;
+}
+
 KappaArgs kappa_args(ald_ctx* c, double tempk) {
   KappaArgs k;
   k.geo = c->geo;
@@ -287,6 +299,11 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   g.nat0 = c->S.nat0;
   g.shifted = c->T.shifted ? 1 : 0;
   g.L = c->T.L;
+  {
+    long long mx = (long long)c->T.L - 1;  // the largest phase sum of a mesh point
+    for (int a = 0; a < 3; ++a) mx += (long long)(g.nc[a] - 1) * (c->T.L - 1);
+    g.L32 = mx < (1LL << 31) ? 1 : 0;
+  }
   cudaStream_t s = c->stream;
   g_h2d = 0;
   // tables
@@ -702,7 +719,7 @@ int ald_collision_matrix(ald_ctx* c, const int ksubset[2], const double* P1, con
   CK(launch_from_fortran5(tmp.p, p2.p, nr, nkc, b, c->stream));
   CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
   CK(launch_collision(c->geo, nibz, ksubset[0] - 1, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p,
-                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, (size_t)cols, 0, c->stream));
+                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, (size_t)cols, 0, nullptr, c->stream));
   CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
   CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -757,6 +774,84 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
   if (funcmin) *funcmin = fm;
   if (iters) *iters = it;
   return r;
+}
+
+int ald_set_isotope_g(ald_ctx* c, const double* g) {
+  if (!c || !g) return fail(ALD_ERR_ARG, "null argument");
+  c->giso.assign(g, g + c->S.nat0);
+  c->giso_ok = true;
+  return ALD_OK;
+}
+
+int ald_get_isotope_g(ald_ctx* c, double* g) {
+  if (!c || !g) return fail(ALD_ERR_ARG, "null argument");
+  if (!c->giso_ok) {
+    std::string e = isotope_g_atoms(c->S, c->giso);
+    if (!e.empty()) return fail(ALD_ERR_UNSUPPORTED, e);
+    c->giso_ok = true;
+  }
+  std::memcpy(g, c->giso.data(), c->giso.size() * sizeof(double));
+  return ALD_OK;
+}
+
+int ald_p_iso_split(ald_ctx* c, const int ksubset[2], double* Piso) {
+  if (!c || !Piso) return fail(ALD_ERR_ARG, "null argument");
+  if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
+  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "isotope scattering: more than 12 bands");
+  CK(cudaSetDevice(c->device));
+  int r = ensure_phonons(c);
+  if (r) return r;
+  // frequencies only (cal_freq); the temperature of the occupations does not enter
+  r = ensure_dist(c, c->dist_tempk > 0 ? c->dist_tempk : c->S.tmin);
+  if (r) return r;
+  r = ensure_giso(c);
+  if (r) return r;
+  const int nr = ksubset[1] - ksubset[0] + 1, b = c->geo.b;
+  DevBuf<double> part, pd;
+  CKA(part.alloc(piso_partial_doubles(c->geo, nr)));
+  CKA(pd.alloc((size_t)nr * b));
+  CK(launch_piso(c->geo, ksubset[0] - 1, nr, c->mapinv.p, c->freq.p, c->evec.p, c->tet_corner.p, c->giso_d.p, part.p,
+                 pd.p, nullptr, nullptr, nullptr, c->stream));
+  std::vector<double> h((size_t)nr * b);
+  CK(cudaMemcpyAsync(h.data(), pd.p, h.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int i = 0; i < nr; ++i)
+    for (int l = 0; l < b; ++l) Piso[i + (size_t)nr * l] = h[(size_t)i * b + l];
+  return check_err_flags(c);
+}
+
+int ald_collision_matrix_iso(ald_ctx* c, const double* P1, const double* P2, const double* Piso, double* CM) {
+  if (!c || !P1 || !P2 || !Piso || !CM) return fail(ALD_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  const int b = c->geo.b, nkc = c->T.nkc, nibz = c->T.nibz, nr = nibz;
+  const size_t n = (size_t)nr * nkc * b * b * b;
+  DevBuf<double> tmp, p1, p2, R1, R2, Qd, pis, cm, cmt;
+  CKA(tmp.alloc(n));
+  CKA(p1.alloc(n));
+  CKA(p2.alloc(n));
+  CKA(R1.alloc((size_t)nr * nkc * b * b));
+  CKA(R2.alloc((size_t)nr * nkc * b * b));
+  CKA(Qd.alloc((size_t)nr * b));
+  CKA(pis.alloc((size_t)nr * b));
+  const int rows = 3 * b * nr, cols = 3 * b * nibz;
+  CKA(cm.alloc((size_t)rows * cols));
+  CKA(cmt.alloc((size_t)rows * cols));
+  std::vector<double> hp((size_t)nr * b);
+  for (int i = 0; i < nr; ++i)
+    for (int l = 0; l < b; ++l) hp[(size_t)i * b + l] = Piso[i + (size_t)nr * l];
+  CK(cudaMemcpyAsync(pis.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(tmp.p, P1, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, p1.p, nr, nkc, b, c->stream));
+  CK(cudaMemcpyAsync(tmp.p, P2, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  CK(launch_from_fortran5(tmp.p, p2.p, nr, nkc, b, c->stream));
+  CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
+  CK(launch_add((size_t)nr * b, Qd.p, pis.p, c->stream));  // the diagonal: -(sum(P1 + P2/2) + Piso)
+  CK(launch_collision(c->geo, nibz, 0, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, Qd.p, R1.p,
+                      R2.p, cm.p, (size_t)cols, 0, pis.p, c->stream));
+  CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
+  CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return ALD_OK;
 }
 
 int ald_update_mpi(ald_ctx* c, const int ksubset[2], const double* P1, const double* P2, const double* Qv,

@@ -36,6 +36,10 @@ struct ald_ctx {
   // pipeline workspaces, kept across calls (allocation outside the timed work)
   DevBuf<double> w_R1, w_R2, w_Q, w_v3, w_F, w_x, w_rhs, w_kr, w_kc, w_cm;
   DevBuf<double> w_R1p, w_R2p, w_Ff, w_Frta, w_part;  // iterative solution: band marginals, F on the mesh
+  // isotope scattering (iso=1): g per primitive atom, Piso [ibz][l1] and its partial sums
+  std::vector<double> giso;
+  bool giso_ok = false;
+  DevBuf<double> giso_d, w_piso, w_piso_part;
   DevBuf<char> w_scratch;
   CgWork cg;
   bool have_phonons = false;
@@ -51,6 +55,8 @@ int ensure_dist(ald_ctx* c, double tempk);
 V3Args v3_args(ald_ctx* c, int first, int nrows, double* out);
 // nlaunch (optional) += the kernels launched
 int run_v3(ald_ctx* c, const V3Args& a, int* nlaunch);
+// g of cal_giso on the device (the element table unless ald_set_isotope_g set it)
+int ensure_giso(ald_ctx* c);
 KappaArgs kappa_args(ald_ctx* c, double tempk);
 int delta_mode(ald_ctx* c);
 double gauss_width(ald_ctx* c);

@@ -305,6 +305,8 @@ std::string read_system(const std::string& dir, System& S) {
     if (ok)
       for (int i = 0; i < ntype; ++i) S.mas.push_back(dval(t[i]));
     ok = ok && R.next(ntype, t);
+    if (ok)
+      for (int i = 0; i < ntype; ++i) S.atname.push_back(t[i]);
     ok = ok && R.next(1, t);
     if (ok) S.nat0 = ival(t[0]);
     if (ok && (S.nat0 < 1 || S.nat0 > 4096)) return "structure.params: bad natoms0";
@@ -842,6 +844,51 @@ std::string build_fc2(const System& S, Fc2Csr& F) {
   F.uidx.resize(F.atom.size());
   for (size_t t = 0; t < F.atom.size(); ++t)
     F.uidx[t] = (int)(std::lower_bound(F.uatom.begin(), F.uatom.end(), F.atom[t]) - F.uatom.begin());
+  return "";
+}
+
+// Natural isotopic compositions (isotope mass in amu, abundance in percent)
+// with the values of the reference's cal_g table (sub.f90:3766-4693), for the
+// elements covered here; others need ald_set_isotope_g.
+namespace {
+struct IsoLine {
+  const char* element;
+  double mass, percent;
+};
+const IsoLine kIsotopes[] = {
+    {"Ar", 35.967546, 0.34},  {"Ar", 37.962732, 0.063},  {"Ar", 39.962383, 99.6},   {"C", 12.0, 98.9},
+    {"C", 13.003355, 1.1},    {"Cl", 34.968853, 75.77},  {"Cl", 36.965903, 24.23},  {"Ge", 69.92425, 20.5},
+    {"Ge", 71.92208, 27.4},   {"Ge", 72.923464, 7.8},    {"Ge", 73.921179, 36.5},   {"Ge", 75.921403, 7.8},
+    {"Na", 22.98977, 100.0},  {"Si", 27.976928, 92.23},  {"Si", 28.976496, 4.67},   {"Si", 29.973772, 3.1},
+};
+}  // namespace
+
+bool isotope_g(const std::string& element, double& g) {
+  // mass variance: mbar = sum m f / 100, g = sum f (1 - m/mbar)^2 / 100
+  double mbar = 0;
+  int n = 0;
+  for (const IsoLine& x : kIsotopes)
+    if (element == x.element) {
+      mbar = mbar + x.mass * x.percent;
+      ++n;
+    }
+  if (n == 0) return false;
+  mbar = mbar / 100;
+  g = 0;
+  for (const IsoLine& x : kIsotopes)
+    if (element == x.element) g = g + x.percent * (1 - (x.mass / mbar)) * (1 - (x.mass / mbar));
+  g = g / 100;
+  return true;
+}
+
+std::string isotope_g_atoms(const System& S, std::vector<double>& g) {
+  g.assign(S.nat0, 0.0);
+  for (int i = 0; i < S.nat0; ++i) {
+    const int t = S.atype[i];
+    if (t < 1 || t > (int)S.atname.size()) return "isotope scattering: atom type without an element name";
+    if (!isotope_g(S.atname[t - 1], g[i]))
+      return "isotope scattering: no isotope data for element " + S.atname[t - 1] + " (ald_set_isotope_g)";
+  }
   return "";
 }
 

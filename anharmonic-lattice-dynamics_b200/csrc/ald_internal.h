@@ -45,6 +45,7 @@ struct System {
   double scale = 0;
   int include_fc[4] = {0};
   std::vector<double> mas;
+  std::vector<std::string> atname;  // element name per type
   int nat0 = 0;
   std::vector<int> atype;
   std::vector<double> mass0;
@@ -162,6 +163,7 @@ struct Geometry {  // passed by value to kernels
   int nat0;
   int shifted;
   int L;
+  int L32;  // 1: every phase sum m.pc + pc3 (m < nc, pc < L) fits in 32 bits
 };
 
 // kernels (implemented in the .cu files)
@@ -295,11 +297,24 @@ cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaS
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s);
 cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s);
-// CM: double, or float when cm_f32 (mixed-precision pipeline); leading dimension ld
+// CM: double, or float when cm_f32 (mixed-precision pipeline); leading dimension ld.
+// piso (optional, [row][l1] of the range): CollisionMatrix_iso's form instead
+// of CollisionMatrix_mpi's (Q must then include Piso)
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
                              const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
-                             cudaStream_t s);
+                             const double* piso, cudaStream_t s);
+// isotope scattering (P_iso_split): Piso[row][l1] of rows n1_first.., and
+// Q, Q_N, Q_U += Piso when Q is given; partial: piso_partial_doubles scratch
+size_t piso_partial_doubles(const Geometry& geo, int nrows);
+cudaError_t launch_piso(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* freq,
+                        const double* evec, const int* tet_corner, const double* giso, double* partial,
+                        double* Piso, double* Q, double* QN, double* QU, cudaStream_t s);
+cudaError_t launch_add(size_t n, double* y, const double* x, cudaStream_t s);
+// the g of cal_g for an element name (false: no isotope data for it), and
+// of every primitive atom (cal_giso)
+bool isotope_g(const std::string& element, double& g);
+std::string isotope_g_atoms(const System& S, std::vector<double>& g);
 
 // layout conversions and the stand-alone stage kernels (ald_util.cu)
 // internal 5-index arrays are [row][q][l1][l2][l3]; the reference's are

@@ -79,6 +79,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
                         double* kappa_rta_modes, double* kappa_cg_modes, double* xo, const IterSpec* it) {
   if (!c || !res) return fail(ALD_ERR_ARG, "null argument");
   if (it && !c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
+  if (it && c->S.iso == 1)
+    return fail(ALD_ERR_UNSUPPORTED, "the iterative solution with isotope scattering (update_iso) is not built");
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
   if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 12 bands is not supported by this build");
   ALD_CK(cudaSetDevice(c->device));
@@ -183,6 +185,18 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   ALD_CK(tm.begin(3));
   ALD_CK(launch_q_from_r(c->geo, 0, nibz, c->mapinv.p, R1.p, R2.p, dQ, dQN, dQU, nibz, s));
   res->launches[3] += 1;
+  // iso=1: isotope scattering (P_iso_split), Q, Q_N, Q_U += Piso as in
+  // calculate_tauRTA_iso (sub.f90:8311-8549)
+  const bool iso = c->S.iso == 1;
+  if (iso) {
+    r = ensure_giso(c);
+    if (r) return r;
+    ALD_CKA(c->w_piso.alloc((size_t)nibz * b));
+    ALD_CKA(c->w_piso_part.alloc(piso_partial_doubles(c->geo, nibz)));
+    ALD_CK(launch_piso(c->geo, 0, nibz, c->mapinv.p, c->freq.p, c->evec.p, c->tet_corner.p, c->giso_d.p,
+                       c->w_piso_part.p, c->w_piso.p, dQ, dQN, dQU, s));
+    res->launches[3] += 2;
+  }
   ALD_CK(tm.end());
   // ---- 4: RTA
   KappaArgs k = kappa_args(c, tempk);
@@ -296,7 +310,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   ALD_CKA(cm.alloc((cm_bytes + sizeof(double) - 1) / sizeof(double)));
   ALD_CK(tm.begin(5));
   ALD_CK(launch_collision(c->geo, nibz, 0, nibz, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, dQ,
-                          R1.p, R2.p, cm.p, ld, cm_f32, s));
+                          R1.p, R2.p, cm.p, ld, cm_f32, iso ? c->w_piso.p : nullptr, s));
   res->launches[5] += 1;
   ALD_CK(tm.end());
   // ---- 6: RHS and the initial guess x0 = F_RTA (kappa.f90:835-843)

@@ -74,9 +74,6 @@ __device__ __forceinline__ int neg_index(const Geometry& g, const int* mw) {
 __device__ __forceinline__ bool at_gamma_index(const Geometry& g, const int* m) {
   return m[0] == g.nc[0] / 2 && m[1] == g.nc[1] / 2 && m[2] == g.nc[2] / 2;
 }
-__device__ __forceinline__ double delta_g(double x, double w) {  // extratools.f90:239
-  return exp(-x * x / 2.0 / w / w) / sqrt(2 * PhysConst::pi) / w;
-}
 
 // make_kp_reg_tet (tetrahedron.f90:2-142): tetrahedron t = 6*cube + l; cube
 // corners pt1..pt8 at offsets (0,0,0) (1,0,0) (0,1,0) (1,1,0) (0,0,1) (1,0,1)
@@ -194,93 +191,134 @@ __global__ void __launch_bounds__(kTetThreads) delta_tet_kernel(Geometry g, int 
   }
 }
 
-// per mesh point: P = F * W, Bose factors, sums over l3
-template <int B, bool F32W>
+// per mesh point: P = F * W, Bose factors, sums over l3.  Two thread maps:
+//   TILE: a CTA takes kPointBlock / b consecutive mesh points w of one IBZ
+//         row and all b bands l2 (thread = (w, l2), l2 fastest), so the loads
+//         of omega, n at (w, l2) and the R1/R2 tile [w][l1][l2] it writes
+//         (staged in shared memory) are contiguous;
+//   else: a CTA takes kPointBlock consecutive w of one row and one l2
+//         (blockIdx.z), so the |V3|^2 loads of a warp are one run of q2.
+// Measured on B200: TILE for the FP64 Gaussian (exp-bound), the other map
+// for the FP32 one (load-latency bound).
+// The Gaussian is delta_g of extratools.f90:239, exp(-x^2/2/w/w)/sqrt(2 pi)/w,
+// with the constant factors formed once (FP64 rounding, not bitwise), and
+// skipped where exp underflows to zero.
+template <int B, bool F32W, bool TILE>
 __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a, const double* __restrict__ W) {
   __shared__ double s_om1[B], s_nb1[B];
+  __shared__ double s_r[2][TILE ? kPointBlock * B : 1];  // R1, R2 tiles: [w local][l1][l2]
   const Geometry& g = a.geo;
   const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
-  const int row = blockIdx.z, l2 = blockIdx.y, tid = threadIdx.x;
+  const int row = blockIdx.y, tid = threadIdx.x;
+  const int nw = TILE ? kPointBlock / b : kPointBlock;  // mesh points per CTA
+  const int wl = TILE ? tid / b : tid, l2 = TILE ? tid % b : (int)blockIdx.z;
+  const int w0 = blockIdx.x * nw;
+  const int w = w0 + wl;
+  const bool ok = wl < nw && w < nkc;
   const int q1 = a.mapinv[a.n1_first + row];
   if (tid < B) {
     s_om1[tid] = tid < b ? a.freq[(size_t)q1 * b + tid] : 0.0;
     s_nb1[tid] = tid < b ? a.dist[(size_t)q1 * b + tid] : 0.0;
   }
   __syncthreads();
-  const int w = blockIdx.x * blockDim.x + tid;
-  if (w >= nkc) return;
-  int m1[3], mw[3];
-  decompose(g, q1, m1);
-  decompose(g, w, mw);
-  int ins1, ins2;
-  const int q3p = pm_index(g, m1, mw, 1, ins1);   // q1 + w
-  const int q3m = pm_index(g, m1, mw, -1, ins2);  // q1 - w
-  const int wneg = neg_index(g, mw);
-  int m3p[3], m3m[3];
-  decompose(g, q3p, m3p);
-  decompose(g, q3m, m3m);
-  const bool w_gamma = at_gamma_index(g, mw);
-  const bool p_gamma = at_gamma_index(g, m3p), m_gamma = at_gamma_index(g, m3m);
-  const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
-  const double n2 = a.dist[(size_t)w * b + l2];
-  const double* v3 = a.v3sq + (size_t)row * nkc * b3;
-  // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
-  const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
-  const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
-  // FP32 Gaussian (mixed-precision pipeline): exp(-(x/w)^2/2) / (sqrt(2 pi) w)
-  const float gi = (float)(1.0 / a.sigma), gn = (float)(1.0 / sqrt(2 * PhysConst::pi) / a.sigma);
   double R1[B], R2[B];
 #pragma unroll
   for (int l = 0; l < B; ++l) R1[l] = R2[l] = 0.0;
-  for (int l3 = 0; l3 < b; ++l3) {
+  if (ok) {
+    int m1[3], mw[3];
+    decompose(g, q1, m1);
+    decompose(g, w, mw);
+    int ins1, ins2;
+    const int q3p = pm_index(g, m1, mw, 1, ins1);   // q1 + w
+    const int q3m = pm_index(g, m1, mw, -1, ins2);  // q1 - w
+    const int wneg = neg_index(g, mw);
+    int m3p[3], m3m[3];
+    decompose(g, q3p, m3p);
+    decompose(g, q3m, m3m);
+    const bool w_gamma = at_gamma_index(g, mw);
+    const bool p_gamma = at_gamma_index(g, m3p), m_gamma = at_gamma_index(g, m3m);
+    const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
+    const double n2 = a.dist[(size_t)w * b + l2];
+    const double w2 = a.freq[(size_t)w * b + l2];
+    const double* v3 = a.v3sq + (size_t)row * nkc * b3;
+    // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
+    const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
+    const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
+    // Gaussian factors: FP64 (exp underflows to 0 beyond 746) and FP32 (beyond 104)
+    const double gc1 = 0.5 / (a.sigma * a.sigma), gc2 = 1.0 / (sqrt(2 * PhysConst::pi) * a.sigma);
+    const float fc1 = (float)gc1, fc2 = (float)gc2;
+    for (int l3 = 0; l3 < b; ++l3) {
 #pragma unroll
-    for (int proc = 0; proc < 2; ++proc) {
-      const int q3 = proc == 0 ? q3p : q3m;
-      const size_t slice = (((size_t)row * b + l2) * b + l3) * 2 + proc;
-      const bool zero = (l2 < 3 && w_gamma) || (l3 < 3 && (proc == 0 ? p_gamma : m_gamma));
-      const int src = proc == 0 ? w : wneg;
-      const double n3 = a.dist[(size_t)q3 * b + l3];
-      const double w2 = a.freq[(size_t)w * b + l2], w3 = a.freq[(size_t)q3 * b + l3];
-      double* Ps = proc == 0 ? a.P1s : a.P2s;
-      double* Pb = proc == 0 ? a.P1 : a.P2;
+      for (int proc = 0; proc < 2; ++proc) {
+        const int q3 = proc == 0 ? q3p : q3m;
+        const size_t slice = (((size_t)row * b + l2) * b + l3) * 2 + proc;
+        const bool zero = (l2 < 3 && w_gamma) || (l3 < 3 && (proc == 0 ? p_gamma : m_gamma));
+        const int src = proc == 0 ? w : wneg;
+        const double n3 = a.dist[(size_t)q3 * b + l3];
+        const double w3 = a.freq[(size_t)q3 * b + l3];
+        double* Ps = proc == 0 ? a.P1s : a.P2s;
+        double* Pb = proc == 0 ? a.P1 : a.P2;
 #pragma unroll
-      for (int l = 0; l < B; ++l) {
-        if (l >= b) continue;
-        double wl;
-        if (a.gauss) {
-          const double x = proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3;
-          if constexpr (F32W) {
-            const float xs = (float)x * gi;
-            wl = (double)(expf(-0.5f * (xs * xs)) * gn);
+        for (int l = 0; l < B; ++l) {
+          if (l >= b) continue;
+          double wl_ = 0.0;
+          if (a.gauss) {
+            const double x = proc == 0 ? s_om1[l] + w2 - w3 : s_om1[l] - w2 - w3;
+            if constexpr (F32W) {
+              const float xf = (float)x, arg = xf * xf * fc1;
+              if (arg < 104.0f) wl_ = (double)(expf(-arg) * fc2);
+            } else {
+              const double arg = x * x * gc1;
+              if (arg < 746.0) wl_ = exp(-arg) * gc2;
+            }
           } else {
-            wl = delta_g(x, a.sigma);
+            wl_ = W[(slice * nkc + w) * b + l];
           }
-        } else {
-          wl = W[(slice * nkc + w) * b + l];
-        }
-        double ps = 0.0;
-        if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * sq + l * s1 + l2 * s2 + l3 * s3] * fnorm);
-        const double nb1 = s_nb1[l];
-        const double Fb = proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1);
-        const double p = ps * Fb;
-        if (proc == 0) R1[l] += p;
-        else R2[l] += p;
-        double* Rpm = proc == 0 ? a.R1p : a.R2p;
-        if (Rpm && p != 0.0) atomicAdd(Rpm + (((size_t)row * nkc + w) * b + l) * b + l3, p);
-        if (Ps || Pb) {
-          size_t o5 = (((size_t)row * nkc + w) * b + l) * b2 + l2 * b + l3;
-          if (Ps) Ps[o5] = ps;
-          if (Pb) Pb[o5] = p;
+          double ps = 0.0;
+          if (wl_ != 0.0 && !zero) ps = wl_ * (v3[(size_t)src * sq + l * s1 + l2 * s2 + l3 * s3] * fnorm);
+          const double nb1 = s_nb1[l];
+          const double Fb = proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1);
+          const double p = ps * Fb;
+          if (proc == 0) R1[l] += p;
+          else R2[l] += p;
+          double* Rpm = proc == 0 ? a.R1p : a.R2p;
+          if (Rpm && p != 0.0) atomicAdd(Rpm + (((size_t)row * nkc + w) * b + l) * b + l3, p);
+          if (Ps || Pb) {
+            size_t o5 = (((size_t)row * nkc + w) * b + l) * b2 + l2 * b + l3;
+            if (Ps) Ps[o5] = ps;
+            if (Pb) Pb[o5] = p;
+          }
         }
       }
     }
   }
+  if constexpr (!TILE) {
+    if (ok) {
 #pragma unroll
-  for (int l = 0; l < B; ++l) {
-    if (l >= b) continue;
-    size_t ri = (((size_t)row * nkc + w) * b + l) * b + l2;
-    a.R1[ri] = R1[l];
-    a.R2[ri] = R2[l];
+      for (int l = 0; l < B; ++l) {
+        if (l >= b) continue;
+        const size_t ri = (((size_t)row * nkc + w) * b + l) * b + l2;
+        a.R1[ri] = R1[l];
+        a.R2[ri] = R2[l];
+      }
+    }
+    return;
+  }
+  if (wl < nw) {
+#pragma unroll
+    for (int l = 0; l < B; ++l) {
+      if (l >= b) continue;
+      s_r[0][(wl * b + l) * b + l2] = R1[l];
+      s_r[1][(wl * b + l) * b + l2] = R2[l];
+    }
+  }
+  __syncthreads();
+  // the tile is one contiguous run of R1/R2: rows w0 .. w0 + nv - 1
+  const int nv = min(nw, nkc - w0);
+  const size_t base = ((size_t)row * nkc + w0) * b2;
+  for (int i = tid; i < nv * b2; i += blockDim.x) {
+    a.R1[base + i] = s_r[0][i];
+    a.R2[base + i] = s_r[1][i];
   }
 }
 
@@ -604,14 +642,15 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) 
     delta_tet_kernel<<<tg, kTetThreads, 0, s>>>(g, a.n1_first, a.mapinv, a.freq, E, Wd);
     W = Wd;
   }
-  dim3 grid((g.nkc + kPointBlock - 1) / kPointBlock, g.b, a.nrows);
+  const int nw = kPointBlock / g.b;
+  dim3 grid_tile((g.nkc + nw - 1) / nw, a.nrows), grid_row((g.nkc + kPointBlock - 1) / kPointBlock, a.nrows, g.b);
   // FP32 weights only for the Gaussian (the tetrahedron weights W are FP64 here)
   const bool fw = a.f32w && a.gauss;
-#define ALD_POINT(BB)                                               \
-  if (fw)                                                           \
-    delta_point_kernel<BB, true><<<grid, kPointBlock, 0, s>>>(a, W); \
-  else                                                              \
-    delta_point_kernel<BB, false><<<grid, kPointBlock, 0, s>>>(a, W);
+#define ALD_POINT(BB)                                                               \
+  if (fw)                                                                           \
+    delta_point_kernel<BB, true, false><<<grid_row, kPointBlock, 0, s>>>(a, W);     \
+  else                                                                              \
+    delta_point_kernel<BB, false, true><<<grid_tile, kPointBlock, 0, s>>>(a, W);
   if (g.b <= 3) {
     ALD_POINT(3)
   } else if (g.b <= 6) {

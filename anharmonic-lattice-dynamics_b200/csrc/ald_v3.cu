@@ -44,7 +44,11 @@ __device__ __forceinline__ void decompose(const Geometry& g, int n, int* m) {
   m[2] = n % g.nc[2];
 }
 
-__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L) {
+__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L, int L32) {
+  if (L32) {  // the sum fits in 32 bits: a 32-bit remainder
+    const unsigned t = (unsigned)(m[0] * pc[0] + m[1] * pc[1] + m[2] * pc[2] + pc[3]);
+    return (int)(t % (unsigned)L);
+  }
   long long t = (long long)m[0] * pc[0] + (long long)m[1] * pc[1] + (long long)m[2] * pc[2] + pc[3];
   return (int)(t % L);
 }
@@ -86,8 +90,8 @@ __global__ void __launch_bounds__(kBlock) v3_fp64_kernel(V3Args a, int ppb, int 
     e3[e] = ev[(size_t)q3 * b2 + e];
   }
   for (int j = lt; j < natoms; j += nt) {
-    tix[j] = phase_index(a.phase_coef + 4 * j, m2, g.L);
-    tix[natoms + j] = phase_index(a.phase_coef + 4 * j, m3, g.L);
+    tix[j] = phase_index(a.phase_coef + 4 * j, m2, g.L, g.L32);
+    tix[natoms + j] = phase_index(a.phase_coef + 4 * j, m3, g.L, g.L32);
   }
   __syncthreads();
   for (int t = lt; t < ntrip; t += nt) {

@@ -76,7 +76,11 @@ __device__ __forceinline__ int idx_q3(const Geometry& g, const int* m1, const in
   for (int a = 0; a < 3; ++a) m3[a] = wrapm(-m1[a] - m2[a] + (g.shifted ? g.nc[a] / 2 : 0), g.nc[a]);
   return m3[2] + g.nc[2] * (m3[1] + g.nc[1] * m3[0]);
 }
-__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L) {
+__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L, int L32) {
+  if (L32) {  // the sum fits in 32 bits: a 32-bit remainder
+    const unsigned t = (unsigned)(m[0] * pc[0] + m[1] * pc[1] + m[2] * pc[2] + pc[3]);
+    return (int)(t % (unsigned)L);
+  }
   long long t = (long long)m[0] * pc[0] + (long long)m[1] * pc[1] + (long long)m[2] * pc[2] + pc[3];
   return (int)(t % L);
 }
@@ -98,7 +102,7 @@ __global__ void v3_row_kernel(V3Args a) {
     double2 acc = make_double2(0.0, 0.0);
     for (int s = a.cls_trip_off[c]; s < a.cls_trip_off[c + 1]; ++s) {
       const int t = a.cls_trip[s], i0 = a.cls_trip_i0[s], k = a.cls_trip_k[s];
-      int ph = phase_index(a.phase_coef + 4 * k, m1, g.L);
+      int ph = phase_index(a.phase_coef + 4 * k, m1, g.L, g.L32);
       const double2 r = roots[ph == 0 ? 0 : g.L - ph];  // exp(-i q1.R_k)
       double2 x = make_double2(0.0, 0.0);
       for (int al = 0; al < 3; ++al) {
@@ -169,7 +173,7 @@ __global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
     const int q = i % QT, c = i / QT;
     int m2[3];
     decompose(g, s_q2[q], m2);
-    P[q * PP + c] = cvt<C>(roots[phase_index(a.cls_pc + 4 * c, m2, g.L)]);
+    P[q * PP + c] = cvt<C>(roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)]);
   }
   __syncthreads();
 

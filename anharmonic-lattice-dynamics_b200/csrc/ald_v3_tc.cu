@@ -66,7 +66,11 @@ __device__ __forceinline__ int idx_q3_fast(const Geometry& g, const int* m1, con
   }
   return m3[2] + g.nc[2] * (m3[1] + g.nc[1] * m3[0]);
 }
-__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L) {
+__device__ __forceinline__ int phase_index(const int* pc, const int* m, int L, int L32) {
+  if (L32) {  // the sum fits in 32 bits: a 32-bit remainder
+    const unsigned t = (unsigned)(m[0] * pc[0] + m[1] * pc[1] + m[2] * pc[2] + pc[3]);
+    return (int)(t % (unsigned)L);
+  }
   long long t = (long long)m[0] * pc[0] + (long long)m[1] * pc[1] + (long long)m[2] * pc[2] + pc[3];
   return (int)(t % L);
 }
@@ -137,7 +141,7 @@ __global__ void v3_ptile_kernel(Geometry g, int ncls, int kp, const int* cls_pc,
     float v = 0.f;
     if (k < 2 * ncls) {
       const int c = k < ncls ? k : k - ncls;
-      const double2 p = roots[phase_index(cls_pc + 4 * c, m2, g.L)];
+      const double2 p = roots[phase_index(cls_pc + 4 * c, m2, g.L, g.L32)];
       v = (float)(k < ncls ? p.x : p.y);
     }
     split_store(hi, lo, kmaj(r, k, kTM), v);

@@ -65,7 +65,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_calculate_w3_ibz_split_sq", "ald_calculate_fgr", "ald_distribution", "ald_calculate_tau_rta",
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
            "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
-           "ald_kappa_iterative"]
+           "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
+           "ald_get_isotope_g"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -240,6 +241,30 @@ class Context:
         _check(lib().ald_collision_matrix(self.h, k, _p(np.asfortranarray(P1, dtype=float)),
                                           _p(np.asfortranarray(P2, dtype=float)), _p(CM)))
         return CM
+
+    def collision_matrix_iso(self, P1, P2, Piso):
+        """CollisionMatrix_iso (sub.f90:3387) over all IBZ rows."""
+        n = self.nibz * self.ndyn * 3
+        CM = np.zeros((n, n), order="F")
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        _check(lib().ald_collision_matrix_iso(self.h, f(P1), f(P2), f(Piso), _p(CM)))
+        return CM
+
+    def p_iso_split(self, ksubset):
+        """P_iso_split (sub.f90:4825): Piso(nk1, ndyn) of IBZ rows ksubset."""
+        k = (C.c_int * 2)(*ksubset)
+        Piso = np.zeros((ksubset[1] - ksubset[0] + 1, self.ndyn), order="F")
+        _check(lib().ald_p_iso_split(self.h, k, _p(Piso)))
+        return Piso
+
+    def set_isotope_g(self, g):
+        """g (mass variance) per primitive atom, in place of the element table."""
+        _check(lib().ald_set_isotope_g(self.h, _p(np.ascontiguousarray(g, dtype=float))))
+
+    def isotope_g(self):
+        g = np.zeros(self.info.natoms0)
+        _check(lib().ald_get_isotope_g(self.h, _p(g)))
+        return g
 
     def rhs(self, tempk):
         r = np.zeros(self.nibz * self.ndyn * 3)

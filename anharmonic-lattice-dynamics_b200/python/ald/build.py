@@ -30,6 +30,7 @@ SOURCES = {
     "ald_v3_tc.cu": [],
     # weight_tet's FP32/FP64 arithmetic must not be contracted into FMAs
     "ald_tetra.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
+    "ald_iso.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
     "ald_bte.cu": [],
     "ald_util.cu": [],
     "ald_cg_static.cu": [],

@@ -148,6 +148,28 @@ int ald_rta_kappa(ald_ctx* ctx, double tempk, const double* Q, double* FFF, doub
  * nibz*ndyn*3) from the Bose-weighted P1, P2 of the same ksubset. */
 int ald_collision_matrix(ald_ctx* ctx, const int ksubset[2], const double* P1, const double* P2, double* CM);
 
+/* CollisionMatrix_iso (sub.f90:3387): the collision matrix of iso=1 over all
+ * IBZ rows, Collision_Matrix(nibz*ndyn*3, nibz*ndyn*3) column-major, from
+ * P1, P2(nibz,nkc,ndyn,ndyn,ndyn) Bose-weighted and Piso(nibz,ndyn).  The
+ * diagonal arm takes -(sum(P1 + P2/2) + Piso), every other arm
+ * sum_l3 (-P1(arm) + P1(q1+arm) + P2(arm)) + Piso, as the reference does. */
+int ald_collision_matrix_iso(ald_ctx* ctx, const double* P1, const double* P2, const double* Piso, double* CM);
+
+/* Isotope scattering (iso=1 in latdyn.params).
+ * ald_p_iso_split replaces P_iso_split (sub.f90:4825-4961): Piso(nk1,ndyn)
+ * of the IBZ rows ksubset, with g per primitive atom from cal_giso
+ * (sub.f90:4695): the mass variance of the element's natural isotopes.
+ * The element table covers Ar, C, Cl, Ge, Na, Si; ald_set_isotope_g sets g
+ * (natoms0 values) for any other, ald_get_isotope_g reads it back
+ * (ALD_ERR_UNSUPPORTED for an element outside the table).  With iso=1 the
+ * pipeline adds Piso to Q, Q_N and Q_U (calculate_tauRTA_iso,
+ * sub.f90:8311-8549) and builds the collision matrix of
+ * ald_collision_matrix_iso; the iterative solution (update_iso) is not
+ * built and returns ALD_ERR_UNSUPPORTED. */
+int ald_p_iso_split(ald_ctx* ctx, const int ksubset[2], double* Piso);
+int ald_set_isotope_g(ald_ctx* ctx, const double* g);
+int ald_get_isotope_g(ald_ctx* ctx, double* g);
+
 /* cal_RHS_IBZ (sub.f90:2618): RHS(nibz*ndyn*3). */
 int ald_rhs(ald_ctx* ctx, double tempk, double* RHS);
 

@@ -251,4 +251,27 @@ int orc_iterative(void* p, double tempk, const double* P1, const double* P2, con
   return iterative_bte(S, tempk, P1, P2, Q, F_RTA, max_iter, mix, FFF, kappa, iters, normk, nthreads);
 }
 
+// cal_giso: g per primitive atom; 0, or 1 with the message in err
+int orc_giso(void* p, double* g, char* err, int errlen) {
+  State& S = *(State*)p;
+  std::string e = cal_giso(S, g);
+  if (!e.empty()) {
+    std::snprintf(err, errlen, "%s", e.c_str());
+    return 1;
+  }
+  return 0;
+}
+
+int orc_p_iso(void* p, int k1, int k2, const double* g, double* Piso, int nthreads) {
+  State& S = *(State*)p;
+  P_iso_split(S, k1, k2, g, Piso, nthreads);
+  return 0;
+}
+
+int orc_collision_iso(void* p, const double* P1, const double* P2, const double* Piso, double* CM, int nthreads) {
+  State& S = *(State*)p;
+  CollisionMatrix_iso(S, P1, P2, Piso, CM, nthreads);
+  return 0;
+}
+
 }  // extern "C"

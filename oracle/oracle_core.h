@@ -106,6 +106,7 @@ struct State {
   std::vector<double> mas;
   int natoms0 = 0;
   std::vector<int> atom_type;   // per primitive atom (1-based type)
+  std::vector<std::string> atname;  // per type (atname, rest.f90:101)
   std::vector<double> mass0;    // atom0(i)%mass
   // ---- lat_fc.dat (rest.f90:164-289)
   double r1[3], r2[3], r3[3], g1[3], g2[3], g3[3];
@@ -193,6 +194,12 @@ int cg_quadratic(int n, const double* a, const double* b, double* vmin, double* 
 int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa);
 void update_mpi(State& S, int k1, int k2, const double* P1, const double* P2, const double* Q,
                 const double* F_RTA, const double* FFF, double* F2mpi, int nthreads);
+// isotope scattering (iso=1): cal_g / cal_giso, P_iso_split, CollisionMatrix_iso
+bool cal_g(const std::string& name, double& g);
+std::string cal_giso(const State& S, double* gis);
+void P_iso_split(State& S, int k1, int k2, const double* g, double* Piso, int nthreads);
+void CollisionMatrix_iso(State& S, const double* P1, const double* P2, const double* Piso, double* CM,
+                         int nthreads);
 int iterative_bte(State& S, double tempk, const double* P1, const double* P2, const double* Q,
                   const double* F_RTA, int max_iter, double update_mix, double* FFF, double* kappa, int* iters,
                   double* normk, int nthreads);

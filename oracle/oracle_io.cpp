@@ -404,7 +404,8 @@ std::string read_inputs(State& S, const std::string& dir) {
     t = r.read(S.natom_type);
     S.mas.resize(S.natom_type);
     for (int i = 0; i < S.natom_type; ++i) S.mas[i] = fnum(t[i]);
-    r.read(S.natom_type);
+    t = r.read(S.natom_type);
+    S.atname.assign(t.begin(), t.end());
     t = r.read(1);
     S.natoms0 = inum(t[0]);
     for (int i = 0; i < 8; ++i) r.read(1);

@@ -38,7 +38,7 @@ def lib():
                      "orc_get_k_info", "orc_getstar", "orc_kstars", "orc_dynmat", "orc_get_freq", "orc_phonons",
                      "orc_get_phonons", "orc_set_phonons", "orc_tet", "orc_v3", "orc_fgr", "orc_distribution",
                      "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d", "orc_update_mpi",
-                     "orc_iterative"]:
+                     "orc_iterative", "orc_giso", "orc_p_iso", "orc_collision_iso"]:
             getattr(L, name).restype = C.c_int
         L.orc_weight_tet_nonperm.restype = C.c_long
         _lib = L
@@ -204,6 +204,28 @@ class Oracle:
                             self.nthreads)
         return CM
 
+    def giso(self):
+        """cal_giso (sub.f90:4695): g per primitive atom from the element names."""
+        g = np.zeros(self.nat0)
+        err = C.create_string_buffer(256)
+        if lib().orc_giso(self.h, _p(g), err, 256):
+            raise RuntimeError(err.value.decode())
+        return g
+
+    def p_iso(self, k1, k2, g):
+        """P_iso_split (sub.f90:4825): Piso(nk1, ndyn) of rows k1..k2."""
+        Piso = np.zeros((k2 - k1 + 1, self.ndyn), order="F")
+        lib().orc_p_iso(self.h, k1, k2, _p(np.ascontiguousarray(g, dtype=float)), _p(Piso), self.nthreads)
+        return Piso
+
+    def collision_iso(self, P1, P2, Piso):
+        """CollisionMatrix_iso (sub.f90:3387) over all IBZ rows."""
+        n = self.nibz * self.ndyn * 3
+        CM = np.zeros((n, n), order="F")
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        lib().orc_collision_iso(self.h, f(P1), f(P2), f(Piso), _p(CM), self.nthreads)
+        return CM
+
     def rhs(self, tempk):
         r = np.zeros(self.nibz * self.ndyn * 3)
         lib().orc_rhs(self.h, C.c_double(tempk), _p(r))
@@ -285,9 +307,18 @@ def run_job1(d: str, tempk=None, gauss=None, k1=1, k2=None, phonons=None, nthrea
     Q, QN, QU, P1, P2 = O.tau(k1, k2, tempk, P1s, P2s)
     out = {"O": O, "v33": v33, "P1s": P1s, "P2s": P2s, "freq": freq, "dist": dist, "Q": Q, "QN": QN, "QU": QU,
            "P1": P1, "P2": P2, "tempk": tempk}
+    # iso=1 (latdyn.params line 11): calculate_tauRTA_iso adds Piso to Q, Q_N
+    # and Q_U (sub.f90:8311-8549); the collision matrix is CollisionMatrix_iso
+    iso = int(open(os.path.join(d, "latdyn.params")).read().split("\n")[10].split()[0]) == 1
+    if iso:
+        g = O.giso()
+        Piso = O.p_iso(k1, k2, g)
+        out.update({"giso": g, "Piso": Piso, "Q3": Q.copy()})
+        Q, QN, QU = Q + Piso, QN + Piso, QU + Piso
+        out.update({"Q": Q, "QN": QN, "QU": QU})
     if k1 == 1 and k2 == O.nibz:
         FFF, krta = O.rta(tempk, Q)
-        CM = O.collision(k1, k2, P1, P2)
+        CM = O.collision_iso(P1, P2, out["Piso"]) if iso else O.collision(k1, k2, P1, P2)
         RHS = O.rhs(tempk)
         x0 = np.array([FFF[i, j, k] for i in range(O.nibz) for j in range(O.ndyn) for k in range(3)])
         x, fmin, it = O.cg(CM, RHS, x0)
