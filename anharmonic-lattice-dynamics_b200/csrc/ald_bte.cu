@@ -295,8 +295,8 @@ struct CgDev {
   double bnorm;
 };
 
-// y = A x for a row-major A (leading dimension ld) of double or float, x
-// and y double; partial[blk] = the block's sum of y*x (and partial_g[blk]
+// y = A x for a row-major A of nrows x n (leading dimension ld) of double or
+// float, x and y double; partial[blk] = the block's sum of y*x (and partial_g[blk]
 // that of g*x).  A block takes
 // kGemvRows rows; its warps split the columns, so each x vector a warp
 // loads serves all the rows, and small matrices still give n/kGemvRows
@@ -322,7 +322,8 @@ struct Vec16<float> {
 };
 
 template <class T>
-__global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld, int vec, const T* __restrict__ A,
+__global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int nrows, int n, size_t ld, int vec,
+                                                               const T* __restrict__ A,
                                                                const double* __restrict__ x, double* __restrict__ y,
                                                                double* partial, const double* g, double* partial_g,
                                                                const CgDev* st) {
@@ -334,7 +335,7 @@ __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld,
   const int row0 = blockIdx.x * kGemvRows;
   const T* Ar[kGemvRows];
 #pragma unroll
-  for (int r = 0; r < kGemvRows; ++r) Ar[r] = A + (size_t)min(row0 + r, n - 1) * ld;  // rows past n: discarded
+  for (int r = 0; r < kGemvRows; ++r) Ar[r] = A + (size_t)min(row0 + r, nrows - 1) * ld;  // rows past nrows: discarded
   double acc[kGemvRows];
 #pragma unroll
   for (int r = 0; r < kGemvRows; ++r) acc[r] = 0.0;
@@ -374,7 +375,7 @@ __global__ void __launch_bounds__(kGemvWarps * 32) gemv_kernel(int n, size_t ld,
   __syncthreads();
   if (threadIdx.x == 0) {
     double dot = 0.0, gdot = 0.0;
-    for (int r = 0; r < kGemvRows && row0 + r < n; ++r) {
+    for (int r = 0; r < kGemvRows && row0 + r < nrows; ++r) {
       double t = 0.0;
       for (int w = 0; w < kGemvWarps; ++w) t += red[w][r];
       y[row0 + r] = t;
@@ -499,6 +500,39 @@ __global__ void __launch_bounds__(kCgThreads) cg_dir_kernel(int n, const double*
   }
 }
 
+// per-CTA partial sums of aux.conj (den) and grad.conj (num) over full
+// vectors, the row-sharded CG's stand-in for the gemv partials
+__global__ void __launch_bounds__(256) cg_dots_kernel(int n, const double* aux, const double* conj,
+                                                      const double* grad, double* pden, double* pnum,
+                                                      const CgDev* st) {
+  if (st->done) return;
+  __shared__ double red[2][8];
+  double d = 0, g = 0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double c = conj[i];
+    d += aux[i] * c;
+    g += grad[i] * c;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    d += __shfl_down_sync(0xffffffffu, d, o);
+    g += __shfl_down_sync(0xffffffffu, g, o);
+  }
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = d;
+    red[1][threadIdx.x >> 5] = g;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double a = 0, b = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+      a += red[0][w];
+      b += red[1][w];
+    }
+    pden[blockIdx.x] = a;
+    pnum[blockIdx.x] = b;
+  }
+}
+
 __global__ void cg_fmin_kernel(int n, const double* x, const double* Ax, const double* b, double* out) {
   double s1 = 0, s2 = 0;
   for (int i = threadIdx.x; i < n; i += blockDim.x) {
@@ -583,7 +617,7 @@ static cudaError_t capture_cg(int iters, int n, size_t ld, int vec, int nblk, co
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
   for (int it = 0; it < iters; ++it) {
-    gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, w.conj.p, w.aux.p, w.partial.p, w.grad.p,
+    gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, n, ld, vec, dA, w.conj.p, w.aux.p, w.partial.p, w.grad.p,
                                                      w.pnum.p, st);
     cg_update_kernel<<<nb, kCgThreads, 0, s>>>(n, w.aux.p, w.partial.p, w.pnum.p, nblk, w.grad.p, w.conj.p, w.v0.p,
                                                dx, w.p4.p, st);
@@ -613,7 +647,7 @@ static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* 
     return ALD_ERR_NOMEM;
   }
   CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
-  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
                                                    nullptr);
   cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, db, w.grad.p, w.conj.p, st);
   cudaError_t e = cudaSuccess;
@@ -653,7 +687,7 @@ static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* 
     msg = std::string("cg: ") + cudaGetErrorString(e);
     return ALD_ERR_CUDA;
   }
-  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
+  gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(n, n, ld, vec, dA, dx, w.aux.p, nullptr, nullptr, nullptr,
                                                    nullptr);
   cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, w.aux.p, db, w.fmin.p);
   CgDev h;
@@ -672,6 +706,87 @@ static int cg_device_t(int n, size_t ld, const T* dA, const double* db, double* 
 int cg_device(int n, const double* dA, const double* db, double* dx, int max_iter, int mode, double tol, int* iters,
               double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
   return cg_device_t<double>(n, (size_t)n, dA, db, dx, max_iter, mode, tol, iters, err_out, funcmin, s, w, msg);
+}
+
+// Row-sharded cg_quadratic: this rank holds rows [row0, row0 + nrows) of A
+// (row-major, leading dimension ld); x, b and the CG vectors are full and
+// replicated.  Per iteration: the local rows of A conj, the all-gather of
+// that product (the caller's exchange), then the same update kernels as
+// cg_device on every rank, so every rank takes the same steps and stops at
+// the same iteration.  No graphs: the exchange runs on the host.
+template <class T>
+static int cg_rows_t(int n, int row0, int nrows, size_t ld, const T* dA, const double* db, double* dx, int max_iter,
+                     int mode, double tol, const CgAllGather& gather, int* iters, double* err_out, double* funcmin,
+                     cudaStream_t s, CgWork& w, std::string& msg) {
+  const int nblk = (nrows + kGemvRows - 1) / kGemvRows;
+  const int nb = std::min(kCgBlocksMax, (n + kCgThreads - 1) / kCgThreads);
+  if (w.grad.alloc(n) || w.conj.alloc(n) || w.aux.alloc(n) || w.v0.alloc(n) || w.partial.alloc(nb) ||
+      w.pnum.alloc(nb) || w.p4.alloc(4 * kCgBlocksMax) || w.fmin.alloc(1) || w.st.alloc(sizeof(CgDev)) ||
+      w.yloc.alloc(std::max(nrows, 1))) {
+    msg = "cg: allocation failed";
+    return ALD_ERR_NOMEM;
+  }
+  const int vec = ((uintptr_t)dA & 15u) == 0 && (ld * sizeof(T)) % 16 == 0;
+  CgDev* st = reinterpret_cast<CgDev*>(w.st.p);
+  auto product = [&](const double* v, const CgDev* stp) -> int {  // aux = A v, all rows
+    if (nrows > 0)
+      gemv_kernel<T><<<nblk, kGemvWarps * 32, 0, s>>>(nrows, n, ld, vec, dA, v, w.yloc.p, nullptr, nullptr, nullptr,
+                                                       stp);
+    if (cudaGetLastError() != cudaSuccess) return ALD_ERR_CUDA;
+    return gather(w.yloc.p, (size_t)nrows, w.aux.p);
+  };
+  int r = product(dx, nullptr);
+  if (r) {
+    msg = "cg: the exchange of A x failed";
+    return r;
+  }
+  cg_init_kernel<<<1, kVecThreads, 0, s>>>(n, w.aux.p, db, w.grad.p, w.conj.p, st);
+  CgDev h{};
+  for (int it = 0; it < max_iter; ++it) {
+    r = product(w.conj.p, nullptr);
+    if (r) {
+      msg = "cg: the exchange of A conj failed";
+      return r;
+    }
+    cg_dots_kernel<<<nb, 256, 0, s>>>(n, w.aux.p, w.conj.p, w.grad.p, w.partial.p, w.pnum.p, st);
+    cg_update_kernel<<<nb, kCgThreads, 0, s>>>(n, w.aux.p, w.partial.p, w.pnum.p, nb, w.grad.p, w.conj.p, w.v0.p, dx,
+                                               w.p4.p, st);
+    cg_dir_kernel<<<nb, kCgThreads, 0, s>>>(n, w.p4.p, w.grad.p, w.conj.p, st, mode, tol);
+    cudaError_t e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) {
+      msg = std::string("cg: ") + cudaGetErrorString(e);
+      return ALD_ERR_CUDA;
+    }
+    if (h.done) break;
+  }
+  r = product(dx, nullptr);
+  if (r) {
+    msg = "cg: the exchange of A x failed";
+    return r;
+  }
+  cg_fmin_kernel<<<1, kVecThreads, 0, s>>>(n, dx, w.aux.p, db, w.fmin.p);
+  cudaError_t e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(funcmin, w.fmin.p, sizeof(double), cudaMemcpyDeviceToHost, s);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+  if (e != cudaSuccess) {
+    msg = std::string("cg: ") + cudaGetErrorString(e);
+    return ALD_ERR_CUDA;
+  }
+  *iters = h.iters;
+  *err_out = h.err;
+  return h.done ? ALD_OK : ALD_WARN_CG_MAXITER;
+}
+
+int cg_device_rows(int n, int row0, int nrows, size_t ld, const void* dA, int a_f32, const double* db, double* dx,
+                   int max_iter, int mode, double tol, const CgAllGather& gather, int* iters, double* err_out,
+                   double* funcmin, cudaStream_t s, CgWork& w, std::string& msg) {
+  (void)row0;
+  if (a_f32)
+    return cg_rows_t<float>(n, row0, nrows, ld, static_cast<const float*>(dA), db, dx, max_iter, mode, tol, gather,
+                            iters, err_out, funcmin, s, w, msg);
+  return cg_rows_t<double>(n, row0, nrows, ld, static_cast<const double*>(dA), db, dx, max_iter, mode, tol, gather,
+                           iters, err_out, funcmin, s, w, msg);
 }
 
 int cg_launched_iterations(int iters, int max_iter) {

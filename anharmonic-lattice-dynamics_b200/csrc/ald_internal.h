@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -353,6 +354,7 @@ cudaError_t launch_update(const Geometry& geo, int n1_first, int nrows, const in
 // (size, pointers, stop rule) changes
 struct CgWork {
   DevBuf<double> grad, conj, aux, v0, partial, pnum, p4, fmin;
+  DevBuf<double> yloc;  // the local rows of A v (row-sharded CG)
   DevBuf<char> st;
   cudaGraphExec_t exec = nullptr;       // kCgChunk iterations
   cudaGraphExec_t exec_tail = nullptr;  // max_iter % kCgChunk iterations
@@ -371,6 +373,12 @@ struct CgWork {
 };
 int cg_device(int n, const double* dA /*row-major*/, const double* db, double* dx, int max_iter, int mode,
               double tol, int* iters, double* err_out, double* funcmin, cudaStream_t s, CgWork& w, std::string& msg);
+// The exchange of the row-sharded CG: gather this rank's `count` values
+// (device) into the full vector `all` (device, rank order); 0 on success.
+using CgAllGather = std::function<int(const double* mine, size_t count, double* all)>;
+int cg_device_rows(int n, int row0, int nrows, size_t ld, const void* dA, int a_f32, const double* db, double* dx,
+                   int max_iter, int mode, double tol, const CgAllGather& gather, int* iters, double* err_out,
+                   double* funcmin, cudaStream_t s, CgWork& w, std::string& msg);
 // CG iterations whose kernels were launched for a solve that stopped after
 // iters (the captured chunks run to their end, as no-ops after the stop)
 int cg_launched_iterations(int iters, int max_iter);

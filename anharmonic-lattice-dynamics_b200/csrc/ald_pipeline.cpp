@@ -75,9 +75,30 @@ struct IterSpec {
   double* F;  // optional out: FFF(nibz, ndyn, 3)
 };
 
+// the row split of the reference's MPI job (kappa.f90:418-428): nibz/nranks
+// rows per rank, the last rank also takes the remainder; 0-based [rb, re)
+static void shard_range(int nibz, int rank, int nranks, int& rb, int& re) {
+  const int local = nibz / nranks;
+  rb = rank * local;
+  re = rank == nranks - 1 ? nibz : rb + local;
+}
+
+// one rank of a row-sharded job=1 (the reference's MPI decomposition): this
+// rank computes V3, the delta, Q and the collision-matrix rows of its IBZ
+// rows; Q and the CG matrix-vector products are exchanged through `gather`
+struct ShardSpec {
+  int rank, nranks;
+  ald_allgather_fn gather;
+  void* user;
+};
+
 static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo, double* QUo,
-                        double* kappa_rta_modes, double* kappa_cg_modes, double* xo, const IterSpec* it) {
+                        double* kappa_rta_modes, double* kappa_cg_modes, double* xo, const IterSpec* it,
+                        const ShardSpec* sh = nullptr) {
   if (!c || !res) return fail(ALD_ERR_ARG, "null argument");
+  if (sh && (sh->nranks < 1 || sh->rank < 0 || sh->rank >= sh->nranks || !sh->gather))
+    return fail(ALD_ERR_ARG, "sharded pipeline: bad rank, rank count or exchange function");
+  if (sh && it) return fail(ALD_ERR_UNSUPPORTED, "the sharded pipeline runs job=1 only");
   if (it && !c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
   if (it && c->S.iso == 1)
     return fail(ALD_ERR_UNSUPPORTED, "the iterative solution with isotope scattering (update_iso) is not built");
@@ -110,8 +131,31 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   r = ensure_dist(c, tempk);
   if (r) return r;
   ALD_CK(tm.end());
-  // ---- 1, 2: V3 and delta/Bose/band sums, chunk by chunk
-  const size_t rsz = (size_t)nibz * nkc * b * b;
+  // this rank's IBZ rows [rb, re) (all rows unless sharded)
+  int rb = 0, re = nibz;
+  if (sh) shard_range(nibz, sh->rank, sh->nranks, rb, re);
+  const int nloc = re - rb;
+  // exchange of per-row blocks of `unit` values through the caller's
+  // all-gather, staged in host memory
+  auto gather_rows = [&](const double* mine, double* all, size_t unit) -> int {
+    std::vector<long long> counts(sh->nranks);
+    for (int k2 = 0; k2 < sh->nranks; ++k2) {
+      int a0, a1;
+      shard_range(nibz, k2, sh->nranks, a0, a1);
+      counts[k2] = (long long)(a1 - a0) * (long long)unit;
+    }
+    std::vector<double> hm((size_t)nloc * unit), ha((size_t)nibz * unit);
+    if (!hm.empty() && cudaMemcpyAsync(hm.data(), mine, hm.size() * sizeof(double), cudaMemcpyDeviceToHost, s))
+      return ALD_ERR_CUDA;
+    if (cudaStreamSynchronize(s) != cudaSuccess) return ALD_ERR_CUDA;
+    if (sh->gather(sh->user, hm.data(), (long long)hm.size(), ha.data(), counts.data(), sh->nranks) != 0)
+      return ALD_ERR_ARG;
+    if (cudaMemcpyAsync(all, ha.data(), ha.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
+      return ALD_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? ALD_OK : ALD_ERR_CUDA;
+  };
+  // ---- 1, 2: V3 and delta/Bose/band sums, chunk by chunk (this rank's rows)
+  const size_t rsz = (size_t)std::max(nloc, 1) * nkc * b * b;
   DevBuf<double>& R1 = c->w_R1;
   DevBuf<double>& R2 = c->w_R2;
   DevBuf<double>& Q = c->w_Q;
@@ -133,8 +177,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
   // class-form V3 kernels write that layout
   const int v3_layout = v3_pair_supported(b, c->opt.precision) ? 1 : 0;
-  for (int r0 = 0; r0 < nibz; r0 += K) {
-    int nr = std::min(K, nibz - r0);
+  for (int r0 = rb; r0 < re; r0 += K) {
+    int nr = std::min(K, re - r0);
     ALD_CK(tm.begin(1));
     V3Args va = v3_args(c, r0, nr, v3.p);
     va.v3_layout = v3_layout;
@@ -155,8 +199,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     a.gauss = gauss;
     a.sigma = gauss_width(c);
     a.f32w = c->opt.precision != ALD_FP64;  // mixed: FP32 delta weights
-    a.R1 = R1.p + (size_t)r0 * nkc * b * b;
-    a.R2 = R2.p + (size_t)r0 * nkc * b * b;
+    a.R1 = R1.p + (size_t)(r0 - rb) * nkc * b * b;
+    a.R2 = R2.p + (size_t)(r0 - rb) * nkc * b * b;
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
     a.R1p = it ? c->w_R1p.p + (size_t)r0 * nkc * b * b : nullptr;
     a.R2p = it ? c->w_R2p.p + (size_t)r0 * nkc * b * b : nullptr;
@@ -183,7 +227,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   double* dQN = Q.p + (size_t)nibz * b;
   double* dQU = Q.p + (size_t)2 * nibz * b;
   ALD_CK(tm.begin(3));
-  ALD_CK(launch_q_from_r(c->geo, 0, nibz, c->mapinv.p, R1.p, R2.p, dQ, dQN, dQU, nibz, s));
+  if (nloc > 0) ALD_CK(launch_q_from_r(c->geo, rb, nloc, c->mapinv.p, R1.p, R2.p, dQ, dQN, dQU, nibz, s));
   res->launches[3] += 1;
   // iso=1: isotope scattering (P_iso_split), Q, Q_N, Q_U += Piso as in
   // calculate_tauRTA_iso (sub.f90:8311-8549)
@@ -191,11 +235,19 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   if (iso) {
     r = ensure_giso(c);
     if (r) return r;
-    ALD_CKA(c->w_piso.alloc((size_t)nibz * b));
-    ALD_CKA(c->w_piso_part.alloc(piso_partial_doubles(c->geo, nibz)));
-    ALD_CK(launch_piso(c->geo, 0, nibz, c->mapinv.p, c->freq.p, c->evec.p, c->tet_corner.p, c->giso_d.p,
-                       c->w_piso_part.p, c->w_piso.p, dQ, dQN, dQU, s));
+    ALD_CKA(c->w_piso.alloc((size_t)std::max(nloc, 1) * b));
+    ALD_CKA(c->w_piso_part.alloc(piso_partial_doubles(c->geo, std::max(nloc, 1))));
+    if (nloc > 0)
+      ALD_CK(launch_piso(c->geo, rb, nloc, c->mapinv.p, c->freq.p, c->evec.p, c->tet_corner.p, c->giso_d.p,
+                         c->w_piso_part.p, c->w_piso.p, dQ + (size_t)rb * b, dQN + (size_t)rb * b,
+                         dQU + (size_t)rb * b, s));
     res->launches[3] += 2;
+  }
+  if (sh) {  // every rank needs Q of every row (MPI_Allgatherv, kappa.f90:641-643)
+    for (double* q : {dQ, dQN, dQU}) {
+      r = gather_rows(q + (size_t)rb * b, q, (size_t)b);
+      if (r) return fail(r, "sharded pipeline: the exchange of Q failed");
+    }
   }
   ALD_CK(tm.end());
   // ---- 4: RTA
@@ -306,11 +358,13 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   // once per iteration, and the products are still summed in FP64.
   const int cm_f32 = c->opt.precision != ALD_FP64;
   const size_t ld = cm_f32 ? (N + 3) / 4 * 4 : (N + 1) / 2 * 2;
-  const size_t cm_bytes = N * ld * (cm_f32 ? sizeof(float) : sizeof(double));
+  const size_t Nloc = (size_t)3 * b * nloc;  // this rank's rows of the matrix
+  const size_t cm_bytes = std::max<size_t>(Nloc, 1) * ld * (cm_f32 ? sizeof(float) : sizeof(double));
   ALD_CKA(cm.alloc((cm_bytes + sizeof(double) - 1) / sizeof(double)));
   ALD_CK(tm.begin(5));
-  ALD_CK(launch_collision(c->geo, nibz, 0, nibz, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, dQ,
-                          R1.p, R2.p, cm.p, ld, cm_f32, iso ? c->w_piso.p : nullptr, s));
+  if (nloc > 0)
+    ALD_CK(launch_collision(c->geo, nibz, rb, nloc, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p,
+                            dQ + (size_t)rb * b, R1.p, R2.p, cm.p, ld, cm_f32, iso ? c->w_piso.p : nullptr, s));
   res->launches[5] += 1;
   ALD_CK(tm.end());
   // ---- 6: RHS and the initial guess x0 = F_RTA (kappa.f90:835-843)
@@ -325,10 +379,20 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   std::string msg;
   double tol = c->opt.cg_stop == ALD_CG_REFERENCE ? 1.0 / std::pow(10.0, 2 * c->opt.cg_ndig) : c->opt.cg_tol;
   ALD_CK(tm.begin(7));
-  int rc = cg_device_ld((int)N, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters,
-                        &cg_err, &fm, s, c->cg, msg);
+  int rc;
+  if (sh) {
+    const CgAllGather gather = [&](const double* mine, size_t, double* all) {
+      return gather_rows(mine, all, (size_t)3 * b);
+    };
+    rc = cg_device_rows((int)N, 3 * b * rb, (int)Nloc, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter,
+                        c->opt.cg_stop, tol, gather, &iters, &cg_err, &fm, s, c->cg, msg);
+    res->launches[7] += 4 + 4 * iters;
+  } else {
+    rc = cg_device_ld((int)N, ld, cm.p, cm_f32, rhs.p, x.p, c->opt.cg_max_iter, c->opt.cg_stop, tol, &iters, &cg_err,
+                      &fm, s, c->cg, msg);
+    res->launches[7] += 4 + 3 * cg_launched_iterations(iters, c->opt.cg_max_iter);
+  }
   if (rc != ALD_OK && rc != ALD_WARN_CG_MAXITER) return fail(rc, msg);
-  res->launches[7] += 4 + 3 * cg_launched_iterations(iters, c->opt.cg_max_iter);
   ALD_CK(tm.end());
   // ---- 8: mode_kappa_d
   ALD_CK(tm.begin(8));
@@ -387,6 +451,22 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
 extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo,
                                   double* QUo, double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
   return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr);
+}
+
+extern "C" int ald_shard_rows(const ald_ctx* c, int rank, int nranks, int ksubset[2]) {
+  if (!c || !ksubset || nranks < 1 || rank < 0 || rank >= nranks) return fail(ALD_ERR_ARG, "bad rank or rank count");
+  int rb, re;
+  shard_range(c->T.nibz, rank, nranks, rb, re);
+  ksubset[0] = rb + 1;
+  ksubset[1] = re;
+  return ALD_OK;
+}
+
+extern "C" int ald_kappa_pipeline_sharded(ald_ctx* c, double tempk, int rank, int nranks, ald_allgather_fn gather,
+                                          void* user, ald_kappa_result* res, double* Qo, double* QNo, double* QUo,
+                                          double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
+  ShardSpec sh{rank, nranks, gather, user};
+  return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr, &sh);
 }
 
 extern "C" int ald_kappa_iterative(ald_ctx* c, double tempk, int max_iter, double update_mix, ald_kappa_result* res,

@@ -66,7 +66,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
            "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
-           "ald_get_isotope_g"]
+           "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -326,6 +326,84 @@ class Context:
         if want_modes:
             out.update({"Q": Q, "QN": QN, "QU": QU, "kappa_rta_modes": kr, "kappa_cg_modes": kc, "x": x})
         return out
+
+    def shard_rows(self, rank: int, nranks: int) -> Tuple[int, int]:
+        k = (C.c_int * 2)()
+        _check(lib().ald_shard_rows(self.h, rank, nranks, k))
+        return k[0], k[1]
+
+    def kappa_pipeline_sharded(self, rank: int, nranks: int, gather, tempk: Optional[float] = None):
+        """One rank of the row-sharded job=1 (ald_kappa_pipeline_sharded).
+        `gather(mine, counts)` is the all-gather: it receives this rank's
+        values (numpy) and the per-rank counts and returns every rank's values
+        concatenated in rank order (e.g. torch_allgather())."""
+        if tempk is None:
+            tempk = self.info.tempk
+        err = []
+
+        def cb(user, mine, count, out, counts, nranks_):
+            try:
+                cn = [counts[k] for k in range(nranks_)]
+                a = np.ctypeslib.as_array(mine, shape=(count,)) if count > 0 else np.zeros(0)
+                allv = np.asarray(gather(a.copy(), cn), dtype=float)
+                if allv.shape != (sum(cn),):
+                    raise ValueError("all-gather returned %s values, expected %d" % (allv.shape, sum(cn)))
+                np.ctypeslib.as_array(out, shape=(sum(cn),))[:] = allv
+                return 0
+            except Exception as ex:  # reported after the call returns
+                err.append(ex)
+                return 1
+
+        fn = ALLGATHER_FN(cb)
+        res = KappaResult()
+        n, ni = self.ndyn, self.nibz
+        Q, QN, QU = (np.zeros((ni, n), order="F") for _ in range(3))
+        kr, kc = np.zeros((n, 3, 3), order="F"), np.zeros((n, 3, 3), order="F")
+        x = np.zeros(ni * n * 3)
+        r = lib().ald_kappa_pipeline_sharded(self.h, C.c_double(tempk), rank, nranks, fn, None, C.byref(res), _p(Q),
+                                             _p(QN), _p(QU), _p(kr), _p(kc), _p(x))
+        if err:
+            raise err[0]
+        _check(r)
+        return {"kappa_rta": np.array(res.kappa_rta).reshape(3, 3, order="F"),
+                "kappa_cg": np.array(res.kappa_cg).reshape(3, 3, order="F"), "cg_iters": res.cg_iters,
+                "status_cg": res.status_cg, "stage_ms": dict(zip(STAGES, list(res.stage_ms))),
+                "Q": Q, "QN": QN, "QU": QU, "kappa_rta_modes": kr, "kappa_cg_modes": kc, "x": x}
+
+
+# int (*)(void* user, const double* mine, long long count, double* all, const long long* counts, int nranks)
+ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_longlong, C.POINTER(C.c_double),
+                           C.POINTER(C.c_longlong), C.c_int)
+
+
+def shard_rows(nibz: int, rank: int, nranks: int) -> Tuple[int, int]:
+    """The 1-based IBZ row range of a rank in the reference's MPI split
+    (kappa.f90:418-428): nibz // nranks rows each, the last rank also takes
+    the remainder (ald_shard_rows computes the same on the library side)."""
+    local = nibz // nranks
+    lo = rank * local + 1
+    hi = nibz if rank == nranks - 1 else rank * local + local
+    return lo, hi
+
+
+def torch_allgather(group=None):
+    """An all-gather for kappa_pipeline_sharded over torch.distributed: the
+    ranks' arrays (different lengths allowed) padded to the longest, gathered
+    with all_gather (on the current CUDA device for NCCL, on the CPU for
+    gloo) and concatenated in rank order."""
+    import torch
+    import torch.distributed as dist
+
+    def gather(mine: np.ndarray, counts: Sequence[int]) -> np.ndarray:
+        dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else "cpu"
+        m = max(counts)
+        buf = torch.zeros(m, dtype=torch.float64, device=dev)
+        buf[:len(mine)] = torch.from_numpy(np.ascontiguousarray(mine)).to(dev)
+        parts = [torch.empty_like(buf) for _ in counts]
+        dist.all_gather(parts, buf, group=group)
+        return np.concatenate([p[:c].cpu().numpy() for p, c in zip(parts, counts)])
+
+    return gather
 
 
 def cg_quadratic(a, b, vmin, max_iter=100, n_dig_accur=2):

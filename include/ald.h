@@ -243,6 +243,28 @@ double ald_h2d_bytes(ald_ctx* ctx);
 int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double* Q, double* QN, double* QU,
                        double* kappa_rta_modes, double* kappa_cg_modes, double* x);
 
+/* Row-sharded job=1, one call per rank (one process per GPU): the MPI
+ * decomposition of kappa_full (kappa.f90:418-428: nibz/nranks IBZ rows per
+ * rank, the last rank also takes the remainder; ald_shard_rows returns a
+ * rank's 1-based range).  Each rank computes V3, the delta, Q, Q_N, Q_U and
+ * the collision-matrix rows of its own IBZ rows.  Two exchanges replace
+ * the reference's MPI_Allgatherv calls (kappa.f90:641-643, 790): Q, Q_N, Q_U
+ * once, and in every CG iteration the local rows of the matrix-vector
+ * product, so the 3 b nibz x 3 b nibz matrix is never gathered.  `gather`
+ * is the caller's all-gather (NCCL, MPI, ...) over host buffers: it
+ * receives this rank's `count` values in `mine` and must fill `all` with
+ * every rank's values in rank order (counts[k] values of rank k), return 0
+ * on success; it is called the same number of times, in the same order,
+ * on every rank.  The CG vectors are replicated, so every rank returns the
+ * same kappa and the full Q/x.  Outputs as ald_kappa_pipeline; iso=1 is
+ * supported, job=3 is not. */
+typedef int (*ald_allgather_fn)(void* user, const double* mine, long long count, double* all,
+                                const long long* counts, int nranks);
+int ald_shard_rows(const ald_ctx* ctx, int rank, int nranks, int ksubset[2]);
+int ald_kappa_pipeline_sharded(ald_ctx* ctx, double tempk, int rank, int nranks, ald_allgather_fn gather,
+                               void* user, ald_kappa_result* res, double* Q, double* QN, double* QU,
+                               double* kappa_rta_modes, double* kappa_cg_modes, double* x);
+
 /* The job=3 sequence (kappa.f90:1046-1487): as ald_kappa_pipeline up to the
  * RTA kappa, then from FFF = F_RTA repeat FFF += update_mix (update_mpi(FFF)
  * - FFF) and kappa = mode_kappa(FFF) until sqrt(sum((kappa_new -
