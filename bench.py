@@ -169,7 +169,7 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8):
     ms = stages[dom] / n
     N = 3 * b * nibz
     b3 = b ** 3
-    # algorithmic bytes per launch ("Rooflines")
+    # algorithmic bytes per launch of the dominant stage
     per = {
         "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n,            # |V3|^2 out + e(q2), e(q3) in
         "delta": nibz * nkc * (b3 * 8 + 2 * b * b * 8 * 2) / n,      # |V3|^2 in + R1/R2 out (read+write)
@@ -185,15 +185,15 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8):
                 "traffic": None, "kernel": dom}
     ach = bytes_ / (ms * 1e-3) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of a 72-row chunk of this
-    # workload (profiles/kappa_pipeline_nacl_morse_mesh16.md), scaled to the rows of a launch
-    ncu_bytes_72rows = {("delta", 4096, 6): 444.64e6, ("v3", 4096, 6): 479.12e6}
+    # workload, scaled to the rows of a launch
+    ncu_bytes_72rows = {("delta", 4096, 6): 450.70e6, ("v3", 4096, 6): 475.61e6}
     traffic = None
     if (dom, nkc, b) in ncu_bytes_72rows:
         traffic = ncu_bytes_72rows[(dom, nkc, b)] * (nibz / n) / 72
     return {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
             "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom, "ms_per_launch": ms,
             "algorithmic_bytes": bytes_, "peak_source": peaks["src"],
-            "note": "the delta and V3 kernels are FP64-ALU bound; ncu FP64-pipe utilisation is in profiles/"}
+            "note": "the delta and V3 kernels are bound by instruction issue (ALU/FMA/FP64 pipes in ncu), not by HBM"}
 
 
 def main():
