@@ -127,7 +127,7 @@ __global__ void v3_row_kernel(V3Args a) {
 // mode product 2 (q, c', l1 block) -> (B/S) x B accumulators;
 // mode product 3 (q, l1, l2 block) -> (B/S) x B accumulators and |V|^2.
 template <class T, int B, int QT, int S, int NT>
-__global__ void __launch_bounds__(NT, 2) v3_pair_kernel(V3Args a) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 2) v3_pair_kernel(V3Args a) {
   using C = typename Cx<T>::t;
   constexpr int NAT = B / 3, B2 = B * B, B3 = B2 * B, NG = NAT * NAT;
   constexpr int AP = B3 | 1, EP = B2 | 1, BS = B / S;
