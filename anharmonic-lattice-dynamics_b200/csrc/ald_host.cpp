@@ -21,6 +21,7 @@
 #include <fstream>
 #include <map>
 #include <numeric>
+#include <thread>
 #include <unordered_map>
 
 #include "ald_internal.h"
@@ -450,6 +451,10 @@ std::string read_system(const std::string& dir, System& S) {
 }
 
 // ======================================================================
+// nearest integer by conversion (no libm call); a fraction of exactly .5
+// rounds away from zero, which the tolerance tests below reject either way
+static inline double round_near(double x) { return (double)(long long)(x + (x >= 0 ? 0.5 : -0.5)); }
+
 std::string build_tables(const System& S, Tables& T) {
   const int N0 = S.nc[0], N1 = S.nc[1], N2 = S.nc[2];
   T.nkc = N0 * N1 * N2;
@@ -528,7 +533,7 @@ std::string build_tables(const System& S, Tables& T) {
     in_cell = true;
     for (int a = 0; a < 3; ++a) {
       double x = f[a] * S.nc[a] + (T.shifted ? 0.5 * S.nc[a] : 0.0);
-      double r = std::nearbyint(x);
+      double r = round_near(x);
       // x is in units of one mesh step; FP32 mesh fractions leave ~1e-6 noise
       if (std::fabs(r - x) > 1e-3) return -1;
       long ir = (long)r;
@@ -542,7 +547,8 @@ std::string build_tables(const System& S, Tables& T) {
   auto star = [&](const double* kc, std::vector<std::array<double, 3>>& arms, std::vector<int>& armop) {
     arms.clear();
     armop.clear();
-    std::vector<std::array<double, 3>> key;
+    std::array<double, 3> key[48];  // at most 48 point operations
+    int nkey = 0;
     for (int o = 0; o < T.npg; ++o) {
       double v[3], v2[3];
       for (int a = 0; a < 3; ++a) {
@@ -556,11 +562,12 @@ std::string build_tables(const System& S, Tables& T) {
         v2[a] = s;
       }
       bool dup = false;
-      for (auto& kk : key) {
+      for (int q = 0; q < nkey && !dup; ++q) {
+        const auto& kk = key[q];
         int c;
         for (c = 0; c < 3; ++c) {
           double d = v2[c] - kk[c];
-          if (std::fabs(d - std::nearbyint(d)) > 1e-6) break;
+          if (std::fabs(d - round_near(d)) > 1e-6) break;
         }
         if (c == 3) {
           dup = true;
@@ -568,7 +575,7 @@ std::string build_tables(const System& S, Tables& T) {
         }
       }
       if (dup) continue;
-      key.push_back({v2[0], v2[1], v2[2]});
+      key[nkey++] = {v2[0], v2[1], v2[2]};
       arms.push_back({v[0], v[1], v[2]});
       armop.push_back(o);
     }
@@ -582,15 +589,38 @@ std::string build_tables(const System& S, Tables& T) {
   std::vector<double> w;
   std::vector<std::array<double, 3>> arms;
   std::vector<int> armop;
+  // The stars of all mesh points are independent: they are found on host
+  // threads first, as per point the mesh index of each arm in star order
+  // (-2: off the mesh or outside its cell, -1: end of the list); the pass
+  // that assigns IBZ points is sequential, as in the reference.
+  const int npg = T.npg;
+  std::vector<int> cand((size_t)T.nkc * npg, -1);
+  {
+    const int nthr = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&, t] {
+        std::vector<std::array<double, 3>> ar;
+        std::vector<int> ao;
+        for (int n = t; n < T.nkc; n += nthr) {
+          star(&T.kpc32[3 * (size_t)n], ar, ao);
+          for (size_t c = 0; c < ar.size(); ++c) {
+            double f[3];
+            reduced(ar[c].data(), f);
+            bool in_cell;
+            const int idx = locate(f, in_cell);
+            cand[(size_t)n * npg + c] = idx >= 0 && in_cell ? idx : -2;
+          }
+        }
+      });
+    for (auto& th : pool) th.join();
+  }
   for (int n = 0; n < T.nkc; ++n) {
-    star(&T.kpc32[3 * (size_t)n], arms, armop);
     int found = -1;
-    for (auto& a : arms) {
-      double f[3];
-      reduced(a.data(), f);
-      bool in_cell;
-      int idx = locate(f, in_cell);
-      if (idx >= 0 && in_cell && idx < n && T.mapibz[idx] > 0) {
+    for (int c = 0; c < npg; ++c) {
+      const int idx = cand[(size_t)n * npg + c];
+      if (idx == -1) break;
+      if (idx >= 0 && idx < n && T.mapibz[idx] > 0) {
         found = T.mapibz[idx];
         break;
       }
@@ -627,26 +657,48 @@ std::string build_tables(const System& S, Tables& T) {
       T.neg_dst.push_back(mk);
     }
   }
-  // ---- star arms per IBZ point: mesh arms (kstarsinfbz1) and folded arms
-  T.arm_off.assign(1, 0);
-  T.star_off.assign(1, 0);
-  for (int i = 0; i < T.nibz; ++i) {
-    star(&T.kibz[3 * (size_t)i], arms, armop);
-    for (size_t s = 0; s < arms.size(); ++s) {
-      double f[3];
-      reduced(arms[s].data(), f);
-      bool in_cell;
-      int idx = locate(f, in_cell);
-      if (idx < 0) return "star arm is not a kpoint";
-      if (in_cell) {
-        T.arm_q.push_back(idx);
-        T.arm_op.push_back(armop[s]);
+  // ---- star arms per IBZ point: mesh arms (kstarsinfbz1) and folded arms.
+  // Per IBZ point (host threads): its arms as (index, op, in cell), or an
+  // index of -1 when an arm is off the mesh; then concatenated in order.
+  {
+    std::vector<int> aq((size_t)T.nibz * npg, -1), ao((size_t)T.nibz * npg, 0), ain((size_t)T.nibz * npg, 0),
+        na(T.nibz, 0);
+    const int nthr = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (int t = 0; t < nthr; ++t)
+      pool.emplace_back([&, t] {
+        std::vector<std::array<double, 3>> ar;
+        std::vector<int> op;
+        for (int i = t; i < T.nibz; i += nthr) {
+          star(&T.kibz[3 * (size_t)i], ar, op);
+          na[i] = (int)ar.size();
+          for (size_t c = 0; c < ar.size(); ++c) {
+            double f[3];
+            reduced(ar[c].data(), f);
+            bool in_cell;
+            aq[(size_t)i * npg + c] = locate(f, in_cell);
+            ao[(size_t)i * npg + c] = op[c];
+            ain[(size_t)i * npg + c] = in_cell ? 1 : 0;
+          }
+        }
+      });
+    for (auto& th : pool) th.join();
+    T.arm_off.assign(1, 0);
+    T.star_off.assign(1, 0);
+    for (int i = 0; i < T.nibz; ++i) {
+      for (int c = 0; c < na[i]; ++c) {
+        const size_t k = (size_t)i * npg + c;
+        if (aq[k] < 0) return "star arm is not a kpoint";
+        if (ain[k]) {
+          T.arm_q.push_back(aq[k]);
+          T.arm_op.push_back(ao[k]);
+        }
+        T.star_q.push_back(aq[k]);
+        T.star_op.push_back(ao[k]);
       }
-      T.star_q.push_back(idx);
-      T.star_op.push_back(armop[s]);
+      T.arm_off.push_back((int)T.arm_q.size());
+      T.star_off.push_back((int)T.star_q.size());
     }
-    T.arm_off.push_back((int)T.arm_q.size());
-    T.star_off.push_back((int)T.star_q.size());
   }
   // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table
   static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
@@ -654,7 +706,10 @@ std::string build_tables(const System& S, Tables& T) {
   static const int off8[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
                                   {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
   T.tet_corner.assign(24 * (size_t)T.nkc, 0);
-  std::vector<std::vector<int>> inc(T.nkc);
+  // incidences (tetrahedron corner (6n+l)*4+k at point p) are generated in
+  // increasing order, so each point's list of 24 comes out sorted
+  T.tet_inc.assign(24 * (size_t)T.nkc, 0);
+  std::vector<int> ninc(T.nkc, 0);
   for (int n = 0; n < T.nkc; ++n) {
     int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
     int pt[8];
@@ -664,15 +719,12 @@ std::string build_tables(const System& S, Tables& T) {
       for (int k = 0; k < 4; ++k) {
         int p = pt[corner_of[l][k]];
         T.tet_corner[4 * (6 * (size_t)n + l) + k] = p;
-        inc[p].push_back((6 * n + l) * 4 + k);
+        if (ninc[p] >= 24) return "tetrahedron incidence count";
+        T.tet_inc[24 * (size_t)p + ninc[p]++] = (6 * n + l) * 4 + k;
       }
   }
-  T.tet_inc.assign(24 * (size_t)T.nkc, 0);
-  for (int p = 0; p < T.nkc; ++p) {
-    if (inc[p].size() != 24) return "tetrahedron incidence count";
-    std::sort(inc[p].begin(), inc[p].end());
-    std::copy(inc[p].begin(), inc[p].end(), T.tet_inc.begin() + 24 * (size_t)p);
-  }
+  for (int p = 0; p < T.nkc; ++p)
+    if (ninc[p] != 24) return "tetrahedron incidence count";
   // ---- exact phases: q(m).R_j = 2 pi sum_a (m_a/N_a - s/2) n_ja
   long L = 1;
   for (int a = 0; a < 3; ++a) L = std::lcm(L, (long)S.nc[a]);
