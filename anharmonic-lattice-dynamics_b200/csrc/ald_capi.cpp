@@ -584,6 +584,7 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   a.gauss = delta_mode(c) == ALD_DELTA_GAUSS;
   a.sigma = gauss_width(c);
   a.f32w = 0;  // the per-stage entry point keeps the reference's FP64 weights
+  a.brange = nullptr;
   a.R1 = R1.p;
   a.R2 = R2.p;
   a.P1s = p1.p;

@@ -40,6 +40,7 @@ struct ald_ctx {
   std::vector<double> giso;
   bool giso_ok = false;
   DevBuf<double> giso_d, w_piso, w_piso_part;
+  DevBuf<double> w_brange;  // omega range of every band over the mesh
   DevBuf<char> w_scratch;
   CgWork cg;
   bool have_phonons = false;

@@ -255,6 +255,7 @@ struct CombineArgs {
   int gauss;
   double sigma;
   int f32w;                  // 1: delta weights in FP32 (mixed-precision pipeline), 0: FP64 as the reference
+  const double* brange;      // optional [2b]: min / max of omega per band over the mesh (slice skipping)
   double* R1;                // [row][q][l1][l2], row local to the chunk
   double* R2;
   double* R1p;               // optional [row][q][l1][l3] = sum_l2 P1 (update_mpi); nullptr = skip
@@ -312,6 +313,8 @@ cudaError_t launch_piso(const Geometry& geo, int n1_first, int nrows, const int*
                         const double* evec, const int* tet_corner, const double* giso, double* partial,
                         double* Piso, double* Q, double* QN, double* QU, cudaStream_t s);
 cudaError_t launch_add(size_t n, double* y, const double* x, cudaStream_t s);
+// brange[l] = min_q omega(q,l), brange[b+l] = max_q omega(q,l)
+cudaError_t launch_band_range(const Geometry& geo, const double* freq, double* brange, cudaStream_t s);
 // the g of cal_g for an element name (false: no isotope data for it), and
 // of every primitive atom (cal_giso)
 bool isotope_g(const std::string& element, double& g);

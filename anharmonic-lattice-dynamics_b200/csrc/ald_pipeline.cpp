@@ -177,6 +177,9 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
   // class-form V3 kernels write that layout
   const int v3_layout = v3_pair_supported(b, c->opt.precision) ? 1 : 0;
+  ALD_CKA(c->w_brange.alloc((size_t)2 * b));
+  ALD_CK(launch_band_range(c->geo, c->freq.p, c->w_brange.p, s));
+  res->launches[2] += 1;
   for (int r0 = rb; r0 < re; r0 += K) {
     int nr = std::min(K, re - r0);
     ALD_CK(tm.begin(1));
@@ -199,6 +202,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     a.gauss = gauss;
     a.sigma = gauss_width(c);
     a.f32w = c->opt.precision != ALD_FP64;  // mixed: FP32 delta weights
+    a.brange = c->w_brange.p;
     a.R1 = R1.p + (size_t)(r0 - rb) * nkc * b * b;
     a.R2 = R2.p + (size_t)(r0 - rb) * nkc * b * b;
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;

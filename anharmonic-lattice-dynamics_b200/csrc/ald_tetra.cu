@@ -324,16 +324,21 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
 
 // Q, Q_N, Q_U from the band sums: Q = sum_{w,l2} R1 + R2/2, split by the
 // normal/umklapp flag of q1+w (process 1) and q1-w (process 2)
-__global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, const double* R1, const double* R2,
-                                double* Q, double* QN, double* QU) {
-  __shared__ double red[3][32];
+__global__ void __launch_bounds__(256) q_from_r_kernel(Geometry g, int n1_first, const int* mapinv,
+                                                       const double* R1, const double* R2, double* Q, double* QN,
+                                                       double* QU) {
+  // one CTA per IBZ row; thread = (w slot, l1) with l1 fastest and a block
+  // size that is a multiple of b, so each thread keeps one l1 and a warp
+  // reads consecutive (w, l1) rows of b doubles: coalesced
+  __shared__ double red[3][256];
   const int b = g.b, nkc = g.nkc;
-  const int row = blockIdx.x, l1 = blockIdx.y;
+  const int row = blockIdx.x, tid = threadIdx.x;
+  const int nslot = blockDim.x / b, l1 = tid % b, slot = tid / b;
   const int q1 = mapinv[n1_first + row];
   int m1[3];
   decompose(g, q1, m1);
   double s = 0, sn = 0, su = 0;
-  for (int w = threadIdx.x; w < nkc; w += blockDim.x) {
+  for (int w = slot; w < nkc; w += nslot) {
     int mw[3], i1, i2;
     decompose(g, w, mw);
     pm_index(g, m1, mw, 1, i1);
@@ -348,18 +353,16 @@ __global__ void q_from_r_kernel(Geometry g, int n1_first, const int* mapinv, con
     sn += (i1 ? r1 : 0.0) + (i2 ? 0.5 * r2 : 0.0);
     su += (i1 ? 0.0 : r1) + (i2 ? 0.0 : 0.5 * r2);
   }
-  double v[3] = {s, sn, su};
-  for (int k = 0; k < 3; ++k) {
-    double x = v[k];
-    for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
-    if ((threadIdx.x & 31) == 0) red[k][threadIdx.x >> 5] = x;
-  }
+  red[0][tid] = s;
+  red[1][tid] = sn;
+  red[2][tid] = su;
   __syncthreads();
-  if (threadIdx.x < 3) {
+  if (tid < 3 * b) {  // thread (k, l1): the slots of one l1 in order
+    const int k = tid / b, l = tid % b;
     double t = 0;
-    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[threadIdx.x][i];
-    double* out = threadIdx.x == 0 ? Q : (threadIdx.x == 1 ? QN : QU);
-    out[(size_t)(n1_first + row) * b + l1] = t;
+    for (int i = 0; i < nslot; ++i) t += red[k][i * b + l];
+    double* out = k == 0 ? Q : (k == 1 ? QN : QU);
+    out[(size_t)(n1_first + row) * b + l] = t;
   }
 }
 
@@ -491,6 +494,24 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
   }
   for (int l3 = 0; l3 < b; ++l3) {
     __syncthreads();  // window staged / previous slice done
+    if (F32W && a.brange) {
+      // The energies of this slice, -+omega(w,l2) + omega(q3,l3), lie within
+      // the bands' ranges over the mesh; when that range misses every
+      // omega1 of the row (with a margin far above the FP32 rounding of E)
+      // no tetrahedron of the slice has weight: skip it (uniform branch).
+      // Measured on B200 (16^3 rock-salt): mixed delta 4.11 -> 4.01 ms, while
+      // the FP64 build of the kernel ran 6.85 -> 7.10 ms with it, so there it
+      // is left out.
+      const double lo2 = a.brange[l2], hi2 = a.brange[b + l2], lo3 = a.brange[l3], hi3 = a.brange[b + l3];
+      const double emin = proc == 0 ? lo3 - hi2 : lo2 + lo3, emax = proc == 0 ? hi3 - lo2 : hi2 + hi3;
+      const double tol = 1e-5 * (fabs(hi2) + fabs(hi3)) + 1e-10;
+      double o1min = s_om[0], o1max = s_om[0];
+      for (int l = 1; l < b; ++l) {
+        o1min = fmin(o1min, s_om[l]);
+        o1max = fmax(o1max, s_om[l]);
+      }
+      if (emax + tol < o1min || emin - tol > o1max) continue;
+    }
     if (tid == 0) {
       s_nrec = 0;
       s_nq = 0;
@@ -703,8 +724,8 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s) {
   (void)nibz;
-  dim3 grid(nrows, geo.b);
-  q_from_r_kernel<<<grid, 256, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU);
+  if (3 * geo.b > 256) return cudaErrorInvalidValue;
+  q_from_r_kernel<<<nrows, 256 / geo.b * geo.b, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU);
   return cudaGetLastError();
 }
 

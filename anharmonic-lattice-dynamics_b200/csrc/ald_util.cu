@@ -169,6 +169,40 @@ __global__ void marginal_l2_kernel(int nrows, int nkc, int b, const double* P1, 
 
 }  // namespace
 
+// per band over the mesh: brange[l] = min omega, brange[b + l] = max omega
+__global__ void band_range_kernel(int nkc, int b, const double* freq, double* brange) {
+  __shared__ double smin[8], smax[8];
+  const int l = blockIdx.x;
+  double mn = 1e300, mx = -1e300;
+  for (int q = threadIdx.x; q < nkc; q += blockDim.x) {
+    const double f = freq[(size_t)q * b + l];
+    mn = fmin(mn, f);
+    mx = fmax(mx, f);
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    mn = fmin(mn, __shfl_down_sync(0xffffffffu, mn, o));
+    mx = fmax(mx, __shfl_down_sync(0xffffffffu, mx, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    smin[threadIdx.x >> 5] = mn;
+    smax[threadIdx.x >> 5] = mx;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < (int)(blockDim.x >> 5); ++w) {
+      mn = fmin(mn, smin[w]);
+      mx = fmax(mx, smax[w]);
+    }
+    brange[l] = fmin(mn, smin[0]);
+    brange[b + l] = fmax(mx, smax[0]);
+  }
+}
+
+cudaError_t launch_band_range(const Geometry& geo, const double* freq, double* brange, cudaStream_t s) {
+  band_range_kernel<<<geo.b, 256, 0, s>>>(geo.nkc, geo.b, freq, brange);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_marginal_l2(const Geometry& geo, int nrows, const double* P1, const double* P2, double* R1p,
                                double* R2p, cudaStream_t s) {
   const size_t total = (size_t)nrows * geo.nkc * geo.b * geo.b;
