@@ -160,7 +160,8 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
 template <class T>
 __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* mapinv, const int* arm_off,
                                  const int* arm_q, const int* arm_op, const double* opk, const double* Q,
-                                 const double* R1, const double* R2, T* CM, size_t ld, const double* piso) {
+                                 const double* R1, const double* R2, T* CM, size_t ld, const double* piso,
+                                 const int4* __restrict__ mesh_m) {
   const int b = g.b, b2 = b * b, nkc = g.nkc;
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   if (t >= nibz * b2) return;
@@ -179,12 +180,20 @@ __global__ void collision_kernel(Geometry g, int nibz, int n1_first, const int* 
     if (n0 == q1 && l1 == l2) {
       C = -Q[(size_t)nl * b + l1];
     } else {
-      int m0[3], mp1[3], mp2[3];
-      decompose(g, n0, m0);
+      // the arm's mesh integers from the table; m1 - m0 + sh and m0 - m1 + sh
+      // lie in (-nc, 3nc/2), so two compares wrap them
+      const int4 mm = __ldg(mesh_m + n0);
+      const int m0[3] = {mm.x, mm.y, mm.z};
+      int mp1[3], mp2[3];
       for (int a = 0; a < 3; ++a) {
-        int sh = g.shifted ? g.nc[a] / 2 : 0;
-        mp1[a] = wrapm(m1[a] - m0[a] + sh, g.nc[a]);  // q1 - arm
-        mp2[a] = wrapm(m0[a] - m1[a] + sh, g.nc[a]);  // arm - q1
+        const int n = g.nc[a], sh = g.shifted ? n / 2 : 0;
+        int v1 = m1[a] - m0[a] + sh, v2 = m0[a] - m1[a] + sh;
+        v1 += v1 < 0 ? n : 0;
+        v1 -= v1 >= n ? n : 0;
+        v2 += v2 < 0 ? n : 0;
+        v2 -= v2 >= n ? n : 0;
+        mp1[a] = v1;  // q1 - arm
+        mp2[a] = v2;  // arm - q1
       }
       int nk3_p1 = compose(g, mp1), nk3_p2 = compose(g, mp2);
       const int bl = l1 * b + l2;
@@ -590,15 +599,16 @@ cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s) {
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
                              const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
-                             const double* piso, cudaStream_t s) {
+                             const double* piso, const int* mesh_m, cudaStream_t s) {
   const int nt = nibz * geo.b * geo.b;
+  const int4* mm = reinterpret_cast<const int4*>(mesh_m);
   dim3 grid((nt + 127) / 128, nrows);
   if (cm_f32)
     collision_kernel<float><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1, R2,
-                                                 static_cast<float*>(CM), ld, piso);
+                                                 static_cast<float*>(CM), ld, piso, mm);
   else
     collision_kernel<double><<<grid, 128, 0, s>>>(geo, nibz, n1_first, mapinv, arm_off, arm_q, arm_op, opk, Q, R1,
-                                                  R2, static_cast<double*>(CM), ld, piso);
+                                                  R2, static_cast<double*>(CM), ld, piso, mm);
   return cudaGetLastError();
 }
 

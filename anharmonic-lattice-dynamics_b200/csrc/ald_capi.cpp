@@ -391,6 +391,15 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
     for (int& v : fop) v = std::max(v, 0);
     CKA(upload(c->mapibz0, m0, s));
     CKA(upload(c->full_op, fop, s));
+    // mesh integers of every point, 4 ints each (the collision kernel's arm lookups)
+    std::vector<int> mm(4 * (size_t)c->T.nkc, 0);
+    const int N1 = c->S.nc[1], N2 = c->S.nc[2];
+    for (int q = 0; q < c->T.nkc; ++q) {
+      mm[4 * (size_t)q] = q / (N1 * N2);
+      mm[4 * (size_t)q + 1] = (q / N2) % N1;
+      mm[4 * (size_t)q + 2] = q % N2;
+    }
+    CKA(upload(c->mesh_m, mm, s));
   }
   {
     std::vector<double> op(48 * 9, 0.0), opi(48 * 9, 0.0);
@@ -720,7 +729,7 @@ int ald_collision_matrix(ald_ctx* c, const int ksubset[2], const double* P1, con
   CK(launch_from_fortran5(tmp.p, p2.p, nr, nkc, b, c->stream));
   CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
   CK(launch_collision(c->geo, nibz, ksubset[0] - 1, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p,
-                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, (size_t)cols, 0, nullptr, c->stream));
+                      c->opk.p, Qd.p, R1.p, R2.p, cm.p, (size_t)cols, 0, nullptr, c->mesh_m.p, c->stream));
   CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
   CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -848,7 +857,7 @@ int ald_collision_matrix_iso(ald_ctx* c, const double* P1, const double* P2, con
   CK(launch_collapse(c->geo, nr, p1.p, p2.p, R1.p, R2.p, Qd.p, c->stream));
   CK(launch_add((size_t)nr * b, Qd.p, pis.p, c->stream));  // the diagonal: -(sum(P1 + P2/2) + Piso)
   CK(launch_collision(c->geo, nibz, 0, nr, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p, Qd.p, R1.p,
-                      R2.p, cm.p, (size_t)cols, 0, pis.p, c->stream));
+                      R2.p, cm.p, (size_t)cols, 0, pis.p, c->mesh_m.p, c->stream));
   CK(launch_transpose(cm.p, cmt.p, rows, cols, c->stream));  // row-major -> Fortran column-major
   CK(cudaMemcpyAsync(CM, cmt.p, (size_t)rows * cols * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

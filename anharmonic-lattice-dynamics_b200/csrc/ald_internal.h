@@ -301,11 +301,11 @@ cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, doub
 cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s);
 // CM: double, or float when cm_f32 (mixed-precision pipeline); leading dimension ld.
 // piso (optional, [row][l1] of the range): CollisionMatrix_iso's form instead
-// of CollisionMatrix_mpi's (Q must then include Piso)
+// of CollisionMatrix_mpi's (Q must then include Piso); mesh_m: 4 mesh integers per point
 cudaError_t launch_collision(const Geometry& geo, int nibz, int n1_first, int nrows, const int* mapinv,
                              const int* arm_off, const int* arm_q, const int* arm_op, const double* opk,
                              const double* Q, const double* R1, const double* R2, void* CM, size_t ld, int cm_f32,
-                             const double* piso, cudaStream_t s);
+                             const double* piso, const int* mesh_m, cudaStream_t s);
 // isotope scattering (P_iso_split): Piso[row][l1] of rows n1_first.., and
 // Q, Q_N, Q_U += Piso when Q is given; partial: piso_partial_doubles scratch
 size_t piso_partial_doubles(const Geometry& geo, int nrows);

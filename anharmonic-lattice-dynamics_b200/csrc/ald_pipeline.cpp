@@ -368,7 +368,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   ALD_CK(tm.begin(5));
   if (nloc > 0)
     ALD_CK(launch_collision(c->geo, nibz, rb, nloc, c->mapinv.p, c->arm_off.p, c->arm_q.p, c->arm_op.p, c->opk.p,
-                            dQ + (size_t)rb * b, R1.p, R2.p, cm.p, ld, cm_f32, iso ? c->w_piso.p : nullptr, s));
+                            dQ + (size_t)rb * b, R1.p, R2.p, cm.p, ld, cm_f32, iso ? c->w_piso.p : nullptr,
+                            c->mesh_m.p, s));
   res->launches[5] += 1;
   ALD_CK(tm.end());
   // ---- 6: RHS and the initial guess x0 = F_RTA (kappa.f90:835-843)
