@@ -44,30 +44,36 @@ constexpr int kTetThreads = 256;
 constexpr int kPointBlock = 128;
 constexpr int kMaxBandsTet = 16;  // queue entries pack l1 into 4 bits
 
-__device__ __forceinline__ int wrapm(int v, int n) {
-  v %= n;
-  return v < 0 ? v + n : v;
-}
 __device__ __forceinline__ void decompose(const Geometry& g, int n, int* m) {
   m[0] = n / (g.nc[1] * g.nc[2]);
   m[1] = (n / g.nc[2]) % g.nc[1];
   m[2] = n % g.nc[2];
 }
 __device__ __forceinline__ int compose(const Geometry& g, const int* m) { return m[2] + g.nc[2] * (m[1] + g.nc[1] * m[0]); }
-// q1 + w (sign=+1) or q1 - w (sign=-1) on the mesh; `inside` is get_k_info's flag
-__device__ __forceinline__ int pm_index(const Geometry& g, const int* m1, const int* mw, int sign, int& inside) {
-  int m[3];
+// v mod n for v in [-n, 2n), by compares
+__device__ __forceinline__ int wrap2(int v, int n) {
+  v += v < 0 ? n : 0;
+  return v >= n ? v - n : v;
+}
+// q1 + w (sign=+1) or q1 - w (sign=-1) on the mesh, and its mesh integers m;
+// `inside` is get_k_info's flag.  m1 + -mw -+ nc/2 lies in [-nc, 2nc).
+__device__ __forceinline__ int pm_index_m(const Geometry& g, const int* m1, const int* mw, int sign, int& inside,
+                                          int* m) {
   inside = 1;
   for (int a = 0; a < 3; ++a) {
     int v = m1[a] + sign * mw[a] + (g.shifted ? -sign * (g.nc[a] / 2) : 0);
     if (v < 0 || v >= g.nc[a]) inside = 0;
-    m[a] = wrapm(v, g.nc[a]);
+    m[a] = wrap2(v, g.nc[a]);
   }
   return compose(g, m);
 }
+__device__ __forceinline__ int pm_index(const Geometry& g, const int* m1, const int* mw, int sign, int& inside) {
+  int m[3];
+  return pm_index_m(g, m1, mw, sign, inside, m);
+}
 __device__ __forceinline__ int neg_index(const Geometry& g, const int* mw) {
   int m[3];
-  for (int a = 0; a < 3; ++a) m[a] = wrapm(-mw[a], g.nc[a]);
+  for (int a = 0; a < 3; ++a) m[a] = wrap2(-mw[a], g.nc[a]);
   return compose(g, m);
 }
 // the reference's acoustic-at-Gamma test: loop indices equal NC/2+1 (sub.f90:7351)
@@ -229,12 +235,10 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
     decompose(g, q1, m1);
     decompose(g, w, mw);
     int ins1, ins2;
-    const int q3p = pm_index(g, m1, mw, 1, ins1);   // q1 + w
-    const int q3m = pm_index(g, m1, mw, -1, ins2);  // q1 - w
-    const int wneg = neg_index(g, mw);
     int m3p[3], m3m[3];
-    decompose(g, q3p, m3p);
-    decompose(g, q3m, m3m);
+    const int q3p = pm_index_m(g, m1, mw, 1, ins1, m3p);   // q1 + w
+    const int q3m = pm_index_m(g, m1, mw, -1, ins2, m3m);  // q1 - w
+    const int wneg = neg_index(g, mw);
     const bool w_gamma = at_gamma_index(g, mw);
     const bool p_gamma = at_gamma_index(g, m3p), m_gamma = at_gamma_index(g, m3m);
     const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
@@ -457,9 +461,8 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
     int mw[3] = {(pi + di) % N0, (j0 + dj) % N1, k};
     const int w = compose(g, mw);
     int ins;
-    const int q3 = pm_index(g, m1, mw, proc == 0 ? 1 : -1, ins);
     int m3[3];
-    decompose(g, q3, m3);
+    const int q3 = pm_index_m(g, m1, mw, proc == 0 ? 1 : -1, ins, m3);
     s_w[p] = w;
     s_q3[p] = q3;
     s_src[p] = proc == 0 ? w : neg_index(g, mw);
