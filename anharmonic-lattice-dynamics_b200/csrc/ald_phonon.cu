@@ -298,44 +298,55 @@ __global__ void __launch_bounds__(kThreads) phonon_kernel(PhononArgs a) {
 }
 
 // ------------------------------------------------------------------
-// Small cells (b <= 12): one warp per matrix, kPhWarps matrices per CTA,
-// synchronised with __syncwarp only.  The same arithmetic as phonon_kernel
+// Small cells (b <= 12): G matrices per warp (32/G lanes each: G = 4 up to 4
+// bands, 2 up to 8, else 1), kPhWarps warps per CTA, synchronised with
+// __syncwarp only.  Every lane runs the same sequence of __syncwarp and
+// shuffle calls: a matrix that has converged (or a slot past the last
+// matrix) just stops doing work.  The same arithmetic as phonon_kernel
 // element by element (FC2 sum in the file's term order, hermitisation,
 // dipole term, cyclic Jacobi rounds, sorts); the q.R phase of every distinct
 // FC2 atom is evaluated once per matrix instead of once per matrix element,
-// and the sweep's off-diagonal and diagonal norms are warp sums.  Each term
-// keeps the reference's (f cos)/sqrt(m m) rounding: the acoustic modes at
-// Gamma are rounding residues of these sums, and a sum rounded differently
-// can reach exactly zero.
+// and the sweep's off-diagonal and diagonal norms are sums over the matrix's
+// lanes.  Each term keeps the reference's (f cos)/sqrt(m m) rounding: the
+// acoustic modes at Gamma are rounding residues of these sums, and a sum
+// rounded differently can reach exactly zero.
 constexpr int kPhWarps = 4;
 constexpr int kPhBMax = 12;
 
-__device__ __forceinline__ double warp_sum(double v) {
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+template <int LPM>
+__device__ __forceinline__ double group_sum(double v) {  // over the LPM aligned lanes of a matrix
+  for (int o = LPM / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
 
+template <int G>
 __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a, int nmat) {
+  constexpr int LPM = 32 / G;  // lanes per matrix
+  constexpr int NS = kPhWarps * G;  // matrix slots per CTA
   extern __shared__ double2 smem[];
-  __shared__ double4 s_rot[kPhWarps][kPhBMax / 2];
-  __shared__ double2 s_nd[kPhWarps][kPhBMax / 2];
-  __shared__ int s_act[kPhWarps][kPhBMax / 2];
-  __shared__ int s_perm[kPhWarps][kPhBMax];
-  __shared__ double s_lam[kPhWarps][kPhBMax], s_lab[kPhWarps][kPhBMax];
-  __shared__ int s_ord[kPhWarps][kPhBMax], s_ord2[kPhWarps][kPhBMax];
+  __shared__ double4 s_rot[NS][kPhBMax / 2];
+  __shared__ double2 s_nd[NS][kPhBMax / 2];
+  __shared__ int s_act[NS][kPhBMax / 2];
+  __shared__ int s_perm[NS][kPhBMax];
+  __shared__ double s_lam[NS][kPhBMax], s_lab[NS][kPhBMax];
+  __shared__ int s_ord[NS][kPhBMax], s_ord2[NS][kPhBMax];
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  const int m = blockIdx.x * kPhWarps + warp;
-  if (m >= nmat) return;  // whole warp; nothing below synchronises the CTA
+  const int sg = lane / LPM, sl = lane % LPM, slot = warp * G + sg;
+  const int m0 = (blockIdx.x * kPhWarps + warp) * G;
+  if (m0 >= nmat) return;  // the whole warp; nothing below synchronises the CTA
+  const int m = m0 + sg;
+  const bool valid = m < nmat;  // a slot past the last matrix repeats the last one and writes nothing
+  const int mc = valid ? m : nmat - 1;
   const int b = a.geo.b, bb = b * b;
-  const int pt = m / 7, d = m % 7;
-  double2* A = smem + (size_t)warp * (2 * bb + a.nuniq);
+  const int pt = mc / 7, d = mc % 7;
+  double2* A = smem + (size_t)slot * (2 * bb + a.nuniq);
   double2* V = A + bb;
   double2* ph = V + bb;
-  double4* rot = s_rot[warp];
-  double2* newdiag = s_nd[warp];
-  int* active = s_act[warp];
-  int* perm = s_perm[warp];
+  double4* rot = s_rot[slot];
+  double2* newdiag = s_nd[slot];
+  int* active = s_act[slot];
+  int* perm = s_perm[slot];
 
   double q[3] = {a.kpc32[3 * pt], a.kpc32[3 * pt + 1], a.kpc32[3 * pt + 2]};
   if (d > 0) {
@@ -343,7 +354,7 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
     q[ax] = (d & 1) ? q[ax] + a.dq : q[ax] - a.dq;
   }
   // ------------------------------------------- phases, then the FC2 sum
-  for (int u = lane; u < a.nuniq; u += 32) {
+  for (int u = sl; u < a.nuniq; u += LPM) {
     const double* rr = a.rr + 3 * a.fc2_uatom[u];
     double x = q[0] * rr[0] + q[1] * rr[1] + q[2] * rr[2];
     double sn, cs;
@@ -351,7 +362,7 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
     ph[u] = make_double2(cs, sn);
   }
   __syncwarp();
-  for (int e = lane; e < bb; e += 32) {
+  for (int e = sl; e < bb; e += LPM) {
     double2 acc = make_double2(0.0, 0.0);
     for (int t = a.fc2_off[e]; t < a.fc2_off[e + 1]; ++t) {
       const double2 p = ph[a.fc2_uidx[t]];
@@ -363,12 +374,12 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
   }
   __syncwarp();
   // ------------------------------------------ hermitisation (rest.f90:513-544)
-  for (int t = lane; t < b; t += 32) {
+  for (int t = sl; t < b; t += LPM) {
     double2 v = A[t * b + t];
     if (fabs(v.y) > 9e-4 * fabs(v.x)) A[t * b + t] = make_double2(v.x, 0.0);
   }
   __syncwarp();
-  for (int e = lane; e < bb; e += 32) {
+  for (int e = sl; e < bb; e += LPM) {
     int t = e / b, j = e % b;
     if (j > t && j <= b - 2) {
       double2 u = A[t * b + j], l = A[j * b + t];
@@ -379,14 +390,14 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
   }
   __syncwarp();
   double sim = 0, sre = 0;
-  for (int e = lane; e < bb; e += 32) {
+  for (int e = sl; e < bb; e += LPM) {
     sim += fabs(A[e].y);
     sre += fabs(A[e].x);
   }
-  sim = warp_sum(sim) / bb;
-  sre = warp_sum(sre) / bb;
+  sim = group_sum<LPM>(sim) / bb;
+  sre = group_sum<LPM>(sre) / bb;
   if (sim < sre * 1e-10)
-    for (int e = lane; e < bb; e += 32) A[e].y = 0.0;
+    for (int e = sl; e < bb; e += LPM) A[e].y = 0.0;
   __syncwarp();
   // --------------------------------------------------- dipole term (nonanal)
   if (a.born_flag != 0) {
@@ -402,7 +413,7 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
                   kh[2] * (eps[2] * kh[0] + eps[5] * kh[1] + eps[8] * kh[2]));
     double q2 = kh[0] * kh[0] + kh[1] * kh[1] + kh[2] * kh[2];
     double ex = exp(-q2 / sc[1]);
-    for (int e = lane; e < bb; e += 32) {
+    for (int e = sl; e < bb; e += LPM) {
       int r = e / b, c = e % b;
       int na = r / 3, i = r % 3, nb = c / 3, j = c % 3;
       const double* za = chg + 9 * na;
@@ -414,32 +425,34 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
     __syncwarp();
   }
   // --------------------- Hermitian matrix of the upper triangle (ZHEEV 'U')
-  for (int e = lane; e < bb; e += 32)
+  for (int e = sl; e < bb; e += LPM)
     if (e / b == e % b) A[e].y = 0.0;
   __syncwarp();
-  for (int e = lane; e < bb; e += 32) {
+  for (int e = sl; e < bb; e += LPM) {
     int i = e / b, j = e % b;
     if (i > j) A[e] = cconj(A[j * b + i]);
   }
   if (d == 0)
-    for (int e = lane; e < bb; e += 32) V[e] = make_double2((e / b) == (e % b) ? 1.0 : 0.0, 0.0);
+    for (int e = sl; e < bb; e += LPM) V[e] = make_double2((e / b) == (e % b) ? 1.0 : 0.0, 0.0);
   __syncwarp();
   // ------------------------------------------------ parallel cyclic Jacobi
   const int n2 = b + (b & 1);
   const int npair = n2 / 2;
+  bool conv = false;  // uniform over the matrix's lanes
   for (int sweep = 0; sweep < kMaxSweeps; ++sweep) {
     double off = 0, dia = 0;
-    for (int e = lane; e < bb; e += 32) {
+    for (int e = sl; e < bb; e += LPM) {
       double m2 = A[e].x * A[e].x + A[e].y * A[e].y;
       if (e / b == e % b) dia += m2;
       else off += m2;
     }
-    off = warp_sum(off);
-    dia = warp_sum(dia);
-    if (off == 0.0 || off <= 1e-32 * dia) break;  // warp-uniform
+    off = group_sum<LPM>(off);
+    dia = group_sum<LPM>(dia);
+    if (!conv && (off == 0.0 || off <= 1e-32 * dia)) conv = true;
+    if (__all_sync(0xffffffffu, conv)) break;  // warp-uniform
     for (int r = 0; r < n2 - 1; ++r) {
-      if (lane < npair) {
-        const int k = lane;
+      if (!conv && sl < npair) {
+        const int k = sl;
         int p, qq;
         rr_pair(r, k, n2, p, qq);
         int act = 0;
@@ -467,39 +480,41 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
       }
       __syncwarp();
       // columns: A <- A J, V <- V J
-      for (int e = lane; e < npair * b; e += 32) {
-        int k = e / b, i = e % b;
-        if (!active[k]) continue;
-        int p = perm[2 * k], qq = perm[2 * k + 1];
-        double4 R = rot[k];
-        double2 wb = make_double2(R.z, -R.w);  // conj(w)
-        double2 aip = A[i * b + p], aiq = A[i * b + qq];
-        double2 t1 = cmul(wb, aiq);
-        A[i * b + p] = make_double2(R.x * aip.x - R.y * t1.x, R.x * aip.y - R.y * t1.y);
-        A[i * b + qq] = make_double2(R.y * aip.x + R.x * t1.x, R.y * aip.y + R.x * t1.y);
-        if (d == 0) {
-          double2 vip = V[i * b + p], viq = V[i * b + qq];
-          double2 t2 = cmul(wb, viq);
-          V[i * b + p] = make_double2(R.x * vip.x - R.y * t2.x, R.x * vip.y - R.y * t2.y);
-          V[i * b + qq] = make_double2(R.y * vip.x + R.x * t2.x, R.y * vip.y + R.x * t2.y);
+      if (!conv)
+        for (int e = sl; e < npair * b; e += LPM) {
+          int k = e / b, i = e % b;
+          if (!active[k]) continue;
+          int p = perm[2 * k], qq = perm[2 * k + 1];
+          double4 R = rot[k];
+          double2 wb = make_double2(R.z, -R.w);  // conj(w)
+          double2 aip = A[i * b + p], aiq = A[i * b + qq];
+          double2 t1 = cmul(wb, aiq);
+          A[i * b + p] = make_double2(R.x * aip.x - R.y * t1.x, R.x * aip.y - R.y * t1.y);
+          A[i * b + qq] = make_double2(R.y * aip.x + R.x * t1.x, R.y * aip.y + R.x * t1.y);
+          if (d == 0) {
+            double2 vip = V[i * b + p], viq = V[i * b + qq];
+            double2 t2 = cmul(wb, viq);
+            V[i * b + p] = make_double2(R.x * vip.x - R.y * t2.x, R.x * vip.y - R.y * t2.y);
+            V[i * b + qq] = make_double2(R.y * vip.x + R.x * t2.x, R.y * vip.y + R.x * t2.y);
+          }
         }
-      }
       __syncwarp();
       // rows: A <- J^H A
-      for (int e = lane; e < npair * b; e += 32) {
-        int k = e / b, j = e % b;
-        if (!active[k]) continue;
-        int p = perm[2 * k], qq = perm[2 * k + 1];
-        double4 R = rot[k];
-        double2 w = make_double2(R.z, R.w);
-        double2 apj = A[p * b + j], aqj = A[qq * b + j];
-        double2 t1 = cmul(w, aqj);
-        A[p * b + j] = make_double2(R.x * apj.x - R.y * t1.x, R.x * apj.y - R.y * t1.y);
-        A[qq * b + j] = make_double2(R.y * apj.x + R.x * t1.x, R.y * apj.y + R.x * t1.y);
-      }
+      if (!conv)
+        for (int e = sl; e < npair * b; e += LPM) {
+          int k = e / b, j = e % b;
+          if (!active[k]) continue;
+          int p = perm[2 * k], qq = perm[2 * k + 1];
+          double4 R = rot[k];
+          double2 w = make_double2(R.z, R.w);
+          double2 apj = A[p * b + j], aqj = A[qq * b + j];
+          double2 t1 = cmul(w, aqj);
+          A[p * b + j] = make_double2(R.x * apj.x - R.y * t1.x, R.x * apj.y - R.y * t1.y);
+          A[qq * b + j] = make_double2(R.y * apj.x + R.x * t1.x, R.y * apj.y + R.x * t1.y);
+        }
       __syncwarp();
-      if (lane < npair && active[lane]) {
-        const int k = lane;
+      if (!conv && sl < npair && active[sl]) {
+        const int k = sl;
         int p = perm[2 * k], qq = perm[2 * k + 1];
         A[p * b + p] = make_double2(newdiag[k].x, 0.0);
         A[qq * b + qq] = make_double2(newdiag[k].y, 0.0);
@@ -510,11 +525,11 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
     }
   }
   // ---------------------------------------------------------- ordering
-  double* lam = s_lam[warp];
-  double* lab = s_lab[warp];
-  int* ord = s_ord[warp];
-  int* ord2 = s_ord2[warp];
-  if (lane == 0) {
+  double* lam = s_lam[slot];
+  double* lab = s_lab[slot];
+  int* ord = s_ord[slot];
+  int* ord2 = s_ord2[slot];
+  if (sl == 0) {
     for (int i = 0; i < b; ++i) {
       lam[i] = A[i * b + i].x;
       ord[i] = i;
@@ -539,24 +554,26 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
         }
   }
   __syncwarp();
-  for (int i = lane; i < b; i += 32) a.w2_all[((size_t)pt * 7 + d) * b + i] = lab[i];
-  if (d == 0) {
-    for (int l = 0; l < b; ++l) {
-      int col = ord[ord2[l]];
-      double sre2 = 0;
-      for (int c = lane; c < b; c += 32) sre2 += fabs(V[c * b + col].x);
-      sre2 = warp_sum(sre2);
-      bool rot90 = sre2 < 1e-3;
-      for (int c = lane; c < b; c += 32) {
+  if (valid)
+    for (int i = sl; i < b; i += LPM) a.w2_all[((size_t)pt * 7 + d) * b + i] = lab[i];
+  for (int l = 0; l < b; ++l) {  // every lane: the sums below shuffle over the matrix's lanes
+    int col = ord[ord2[l]];
+    double sre2 = 0;
+    if (d == 0)
+      for (int c = sl; c < b; c += LPM) sre2 += fabs(V[c * b + col].x);
+    sre2 = group_sum<LPM>(sre2);
+    bool rot90 = sre2 < 1e-3;
+    if (valid && d == 0)
+      for (int c = sl; c < b; c += LPM) {
         double2 v = V[c * b + col];
         if (rot90) v = make_double2(-v.y, v.x);
         size_t o = (((size_t)pt * b + l) * b + c) * 2;
         a.evec[o] = v.x;
         a.evec[o + 1] = v.y;
       }
-    }
-    for (int l = lane; l < b; l += 32) a.w2[(size_t)pt * b + l] = lab[ord2[l]];
   }
+  if (valid && d == 0)
+    for (int l = sl; l < b; l += LPM) a.w2[(size_t)pt * b + l] = lab[ord2[l]];
 }
 
 // finite differences use the get_freq order (before the second sort)
@@ -614,14 +631,25 @@ __global__ void freq_dist_kernel(Geometry geo, const double* w2, double cnst, do
 
 cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
   int b = a.geo.b;
-  const size_t smw = (size_t)kPhWarps * (2 * (size_t)b * b + a.nuniq) * sizeof(double2);
+  const int G = b <= 4 ? 4 : (b <= 8 ? 2 : 1);  // matrices per warp
+  const size_t smw = (size_t)kPhWarps * G * (2 * (size_t)b * b + a.nuniq) * sizeof(double2);
   if (b <= kPhBMax && smw <= 160 * 1024) {
-    if (smw > 48 * 1024) {
-      cudaError_t e = cudaFuncSetAttribute(phonon_warp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);
-      if (e != cudaSuccess) return e;
-    }
     const int nmat = a.geo.nkc * 7;
-    phonon_warp_kernel<<<(nmat + kPhWarps - 1) / kPhWarps, kPhWarps * 32, smw, s>>>(a, nmat);
+    const int per_cta = kPhWarps * G;
+    cudaError_t e = cudaSuccess;
+#define ALD_PHW(GG)                                                                                            \
+  if (smw > 48 * 1024)                                                                                         \
+    e = cudaFuncSetAttribute(phonon_warp_kernel<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);    \
+  if (e != cudaSuccess) return e;                                                                              \
+  phonon_warp_kernel<GG><<<(nmat + per_cta - 1) / per_cta, kPhWarps * 32, smw, s>>>(a, nmat);
+    if (G == 4) {
+      ALD_PHW(4)
+    } else if (G == 2) {
+      ALD_PHW(2)
+    } else {
+      ALD_PHW(1)
+    }
+#undef ALD_PHW
     return cudaGetLastError();
   }
   size_t sm = 2 * (size_t)b * b * sizeof(double2);
