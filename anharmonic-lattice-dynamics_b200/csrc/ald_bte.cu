@@ -98,12 +98,20 @@ __global__ void rhs_kernel(KappaArgs a, double* rhs) {
 }
 
 // one CTA per band l; threads over IBZ points; 9 sums reduced in the block
-__global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double* kappa_modes, int* err) {
-  __shared__ double red[9][32];
-  const int b = a.geo.b, l = blockIdx.x;
+// kappa per band: a thread per (arm of an IBZ point, band), a CTA per
+// (block of kKapThreads arms, band); per-CTA partial sums of the 9
+// components, added in CTA order by kappa_final_kernel
+constexpr int kKapThreads = 128;
+
+__global__ void __launch_bounds__(kKapThreads) kappa_arm_kernel(KappaArgs a, const double* F, int averaged,
+                                                                int narm, int* err) {
+  __shared__ double red[9][kKapThreads / 32];
+  const int b = a.geo.b, l = blockIdx.y;
+  const int s = blockIdx.x * kKapThreads + threadIdx.x;
   double acc[9];
   for (int k = 0; k < 9; ++k) acc[k] = 0.0;
-  for (int i = threadIdx.x; i < a.nibz; i += blockDim.x) {
+  if (s < narm) {
+    const int i = a.arm_owner[s];
     double f[3] = {F[((size_t)i * b + l) * 3], F[((size_t)i * b + l) * 3 + 1], F[((size_t)i * b + l) * 3 + 2]};
     double vv[3];
     if (averaged) {
@@ -111,10 +119,10 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
       int s0 = a.star_off[i], s1 = a.star_off[i + 1];
       double narms = (double)(s1 - s0);
       double va[3] = {0, 0, 0};
-      for (int s = s0; s < s1; ++s) {
-        const double* vq = a.vel + ((size_t)a.star_q[s] * b + l) * 3;
+      for (int t = s0; t < s1; ++t) {
+        const double* vq = a.vel + ((size_t)a.star_q[t] * b + l) * 3;
         double vin[3] = {vq[0], vq[1], vq[2]}, vr[3];
-        opmul(a.opk_inv + 9 * a.star_op[s], vin, vr);
+        opmul(a.opk_inv + 9 * a.star_op[t], vin, vr);
         for (int x = 0; x < 3; ++x) va[x] = va[x] + (vr[x] / narms);
       }
       for (int x = 0; x < 3; ++x) vv[x] = va[x];
@@ -124,18 +132,16 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
       vv[1] = vq[1];
       vv[2] = vq[2];
     }
-    for (int s = a.arm_off[i]; s < a.arm_off[i + 1]; ++s) {
-      const double* op = a.opk + 9 * a.arm_op[s];
-      double F12[3], velocc[3];
-      opmul(op, f, F12);
-      opmul(op, vv, velocc);
-      int n0 = a.arm_q[s];
-      double omega = sqrt(a.w2[(size_t)n0 * b + l]) * PhysConst::cnst();
-      double nb0 = nbe_dev(omega, a.temp, a.classical, err);
-      for (int j = 0; j < 3; ++j)
-        for (int jj = 0; jj < 3; ++jj)
-          acc[j + 3 * jj] -= ((((a.const1 * omega) * velocc[j]) * nb0) * (nb0 + 1)) * F12[jj];
-    }
+    const double* op = a.opk + 9 * a.arm_op[s];
+    double F12[3], velocc[3];
+    opmul(op, f, F12);
+    opmul(op, vv, velocc);
+    int n0 = a.arm_q[s];
+    double omega = sqrt(a.w2[(size_t)n0 * b + l]) * PhysConst::cnst();
+    double nb0 = nbe_dev(omega, a.temp, a.classical, err);
+    for (int j = 0; j < 3; ++j)
+      for (int jj = 0; jj < 3; ++jj)
+        acc[j + 3 * jj] -= ((((a.const1 * omega) * velocc[j]) * nb0) * (nb0 + 1)) * F12[jj];
   }
   for (int k = 0; k < 9; ++k) {
     double v = acc[k];
@@ -144,11 +150,20 @@ __global__ void kappa_kernel(KappaArgs a, const double* F, int averaged, double*
   }
   __syncthreads();
   if (threadIdx.x < 9) {
-    double s = 0;
-    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) s += red[threadIdx.x][w];
-    int j = threadIdx.x % 3, jj = threadIdx.x / 3;
-    kappa_modes[l + b * (j + 3 * jj)] = s;  // kappa(ndyn,3,3) column-major
+    double t = 0;
+    for (int w = 0; w < kKapThreads / 32; ++w) t += red[threadIdx.x][w];
+    a.part[((size_t)l * gridDim.x + blockIdx.x) * 9 + threadIdx.x] = t;
   }
+}
+
+__global__ void kappa_final_kernel(int b, int nblk, const double* part, double* kappa_modes) {
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= 9 * b) return;
+  const int l = t / 9, k = t % 9;
+  double s = 0;
+  for (int q = 0; q < nblk; ++q) s += part[((size_t)l * nblk + q) * 9 + k];
+  const int j = k % 3, jj = k / 3;
+  kappa_modes[l + b * (j + 3 * jj)] = s;  // kappa(ndyn,3,3) column-major
 }
 
 // collision matrix: thread per (n1, n2, l1, l2), l2 fastest, so that the b*b
@@ -561,9 +576,17 @@ cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaS
   return cudaGetLastError();
 }
 
+size_t kappa_partial_doubles(int b, int narm) {
+  return (size_t)b * std::max(1, (narm + kKapThreads - 1) / kKapThreads) * 9;
+}
+
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s) {
-  kappa_kernel<<<a.geo.b, 256, 0, s>>>(a, F, averaged, kappa_modes, err);
+  if (!a.part) return cudaErrorMemoryAllocation;
+  const int narm = a.narm;
+  const int nblk = std::max(1, (narm + kKapThreads - 1) / kKapThreads);
+  kappa_arm_kernel<<<dim3(nblk, a.geo.b), kKapThreads, 0, s>>>(a, F, averaged, narm, err);
+  kappa_final_kernel<<<(9 * a.geo.b + 127) / 128, 128, 0, s>>>(a.geo.b, nblk, a.part, kappa_modes);
   return cudaGetLastError();
 }
 

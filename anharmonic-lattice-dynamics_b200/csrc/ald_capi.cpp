@@ -224,6 +224,9 @@ KappaArgs kappa_args(ald_ctx* c, double tempk) {
   k.const1 = PhysConst::h_plank * PhysConst::c_light * 100 * PhysConst::c_light /
              (c->T.nkc * c->S.volume_r / 1e30);
   k.classical = c->S.classical;
+  k.arm_owner = c->arm_owner.p;
+  k.narm = (int)c->T.arm_q.size();
+  k.part = c->w_kpart.alloc(kappa_partial_doubles(c->geo.b, k.narm)) == cudaSuccess ? c->w_kpart.p : nullptr;
   return k;
 }
 
@@ -400,6 +403,10 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
       mm[4 * (size_t)q + 2] = q % N2;
     }
     CKA(upload(c->mesh_m, mm, s));
+    std::vector<int> own(c->T.arm_q.size());
+    for (int i = 0; i < c->T.nibz; ++i)
+      for (int a = c->T.arm_off[i]; a < c->T.arm_off[i + 1]; ++a) own[a] = i;
+    CKA(upload(c->arm_owner, own, s));
   }
   {
     std::vector<double> op(48 * 9, 0.0), opi(48 * 9, 0.0);

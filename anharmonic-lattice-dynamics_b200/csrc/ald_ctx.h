@@ -25,6 +25,7 @@ struct ald_ctx {
   DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,
       arm_op, star_off, star_q, star_op, tet_corner, tet_inc, err;
   DevBuf<int> cls_grp_off, cls_pc, cls_trip_off, cls_trip, cls_trip_i0, cls_trip_k;
+  DevBuf<int> arm_owner;              // per arm: its IBZ point (kappa over arms)
   DevBuf<int> mesh_m;                 // per mesh point: its three mesh integers (+ 1 pad)
   DevBuf<int> mapibz0, full_op;       // per mesh point: IBZ point and the op of its star arm (job=3)
   bool full_op_ok = false;
@@ -41,6 +42,7 @@ struct ald_ctx {
   std::vector<double> giso;
   bool giso_ok = false;
   DevBuf<double> giso_d, w_piso, w_piso_part;
+  DevBuf<double> w_kpart;   // per-CTA partial sums of kappa
   DevBuf<double> w_brange;  // omega range of every band over the mesh
   DevBuf<char> w_scratch;
   CgWork cg;

@@ -294,7 +294,11 @@ struct KappaArgs {
   const double* opk_inv;     // 48*9
   double tempk, temp, const1;
   int classical;
+  const int* arm_owner;      // per arm (arm_q entry): its IBZ point
+  int narm;                  // arm_off[nibz]
+  double* part;              // scratch: kappa_partial_doubles(b, narm) (per-CTA partial sums)
 };
+size_t kappa_partial_doubles(int b, int narm);
 cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaStream_t s);
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s);
