@@ -326,6 +326,79 @@ __global__ void __launch_bounds__(kPointBlock) delta_point_kernel(CombineArgs a,
   }
 }
 
+// The FP32 Gaussian of the mixed pipeline with both processes per thread:
+// a thread takes mesh point q and band l2 and reads each |V3|^2(q) once for
+// process 1 at w = q (q3 = q1 + q) and for process 2 at w = -q, whose q3 =
+// q1 - w is the same point and whose |V3|^2 source is q again.  It writes
+// R1 at w = q and R2 at w = -q (the map q -> -q is a permutation of the
+// mesh).  P1s/P2s/P1/P2 are not produced (pipeline only).
+template <int B>
+__global__ void __launch_bounds__(kPointBlock) delta_point_pair_kernel(CombineArgs a) {
+  __shared__ double s_om1[B], s_nb1[B];
+  const Geometry& g = a.geo;
+  const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
+  const int row = blockIdx.y, l2 = blockIdx.z, tid = threadIdx.x;
+  const int q1 = a.mapinv[a.n1_first + row];
+  if (tid < B) {
+    s_om1[tid] = tid < b ? a.freq[(size_t)q1 * b + tid] : 0.0;
+    s_nb1[tid] = tid < b ? a.dist[(size_t)q1 * b + tid] : 0.0;
+  }
+  __syncthreads();
+  const int q = blockIdx.x * blockDim.x + tid;
+  if (q >= nkc) return;  // no barrier below
+  int m1[3], mq[3], m3[3], mn[3];
+  decompose(g, q1, m1);
+  decompose(g, q, mq);
+  int ins;
+  const int q3 = pm_index_m(g, m1, mq, 1, ins, m3);  // q1 + q = q1 - (-q)
+  for (int x = 0; x < 3; ++x) mn[x] = wrap2(-mq[x], g.nc[x]);
+  const int wn = compose(g, mn);  // -q
+  const bool gq = at_gamma_index(g, mq), gn = at_gamma_index(g, mn), g3 = at_gamma_index(g, m3);
+  const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
+  const double n2a = a.dist[(size_t)q * b + l2], w2a = a.freq[(size_t)q * b + l2];
+  const double n2b = a.dist[(size_t)wn * b + l2], w2b = a.freq[(size_t)wn * b + l2];
+  const double* v3 = a.v3sq + (size_t)row * nkc * b3;
+  const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
+  const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
+  const float fc1 = (float)(0.5 / (a.sigma * a.sigma)), fc2 = (float)(1.0 / (sqrt(2 * PhysConst::pi) * a.sigma));
+  double R1[B], R2[B];
+#pragma unroll
+  for (int l = 0; l < B; ++l) R1[l] = R2[l] = 0.0;
+  for (int l3 = 0; l3 < b; ++l3) {
+    const double n3 = a.dist[(size_t)q3 * b + l3], w3 = a.freq[(size_t)q3 * b + l3];
+    const bool zero1 = (l2 < 3 && gq) || (l3 < 3 && g3);
+    const bool zero2 = (l2 < 3 && gn) || (l3 < 3 && g3);
+#pragma unroll
+    for (int l = 0; l < B; ++l) {
+      if (l >= b) continue;
+      const double v = v3[(size_t)q * sq + l * s1 + l2 * s2 + l3 * s3] * fnorm;
+      const double nb1 = s_nb1[l];
+      {  // process 1 at w = q
+        const float xf = (float)(s_om1[l] + w2a - w3), arg = xf * xf * fc1;
+        if (arg < 104.0f && !zero1) {
+          const double p = ((double)(expf(-arg) * fc2) * v) * (nb1 * n2a * (n3 + 1));
+          R1[l] += p;
+          if (a.R1p && p != 0.0) atomicAdd(a.R1p + (((size_t)row * nkc + q) * b + l) * b + l3, p);
+        }
+      }
+      {  // process 2 at w = -q
+        const float xf = (float)(s_om1[l] - w2b - w3), arg = xf * xf * fc1;
+        if (arg < 104.0f && !zero2) {
+          const double p = ((double)(expf(-arg) * fc2) * v) * (nb1 * (n2b + 1) * (n3 + 1));
+          R2[l] += p;
+          if (a.R2p && p != 0.0) atomicAdd(a.R2p + (((size_t)row * nkc + wn) * b + l) * b + l3, p);
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < B; ++l) {
+    if (l >= b) continue;
+    a.R1[(((size_t)row * nkc + q) * b + l) * b + l2] = R1[l];
+    a.R2[(((size_t)row * nkc + wn) * b + l) * b + l2] = R2[l];
+  }
+}
+
 // Q, Q_N, Q_U from the band sums: Q = sum_{w,l2} R1 + R2/2, split by the
 // normal/umklapp flag of q1+w (process 1) and q1-w (process 2)
 __global__ void __launch_bounds__(256) q_from_r_kernel(Geometry g, int n1_first, const int* mapinv,
@@ -670,8 +743,11 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s) 
   dim3 grid_tile((g.nkc + nw - 1) / nw, a.nrows), grid_row((g.nkc + kPointBlock - 1) / kPointBlock, a.nrows, g.b);
   // FP32 weights only for the Gaussian (the tetrahedron weights W are FP64 here)
   const bool fw = a.f32w && a.gauss;
+  const bool pair = fw && !a.P1s && !a.P2s && !a.P1 && !a.P2;
 #define ALD_POINT(BB)                                                               \
-  if (fw)                                                                           \
+  if (pair)                                                                         \
+    delta_point_pair_kernel<BB><<<grid_row, kPointBlock, 0, s>>>(a);                \
+  else if (fw)                                                                      \
     delta_point_kernel<BB, true, false><<<grid_row, kPointBlock, 0, s>>>(a, W);     \
   else                                                                              \
     delta_point_kernel<BB, false, true><<<grid_tile, kPointBlock, 0, s>>>(a, W);
