@@ -59,10 +59,12 @@ __device__ __forceinline__ double nbe_dev(double w, double t, int m, int* err) {
   return 1 / z;
 }
 
-__device__ __forceinline__ void opmul(const double* op, const double* v, double* out) {  // column-major 3x3
+// syop_f's product (column-major 3x3), rounded as the Fortran rounds it (no
+// fused multiply-add), so that near-cancelling components come out the same
+__device__ __forceinline__ void opmul(const double* op, const double* v, double* out) {
   for (int i = 0; i < 3; ++i) {
     double x = 0;
-    for (int j = 0; j < 3; ++j) x = x + op[i + 3 * j] * v[j];
+    for (int j = 0; j < 3; ++j) x = __dadd_rn(x, __dmul_rn(op[i + 3 * j], v[j]));
     out[i] = x;
   }
 }
@@ -103,6 +105,29 @@ __global__ void rhs_kernel(KappaArgs a, double* rhs) {
 // components, added in CTA order by kappa_final_kernel
 constexpr int kKapThreads = 128;
 
+// velocity of IBZ mode (i, l): veloc at mapinv(i) (mode_kappa), or the star
+// average with inverse operations (veloc_avergeIBZ_invsyFBZ, sub.f90:5479)
+__device__ __forceinline__ void mode_velocity(const KappaArgs& a, int i, int l, int averaged, double vv[3]) {
+  const int b = a.geo.b;
+  if (averaged) {
+    int s0 = a.star_off[i], s1 = a.star_off[i + 1];
+    double narms = (double)(s1 - s0);
+    double va[3] = {0, 0, 0};
+    for (int t = s0; t < s1; ++t) {
+      const double* vq = a.vel + ((size_t)a.star_q[t] * b + l) * 3;
+      double vin[3] = {vq[0], vq[1], vq[2]}, vr[3];
+      opmul(a.opk_inv + 9 * a.star_op[t], vin, vr);
+      for (int x = 0; x < 3; ++x) va[x] = va[x] + (vr[x] / narms);
+    }
+    for (int x = 0; x < 3; ++x) vv[x] = va[x];
+  } else {
+    const double* vq = a.vel + ((size_t)a.mapinv[i] * b + l) * 3;
+    vv[0] = vq[0];
+    vv[1] = vq[1];
+    vv[2] = vq[2];
+  }
+}
+
 __global__ void __launch_bounds__(kKapThreads) kappa_arm_kernel(KappaArgs a, const double* F, int averaged,
                                                                 int narm, int* err) {
   __shared__ double red[9][kKapThreads / 32];
@@ -114,24 +139,7 @@ __global__ void __launch_bounds__(kKapThreads) kappa_arm_kernel(KappaArgs a, con
     const int i = a.arm_owner[s];
     double f[3] = {F[((size_t)i * b + l) * 3], F[((size_t)i * b + l) * 3 + 1], F[((size_t)i * b + l) * 3 + 2]};
     double vv[3];
-    if (averaged) {
-      // star average with inverse operations (veloc_avergeIBZ_invsyFBZ)
-      int s0 = a.star_off[i], s1 = a.star_off[i + 1];
-      double narms = (double)(s1 - s0);
-      double va[3] = {0, 0, 0};
-      for (int t = s0; t < s1; ++t) {
-        const double* vq = a.vel + ((size_t)a.star_q[t] * b + l) * 3;
-        double vin[3] = {vq[0], vq[1], vq[2]}, vr[3];
-        opmul(a.opk_inv + 9 * a.star_op[t], vin, vr);
-        for (int x = 0; x < 3; ++x) va[x] = va[x] + (vr[x] / narms);
-      }
-      for (int x = 0; x < 3; ++x) vv[x] = va[x];
-    } else {
-      const double* vq = a.vel + ((size_t)a.mapinv[i] * b + l) * 3;
-      vv[0] = vq[0];
-      vv[1] = vq[1];
-      vv[2] = vq[2];
-    }
+    mode_velocity(a, i, l, averaged, vv);
     const double* op = a.opk + 9 * a.arm_op[s];
     double F12[3], velocc[3];
     opmul(op, f, F12);
@@ -164,6 +172,49 @@ __global__ void kappa_final_kernel(int b, int nblk, const double* part, double* 
   for (int q = 0; q < nblk; ++q) s += part[((size_t)l * nblk + q) * 9 + k];
   const int j = k % 3, jj = k / 3;
   kappa_modes[l + b * (j + 3 * jj)] = s;  // kappa(ndyn,3,3) column-major
+}
+
+// tauinv_eff(i, l): a thread per IBZ mode, its star arms in table order.
+//   mode_kappa   (averaged = 0, sub.f90:1360-1365): per arm and j,
+//     -= const2 F12(j)/omega/0.01 where velocc(j) == 0, else
+//     -= const2 F12(j)/omega/velocc(j)/(3 narms);
+//   mode_kappa_d (averaged = 1, sub.f90:1497): per arm, three times (the j
+//     loop around it), -= const2 (F12.velocc)/omega/(velocc.velocc)/(3 narms).
+// F12 and velocc are F and the velocity rotated onto the arm (syop_f).
+__global__ void tau_eff_kernel(KappaArgs a, const double* F, int averaged, double* tinv) {
+  const int b = a.geo.b;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= a.nibz * b) return;
+  const int i = idx / b, l = idx % b;
+  const double f[3] = {F[(size_t)idx * 3], F[(size_t)idx * 3 + 1], F[(size_t)idx * 3 + 2]};
+  double vv[3];
+  mode_velocity(a, i, l, averaged, vv);
+  const int s0 = a.arm_off[i], s1 = a.arm_off[i + 1];
+  const double narms3 = (double)(s1 - s0) * 3.0;
+  double t = 0.0;
+  for (int s = s0; s < s1; ++s) {
+    const double* op = a.opk + 9 * a.arm_op[s];
+    double F12[3], velocc[3];
+    opmul(op, f, F12);
+    opmul(op, vv, velocc);
+    const double omega = sqrt(a.w2[(size_t)a.arm_q[s] * b + l]) * PhysConst::cnst();
+    if (averaged) {
+      const double fv = __dadd_rn(__dadd_rn(__dmul_rn(F12[0], velocc[0]), __dmul_rn(F12[1], velocc[1])),
+                                  __dmul_rn(F12[2], velocc[2]));
+      const double v2 = __dadd_rn(__dadd_rn(__dmul_rn(velocc[0], velocc[0]), __dmul_rn(velocc[1], velocc[1])),
+                                  __dmul_rn(velocc[2], velocc[2]));
+      const double term = (((a.const2 * fv) / omega) / v2) / narms3;
+      for (int j = 0; j < 3; ++j) t = t - term;
+    } else {
+      for (int j = 0; j < 3; ++j) {
+        if (velocc[j] == 0.0)
+          t = t - ((a.const2 * F12[j]) / omega) / 0.01;
+        else
+          t = t - (((a.const2 * F12[j]) / omega) / velocc[j]) / narms3;
+      }
+    }
+  }
+  tinv[idx] = t;
 }
 
 // collision matrix: thread per (n1, n2, l1, l2), l2 fastest, so that the b*b
@@ -587,6 +638,13 @@ cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, doub
   const int nblk = std::max(1, (narm + kKapThreads - 1) / kKapThreads);
   kappa_arm_kernel<<<dim3(nblk, a.geo.b), kKapThreads, 0, s>>>(a, F, averaged, narm, err);
   kappa_final_kernel<<<(9 * a.geo.b + 127) / 128, 128, 0, s>>>(a.geo.b, nblk, a.part, kappa_modes);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_tau_eff(const KappaArgs& a, const double* F, int averaged, double* tauinv_eff,
+                           cudaStream_t s) {
+  const int n = a.nibz * a.geo.b;
+  tau_eff_kernel<<<(n + 127) / 128, 128, 0, s>>>(a, F, averaged, tauinv_eff);
   return cudaGetLastError();
 }
 

@@ -223,6 +223,7 @@ KappaArgs kappa_args(ald_ctx* c, double tempk) {
   k.temp = temp_cm(tempk);
   k.const1 = PhysConst::h_plank * PhysConst::c_light * 100 * PhysConst::c_light /
              (c->T.nkc * c->S.volume_r / 1e30);
+  k.const2 = PhysConst::k_b * (tempk * tempk) / (PhysConst::h_plank * PhysConst::c_light * 100) / PhysConst::c_light;
   k.classical = c->S.classical;
   k.arm_owner = c->arm_owner.p;
   k.narm = (int)c->T.arm_q.size();

@@ -293,6 +293,7 @@ struct KappaArgs {
   const double* opk;         // 48*9
   const double* opk_inv;     // 48*9
   double tempk, temp, const1;
+  double const2;             // k_b T^2/(h c 100)/c (mode_kappa's tauinv_eff)
   int classical;
   const int* arm_owner;      // per arm (arm_q entry): its IBZ point
   int narm;                  // arm_off[nibz]
@@ -303,6 +304,10 @@ cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaS
 cudaError_t launch_kappa(const KappaArgs& a, const double* F, int averaged, double* kappa_modes, int* err,
                          cudaStream_t s);
 cudaError_t launch_rhs(const KappaArgs& a, double* rhs, cudaStream_t s);
+// tauinv_eff(nibz, b) [i*b + l] of mode_kappa (averaged = 0, F = F_RTA) or
+// mode_kappa_d (averaged = 1, F = the CG solution), both [(i*b + l)*3 + x]
+cudaError_t launch_tau_eff(const KappaArgs& a, const double* F, int averaged, double* tauinv_eff,
+                           cudaStream_t s);
 // CM: double, or float when cm_f32 (mixed-precision pipeline); leading dimension ld.
 // piso (optional, [row][l1] of the range): CollisionMatrix_iso's form instead
 // of CollisionMatrix_mpi's (Q must then include Piso); mesh_m: 4 mesh integers per point

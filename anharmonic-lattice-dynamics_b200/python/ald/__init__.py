@@ -66,7 +66,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
            "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
-           "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded"]
+           "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_tau_eff", "ald_qandtau",
+           "ald_write_kappa", "ald_write_job1_files", "ald_format_value"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -87,11 +88,23 @@ def lib():
         L.ald_set_stream.argtypes = [C.c_void_p, C.c_void_p]
         L.ald_cg_quadratic_static.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                               C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p]
+        L.ald_format_value.argtypes = [C.c_char_p, C.c_double, C.c_char_p, C.c_int]
         for n in EXPORTS[2:]:
             if n not in ("ald_destroy", "ald_h2d_bytes"):
                 getattr(L, n).restype = C.c_int
         _lib = L
     return _lib
+
+
+def format_value(edit: str, value) -> str:
+    """One value formatted as the output writers format it (host only):
+    edit "Iw", "Fw.d", "Ew.d", "Gw.d", "*" (list-directed REAL(8)) or "*I"
+    (list-directed INTEGER)."""
+    buf = C.create_string_buffer(512)
+    n = lib().ald_format_value(edit.encode(), C.c_double(value), buf, 512)
+    if n < 0:
+        raise ValueError("bad edit descriptor %r" % edit)
+    return buf.value.decode()
 
 
 def _p(a):
@@ -303,6 +316,44 @@ class Context:
         kap = np.zeros((self.ndyn, 3, 3), order="F")
         _check(lib().ald_mode_kappa_d(self.h, C.c_double(tempk), _p(np.ascontiguousarray(x, dtype=float)), _p(kap)))
         return kap
+
+    def tau_eff(self, tempk, F, solution: int):
+        """tauinv_eff(nibz, ndyn) per mode: mode_kappa's sum (solution 0, F =
+        FFF(nibz,ndyn,3)) or mode_kappa_d's (solution 1, F = the CG solution)."""
+        t = np.zeros((self.nibz, self.ndyn), order="F")
+        f = np.asfortranarray(F, dtype=float) if solution == 0 else np.ascontiguousarray(F, dtype=float)
+        _check(lib().ald_tau_eff(self.h, C.c_double(tempk), _p(f), int(solution), _p(t)))
+        return t
+
+    def qandtau(self, tempk, Q, QN, QU, qvalue_path: Optional[str] = None):
+        """Qandtau (sub.f90:8198): tauinv_N, tauinv_U, tauinv_tot(nibz, ndyn) in
+        1/s; writes Qvalue.dat to qvalue_path when given."""
+        tN, tU, tT = (np.zeros((self.nibz, self.ndyn), order="F") for _ in range(3))
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        _check(lib().ald_qandtau(self.h, C.c_double(tempk), f(Q), f(QN), f(QU),
+                                 qvalue_path.encode() if qvalue_path else None, _p(tN), _p(tU), _p(tT)))
+        return tN, tU, tT
+
+    def write_kappa(self, tempk, kappa_modes, tauinv_N, tauinv_U, tauinv_tot, tauinv_eff,
+                    kappa_path: Optional[str] = None, tau_path: Optional[str] = None):
+        """write_kappa (sub.f90:1818).  tauinv_N and tauinv_U must be float64
+        Fortran-ordered arrays: zero entries become 1e10 in place, as in the
+        reference."""
+        for a in (tauinv_N, tauinv_U):
+            if not (isinstance(a, np.ndarray) and a.dtype == np.float64 and a.flags.f_contiguous):
+                raise TypeError("tauinv_N and tauinv_U must be float64 arrays in Fortran order")
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        _check(lib().ald_write_kappa(self.h, C.c_double(tempk), f(kappa_modes), _p(tauinv_N), _p(tauinv_U),
+                                     f(tauinv_tot), f(tauinv_eff), kappa_path.encode() if kappa_path else None,
+                                     tau_path.encode() if tau_path else None))
+
+    def write_job1_files(self, out_dir: str, tempk, res: dict):
+        """The five output files of kappa_full's job=1 block, from the dict
+        kappa_pipeline() returns (it needs the per-mode arrays)."""
+        f = lambda a: _p(np.asfortranarray(a, dtype=float))
+        _check(lib().ald_write_job1_files(self.h, out_dir.encode(), C.c_double(tempk), f(res["Q"]), f(res["QN"]),
+                                          f(res["QU"]), f(res["kappa_rta_modes"]), f(res["kappa_cg_modes"]),
+                                          _p(np.ascontiguousarray(res["x"], dtype=float))))
 
     def kappa_pipeline(self, tempk: Optional[float] = None, want_modes=True):
         if tempk is None:

@@ -34,6 +34,7 @@ SOURCES = {
     "ald_bte.cu": [],
     "ald_util.cu": [],
     "ald_cg_static.cu": [],
+    "ald_writers.cpp": [],
 }
 
 

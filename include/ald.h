@@ -276,6 +276,54 @@ int ald_kappa_pipeline_sharded(ald_ctx* ctx, double tempk, int rank, int nranks,
 int ald_kappa_iterative(ald_ctx* ctx, double tempk, int max_iter, double update_mix, ald_kappa_result* res,
                         double* Q, double* kappa_rta_modes, double* kappa_iter_modes, double* FFF);
 
+/* Output files of a job=1 run, as the reference's gfortran build writes
+ * them (list-directed records: I11 integers, REAL(8) with 17 significant
+ * digits in 25 columns; formatted records: the Fortran Iw/Fw.d/Ew.d/Gw.d
+ * rules).
+ *
+ * ald_tau_eff: tauinv_eff(nibz,ndyn) per mode, the sum mode_kappa
+ * (solution = 0, sub.f90:1336-1366; F = FFF(nibz,ndyn,3) of
+ * ald_rta_kappa, velocities at mapinv, velocc(j) == 0 -> /0.01) or
+ * mode_kappa_d (solution = 1, sub.f90:1497; F = the CG solution
+ * Fi_x(nibz*ndyn*3), star-averaged velocities) adds for that mode.
+ *
+ * ald_qandtau replaces Qandtau (sub.f90:8198-8305): tauinv_N, tauinv_U,
+ * tauinv_tot(nibz,ndyn) in 1/s from Q, Q_N, Q_U(nibz,ndyn), and the file
+ * Qvalue.dat ("nk,la,Q", then ibz, la, Q, Q/(n(n+1))) when qvalue_path is
+ * not NULL.
+ *
+ * ald_write_kappa replaces write_kappa (sub.f90:1818-1916): kappa_path
+ * gets the per-band tensor, tot_kap and the diagonal sums, tau_path one
+ * line per IBZ mode (tempk, i, kibz, la, omega, n, 1/tauinv_N,
+ * 1/tauinv_U, 1/tauinv_tot, tauinv_eff, veloc at mapinv).  Like the
+ * reference it sets zero entries of tauinv_N and tauinv_U to 1e10 in
+ * place.  Either path may be NULL.
+ *
+ * ald_write_job1_files writes, into directory dir, the five files of
+ * kappa_full's job=1 block (kappa.f90:559-870) from the outputs of
+ * ald_kappa_pipeline (Q, QN, QU, the two per-band tensors and x):
+ * Qvalue.dat; tau_RTA.dat and kappa_RTA.dat; tau_RTAandeff-cg.dat and
+ * kappa_direct-cg.dat.  tauinv_eff follows the reference's array: mode_kappa
+ * clears the whole array before each mode, so the RTA file carries only the
+ * last mode's value (nibz, ndyn) and zeros elsewhere; mode_kappa_d adds its
+ * sums on top of that.
+ *
+ * ald_format_value formats one value as the writers do, host only: edit
+ * "Iw", "Fw.d", "Ew.d", "Gw.d", "*" (a list-directed REAL(8) field, 25
+ * characters, no separator) or "*I" (a list-directed INTEGER field, 11
+ * characters).  Returns the length written into out (NUL-terminated), -1
+ * for a bad edit or a short buffer. */
+int ald_tau_eff(ald_ctx* ctx, double tempk, const double* F, int solution, double* tauinv_eff);
+int ald_qandtau(ald_ctx* ctx, double tempk, const double* Q, const double* QN, const double* QU,
+                const char* qvalue_path, double* tauinv_N, double* tauinv_U, double* tauinv_tot);
+int ald_write_kappa(ald_ctx* ctx, double tempk, const double* kappa, double* tauinv_N, double* tauinv_U,
+                    const double* tauinv_tot, const double* tauinv_eff, const char* kappa_path,
+                    const char* tau_path);
+int ald_write_job1_files(ald_ctx* ctx, const char* dir, double tempk, const double* Q, const double* QN,
+                         const double* QU, const double* kappa_rta_modes, const double* kappa_cg_modes,
+                         const double* x);
+int ald_format_value(const char* edit, double value, char* out, int cap);
+
 #ifdef __cplusplus
 }
 #endif

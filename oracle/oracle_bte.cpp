@@ -487,12 +487,19 @@ static void syop_f(const State& S, int s, const double* ff, double* fs) {
   }
 }
 
+// teff (optional) is the module array tauinv_eff(nibz,ndn): mode_kappa
+// (averaged = false) clears all of it before each mode (sub.f90:1337) and
+// adds per arm and j const2 F12(j)/omega/velocc(j)/(3 narms), or /0.01 where
+// velocc(j) == 0 (sub.f90:1360-1365); mode_kappa_d (averaged = true) adds to
+// what it holds, per arm and j, const2 (F12.velocc)/omega/(velocc.velocc)/(3
+// narms) (sub.f90:1497).
 static int kappa_core(State& S, double tempk, const double* FFF, const double* velsrc, bool averaged,
-                      double* kappa) {
+                      double* kappa, double* teff = nullptr, bool reset = true) {
   int ndn = S.ndyn, nkc = S.nkc, nibz = S.nibz;
   const Consts& K = S.K;
   double temp = tempk * K.k_b / (100 * K.h_plank * K.c_light);
   double const1 = K.h_plank * K.c_light * 100 * K.c_light / (nkc * S.volume_r / 1e30);
+  double const2 = K.k_b * (tempk * tempk) / (K.h_plank * K.c_light * 100) / K.c_light;
   std::fill(kappa, kappa + ndn * 9, 0.0);
   int err = 0;
   for (int i = 1; i <= nibz; ++i) {
@@ -500,7 +507,8 @@ static int kappa_core(State& S, double tempk, const double* FFF, const double* v
     int narms, kvecop[48];
     double kvecstar[48][3];
     kstarsinfbz1(S, q, narms, kvecstar, kvecop);
-    for (int ii = 1; ii <= ndn; ++ii)
+    for (int ii = 1; ii <= ndn; ++ii) {
+      if (teff && !averaged && reset) std::fill(teff, teff + (size_t)nibz * ndn, 0.0);
       for (int s = 1; s <= narms; ++s) {
         double F12[3], velocc[3], f[3], vv[3];
         for (int c = 0; c < 3; ++c) f[c] = FFF[F3(i, ii, c + 1, nibz, ndn)];
@@ -514,20 +522,35 @@ static int kappa_core(State& S, double tempk, const double* FFF, const double* v
         get_k_info(S, kvecstar[s - 1], n0, a1, a2, a3, ins);
         double omega = std::sqrt(S.eigenval[F2(ii, n0, ndn)]) * K.cnst;
         double nb0 = nbe(omega, temp, S.classical, &err);
-        for (int j = 1; j <= 3; ++j)
+        for (int j = 1; j <= 3; ++j) {
           for (int jj = 1; jj <= 3; ++jj)
             kappa[F3(ii, j, jj, ndn, 3)] = kappa[F3(ii, j, jj, ndn, 3)] -
                                            ((((const1 * omega) * velocc[j - 1]) * nb0) * (nb0 + 1)) * F12[jj - 1];
+          if (!teff) continue;
+          double& t = teff[F2(i, ii, nibz)];
+          if (!averaged) {
+            if (velocc[j - 1] == 0.0)
+              t = t - const2 * F12[j - 1] / omega / 0.01;
+            else
+              t = t - const2 * F12[j - 1] / omega / velocc[j - 1] / (narms * 3.0);
+          } else {
+            double fv = 0, v2 = 0;  // dot_product
+            for (int c = 0; c < 3; ++c) fv = fv + F12[c] * velocc[c];
+            for (int c = 0; c < 3; ++c) v2 = v2 + velocc[c] * velocc[c];
+            t = t - const2 * fv / omega / v2 / (narms * 3.0);
+          }
+        }
       }
+    }
   }
   return err;
 }
 
-int mode_kappa(State& S, double tempk, const double* FFF, double* kappa) {
-  return kappa_core(S, tempk, FFF, S.veloc.data(), false, kappa);
+int mode_kappa(State& S, double tempk, const double* FFF, double* kappa, double* teff, bool reset) {
+  return kappa_core(S, tempk, FFF, S.veloc.data(), false, kappa, teff, reset);
 }
 
-int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa) {
+int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa, double* teff) {
   int ndn = S.ndyn, nibz = S.nibz;
   std::vector<double> FFF((size_t)nibz * ndn * 3);
   int r = 0;
@@ -576,7 +599,7 @@ int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa) {
       for (int c = 0; c < 3; ++c) veloci[F3(c + 1, j, i, 3, ndn)] = veli_a[c];
     }
   }
-  return kappa_core(S, tempk, FFF.data(), veloci.data(), true, kappa);
+  return kappa_core(S, tempk, FFF.data(), veloci.data(), true, kappa, teff);
 }
 
 // ------------------------------------------------------- collision matrix

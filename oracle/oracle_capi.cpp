@@ -238,6 +238,20 @@ int orc_kappa_d(void* p, double tempk, const double* x, double* kappa) {
   return mode_kappa_d(S, tempk, x, kappa);
 }
 
+// mode_kappa from FFF(nibz,ndn,3) with the module array tauinv_eff(nibz,ndn)
+// as it leaves it (teff in/out); keep_all = 1 skips the per-mode clearing,
+// so that every mode keeps its own sum
+int orc_mode_kappa_teff(void* p, double tempk, const double* FFF, double* kappa, double* teff, int keep_all) {
+  State& S = *(State*)p;
+  return mode_kappa(S, tempk, FFF, kappa, teff, keep_all == 0);
+}
+
+// mode_kappa_d adding to tauinv_eff(nibz,ndn) (teff in/out)
+int orc_kappa_d_teff(void* p, double tempk, const double* x, double* kappa, double* teff) {
+  State& S = *(State*)p;
+  return mode_kappa_d(S, tempk, x, kappa, teff);
+}
+
 int orc_update_mpi(void* p, int k1, int k2, const double* P1, const double* P2, const double* Q,
                    const double* F_RTA, const double* FFF, double* F2, int nthreads) {
   State& S = *(State*)p;

@@ -184,14 +184,17 @@ void calculate_tauRTA_mpi2(State& S, int k1, int k2, double tempk, const double*
                            const double* P2smpi, double* Q, double* QN, double* QU, double* P1, double* P2,
                            int nthreads);
 void calculate_RTA_distributionfunction(State& S, double tempk, const double* Q, double* FFF);
-int mode_kappa(State& S, double tempk, const double* FFF, double* kappa);
+// teff: tauinv_eff(nibz,ndn) in/out; reset = false keeps every mode's sum
+// (a checker mode: the reference clears the array before each mode)
+int mode_kappa(State& S, double tempk, const double* FFF, double* kappa, double* teff = nullptr,
+               bool reset = true);
 void kstarsinfbz1(const State& S, const double q[3], int& ds, double kvecstars[][3], int kvecops[]);
 void CollisionMatrix_mpi(State& S, int k1, int k2, const double* P1, const double* P2, double* CM,
                          int nthreads);
 void cal_RHS_IBZ(State& S, double tempk, double* RHS);
 int cg_quadratic(int n, const double* a, const double* b, double* vmin, double* funcmin, int max_iter,
                  int n_dig_accur, int nthreads);
-int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa);
+int mode_kappa_d(State& S, double tempk, const double* Fi_x, double* kappa, double* teff = nullptr);
 void update_mpi(State& S, int k1, int k2, const double* P1, const double* P2, const double* Q,
                 const double* F_RTA, const double* FFF, double* F2mpi, int nthreads);
 // isotope scattering (iso=1): cal_g / cal_giso, P_iso_split, CollisionMatrix_iso

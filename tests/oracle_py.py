@@ -38,7 +38,8 @@ def lib():
                      "orc_get_k_info", "orc_getstar", "orc_kstars", "orc_dynmat", "orc_get_freq", "orc_phonons",
                      "orc_get_phonons", "orc_set_phonons", "orc_tet", "orc_v3", "orc_fgr", "orc_distribution",
                      "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d", "orc_update_mpi",
-                     "orc_iterative", "orc_giso", "orc_p_iso", "orc_collision_iso"]:
+                     "orc_iterative", "orc_giso", "orc_p_iso", "orc_collision_iso", "orc_mode_kappa_teff",
+                     "orc_kappa_d_teff"]:
             getattr(L, name).restype = C.c_int
         L.orc_weight_tet_nonperm.restype = C.c_long
         _lib = L
@@ -259,6 +260,28 @@ class Oracle:
         if e:
             raise RuntimeError("nbe error %d" % e)
         return F, kap, it.value, nk.value
+
+    def mode_kappa_teff(self, tempk, FFF, teff=None, keep_all=False):
+        """mode_kappa (sub.f90:1292) and the module array tauinv_eff(nibz,ndn)
+        as it leaves it: only the last mode keeps its sum (keep_all: every
+        mode keeps its own sum)."""
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        t = np.zeros((self.nibz, self.ndyn), order="F") if teff is None else np.asfortranarray(teff).copy()
+        e = lib().orc_mode_kappa_teff(self.h, C.c_double(tempk), _p(np.asfortranarray(FFF)), _p(kap), _p(t),
+                                      int(keep_all))
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return kap, t
+
+    def kappa_d_teff(self, tempk, x, teff):
+        """mode_kappa_d (sub.f90:1407) adding to tauinv_eff (a copy of teff)."""
+        kap = np.zeros((self.ndyn, 3, 3), order="F")
+        t = np.asfortranarray(teff, dtype=float).copy()
+        e = lib().orc_kappa_d_teff(self.h, C.c_double(tempk), _p(np.ascontiguousarray(x, dtype=float)), _p(kap),
+                                   _p(t))
+        if e:
+            raise RuntimeError("nbe error %d" % e)
+        return kap, t
 
     def kappa_d(self, tempk, x):
         kap = np.zeros((self.ndyn, 3, 3), order="F")
