@@ -266,7 +266,7 @@ class Oracle:
         as it leaves it: only the last mode keeps its sum (keep_all: every
         mode keeps its own sum)."""
         kap = np.zeros((self.ndyn, 3, 3), order="F")
-        t = np.zeros((self.nibz, self.ndyn), order="F") if teff is None else np.asfortranarray(teff).copy()
+        t = np.zeros((self.nibz, self.ndyn), order="F") if teff is None else np.array(teff, dtype=float, order="F")
         e = lib().orc_mode_kappa_teff(self.h, C.c_double(tempk), _p(np.asfortranarray(FFF)), _p(kap), _p(t),
                                       int(keep_all))
         if e:
@@ -276,7 +276,7 @@ class Oracle:
     def kappa_d_teff(self, tempk, x, teff):
         """mode_kappa_d (sub.f90:1407) adding to tauinv_eff (a copy of teff)."""
         kap = np.zeros((self.ndyn, 3, 3), order="F")
-        t = np.asfortranarray(teff, dtype=float).copy()
+        t = np.array(teff, dtype=float, order="F")
         e = lib().orc_kappa_d_teff(self.h, C.c_double(tempk), _p(np.ascontiguousarray(x, dtype=float)), _p(kap),
                                    _p(t))
         if e:

@@ -5,10 +5,12 @@ oracle's restatement of Qandtau / write_kappa (oracle/writers.py), GPU.
 The oracle's eigenpairs are injected into the context (identical inputs, as
 in the stage parity tests).  Records must agree in layout (line count, line
 lengths, token count, every integer, every non-numeric token) and in value:
-equal text, or numbers within one unit of the last printed digit plus the
-stated relative tolerance (1e-10 given the oracle's results; 1e-8 for the
-files from the library's own pipeline, the kappa_cg tolerance of the
-pipeline parity test).
+equal text, or numbers within one unit of the last printed digit plus
+rtol |value| + atol max|column| (rtol 1e-10, atol 1e-12 given the oracle's
+results; rtol 1e-8, atol 1e-10 for the files from the library's own
+pipeline, the kappa_cg tolerance of the pipeline parity test; there the
+1/tauinv columns are compared as rates, since the inverse of a rate near
+zero is arbitrarily large).
 
 tauinv_eff of mode_kappa_d divides by |v|^2 of the star-averaged velocity:
 where that velocity is rounding noise (|v| < 1e-9 max|v|) both codes return
@@ -47,10 +49,34 @@ def last_unit(t):
     return 10.0 ** (-len(m.group(3)) + int(m.group(4) or 0))
 
 
-def compare(a_path, b_path, rtol, skip=lambda line, col: False):
+def _val(t, inverse):
+    v = num(t)
+    if inverse:  # 1/rate -> rate
+        return 0.0 if math.isinf(v) else 1.0 / v
+    return v
+
+
+def column_scale(lines, inverse=()):
+    """max |value| per token column over the finite numbers of a file."""
+    sc = {}
+    for y in lines:
+        for c, v in enumerate(y.split()):
+            if NUM.match(v) and "." in v:
+                f = abs(_val(v, c in inverse))
+                if math.isfinite(f):
+                    sc[c] = max(sc.get(c, 0.0), f)
+    return sc
+
+
+def compare(a_path, b_path, rtol, atol, skip=lambda line, col: False, inverse=()):
+    """a (library) vs b (oracle): |a - b| <= one unit of b's last digit +
+    rtol |b| + atol max|column of b|, or equal text.  Columns in `inverse`
+    hold 1/rate and are compared as rates (a rate near zero makes its
+    inverse arbitrarily large)."""
     A = open(a_path).read().split("\n")
     B = open(b_path).read().split("\n")
     assert len(A) == len(B), (a_path, len(A), len(B))
+    scale = column_scale(B, inverse)
     worst = 0.0
     for k, (x, y) in enumerate(zip(A, B)):
         if x == y:
@@ -63,8 +89,10 @@ def compare(a_path, b_path, rtol, skip=lambda line, col: False):
                 continue
             assert NUM.match(u) and NUM.match(v), (a_path, k, c, u, v)
             assert "." in u, (a_path, k, c, u, v)  # integers must match exactly
-            fu, fv = num(u), num(v)
-            err = abs(fu - fv) - 1.01 * last_unit(v) - rtol * abs(fv)
+            inv = c in inverse
+            fu, fv = _val(u, inv), _val(v, inv)
+            unit = last_unit(v) * (abs(fv) / abs(num(v)) if inv and fv != 0 else 1.0)
+            err = abs(fu - fv) - 1.01 * unit - rtol * abs(fv) - atol * scale.get(c, 0.0)
             worst = max(worst, abs(fu - fv) / (abs(fv) + 1e-300))
             assert err <= 0, (a_path, k, c, u, v)
     return worst
@@ -124,7 +152,7 @@ def test_qandtau(case, tmp_path):
                             str(tmp_path / "Qvalue_oracle.dat"))
     for g, r in ((tN, oN), (tU, oU), (tT, oT)):
         assert np.allclose(g, r, rtol=1e-12, atol=0)
-    compare(str(tmp_path / "Qvalue.dat"), str(tmp_path / "Qvalue_oracle.dat"), 1e-12)
+    compare(str(tmp_path / "Qvalue.dat"), str(tmp_path / "Qvalue_oracle.dat"), 1e-12, 0.0)
 
 
 def _skip_for(mapinv, vel, ndn):
@@ -151,7 +179,7 @@ def test_files_given_oracle_results(case, tmp_path):
                           ref["x"])
     skip = _skip_for(mapinv, vel, ctx.ndyn)
     for f in FILES:
-        compare(os.path.join(lib_dir, f), os.path.join(orc_dir, f), 1e-10,
+        compare(os.path.join(lib_dir, f), os.path.join(orc_dir, f), 1e-10, 1e-12,
                 skip if f == "tau_RTAandeff-cg.dat" else (lambda line, col: False))
     # the layout of kappa_full's files: one record per IBZ mode plus a header
     n = ref["O"].nibz * ctx.ndyn
@@ -171,5 +199,6 @@ def test_files_from_pipeline(case, tmp_path):
                           ref["x"])
     skip = _skip_for(mapinv, vel, ctx.ndyn)
     for f in FILES:
-        compare(os.path.join(lib_dir, f), os.path.join(orc_dir, f), 1e-8,
-                skip if f == "tau_RTAandeff-cg.dat" else (lambda line, col: False))
+        compare(os.path.join(lib_dir, f), os.path.join(orc_dir, f), 1e-8, 1e-10,
+                skip if f == "tau_RTAandeff-cg.dat" else (lambda line, col: False),
+                inverse=(8, 9, 10) if f.startswith("tau") else ())
