@@ -288,4 +288,51 @@ int orc_collision_iso(void* p, const double* P1, const double* P2, const double*
   return 0;
 }
 
+// make_kp_bs from dir/kpbs.params: *nkp points; kp (3,nkp) and dk (nkp)
+// filled when cap >= nkp.  Returns 0, or 1 (message in err).
+int orc_make_kp_bs(void* p, const char* dir, int* nkp, double* kp, double* dk, int cap, char* err, int errlen) {
+  State& S = *(State*)p;
+  std::vector<double> k, d;
+  std::string e = make_kp_bs(S, dir, k, d);
+  if (!e.empty()) {
+    std::snprintf(err, errlen, "%s", e.c_str());
+    return 1;
+  }
+  *nkp = (int)d.size();
+  if (cap >= *nkp) {
+    std::memcpy(kp, k.data(), k.size() * sizeof(double));
+    std::memcpy(dk, d.data(), d.size() * sizeof(double));
+  }
+  return 0;
+}
+
+// get_frequencies at np points: eival (ndyn,np), eivec (ndyn,ndyn,np) complex
+int orc_frequencies_at(void* p, int np, const double* kp, double* eival, double* eivec, int nthreads) {
+  State& S = *(State*)p;
+  frequencies_at(S, np, kp, eival, (cplx*)eivec, nthreads);
+  return 0;
+}
+
+// function_self_w3 (gauss 0) / function_self_w4 (gauss 1) for each of np
+// (point, la, omega) jobs: q (3,np), la (np, 1-based), omega (np), temp in
+// cm^-1; out (4,np) = nself re, im, uself re, im.  Returns the first error.
+int orc_self_w(void* p, int np, const double* q, const int* la, const double* omega, double temp, int gauss,
+               double* out, int nthreads) {
+  State& S = *(State*)p;
+  std::vector<int> errs(np, 0);
+  parfor(0, np - 1, nthreads, [&](int j) {
+    cplx ns, us;
+    errs[j] = function_self_w(S, &q[3 * j], la[j], omega[j], temp, gauss != 0, ns, us);
+    out[4 * j] = ns.real();
+    out[4 * j + 1] = ns.imag();
+    out[4 * j + 2] = us.real();
+    out[4 * j + 3] = us.imag();
+  });
+  for (int e : errs)
+    if (e) return e;
+  return 0;
+}
+
+int orc_check_inside_bz(void* p, const double* q) { return check_inside_bz(*(State*)p, q); }
+
 }  // extern "C"

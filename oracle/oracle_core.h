@@ -110,6 +110,7 @@ struct State {
   std::vector<double> mass0;    // atom0(i)%mass
   // ---- lat_fc.dat (rest.f90:164-289)
   double r1[3], r2[3], r3[3], g1[3], g2[3], g3[3];
+  double g1conv[3], g2conv[3], g3conv[3];  // reciprocal of the conventional cell, with 2 pi
   // make_reciprocal_lattice of g1..g3 (no 2*pi): the dual basis get_k_info
   // projects on (extratools.f90:188-207); set by set_k_dual once g is known
   double gd1[3], gd2[3], gd3[3];
@@ -159,6 +160,11 @@ inline size_t F5(int a, int b, int c, int d, int e, int n1, int n2, int n3, int 
 
 // ----------------------------------------------------------------- routines
 std::string read_inputs(State& S, const std::string& dir);
+// make_reciprocal_lattice (extratools.f90:188-207): no factor of 2 pi
+struct RecipNo2pi {
+  double rr1[3], rr2[3], rr3[3];
+};
+RecipNo2pi make_reciprocal_lattice(const double* g1, const double* g2, const double* g3);
 void make_kp_reg(State& S);
 void get_negatives(State& S);
 void getstar(const State& S, const double kvec[3], int& narms, double kvecstar[][3], int kvecop[]);
@@ -169,6 +175,16 @@ void set_dynamical_matrix(const State& S, const double kpt[3], cplx* dynmat);
 void hermitian_eigen(int n, const cplx* upper, double* eival, cplx* eivec);
 void get_freq(const State& S, const double kp[3], double* eival, cplx* eivec);
 void finitedif_vel(const State& S, const double q0[3], double* vgr, double* evl0, cplx* evc0);
+void fsort(int n, const double* r, int* mcor);
+// three-phonon self-energy along the band path (oracle_self.cpp)
+std::string make_kp_bs(const State& S, const std::string& dir, std::vector<double>& kp_bs,
+                       std::vector<double>& dk_bs);
+int check_inside_bz(const State& S, const double q[3]);
+bool matrix_elt_full(const State& S, const double* q2, const double* q3, double omq, double om2, double om3,
+                     const cplx* evq, const cplx* ev2, const cplx* ev3, cplx& w33);
+int function_self_w(const State& S, const double q[3], int la, double omega, double temp, bool gauss,
+                    cplx& nself, cplx& uself);
+void frequencies_at(const State& S, int np, const double* kp, double* eival, cplx* eivec, int nthreads);
 void get_frequencies(State& S, int nthreads);
 void subst_eivecs(State& S);
 void make_kp_reg_tet(State& S);

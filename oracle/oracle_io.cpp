@@ -512,6 +512,26 @@ std::string read_inputs(State& S, const std::string& dir) {
                                 std::sin(latp[5]);
     conv_to_cart[F2(3, 3, 3)] = std::sqrt(latp[2] * latp[2] - conv_to_cart[F2(1, 3, 3)] * conv_to_cart[F2(1, 3, 3)] -
                                           conv_to_cart[F2(2, 3, 3)] * conv_to_cart[F2(2, 3, 3)]);
+    {  // make_reciprocal_lattice_2pi of the conventional cell (force_constants.f90:100-104)
+      const double* c1 = &conv_to_cart[0];
+      const double* c2 = &conv_to_cart[3];
+      const double* c3 = &conv_to_cart[6];
+      double c23[3], c31[3], c12[3];
+      auto cross = [](const double* a, const double* b, double* c) {
+        c[0] = a[1] * b[2] - a[2] * b[1];
+        c[1] = a[2] * b[0] - a[0] * b[2];
+        c[2] = a[0] * b[1] - a[1] * b[0];
+      };
+      cross(c2, c3, c23);
+      cross(c3, c1, c31);
+      cross(c1, c2, c12);
+      const double om = c1[0] * c23[0] + c1[1] * c23[1] + c1[2] * c23[2];
+      for (int i = 0; i < 3; ++i) {
+        S.g1conv[i] = 2 * S.K.pi * c23[i] / om;
+        S.g2conv[i] = 2 * S.K.pi * c31[i] / om;
+        S.g3conv[i] = 2 * S.K.pi * c12[i] / om;
+      }
+    }
     double prim_to_conv[9], prim_to_cart[9], cart_to_prim[9], conv_to_prim[9];
     std::memcpy(prim_to_conv, S.primitivelattice, sizeof prim_to_conv);
     xmatmlt3(conv_to_cart, prim_to_conv, prim_to_cart);

@@ -26,10 +26,7 @@ namespace {
 inline double dot3(const double* v, const double* w) {  // dotproduct_av (modules.f90:133)
   return v[0] * w[0] + v[1] * w[1] + v[2] * w[2];
 }
-
-struct RecipNo2pi {
-  double rr1[3], rr2[3], rr3[3];
-};
+}  // namespace
 
 RecipNo2pi make_reciprocal_lattice(const double* g1, const double* g2, const double* g3) {
   auto cross = [](const double* a, const double* b, double* c) {
@@ -69,7 +66,6 @@ void fsort(int n, const double* r, int* mcor) {
     for (int j = i + 1; j <= n; ++j)
       if (r[mcor[i - 1] - 1] > r[mcor[j - 1] - 1]) std::swap(mcor[i - 1], mcor[j - 1]);
 }
-}  // namespace
 
 void set_k_dual(State& S) {
   RecipNo2pi r = make_reciprocal_lattice(S.g1, S.g2, S.g3);

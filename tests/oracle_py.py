@@ -39,7 +39,8 @@ def lib():
                      "orc_get_phonons", "orc_set_phonons", "orc_tet", "orc_v3", "orc_fgr", "orc_distribution",
                      "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d", "orc_update_mpi",
                      "orc_iterative", "orc_giso", "orc_p_iso", "orc_collision_iso", "orc_mode_kappa_teff",
-                     "orc_kappa_d_teff"]:
+                     "orc_kappa_d_teff", "orc_make_kp_bs", "orc_frequencies_at", "orc_self_w",
+                     "orc_check_inside_bz"]:
             getattr(L, name).restype = C.c_int
         L.orc_weight_tet_nonperm.restype = C.c_long
         _lib = L
@@ -282,6 +283,44 @@ class Oracle:
         if e:
             raise RuntimeError("nbe error %d" % e)
         return kap, t
+
+    def make_kp_bs(self, d):
+        """make_kp_bs (modules.f90:1507) from d/kpbs.params: kp_bs (3,nkp), dk_bs."""
+        n = C.c_int(0)
+        err = C.create_string_buffer(256)
+        if lib().orc_make_kp_bs(self.h, d.encode(), C.byref(n), None, None, 0, err, 256):
+            raise RuntimeError(err.value.decode())
+        kp = np.zeros((3, n.value), order="F")
+        dk = np.zeros(n.value)
+        lib().orc_make_kp_bs(self.h, d.encode(), C.byref(n), _p(kp), _p(dk), n.value, err, 256)
+        return kp, dk
+
+    def frequencies_at(self, kp):
+        """get_frequencies at the points kp (3,np): eival (ndyn,np), eivec."""
+        kp = np.asfortranarray(kp, dtype=float)
+        np_ = kp.shape[1]
+        ev = np.zeros((self.ndyn, np_), order="F")
+        vec = np.zeros((self.ndyn, self.ndyn, np_), dtype=complex, order="F")
+        lib().orc_frequencies_at(self.h, np_, _p(kp), _p(ev), vec.ctypes.data_as(dp), self.nthreads)
+        return ev, vec
+
+    def self_w(self, q, la, omega, temp, gauss=False):
+        """function_self_w3 (gauss False) / function_self_w4 (True) per job:
+        q (3,n), la (n, 1-based), omega (n) and temp in cm^-1.  Returns
+        nself, uself (n,) complex."""
+        q = np.asfortranarray(q, dtype=float)
+        n = q.shape[1]
+        la = np.ascontiguousarray(la, dtype=np.int32)
+        om = np.ascontiguousarray(omega, dtype=float)
+        out = np.zeros((4, n), order="F")
+        e = lib().orc_self_w(self.h, n, _p(q), _p(la, ip), _p(om), C.c_double(temp), int(gauss), _p(out),
+                             self.nthreads)
+        if e:
+            raise RuntimeError("self-energy error %d" % e)
+        return out[0] + 1j * out[1], out[2] + 1j * out[3]
+
+    def check_inside_bz(self, q):
+        return lib().orc_check_inside_bz(self.h, _p(np.ascontiguousarray(q, dtype=float)))
 
     def kappa_d(self, tempk, x):
         kap = np.zeros((self.ndyn, 3, 3), order="F")
