@@ -473,6 +473,22 @@ std::string build_tables(const System& S, Tables& T) {
   conv_to_cart[cm(1, 2)] = latp[2] * (std::cos(latp[3]) - std::cos(latp[5]) * std::cos(latp[4])) / std::sin(latp[5]);
   conv_to_cart[cm(2, 2)] = std::sqrt(latp[2] * latp[2] - conv_to_cart[cm(0, 2)] * conv_to_cart[cm(0, 2)] -
                                      conv_to_cart[cm(1, 2)] * conv_to_cart[cm(1, 2)]);
+  {  // make_reciprocal_lattice_2pi of the conventional cell (force_constants.f90:100-104)
+    const double* c1 = &conv_to_cart[0];
+    const double* c2 = &conv_to_cart[3];
+    const double* c3 = &conv_to_cart[6];
+    const double* cc[3][2] = {{c2, c3}, {c3, c1}, {c1, c2}};
+    double x[3][3];
+    for (int v = 0; v < 3; ++v) {
+      const double *u = cc[v][0], *w = cc[v][1];
+      x[v][0] = u[1] * w[2] - u[2] * w[1];
+      x[v][1] = u[2] * w[0] - u[0] * w[2];
+      x[v][2] = u[0] * w[1] - u[1] * w[0];
+    }
+    const double om = c1[0] * x[0][0] + c1[1] * x[0][1] + c1[2] * x[0][2];
+    for (int v = 0; v < 3; ++v)
+      for (int i = 0; i < 3; ++i) T.gconv[v][i] = 2 * PhysConst::pi * x[v][i] / om;
+  }
   double prim_to_cart[9], conv_to_prim[9];
   mat3mul(conv_to_cart, S.primlatt, prim_to_cart);
   if (!mat3inv(S.primlatt, conv_to_prim)) return "primitive_lattice is singular";

@@ -80,6 +80,7 @@ struct Tables {
   int nkc = 0, nibz = 0, b = 0, npg = 0;
   bool shifted = false;            // all mesh divisions even: q = (m/N - 1/2) g
   double opk[48][9];               // op_kmatrix, column-major
+  double gconv[3][3];              // reciprocal vectors of the conventional cell, 2 pi included
   std::vector<double> kpc32;       // 3*nkc: mesh of make_kp_reg (FP32 fractions)
   std::vector<int> mapibz;         // nkc, 1-based
   std::vector<int> mapinv;         // nibz, 1-based
@@ -183,7 +184,8 @@ struct PhononArgs {
   int born_flag;
   const double* born;        // epsil(9), charge(9*nat0), masses(nat0), scalars(4): eps_scale, rho2, om0, pad
   double dq;
-  double* w2_all;            // nkc*7*b |lambda| in get_freq order
+  int ndisp = 7;             // matrices per point: 7 (the point and its six +-dq, velocities) or 1
+  double* w2_all;            // nkc*ndisp*b |lambda| in get_freq order
   double* w2;                // nkc*b eigenval after get_frequencies' sort
   double* evec;              // 2*b*b*nkc (complex) for the central point
   int* err;
@@ -195,6 +197,37 @@ cudaError_t launch_subst_eivecs(const Geometry& geo, const int* src, const int* 
                                 cudaStream_t s);
 cudaError_t launch_freq_dist(const Geometry& geo, const double* w2, double cnst, double temp, int classical,
                              double* freq, double* dist, int* err, cudaStream_t s);
+
+// Three-phonon self-energy at arbitrary q (function_self_w3/w4), ald_self.cu
+struct SelfArgs {
+  int b, nkc, nat0, np;      // bands, mesh points, primitive atoms, path points of the chunk
+  const double* qp;          // 3*np path points (Cartesian, 2 pi included)
+  const double* omega;       // np*b target frequencies (cm^-1), [p*b + la]
+  const double* evq;         // complex [p][la][comp] eigenvectors at the path points
+  const double* wq;          // np*b |lambda| at the path points
+  const double* kpc;         // 3*nkc mesh points
+  const double* ev2;         // complex [k][l][comp] mesh eigenvectors
+  const double* w2;          // nkc*b mesh eigenvalues
+  const double* ev3;         // complex [p*nkc + k][l][comp] at k3 = -q - k2
+  const double* w3;          // [(p*nkc + k)*b + l] |lambda| at k3
+  int ntrip, natoms;
+  const int* blk_off;
+  const int* trip_j;
+  const int* trip_k;
+  const double* fc3w;
+  const double* rr;          // 3*natoms: atompos(j) - atompos(j0)
+  double gd[9];              // dual basis of g1..g3 without 2 pi (make_reciprocal_lattice), rows
+  double ghalf[3];           // (g1+g2+g3)/2
+  double temp, eta, etacut, cnst, const33, pi, v3thr;
+  int classical, gauss;      // gauss: function_self_w4, else function_self_w3
+  double* part;              // self_partial_doubles(*this)
+  int* err;
+};
+size_t self_smem_bytes(const SelfArgs& a, int* ppb);
+size_t self_partial_doubles(const SelfArgs& a);
+cudaError_t launch_k3_points(int np, int nkc, const double* qp, const double* kpc, double* k3, cudaStream_t s);
+// out: np*b*4 = nself re, im, uself re, im per (p, la), already /nkc*pi
+cudaError_t launch_self(const SelfArgs& a, double* out, cudaStream_t s);
 
 struct V3Args {
   Geometry geo;

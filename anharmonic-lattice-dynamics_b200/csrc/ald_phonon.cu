@@ -70,7 +70,7 @@ __global__ void __launch_bounds__(kThreads) phonon_kernel(PhononArgs a) {
 
   const int b = a.geo.b;
   const int bb = b * b;
-  const int pt = blockIdx.x / 7, d = blockIdx.x % 7;
+  const int pt = blockIdx.x / a.ndisp, d = blockIdx.x % a.ndisp;
   double2* A = smem;        // row-major b x b
   double2* V = smem + bb;   // eigenvectors (columns), only for d == 0
 
@@ -276,7 +276,7 @@ __global__ void __launch_bounds__(kThreads) phonon_kernel(PhononArgs a) {
         }
   }
   __syncthreads();
-  for (int i = threadIdx.x; i < b; i += blockDim.x) a.w2_all[((size_t)pt * 7 + d) * b + i] = lab[i];
+  for (int i = threadIdx.x; i < b; i += blockDim.x) a.w2_all[((size_t)pt * a.ndisp + d) * b + i] = lab[i];
   if (d == 0) {
     // eigenvector of final band l: column ord[ord2[l]]; pure-imaginary fix
     for (int l = threadIdx.x >> 5; l < b; l += blockDim.x >> 5) {
@@ -339,7 +339,7 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
   const bool valid = m < nmat;  // a slot past the last matrix repeats the last one and writes nothing
   const int mc = valid ? m : nmat - 1;
   const int b = a.geo.b, bb = b * b;
-  const int pt = mc / 7, d = mc % 7;
+  const int pt = mc / a.ndisp, d = mc % a.ndisp;
   double2* A = smem + (size_t)slot * (2 * bb + a.nuniq);
   double2* V = A + bb;
   double2* ph = V + bb;
@@ -555,7 +555,7 @@ __global__ void __launch_bounds__(kPhWarps * 32) phonon_warp_kernel(PhononArgs a
   }
   __syncwarp();
   if (valid)
-    for (int i = sl; i < b; i += LPM) a.w2_all[((size_t)pt * 7 + d) * b + i] = lab[i];
+    for (int i = sl; i < b; i += LPM) a.w2_all[((size_t)pt * a.ndisp + d) * b + i] = lab[i];
   for (int l = 0; l < b; ++l) {  // every lane: the sums below shuffle over the matrix's lanes
     int col = ord[ord2[l]];
     double sre2 = 0;
@@ -634,7 +634,7 @@ cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
   const int G = b <= 4 ? 4 : (b <= 8 ? 2 : 1);  // matrices per warp
   const size_t smw = (size_t)kPhWarps * G * (2 * (size_t)b * b + a.nuniq) * sizeof(double2);
   if (b <= kPhBMax && smw <= 160 * 1024) {
-    const int nmat = a.geo.nkc * 7;
+    const int nmat = a.geo.nkc * a.ndisp;
     const int per_cta = kPhWarps * G;
     cudaError_t e = cudaSuccess;
 #define ALD_PHW(GG)                                                                                            \
@@ -658,7 +658,7 @@ cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
     cudaError_t e = cudaFuncSetAttribute(phonon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
   }
-  phonon_kernel<<<a.geo.nkc * 7, kThreads, sm, s>>>(a);
+  phonon_kernel<<<a.geo.nkc * a.ndisp, kThreads, sm, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -34,6 +34,7 @@
 #include <vector>
 
 #include "ald_ctx.h"
+#include "ald_fortran_io.h"
 
 using namespace ald;
 using namespace ald::capi;
@@ -134,24 +135,6 @@ std::string list_real(double x) {
 
 std::string list_int(long long v) { return pad_left(std::to_string(v), 11); }
 
-// A list-directed record: items separated as write(u,*) separates them.
-class ListRecord {
- public:
-  ListRecord& i(long long v) { return item(list_int(v), false); }
-  ListRecord& r(double v) { return item(list_real(v), false); }
-  ListRecord& c(const char* t) { return item(t, true); }
-  const std::string& str() const { return s_; }
-
- private:
-  ListRecord& item(const std::string& t, bool chr) {
-    if (!(chr && last_chr_) || s_.empty()) s_ += ' ';
-    s_ += t;
-    last_chr_ = chr;
-    return *this;
-  }
-  std::string s_;
-  bool last_chr_ = false;
-};
 
 }  // namespace fio
 }  // namespace ald

@@ -67,7 +67,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_tau_eff", "ald_qandtau",
-           "ald_write_kappa", "ald_write_job1_files", "ald_format_value"]
+           "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
+           "ald_function_self_w", "ald_self_energy_bs"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -354,6 +355,43 @@ class Context:
         _check(lib().ald_write_job1_files(self.h, out_dir.encode(), C.c_double(tempk), f(res["Q"]), f(res["QN"]),
                                           f(res["QU"]), f(res["kappa_rta_modes"]), f(res["kappa_cg_modes"]),
                                           _p(np.ascontiguousarray(res["x"], dtype=float))))
+
+    def make_kp_bs(self, d: str):
+        """make_kp_bs (modules.f90:1507): kp_bs (3, nkp), dk_bs (nkp) of d/kpbs.params."""
+        n = C.c_int(0)
+        _check(lib().ald_make_kp_bs(self.h, d.encode(), C.byref(n), None, None, 0))
+        kp = np.zeros((3, n.value), order="F")
+        dk = np.zeros(n.value)
+        _check(lib().ald_make_kp_bs(self.h, d.encode(), C.byref(n), _p(kp), _p(dk), n.value))
+        return kp, dk
+
+    def function_self_w(self, q, la, omega, temp, gauss=False):
+        """function_self_w3 (gauss False) / function_self_w4 (True) for jobs
+        q (3,n), la (n, 1-based), omega (n) and temp in cm^-1: nself, uself
+        (n,) complex."""
+        q = np.asfortranarray(q, dtype=float)
+        n = q.shape[1]
+        la = np.ascontiguousarray(la, dtype=np.int32)
+        om = np.ascontiguousarray(omega, dtype=float)
+        ns = np.zeros(2 * n)
+        us = np.zeros(2 * n)
+        _check(lib().ald_function_self_w(self.h, n, _p(q), la.ctypes.data_as(C.POINTER(C.c_int)), _p(om),
+                                         C.c_double(temp), int(gauss), _p(ns), _p(us)))
+        return ns[0::2] + 1j * ns[1::2], us[0::2] + 1j * us[1::2]
+
+    def self_energy_bs(self, d: str, tempk, gauss=False, out_dir: Optional[str] = None):
+        """The job=2 block: omega0 (ndyn, nkp), nself, uself (ndyn, nkp) complex
+        along the path of d/kpbs.params; writes the lw-selfenergy files to
+        out_dir when given."""
+        kp, dk = self.make_kp_bs(d)
+        n = kp.shape[1]
+        om = np.zeros((self.ndyn, n), order="F")
+        ns = np.zeros(2 * self.ndyn * n)
+        us = np.zeros(2 * self.ndyn * n)
+        _check(lib().ald_self_energy_bs(self.h, d.encode(), C.c_double(tempk), int(gauss), n, _p(om), _p(ns),
+                                        _p(us), out_dir.encode() if out_dir else None))
+        f = lambda a: (a[0::2] + 1j * a[1::2]).reshape(n, self.ndyn).T
+        return {"kp_bs": kp, "dk_bs": dk, "omega0": om, "nself": f(ns), "uself": f(us)}
 
     def kappa_pipeline(self, tempk: Optional[float] = None, want_modes=True):
         if tempk is None:

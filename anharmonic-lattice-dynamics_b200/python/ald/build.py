@@ -35,6 +35,9 @@ SOURCES = {
     "ald_util.cu": [],
     "ald_cg_static.cu": [],
     "ald_writers.cpp": [],
+    # the self terms follow the reference's operation order: no contraction
+    "ald_self.cu": ["-fmad=false"],
+    "ald_self.cpp": [],
 }
 
 

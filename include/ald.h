@@ -324,6 +324,38 @@ int ald_write_job1_files(ald_ctx* ctx, const char* dir, double tempk, const doub
                          const double* x);
 int ald_format_value(const char* edit, double value, char* out, int cap);
 
+/* Three-phonon self-energy at arbitrary q: THERMACOND's job=2 block
+ * (kappa.f90:874-1040).
+ *
+ * ald_make_kp_bs replaces make_kp_bs (modules.f90:1507-1652): the band path
+ * of dir/kpbs.params (units 0 = conventional reciprocal coordinates, else
+ * primitive; nkdir points per segment; ndir segments), kp_bs(3,nkp_bs)
+ * Cartesian (2 pi included) and dk_bs(nkp_bs).  *nkp_bs = ndir*nkdir is
+ * always set; kp_bs/dk_bs are filled when not NULL (cap >= nkp_bs).
+ *
+ * ald_function_self_w replaces function_self_w3 (gauss = 0; Lorentzian
+ * of width etaz, four terms, real and imaginary parts; rest.f90:4012) and
+ * function_self_w4 (gauss = 1; Gaussian, three terms, imaginary part only;
+ * rest.f90:4126) for n jobs: point q(3,n), mode la(n) (1-based), frequency
+ * omega(n) and temperature temp, both in cm^-1.  nself, uself (2,n) are
+ * the normal and umklapp parts (complex: re, im), already /nkc*pi.  The
+ * sum runs over the mesh q2 and the bands at q2 and q3 = -q - q2, whose
+ * eigenpairs come from the same eigensolver as the mesh's.  Eigenpairs at q
+ * and q3 are taken in |lambda| order (get_frequencies') for both the
+ * eigenvalue and the eigenvector.
+ *
+ * ald_self_energy_bs runs the job=2 block at temperature tempk (K): the path
+ * of dir/kpbs.params, omega0(ndyn,nkp_bs) = sqrt|lambda|*cnst at the path
+ * points, nself/uself (2,ndyn,nkp_bs) of function_self_w3 (gauss = 0) or
+ * function_self_w4 (gauss = 1) at omega = omega0, and, when out_dir is not
+ * NULL, lw-selfenergy.dat and lw-selfenergy2.dat there (kappa.f90:1019-1031:
+ * isempi = 2 Im(nself + uself), tsempi = 1e10/c_light/isempi). */
+int ald_make_kp_bs(ald_ctx* ctx, const char* dir, int* nkp_bs, double* kp_bs, double* dk_bs, int cap);
+int ald_function_self_w(ald_ctx* ctx, int n, const double* q, const int* la, const double* omega, double temp,
+                        int gauss, double* nself, double* uself);
+int ald_self_energy_bs(ald_ctx* ctx, const char* dir, double tempk, int gauss, int nkp_bs, double* omega0,
+                       double* nself, double* uself, const char* out_dir);
+
 #ifdef __cplusplus
 }
 #endif
