@@ -9,7 +9,12 @@ groups of la (|omega_i - omega_j| < 1e-6 max omega): a sum over a degenerate
 subspace does not depend on the basis chosen in it, and the sums over l3
 inside each value are basis-free in the same way.  Acoustic modes at Gamma
 (omega0 < 1e-3 max omega) are left out: there omega -> 0 makes the matrix
-element 0/0 in both codes.
+element 0/0 in both codes.  Values are compared at the path points strictly
+inside the segments: at a segment end (Gamma, X, L, all points of the 4^3
+mesh, or within 3e-9 of one: make_kp_bs divides by nkdir-1+1e-8) there is a
+q2 with q3 = -q - q2 within rounding of Gamma, where om3 and the matrix
+element are rounding noise amplified by 1/om3 and n(om3), in the reference as
+here.  The files are still checked at every point for their layout.
 
 Tolerance: |gpu - ref| <= 1e-8 |ref| + 1e-9 max|ref| over the compared values
 (the orders of the sums differ; the real part of function_self_w3 is a
@@ -29,7 +34,9 @@ import writers as OW  # noqa: E402
 pytestmark = pytest.mark.gpu
 
 CASES = [(1, (4, 4, 4), {}), (0, (4, 4, 4), {})]
-KPBS = "0\n4\n2\nG 0 0 0\nX 0 0 1\nL 0.5 0.5 0.5\n"
+NKDIR = 4
+KPBS = "0\n%d\n2\nG 0 0 0\nX 0 0 1\nL 0.5 0.5 0.5\n" % NKDIR
+INTERIOR = [p for p in range(2 * NKDIR) if 0 < p % NKDIR < NKDIR - 1]
 KB, H, CL = 1.3806504e-23, 6.62606896e-34, 2.99792458e+8
 
 
@@ -102,7 +109,7 @@ def test_function_self_w(case, gauss):
     skip = 1e-3 * om0.max()
     for part_g, part_o in ((ns_g, ns_o), (us_g, us_o)):
         G, R = [], []
-        for p in range(kp.shape[1]):
+        for p in INTERIOR:
             sl = slice(p * n, (p + 1) * n)
             G.append(grouped(part_g[sl], om0[:, p], skip))
             R.append(grouped(part_o[sl], om0[:, p], skip))
@@ -130,8 +137,8 @@ def test_self_energy_bs_files(case, tmp_path):
     ise_o = 2 * np.imag(ns_o + us_o).reshape(npt, n).T
     ise_g = 2 * np.imag(res["nself"] + res["uself"])
     skip = 1e-3 * om0.max()
-    G = np.concatenate([grouped(ise_g[:, p], om0[:, p], skip) for p in range(npt)])
-    R = np.concatenate([grouped(ise_o[:, p], om0[:, p], skip) for p in range(npt)])
+    G = np.concatenate([grouped(ise_g[:, p], om0[:, p], skip) for p in INTERIOR])
+    R = np.concatenate([grouped(ise_o[:, p], om0[:, p], skip) for p in INTERIOR])
     ok, worst = close(G, R)
     assert ok, worst
     # file layout: one lw-selfenergy.dat record per (point, mode), one
