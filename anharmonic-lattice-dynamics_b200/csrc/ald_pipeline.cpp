@@ -100,8 +100,12 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     return fail(ALD_ERR_ARG, "sharded pipeline: bad rank, rank count or exchange function");
   if (sh && it) return fail(ALD_ERR_UNSUPPORTED, "the sharded pipeline runs job=1 only");
   if (it && !c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
+  // job=3 with iso=1 has no defined result to reproduce: kappa_full deallocates
+  // Piso (kappa.f90:1252) before update_iso reads it (sub.f90:2598)
   if (it && c->S.iso == 1)
-    return fail(ALD_ERR_UNSUPPORTED, "the iterative solution with isotope scattering (update_iso) is not built");
+    return fail(ALD_ERR_UNSUPPORTED,
+                "job=3 with iso=1: the reference frees Piso (kappa.f90:1252) before update_iso reads it "
+                "(sub.f90:2598), so there is no defined result to reproduce");
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
   if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 12 bands is not supported by this build");
   ALD_CK(cudaSetDevice(c->device));

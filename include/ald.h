@@ -164,8 +164,10 @@ int ald_collision_matrix_iso(ald_ctx* ctx, const double* P1, const double* P2, c
  * (ALD_ERR_UNSUPPORTED for an element outside the table).  With iso=1 the
  * pipeline adds Piso to Q, Q_N and Q_U (calculate_tauRTA_iso,
  * sub.f90:8311-8549) and builds the collision matrix of
- * ald_collision_matrix_iso; the iterative solution (update_iso) is not
- * built and returns ALD_ERR_UNSUPPORTED. */
+ * ald_collision_matrix_iso.  The iterative solution with isotopes
+ * (update_iso) returns ALD_ERR_UNSUPPORTED: kappa_full frees Piso
+ * (kappa.f90:1252) before update_iso reads it (sub.f90:2598), so the
+ * reference has no defined result there. */
 int ald_p_iso_split(ald_ctx* ctx, const int ksubset[2], double* Piso);
 int ald_set_isotope_g(ald_ctx* ctx, const double* g);
 int ald_get_isotope_g(ald_ctx* ctx, double* g);
