@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <array>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
@@ -42,10 +43,20 @@ namespace {
 class Records {
  public:
   bool load(const std::string& path) {
-    std::ifstream f(path);
+    FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) return false;
-    std::string l;
-    while (std::getline(f, l)) rec_.push_back(l);
+    std::string buf;
+    char chunk[1 << 16];
+    size_t n;
+    while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) buf.append(chunk, n);
+    std::fclose(f);
+    size_t b = 0;
+    while (b < buf.size()) {  // lines as getline gives them
+      size_t e = buf.find('\n', b);
+      if (e == std::string::npos) e = buf.size();
+      rec_.emplace_back(buf, b, e - b);
+      b = e + 1;
+    }
     return true;
   }
   bool next(size_t n, std::vector<std::string>& out) {
@@ -63,31 +74,35 @@ class Records {
   }
   size_t remaining_nonblank() const {
     size_t c = 0;
-    std::vector<std::string> t;
-    for (size_t i = at_; i < rec_.size(); ++i) {
-      t.clear();
-      split(rec_[i], t, 1);
-      if (!t.empty()) ++c;
-    }
+    for (size_t i = at_; i < rec_.size(); ++i)
+      for (char ch : rec_[i]) {
+        if (ch == '/') break;
+        if (!is_sep(ch)) {
+          ++c;
+          break;
+        }
+      }
     return c;
   }
 
  private:
+  static bool is_sep(char c) { return c == ' ' || c == '\t' || c == ',' || c == '\r'; }
   static void split(const std::string& l, std::vector<std::string>& out, size_t cap) {
-    std::string tok;
-    auto flush = [&]() {
-      if (!tok.empty() && out.size() < cap) out.push_back(tok);
-      tok.clear();
-    };
-    for (char c : l) {
-      if (c == '/') break;
-      if (c == ' ' || c == '\t' || c == ',' || c == '\r') {
-        flush();
-      } else {
-        tok += c;
+    const char* p = l.data();
+    const size_t n = l.size();
+    size_t i = 0;
+    while (i < n && out.size() < cap) {
+      if (p[i] == '/') return;
+      if (is_sep(p[i])) {
+        ++i;
+        continue;
       }
+      size_t j = i;
+      while (j < n && p[j] != '/' && !is_sep(p[j])) ++j;
+      out.emplace_back(p + i, j - i);
+      if (j < n && p[j] == '/') return;
+      i = j;
     }
-    flush();
   }
   std::vector<std::string> rec_;
   size_t at_ = 0;
@@ -565,6 +580,13 @@ std::string build_tables(const System& S, Tables& T) {
     armop.clear();
     std::array<double, 3> key[48];  // at most 48 point operations
     int nkey = 0;
+    // keys hashed by the bucket of their first fractional part (width 2^-16 >
+    // 2e-6): a key within 1e-6 of fr[0] (mod 1) sits in the same or a
+    // neighbouring bucket, so only the keys of those three buckets are compared
+    constexpr int kBuckets = 1 << 16, kSlots = 128;
+    int head[kSlots], nxt[48], kb[48];
+    std::fill(head, head + kSlots, -1);
+    auto bucket = [&](double f) { return std::min(kBuckets - 1, (int)(f * kBuckets)); };
     for (int o = 0; o < T.npg; ++o) {
       double v[3], v2[3];
       for (int a = 0; a < 3; ++a) {
@@ -577,21 +599,30 @@ std::string build_tables(const System& S, Tables& T) {
         for (int k = 0; k < 3; ++k) s = s + v[k] * S.primlatt[cm(k, a)];
         v2[a] = s;
       }
+      // v2 - key within 1e-6 of integers in every component: compared on the
+      // fractional parts, |fa - fb| <= 1e-6 or >= 1 - 1e-6
+      double fr[3];
+      for (int c = 0; c < 3; ++c) fr[c] = v2[c] - std::floor(v2[c]);
+      const int bk = bucket(fr[0]);
       bool dup = false;
-      for (int q = 0; q < nkey && !dup; ++q) {
-        const auto& kk = key[q];
-        int c;
-        for (c = 0; c < 3; ++c) {
-          double d = v2[c] - kk[c];
-          if (std::fabs(d - round_near(d)) > 1e-6) break;
-        }
-        if (c == 3) {
-          dup = true;
-          break;
+      for (int db = -1; db <= 1 && !dup; ++db) {
+        const int bb = (bk + db + kBuckets) % kBuckets;  // the mod-1 wrap
+        for (int q = head[bb % kSlots]; q >= 0 && !dup; q = nxt[q]) {
+          if (kb[q] != bb) continue;
+          const auto& kk = key[q];
+          int c;
+          for (c = 0; c < 3; ++c) {
+            const double d = std::fabs(fr[c] - kk[c]);
+            if (d > 1e-6 && d < 1 - 1e-6) break;
+          }
+          if (c == 3) dup = true;
         }
       }
       if (dup) continue;
-      key[nkey++] = {v2[0], v2[1], v2[2]};
+      kb[nkey] = bk;
+      nxt[nkey] = head[bk % kSlots];
+      head[bk % kSlots] = nkey;
+      key[nkey++] = {fr[0], fr[1], fr[2]};
       arms.push_back({v[0], v[1], v[2]});
       armop.push_back(o);
     }
