@@ -258,7 +258,10 @@ __global__ void self_final_kernel(int np, int b, int nblk, int nkc, double pi, c
 
 size_t self_smem_bytes(const SelfArgs& a, int* ppb_out) {
   const int b = a.b, b2 = b * b, b3 = b2 * b;
-  int nt = std::min(kSelfBlock, ((b3 + 31) / 32) * 32);
+  // 3 bands: a warp per pair (8 pairs per CTA); 4 to 6 bands: 64 threads per
+  // pair, 4 pairs per CTA (the stages between barriers are short; one pair per
+  // CTA left the CTA waiting at them)
+  int nt = b3 <= 32 ? 32 : b <= 6 ? 64 : std::min(kSelfBlock, ((b3 + 31) / 32) * 32);
   int ppb = std::max(1, kSelfBlock / nt);
   while (kSelfBlock % ppb) --ppb;
   const size_t per_pair = 2 * (size_t)b2 + 4 * (size_t)b3 + a.ntrip + a.natoms;
