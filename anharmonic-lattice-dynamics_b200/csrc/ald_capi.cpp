@@ -9,7 +9,9 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
 #include <memory>
+#include <mutex>
 #include <string>
 
 #include "ald_internal.h"
@@ -20,6 +22,96 @@ using namespace ald;
 
 
 namespace ald {
+
+namespace {
+constexpr size_t kCacheMin = (size_t)1 << 20, kCacheMax = (size_t)32 << 30;
+struct DevCache {
+  std::mutex m;
+  std::map<std::pair<int, size_t>, std::vector<void*>> blocks;  // (device, bytes) -> free blocks
+  std::map<int, size_t> held;                                   // bytes held per device
+};
+DevCache& dev_cache() {
+  static DevCache* c = new DevCache;  // never destroyed: no CUDA calls in static destructors
+  return *c;
+}
+void release_device(DevCache& c, int dev) {  // caller holds c.m
+  for (auto it = c.blocks.begin(); it != c.blocks.end();) {
+    if (it->first.first == dev) {
+      for (void* p : it->second) cudaFree(p);
+      it = c.blocks.erase(it);
+    } else {
+      ++it;
+    }
+  }
+  c.held[dev] = 0;
+}
+}  // namespace
+
+cudaError_t dev_alloc(void** p, size_t bytes) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  DevCache& c = dev_cache();
+  if (bytes >= kCacheMin) {
+    std::lock_guard<std::mutex> g(c.m);
+    auto it = c.blocks.find({dev, bytes});
+    if (it != c.blocks.end() && !it->second.empty()) {
+      *p = it->second.back();
+      it->second.pop_back();
+      c.held[dev] -= bytes;
+      return cudaSuccess;
+    }
+  }
+  e = cudaMalloc(p, bytes);
+  if (e == cudaErrorMemoryAllocation) {
+    (void)cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> g(c.m);
+      release_device(c, dev);
+    }
+    e = cudaMalloc(p, bytes);
+  }
+  return e;
+}
+
+void dev_free(void* p, size_t bytes) {
+  if (!p) return;
+  cudaPointerAttributes at;
+  if (bytes >= kCacheMin && cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeDevice) {
+    const int dev = at.device;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    DevCache& c = dev_cache();
+    std::lock_guard<std::mutex> g(c.m);
+    bool keep = c.held[dev] + bytes <= kCacheMax;
+    if (keep) {  // no queued work of this device may still use the block
+      if (dev != cur) cudaSetDevice(dev);
+      keep = cudaDeviceSynchronize() == cudaSuccess;
+      if (dev != cur) cudaSetDevice(cur);
+    }
+    if (keep) {
+      c.blocks[{dev, bytes}].push_back(p);
+      c.held[dev] += bytes;
+      return;
+    }
+  }
+  cudaFree(p);
+}
+
+void dev_trim() {
+  DevCache& c = dev_cache();
+  std::lock_guard<std::mutex> g(c.m);
+  int cur = 0;
+  cudaGetDevice(&cur);
+  std::vector<int> devs;
+  for (auto& kv : c.held) devs.push_back(kv.first);
+  for (int d : devs) {
+    cudaSetDevice(d);
+    release_device(c, d);
+  }
+  cudaSetDevice(cur);
+}
+
 namespace capi {
 
 thread_local std::string g_err;
@@ -457,6 +549,8 @@ int ald_set_stream(ald_ctx* c, void* stream) {
 }
 
 double ald_h2d_bytes(ald_ctx* c) { return c ? c->h2d_bytes : 0.0; }
+
+void ald_release_cached_memory(void) { ald::dev_trim(); }
 
 int ald_get_info(ald_ctx* c, ald_info* info) {
   if (!c || !info) return fail(ALD_ERR_ARG, "null argument");

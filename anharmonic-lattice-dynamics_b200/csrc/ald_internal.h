@@ -139,6 +139,17 @@ struct Fc2Csr {
 std::string build_fc2(const System& S, Fc2Csr& F);
 
 // ------------------------------------------------------------ device side
+// Device memory of the library.  Blocks of 1 MiB or more that are freed are
+// kept per device (after a device synchronisation, so no queued work still
+// uses them) and handed out again to an allocation of the same byte size:
+// contexts created one after another reuse their workspaces without
+// cudaMalloc/cudaFree.  The cache holds at most 32 GiB per device; when
+// cudaMalloc runs out of memory the device's cached blocks are released and
+// the allocation retried.  dev_trim releases every cached block.
+cudaError_t dev_alloc(void** p, size_t bytes);
+void dev_free(void* p, size_t bytes);
+void dev_trim();
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;
@@ -148,10 +159,10 @@ struct DevBuf {
     free();
     n = count;
     if (count == 0) return cudaSuccess;
-    return cudaMalloc((void**)&p, count * sizeof(T));
+    return dev_alloc((void**)&p, count * sizeof(T));
   }
   void free() {
-    if (p) cudaFree(p);
+    if (p) dev_free(p, n * sizeof(T));
     p = nullptr;
     n = 0;
   }

@@ -68,7 +68,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
-           "ald_function_self_w", "ald_self_energy_bs"]
+           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -90,11 +90,17 @@ def lib():
         L.ald_cg_quadratic_static.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.POINTER(C.c_double),
                                               C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p]
         L.ald_format_value.argtypes = [C.c_char_p, C.c_double, C.c_char_p, C.c_int]
+        L.ald_release_cached_memory.restype = None
         for n in EXPORTS[2:]:
-            if n not in ("ald_destroy", "ald_h2d_bytes"):
+            if n not in ("ald_destroy", "ald_h2d_bytes", "ald_release_cached_memory"):
                 getattr(L, n).restype = C.c_int
         _lib = L
     return _lib
+
+
+def release_cached_memory() -> None:
+    """Return the device blocks the library keeps for reuse to the driver."""
+    lib().ald_release_cached_memory()
 
 
 def format_value(edit: str, value) -> str:
