@@ -705,6 +705,7 @@ static cudaError_t capture_cg(int iters, int n, size_t ld, int vec, int nblk, co
                               int mode, double tol, cudaStream_t s, cudaGraphExec_t* out) {
   cudaGraph_t graph = nullptr;
   const int nb = std::min(kCgBlocksMax, (n + kCgThreads - 1) / kCgThreads);
+  std::lock_guard<std::mutex> cap(capture_mutex());
   cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
   if (e != cudaSuccess) return e;
   for (int it = 0; it < iters; ++it) {

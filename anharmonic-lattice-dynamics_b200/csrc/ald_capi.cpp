@@ -47,6 +47,11 @@ void release_device(DevCache& c, int dev) {  // caller holds c.m
 }
 }  // namespace
 
+std::mutex& capture_mutex() {
+  static std::mutex* m = new std::mutex;
+  return *m;
+}
+
 cudaError_t dev_alloc(void** p, size_t bytes) {
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
@@ -76,6 +81,7 @@ cudaError_t dev_alloc(void** p, size_t bytes) {
 
 void dev_free(void* p, size_t bytes) {
   if (!p) return;
+  std::lock_guard<std::mutex> cap(capture_mutex());
   cudaPointerAttributes at;
   if (bytes >= kCacheMin && cudaPointerGetAttributes(&at, p) == cudaSuccess && at.type == cudaMemoryTypeDevice) {
     const int dev = at.device;
@@ -99,6 +105,7 @@ void dev_free(void* p, size_t bytes) {
 }
 
 void dev_trim() {
+  std::lock_guard<std::mutex> cap(capture_mutex());
   DevCache& c = dev_cache();
   std::lock_guard<std::mutex> g(c.m);
   int cur = 0;

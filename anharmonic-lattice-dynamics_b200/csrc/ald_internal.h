@@ -5,6 +5,7 @@
 
 #include <cstdint>
 #include <functional>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -149,6 +150,10 @@ std::string build_fc2(const System& S, Fc2Csr& F);
 cudaError_t dev_alloc(void** p, size_t bytes);
 void dev_free(void* p, size_t bytes);
 void dev_trim();
+// Held while a stream of the library is being captured into a CUDA graph and
+// while dev_free synchronises the device, so that contexts driven from
+// different host threads never synchronise the device during a capture.
+std::mutex& capture_mutex();
 
 template <class T>
 struct DevBuf {

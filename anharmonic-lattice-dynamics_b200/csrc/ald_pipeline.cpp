@@ -19,6 +19,7 @@
 #include <cmath>
 #include <cstring>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "ald_ctx.h"
@@ -460,6 +461,37 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
 extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double* Qo, double* QNo,
                                   double* QUo, double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
   return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr);
+}
+
+extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res,
+                                 int* status) {
+  if (n <= 0 || !ctx || !tempk || !res) return fail(ALD_ERR_ARG, "bad argument");
+  for (int i = 0; i < n; ++i) {
+    if (!ctx[i]) return fail(ALD_ERR_ARG, "null context");
+    for (int j = 0; j < i; ++j)
+      if (ctx[j] == ctx[i]) return fail(ALD_ERR_ARG, "a context appears twice in the batch");
+  }
+  // one host thread per structure: each context issues its work on its own
+  // stream, so the structures' kernels overlap on the device
+  std::vector<int> st(n, ALD_OK);
+  std::vector<std::string> msg(n);
+  std::vector<std::thread> th;
+  th.reserve(n);
+  for (int i = 0; i < n; ++i)
+    th.emplace_back([&, i] {
+      st[i] = run_pipeline(ctx[i], tempk[i], &res[i], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
+      if (st[i] != ALD_OK) msg[i] = ald_last_error();
+    });
+  for (auto& t : th) t.join();
+  int first = ALD_OK;
+  for (int i = 0; i < n; ++i) {
+    if (status) status[i] = st[i];
+    if (first == ALD_OK && st[i] != ALD_OK) {
+      first = st[i];
+      fail(first, "structure " + std::to_string(i) + ": " + msg[i]);
+    }
+  }
+  return first;
 }
 
 extern "C" int ald_shard_rows(const ald_ctx* c, int rank, int nranks, int ksubset[2]) {

@@ -68,7 +68,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
-           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory"]
+           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -96,6 +96,24 @@ def lib():
                 getattr(L, n).restype = C.c_int
         _lib = L
     return _lib
+
+
+def kappa_batched(contexts, tempk):
+    """ald_kappa_batched: the job=1 pipeline on several contexts at once.
+    Returns one dict per context (kappa_rta, kappa_cg, cg_iters, status_cg,
+    stage_ms, triplet_bands) and the per-context status codes."""
+    n = len(contexts)
+    hs = (C.c_void_p * n)(*[c.h.value for c in contexts])
+    tk = (C.c_double * n)(*([float(tempk)] * n if np.isscalar(tempk) else [float(t) for t in tempk]))
+    res = (KappaResult * n)()
+    st = (C.c_int * n)()
+    r = lib().ald_kappa_batched(n, hs, tk, res, st)
+    _check(r)
+    out = [{"kappa_rta": np.array(x.kappa_rta).reshape(3, 3, order="F"),
+            "kappa_cg": np.array(x.kappa_cg).reshape(3, 3, order="F"), "cg_iters": x.cg_iters,
+            "status_cg": x.status_cg, "stage_ms": dict(zip(STAGES, list(x.stage_ms))),
+            "triplet_bands": x.triplet_bands} for x in res]
+    return out, list(st)
 
 
 def release_cached_memory() -> None:

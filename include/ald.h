@@ -252,6 +252,15 @@ double ald_h2d_bytes(ald_ctx* ctx);
 int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double* Q, double* QN, double* QU,
                        double* kappa_rta_modes, double* kappa_cg_modes, double* x);
 
+/* ald_kappa_batched: ald_kappa_pipeline on n structures at once (the batched
+ * configurations of many small cells), one host thread per context; each
+ * context runs on its own stream, so the structures' kernels overlap on the
+ * device.  tempk[n], res[n]; status[n] (may be NULL) receives each
+ * structure's return code.  Returns ALD_OK, or the first structure's error
+ * (ald_last_error names the structure).  The contexts must be distinct; each
+ * structure's limits are those of ald_kappa_pipeline (at most 12 bands). */
+int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res, int* status);
+
 /* Row-sharded job=1, one call per rank (one process per GPU): the MPI
  * decomposition of kappa_full (kappa.f90:418-428: nibz/nranks IBZ rows per
  * rank, the last rank also takes the remainder; ald_shard_rows returns a

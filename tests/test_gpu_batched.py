@@ -1,0 +1,43 @@
+"""ald_kappa_batched: several structures through the job=1 pipeline at once
+(one host thread and one stream per context) must give what each context gives
+alone, GPU.  The delta kernel accumulates with floating-point atomics, so runs
+differ in the last bits; kappa is compared to 1e-12 relative (plus 1e-14 of
+its largest component) and the CG iteration counts exactly."""
+import numpy as np
+import pytest
+
+from conftest import make_case
+
+pytestmark = pytest.mark.gpu
+
+CASES = [(1, (4, 4, 4), {}), (0, (6, 6, 6), {"delta": "gauss"}), (1, (6, 6, 6), {}),
+         (3, (4, 4, 4), {"delta": "gauss", "width_cm": 5.0, "rc_sigma": 1.2})]
+
+
+def test_batched_equals_single(ald_lib, workdir):
+    dirs = [make_case(workdir, cfg, mesh, **kw) for cfg, mesh, kw in CASES]
+    single = []
+    for d in dirs:
+        ctx = ald_lib.Context(d)
+        single.append(ctx.kappa_pipeline(want_modes=False))
+        ctx.close()
+    ctxs = [ald_lib.Context(d) for d in dirs]
+    tempk = [c.info.tempk for c in ctxs]
+    for rep in range(2):  # the second pass reuses every context's workspaces and graphs
+        out, st = ald_lib.kappa_batched(ctxs, tempk)
+        assert st == [0] * len(dirs)
+        for o, s in zip(out, single):
+            assert o["cg_iters"] == s["cg_iters"]
+            for k in ("kappa_rta", "kappa_cg"):
+                assert np.allclose(o[k], s[k], rtol=1e-12, atol=1e-14 * np.abs(s[k]).max()), k
+            assert o["triplet_bands"] == s["triplet_bands"]
+    for c in ctxs:
+        c.close()
+
+
+def test_batched_rejects_a_repeated_context(ald_lib, workdir):
+    d = make_case(workdir, 1, (4, 4, 4))
+    ctx = ald_lib.Context(d)
+    with pytest.raises(RuntimeError):
+        ald_lib.kappa_batched([ctx, ctx], 300.0)
+    ctx.close()
