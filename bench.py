@@ -186,7 +186,7 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8):
     ach = bytes_ / (ms * 1e-3) / 1e9
     # DRAM bytes (read + write) per launch from one ncu capture of a 72-row chunk of this
     # workload, scaled to the rows of a launch
-    ncu_bytes_72rows = {("delta", 4096, 6): 450.70e6, ("v3", 4096, 6): 475.61e6}
+    ncu_bytes_72rows = {("delta", 4096, 6): 452.72e6, ("v3", 4096, 6): 477.53e6}
     traffic = None
     if (dom, nkc, b) in ncu_bytes_72rows:
         traffic = ncu_bytes_72rows[(dom, nkc, b)] * (nibz / n) / 72
