@@ -41,3 +41,24 @@ def test_batched_rejects_a_repeated_context(ald_lib, workdir):
     with pytest.raises(RuntimeError):
         ald_lib.kappa_batched([ctx, ctx], 300.0)
     ctx.close()
+
+
+def test_device_memory_cache_reuse_and_release(ald_lib, workdir):
+    """Workspaces freed by one context are reused by the next one of the same
+    system; after ald_release_cached_memory a new context still runs, with
+    the same results."""
+    d = make_case(workdir, 1, (6, 6, 6))
+    runs = []
+    for release in (False, False, True):
+        ctx = ald_lib.Context(d)
+        runs.append(ctx.kappa_pipeline(want_modes=False))
+        ctx.close()
+        if release:
+            ald_lib.release_cached_memory()
+    ctx = ald_lib.Context(d)
+    runs.append(ctx.kappa_pipeline(want_modes=False))
+    ctx.close()
+    for r in runs[1:]:
+        assert r["cg_iters"] == runs[0]["cg_iters"]
+        for k in ("kappa_rta", "kappa_cg"):
+            assert np.allclose(r[k], runs[0][k], rtol=1e-12, atol=1e-14 * np.abs(runs[0][k]).max())
