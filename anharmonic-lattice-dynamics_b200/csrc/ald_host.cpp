@@ -630,6 +630,43 @@ std::string build_tables(const System& S, Tables& T) {
   auto reduced = [&](const double* kc, double* f) {
     for (int a = 0; a < 3; ++a) f[a] = Ginv[cm(a, 0)] * kc[0] + Ginv[cm(a, 1)] * kc[1] + Ginv[cm(a, 2)] * kc[2];
   };
+  // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table.  They
+  // depend on the mesh only, so a host thread builds them while the IBZ and
+  // the stars are found.
+  auto build_tet = [&]() -> std::string {
+    static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
+                                        {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
+    static const int off8[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
+                                    {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+    T.tet_corner.assign(24 * (size_t)T.nkc, 0);
+    // incidences (tetrahedron corner (6n+l)*4+k at point p) are generated in
+    // increasing order, so each point's list of 24 comes out sorted
+    T.tet_inc.assign(24 * (size_t)T.nkc, 0);
+    std::vector<int> ninc(T.nkc, 0);
+    for (int n = 0; n < T.nkc; ++n) {
+      int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
+      int pt[8];
+      for (int c = 0; c < 8; ++c)
+        pt[c] = mesh_index(wrap(m[0] + off8[c][0], N0), wrap(m[1] + off8[c][1], N1), wrap(m[2] + off8[c][2], N2));
+      for (int l = 0; l < 6; ++l)
+        for (int k = 0; k < 4; ++k) {
+          int p = pt[corner_of[l][k]];
+          T.tet_corner[4 * (6 * (size_t)n + l) + k] = p;
+          if (ninc[p] >= 24) return std::string("tetrahedron incidence count");
+          T.tet_inc[24 * (size_t)p + ninc[p]++] = (6 * n + l) * 4 + k;
+        }
+    }
+    for (int p = 0; p < T.nkc; ++p)
+      if (ninc[p] != 24) return std::string("tetrahedron incidence count");
+    return std::string();
+  };
+  std::string tet_err;
+  struct Joiner {
+    std::thread t;
+    ~Joiner() {
+      if (t.joinable()) t.join();
+    }
+  } tet_thread{std::thread([&] { tet_err = build_tet(); })};
   // ---- IBZ (get_weights): first mesh point of each exact (unfolded) orbit
   T.mapibz.assign(T.nkc, 0);
   T.mapinv.clear();
@@ -747,31 +784,8 @@ std::string build_tables(const System& S, Tables& T) {
       T.star_off.push_back((int)T.star_q.size());
     }
   }
-  // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table
-  static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
-                                      {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
-  static const int off8[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
-                                  {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-  T.tet_corner.assign(24 * (size_t)T.nkc, 0);
-  // incidences (tetrahedron corner (6n+l)*4+k at point p) are generated in
-  // increasing order, so each point's list of 24 comes out sorted
-  T.tet_inc.assign(24 * (size_t)T.nkc, 0);
-  std::vector<int> ninc(T.nkc, 0);
-  for (int n = 0; n < T.nkc; ++n) {
-    int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
-    int pt[8];
-    for (int c = 0; c < 8; ++c)
-      pt[c] = mesh_index(wrap(m[0] + off8[c][0], N0), wrap(m[1] + off8[c][1], N1), wrap(m[2] + off8[c][2], N2));
-    for (int l = 0; l < 6; ++l)
-      for (int k = 0; k < 4; ++k) {
-        int p = pt[corner_of[l][k]];
-        T.tet_corner[4 * (6 * (size_t)n + l) + k] = p;
-        if (ninc[p] >= 24) return "tetrahedron incidence count";
-        T.tet_inc[24 * (size_t)p + ninc[p]++] = (6 * n + l) * 4 + k;
-      }
-  }
-  for (int p = 0; p < T.nkc; ++p)
-    if (ninc[p] != 24) return "tetrahedron incidence count";
+  tet_thread.t.join();
+  if (!tet_err.empty()) return tet_err;
   // ---- exact phases: q(m).R_j = 2 pi sum_a (m_a/N_a - s/2) n_ja
   long L = 1;
   for (int a = 0; a < 3; ++a) L = std::lcm(L, (long)S.nc[a]);
