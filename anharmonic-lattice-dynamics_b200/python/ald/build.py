@@ -44,22 +44,35 @@ SOURCES = {
 def _compile(src: str, extra) -> str:
     obj = os.path.join(OBJDIR, src + ".o")
     path = os.path.join(CSRC, src)
+    # the compiler writes the object's header dependencies beside it (obj.d)
+    dep = ["-MD", "-MF", obj + ".d"]
     if src.endswith(".cu"):
-        cmd = [NVCC] + ARCH + COMMON + extra + ["-c", path, "-o", obj]
+        cmd = [NVCC] + ARCH + COMMON + extra + dep + ["-c", path, "-o", obj]
     else:
         cmd = [os.environ.get("CXX", "g++"), "-std=c++17", "-O2", "-fPIC", "-Wall", "-I/usr/local/cuda/include",
-               "-c", path, "-o", obj] + extra
+               "-c", path, "-o", obj] + dep + extra
     subprocess.run(cmd, check=True)
     return obj
+
+
+def _deps(obj: str, src: str):
+    """The source and every header the compiler read for obj (from obj.d),
+    system headers included; without a dependency file, every header of the
+    package and include/."""
+    d = obj + ".d"
+    if os.path.exists(d):
+        text = open(d).read().replace("\\\n", " ")
+        files = text.split(":", 1)[1].split() if ":" in text else []
+        return [os.path.join(CSRC, src)] + files
+    hdr = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".h")]
+    return [os.path.join(CSRC, src), os.path.join(os.path.dirname(PKG), "include", "ald.h")] + hdr
 
 
 def _stale(obj: str, src: str) -> bool:
     if not os.path.exists(obj):
         return True
     t = os.path.getmtime(obj)
-    deps = [os.path.join(CSRC, src), os.path.join(CSRC, "ald_internal.h"), os.path.join(CSRC, "ald_ctx.h"),
-            os.path.join(os.path.dirname(PKG), "include", "ald.h")]
-    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+    return any(os.path.getmtime(d) > t for d in _deps(obj, src) if os.path.exists(d))
 
 
 def build(force: bool = False, verbose: bool = False) -> str:

@@ -20,7 +20,7 @@ most 40 per edge and file, and an evenly spaced sample.  The test rebuilds
 each record from its own numbers and must get the same bytes.
 
 Run where the reference is mounted:
-    python tests/golden/make_format_golden.py /root/reference
+    python tests/golden/make_format_golden.py <path of the reference checkout>
 It writes tests/golden/fortran_records.json.
 """
 from __future__ import annotations
@@ -77,4 +77,6 @@ def main(ref: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s <path of the reference checkout>" % sys.argv[0])
+    main(sys.argv[1])

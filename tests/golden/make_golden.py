@@ -19,7 +19,7 @@ FC2 terms) and keeps the reference's outputs that depend only on them:
 No example ships fc3.dat, so nothing here pins V3 or later stages.
 
 Run in a container that has the reference mounted:
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference checkout>
 It writes tests/golden/{ge,gese}_example.npz.
 """
 from __future__ import annotations
@@ -144,4 +144,6 @@ def main(ref_root: str):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: %s <path of the reference checkout>" % sys.argv[0])
+    main(sys.argv[1])
