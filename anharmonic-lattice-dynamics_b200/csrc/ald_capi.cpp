@@ -5,6 +5,8 @@
 // buffers across the boundary.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+
 #include <algorithm>
 #include <chrono>
 #include <cmath>
@@ -162,6 +164,7 @@ int check_err_flags(ald_ctx* c) {
   if (h) {
     CK(cudaMemsetAsync(c->err.p, 0, sizeof(int), c->stream));
     if (h & 16) return fail(ALD_ERR_CUDA, "V3: a tensor-core wait timed out (MMA completion not observed)");
+    if (h & 32) return fail(ALD_ERR_CUDA, "eigensolver: the QL iteration did not converge in 60 sweeps");
     if (h & 2) return fail(ALD_ERR_DEN_ZERO, "MATRIX_ELT: den=0 (an eigenvalue is exactly zero)");
     if (h & 1) return fail(ALD_ERR_NBE, "ERROR in N_BE: w=<0 or t=<0");
   }
@@ -171,7 +174,8 @@ int check_err_flags(ald_ctx* c) {
 int ensure_phonons(ald_ctx* c) {
   if (c->have_phonons) return ALD_OK;
   const int b = c->geo.b, nkc = c->geo.nkc;
-  if (b > 64) return fail(ALD_ERR_UNSUPPORTED, "eigensolver: more than 64 bands is not supported by this build");
+  if (b > kHeevMaxBands)
+    return fail(ALD_ERR_UNSUPPORTED, "eigensolver: more than 256 bands is not supported by this build");
   CKA(c->w2_all.alloc((size_t)nkc * 7 * b));
   CKA(c->w2.alloc((size_t)nkc * b));
   CKA(c->evec.alloc((size_t)nkc * b * b * 2));
@@ -195,7 +199,18 @@ int ensure_phonons(ald_ctx* c) {
   a.w2 = c->w2.p;
   a.evec = c->evec.p;
   a.err = c->err.p;
-  CK(launch_phonons(a, c->stream));
+  // the shared-memory Jacobi up to 64 bands, else Householder + QL on global
+  // workspace; ALD_EIGENSOLVER=householder selects the latter at any size
+  const char* es = getenv("ALD_EIGENSOLVER");
+  if (b > 64 || (es && std::string(es) == "householder")) {
+    a.ndisp = 7;
+    a.he_slots = heev_slots(nkc * a.ndisp);
+    CKA(c->w_heev.alloc(heev_work_doubles(b, a.he_slots)));
+    a.he_work = c->w_heev.p;
+    CK(launch_heev(a, c->stream));
+  } else {
+    CK(launch_phonons(a, c->stream));
+  }
   CK(launch_phonon_post(c->geo, c->w2_all.p, a.dq, PhysConst::cnst(), c->vel.p, c->stream));
   CK(launch_subst_eivecs(c->geo, c->neg_src.p, c->neg_dst.p, (int)c->T.neg_src.size(), c->evec.p, c->stream));
   c->have_phonons = true;
@@ -252,11 +267,23 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
 int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
   int nl = 0;
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
-  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "V3: more than 12 bands is not supported by this build");
+  if (c->geo.b > kHeevMaxBands)
+    return fail(ALD_ERR_UNSUPPORTED, "V3: more than 256 bands is not supported by this build");
   const int prec = c->opt.precision;
   V3Args a = a0;
   cudaError_t e;
-  if (prec == ALD_MIXED && v3_tc_supported(c->geo.b, c->VC.ncls)) {
+  if (v3_dense_supported(c->geo.b)) {
+    // more than 12 bands: batched GEMMs per pair (FP64)
+    const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, ALD_FP64);
+    if (c->w_h.n < need) CKA(c->w_h.alloc(need));
+    a.hbuf = c->w_h.p;
+    const size_t wb = v3_dense_work_bytes(c->geo.b, (long long)a.nrows * c->geo.nkc, (size_t)2 << 30);
+    if (c->w_v3work.n < wb) CKA(c->w_v3work.alloc(wb));
+    e = launch_v3_rows_f64(a, c->stream);
+    if (e == cudaSuccess) e = launch_v3_dense(a, c->w_v3work.p, c->w_v3work.n, c->stream);
+    const long long per = (long long)(c->w_v3work.n / (2 * (size_t)c->geo.b * c->geo.b * c->geo.b * 16));
+    nl += 1 + 3 * (int)(((long long)a.nrows * c->geo.nkc + per - 1) / per);
+  } else if (prec == ALD_MIXED && v3_tc_supported(c->geo.b, c->VC.ncls)) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
@@ -670,7 +697,8 @@ int ald_calculate_w3_ibz_split_sq(ald_ctx* c, const int ksubset[2], double* v33s
 int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, double* P1smpi, double* P2smpi) {
   if (!c || !v33s8 || !P1smpi || !P2smpi) return fail(ALD_ERR_ARG, "null argument");
   if (!ksub_ok(c, ksubset)) return fail(ALD_ERR_ARG, "ksubset out of range");
-  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "delta stage: more than 12 bands is not supported by this build");
+  if (c->geo.b > kHeevMaxBands)
+    return fail(ALD_ERR_UNSUPPORTED, "delta stage: more than 256 bands is not supported by this build");
   CK(cudaSetDevice(c->device));
   int r = ensure_phonons(c);
   if (r) return r;
@@ -686,7 +714,7 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   CKA(p2.alloc(n));
   CKA(R1.alloc((size_t)nr * nkc * b * b));
   CKA(R2.alloc((size_t)nr * nkc * b * b));
-  CKA(scratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, nr, 0))));
+  if (b <= kDeltaSmallBands) CKA(scratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, nr, 0))));
   CK(cudaMemcpyAsync(vf.p, v33s8, n * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(launch_from_fortran5(vf.p, v.p, nr, nkc, b, c->stream));
   CombineArgs a;
@@ -711,7 +739,14 @@ int ald_calculate_fgr(ald_ctx* c, const int ksubset[2], const double* v33s8, dou
   a.P2 = nullptr;
   a.R1p = a.R2p = nullptr;
   a.v3_layout = 0;
-  CK(launch_combine(a, scratch.p, c->stream));
+  if (b > kDeltaSmallBands) {  // band-generic kernels: P1smpi/P2smpi only
+    CK(cudaMemsetAsync(p1.p, 0, n * sizeof(double), c->stream));
+    CK(cudaMemsetAsync(p2.p, 0, n * sizeof(double), c->stream));
+    a.R1 = a.R2 = nullptr;
+    CK(launch_delta_any(a, c->stream));
+  } else {
+    CK(launch_combine(a, scratch.p, c->stream));
+  }
   CK(launch_to_fortran5(p1.p, vf.p, nr, nkc, b, c->stream));
   CK(cudaMemcpyAsync(P1smpi, vf.p, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));

@@ -32,6 +32,7 @@ struct ald_ctx {
   DevBuf<char> w_h;                   // per-row phase-class sums of the pair kernel
   DevBuf<char> w_ptiles;              // phase tiles of the tensor-core V3 (mesh-only, built once)
   DevBuf<char> w_btiles;              // per-row B operands of the tensor-core V3
+  DevBuf<char> w_v3work;              // T1/T2 of the large-cell V3 GEMMs
   bool ptiles_ok = false;
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;
@@ -45,6 +46,7 @@ struct ald_ctx {
   DevBuf<double> w_kpart;   // per-CTA partial sums of kappa
   DevBuf<double> w_brange;  // omega range of every band over the mesh
   DevBuf<char> w_scratch;
+  DevBuf<double> w_heev;    // Householder eigensolver workspace (large cells)
   CgWork cg;
   bool have_phonons = false;
   double dist_tempk = -1;

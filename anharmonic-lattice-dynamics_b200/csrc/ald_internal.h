@@ -205,8 +205,16 @@ struct PhononArgs {
   double* w2;                // nkc*b eigenval after get_frequencies' sort
   double* evec;              // 2*b*b*nkc (complex) for the central point
   int* err;
+  double* he_work = nullptr; // Householder solver: heev_work_doubles(b, he_slots) doubles
+  int he_slots = 0;
 };
 cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s);
+// Householder + implicit QL eigensolver (ald_heev.cu), for cells whose
+// matrices do not fit the shared-memory Jacobi (more than 64 bands, up to 256)
+constexpr int kHeevMaxBands = 256;
+int heev_slots(int nmat);
+size_t heev_work_doubles(int b, int slots);
+cudaError_t launch_heev(const PhononArgs& a, cudaStream_t s);
 cudaError_t launch_phonon_post(const Geometry& geo, const double* w2_all, double dq, double cnst, double* vel,
                                cudaStream_t s);
 cudaError_t launch_subst_eivecs(const Geometry& geo, const int* src, const int* dst, int n, double* evec,
@@ -279,8 +287,15 @@ cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s);
 bool v3_pair_supported(int b, int precision);
 size_t v3_hbuf_bytes(int b, int ncls, int nrows, int precision);
 cudaError_t launch_v3_pair(const V3Args& a, int precision, cudaStream_t s);
-// row stage alone, H in FP32 (for the tensor-core class sums)
+// row stage alone, H in FP32 (for the tensor-core class sums) or FP64
 cudaError_t launch_v3_rows_f32(const V3Args& a, cudaStream_t s);
+cudaError_t launch_v3_rows_f64(const V3Args& a, cudaStream_t s);
+// more than 12 bands (ald_v3_dense.cu): the class sums and both mode products
+// as batched complex GEMMs per (q1, q2) pair; hbuf from launch_v3_rows_f64;
+// work: v3_dense_work_bytes(b, pairs of the chunk, budget) bytes
+bool v3_dense_supported(int b);
+size_t v3_dense_work_bytes(int b, long long npairs, size_t budget);
+cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s);
 // 3 bands, ALD_MIXED: class sums on tcgen05 (ald_v3_tc.cu); hbuf from launch_v3_rows_f32
 bool v3_tc_supported(int b, int ncls);
 // the row-independent phase tiles (split FP16, canonical layout), built once per context
@@ -321,6 +336,11 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s);
 // R1/R2 of the chunk must be zero on entry
 bool delta_fused_supported(const Geometry& g);
 cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s);
+// any number of bands (large cells): the tetrahedron or Gaussian delta into
+// R1/R2 and/or P1s/P2s straight from |V3|^2 of the chunk; for the tetrahedron
+// R1/R2/P1s/P2s (and R1p/R2p) must be zero on entry; P1/P2 are not produced
+constexpr int kDeltaSmallBands = 16;  // up to here the band-templated kernels
+cudaError_t launch_delta_any(const CombineArgs& a, cudaStream_t s);
 // Q/QN/QU[(n1_first+row)*b + l1] from R1/R2 of rows [0, nrows)
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s);

@@ -108,7 +108,10 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
                 "job=3 with iso=1: the reference frees Piso (kappa.f90:1252) before update_iso reads it "
                 "(sub.f90:2598), so there is no defined result to reproduce");
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
-  if (c->geo.b > 12) return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 12 bands is not supported by this build");
+  if (c->geo.b > kHeevMaxBands)
+    return fail(ALD_ERR_UNSUPPORTED, "pipeline: more than 256 bands is not supported by this build");
+  if (it && c->geo.b > kDeltaSmallBands)
+    return fail(ALD_ERR_UNSUPPORTED, "job=3: more than 16 bands is not supported by this build");
   ALD_CK(cudaSetDevice(c->device));
   std::memset(res, 0, sizeof *res);
   cudaStream_t s = c->stream;
@@ -178,10 +181,12 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
   const bool fused = !gauss && delta_fused_supported(c->geo);
-  if (!fused) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
+  // more than 16 bands: the band-generic delta kernels, straight into R1/R2
+  const bool any = !fused && b > kDeltaSmallBands;
+  if (!fused && !any) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
   // class-form V3 kernels write that layout
-  const int v3_layout = v3_pair_supported(b, c->opt.precision) ? 1 : 0;
+  const int v3_layout = v3_pair_supported(b, c->opt.precision) || v3_dense_supported(b) ? 1 : 0;
   ALD_CKA(c->w_brange.alloc((size_t)2 * b));
   ALD_CK(launch_band_range(c->geo, c->freq.p, c->w_brange.p, s));
   res->launches[2] += 1;
@@ -224,6 +229,13 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
       ALD_CK(cudaMemsetAsync(a.R1, 0, n, s));
       ALD_CK(cudaMemsetAsync(a.R2, 0, n, s));
       ALD_CK(launch_delta_fused(a, s));
+      res->launches[2] += 1;
+    } else if (any) {
+      if (!gauss) {  // the tetrahedron kernel adds into R1/R2
+        ALD_CK(cudaMemsetAsync(a.R1, 0, rbytes, s));
+        ALD_CK(cudaMemsetAsync(a.R2, 0, rbytes, s));
+      }
+      ALD_CK(launch_delta_any(a, s));
       res->launches[2] += 1;
     } else {
       ALD_CK(launch_combine(a, escratch.p, s));

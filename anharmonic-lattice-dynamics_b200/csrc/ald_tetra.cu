@@ -712,6 +712,218 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
   }
 }
 
+// ---------------------------------------------------------------------------
+// Any number of bands (the large cells): the delta straight from the slice
+// energies, no per-band register arrays.
+//
+// Tetrahedron: a thread per (slice, tetrahedron); its four corner energies
+// E = -+omega(w,l2) + omega(q1+-w,l3) as default REAL, one sort, the bands
+// l1 whose omega1 lies in [E_min, E_max] by binary search (omega1 ascending),
+// and for each one weight_tet's corner weights c (bitwise, ald_tet.h) added
+// at the four corners w:
+//   P1s/P2s(row, w, l1, l2, l3) += c/6 |V3|^2(src(w)) (2pi)^2/nkc        (if given)
+//   R(row, w, l1, l2)           += that * n1 G(w)                       (if given)
+// with G and the Gamma-acoustic zeros of the fused kernel.  FP64 atomics:
+// the sums agree with the reference to FP64 rounding, not bitwise.
+template <bool F32W>
+__global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
+  extern __shared__ double s_any[];  // omega1[b], n1[b]
+  const Geometry& g = a.geo;
+  const int b = g.b, nkc = g.nkc, b2 = b * b;
+  const int slice = blockIdx.x;  // x: up to 2^31 - 1 slices; y: blocks of tetrahedra
+  const int proc = slice & 1, l3 = (slice >> 1) % b, l2 = (slice / (2 * b)) % b, row = slice / (2 * b2);
+  const int q1 = a.mapinv[a.n1_first + row];
+  double* s_om = s_any;
+  double* s_nb = s_any + b;
+  for (int l = threadIdx.x; l < b; l += blockDim.x) {
+    s_om[l] = a.freq[(size_t)q1 * b + l];
+    s_nb[l] = a.dist[(size_t)q1 * b + l];
+  }
+  __syncthreads();
+  const int t = blockIdx.y * blockDim.x + threadIdx.x;
+  if (t >= 6 * nkc) return;
+  int m1[3];
+  decompose(g, q1, m1);
+  int c[4], src[4];
+  float en[4];
+  double G[4];
+  tet_corners(g, t, c);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    int mw[3], m3[3], ins;
+    decompose(g, c[k], mw);
+    const int q3 = pm_index_m(g, m1, mw, proc == 0 ? 1 : -1, ins, m3);
+    const double fw = a.freq[(size_t)c[k] * b + l2], f3 = a.freq[(size_t)q3 * b + l3];
+    en[k] = (float)(proc == 0 ? -fw + f3 : fw + f3);
+    const bool zero = (l2 < 3 && at_gamma_index(g, mw)) || (l3 < 3 && at_gamma_index(g, m3));
+    const double n2 = a.dist[(size_t)c[k] * b + l2], n3 = a.dist[(size_t)q3 * b + l3];
+    G[k] = zero ? -1.0 : (proc == 0 ? n2 * (n3 + 1) : (n2 + 1) * (n3 + 1));
+    src[k] = proc == 0 ? c[k] : neg_index(g, mw);
+  }
+  const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+  const double E1 = ts.e1, E4 = ts.e4;
+  // first band with omega1 >= E1, first band with omega1 > E4
+  int lo = 0, hi = b;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (s_om[mid] < E1) lo = mid + 1;
+    else hi = mid;
+  }
+  int lo2 = lo, hi2 = b;
+  while (lo2 < hi2) {
+    const int mid = (lo2 + hi2) >> 1;
+    if (s_om[mid] > E4) hi2 = mid;
+    else lo2 = mid + 1;
+  }
+  const int lend = lo2;
+  const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
+  size_t sq, s1, s2, s3;
+  if (a.v3_layout == 1) {
+    sq = 1;
+    s1 = nkc;
+    s3 = (size_t)b * nkc;
+    s2 = (size_t)b2 * nkc;
+  } else {
+    s3 = 1;
+    s2 = b;
+    s1 = (size_t)b2;
+    sq = (size_t)b2 * b;
+  }
+  const double* v3 = a.v3sq + (size_t)row * nkc * b2 * b + l2 * s2 + l3 * s3;
+  double* Ps = proc == 0 ? a.P1s : a.P2s;
+  double* Rp = proc == 0 ? a.R1 : a.R2;
+  double* Rpp = proc == 0 ? a.R1p : a.R2p;
+  int pos[4];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) pos[k] = tet_pos(en, k);
+  for (int l1 = lo; l1 < lend; ++l1) {
+    double cp[4];
+    if constexpr (F32W) {
+      float cf[4];
+      if (!tet_weights4_f32(ts, s_om[l1], cf)) continue;
+#pragma unroll
+      for (int k = 0; k < 4; ++k) cp[k] = cf[k];
+    } else {
+      if (!tet_weights4(ts, s_om[l1], cp)) continue;
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const double cw = cp[pos[k]];
+      if (cw == 0.0 || G[k] < 0.0) continue;
+      const double ps = (cw / 6.0) * (__ldg(v3 + (size_t)src[k] * sq + l1 * s1) * fnorm);
+      const size_t w = (size_t)row * nkc + c[k];
+      if (Ps) atomicAdd(Ps + (w * b + l1) * b2 + l2 * b + l3, ps);
+      if (Rp) {
+        const double p = ps * (s_nb[l1] * G[k]);
+        atomicAdd(Rp + (w * b + l1) * b + l2, p);
+        if (Rpp) atomicAdd(Rpp + (w * b + l1) * b + l3, p);
+      }
+    }
+  }
+}
+
+// Gaussian: a thread per (row, w, l1, l2), w fastest; the sums over l3 of
+// both processes (R1, R2 at w) in registers, P1s/P2s written when given.
+// The Gaussian is delta_g of extratools.f90:239 as in delta_point_kernel.
+template <bool F32W>
+__global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
+  const Geometry& g = a.geo;
+  const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
+  // x: (l1, l2, block of w) with w blocks fastest; y: row
+  const int nwb = (nkc + blockDim.x - 1) / blockDim.x;
+  const int l12 = (int)(blockIdx.x / nwb), w = (int)(blockIdx.x % nwb) * blockDim.x + threadIdx.x, row = blockIdx.y;
+  const int l1 = l12 / b, l2 = l12 % b;
+  if (w >= nkc) return;
+  const int q1 = a.mapinv[a.n1_first + row];
+  int m1[3], mw[3], m3p[3], m3m[3], ins1, ins2;
+  decompose(g, q1, m1);
+  decompose(g, w, mw);
+  const int q3p = pm_index_m(g, m1, mw, 1, ins1, m3p);
+  const int q3m = pm_index_m(g, m1, mw, -1, ins2, m3m);
+  const int wneg = neg_index(g, mw);
+  const bool w_gamma = at_gamma_index(g, mw), p_gamma = at_gamma_index(g, m3p), m_gamma = at_gamma_index(g, m3m);
+  const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
+  const double om1 = a.freq[(size_t)q1 * b + l1], nb1 = a.dist[(size_t)q1 * b + l1];
+  const double n2 = a.dist[(size_t)w * b + l2], w2 = a.freq[(size_t)w * b + l2];
+  const double* v3 = a.v3sq + (size_t)row * nkc * b3;
+  const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
+  const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
+  const double gc1 = 0.5 / (a.sigma * a.sigma), gc2 = 1.0 / (sqrt(2 * PhysConst::pi) * a.sigma);
+  const float fc1 = (float)gc1, fc2 = (float)gc2;
+  double R[2] = {0.0, 0.0};
+  for (int l3 = 0; l3 < b; ++l3) {
+#pragma unroll
+    for (int proc = 0; proc < 2; ++proc) {
+      const int q3 = proc == 0 ? q3p : q3m;
+      const bool zero = (l2 < 3 && w_gamma) || (l3 < 3 && (proc == 0 ? p_gamma : m_gamma));
+      const int src = proc == 0 ? w : wneg;
+      const double n3 = a.dist[(size_t)q3 * b + l3], w3 = a.freq[(size_t)q3 * b + l3];
+      const double x = proc == 0 ? om1 + w2 - w3 : om1 - w2 - w3;
+      double wl = 0.0;
+      if constexpr (F32W) {
+        const float xf = (float)x, arg = xf * xf * fc1;
+        if (arg < 104.0f) wl = (double)(expf(-arg) * fc2);
+      } else {
+        const double arg = x * x * gc1;
+        if (arg < 746.0) wl = exp(-arg) * gc2;
+      }
+      double ps = 0.0;
+      if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * sq + l1 * s1 + l2 * s2 + l3 * s3] * fnorm);
+      const double p = ps * (proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1));
+      R[proc] += p;
+      double* Rpm = proc == 0 ? a.R1p : a.R2p;
+      if (Rpm && p != 0.0) atomicAdd(Rpm + (((size_t)row * nkc + w) * b + l1) * b + l3, p);
+      double* Ps = proc == 0 ? a.P1s : a.P2s;
+      if (Ps) Ps[(((size_t)row * nkc + w) * b + l1) * b2 + l2 * b + l3] = ps;
+    }
+  }
+  const size_t ri = (((size_t)row * nkc + w) * b + l1) * b + l2;
+  if (a.R1) a.R1[ri] = R[0];
+  if (a.R2) a.R2[ri] = R[1];
+}
+
+// Q, Q_N, Q_U of any number of bands: a CTA per (row, l1), threads over w
+__global__ void __launch_bounds__(256) q_from_r_any_kernel(Geometry g, int n1_first, const int* mapinv,
+                                                           const double* R1, const double* R2, double* Q,
+                                                           double* QN, double* QU) {
+  __shared__ double red[3][256];
+  const int b = g.b, nkc = g.nkc, row = blockIdx.x, l1 = blockIdx.y, tid = threadIdx.x;
+  const int q1 = mapinv[n1_first + row];
+  int m1[3];
+  decompose(g, q1, m1);
+  double s = 0, sn = 0, su = 0;
+  for (int w = tid; w < nkc; w += blockDim.x) {
+    int mw[3], i1, i2;
+    decompose(g, w, mw);
+    pm_index(g, m1, mw, 1, i1);
+    pm_index(g, m1, mw, -1, i2);
+    double r1 = 0, r2 = 0;
+    const size_t base = (((size_t)row * nkc + w) * b + l1) * b;
+    for (int l2 = 0; l2 < b; ++l2) {
+      r1 += R1[base + l2];
+      r2 += R2[base + l2];
+    }
+    s += r1 + 0.5 * r2;
+    sn += (i1 ? r1 : 0.0) + (i2 ? 0.5 * r2 : 0.0);
+    su += (i1 ? 0.0 : r1) + (i2 ? 0.0 : 0.5 * r2);
+  }
+  red[0][tid] = s;
+  red[1][tid] = sn;
+  red[2][tid] = su;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {  // fixed tree: deterministic
+    if (tid < o)
+      for (int k = 0; k < 3; ++k) red[k][tid] += red[k][tid + o];
+    __syncthreads();
+  }
+  if (tid == 0) {
+    const size_t o = (size_t)(n1_first + row) * b + l1;
+    Q[o] = red[0][0];
+    QN[o] = red[1][0];
+    QU[o] = red[2][0];
+  }
+}
+
 }  // namespace
 
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss) {
@@ -800,10 +1012,34 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_delta_any(const CombineArgs& a, cudaStream_t s) {
+  const Geometry& g = a.geo;
+  if (g.b > 256) return cudaErrorInvalidValue;
+  if (a.gauss) {
+    const long long nx = (long long)((g.nkc + 127) / 128) * g.b * g.b;
+    if (nx > 2147483647LL || a.nrows > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)nx, a.nrows);
+    if (a.f32w) delta_gauss_any_kernel<true><<<grid, 128, 0, s>>>(a);
+    else delta_gauss_any_kernel<false><<<grid, 128, 0, s>>>(a);
+  } else {
+    const long long nslice = (long long)a.nrows * g.b * g.b * 2;
+    if (nslice > 2147483647LL) return cudaErrorInvalidValue;
+    if ((6LL * g.nkc + 255) / 256 > 65535) return cudaErrorInvalidValue;
+    const dim3 grid((unsigned)nslice, (6 * g.nkc + 255) / 256);
+    const size_t smem = 2 * (size_t)g.b * sizeof(double);
+    if (a.f32w) delta_tet_any_kernel<true><<<grid, 256, smem, s>>>(a);
+    else delta_tet_any_kernel<false><<<grid, 256, smem, s>>>(a);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_q_from_r(const Geometry& geo, int n1_first, int nrows, const int* mapinv, const double* R1,
                             const double* R2, double* Q, double* QN, double* QU, int nibz, cudaStream_t s) {
   (void)nibz;
-  if (3 * geo.b > 256) return cudaErrorInvalidValue;
+  if (3 * geo.b > 256) {
+    q_from_r_any_kernel<<<dim3(nrows, geo.b), 256, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU);
+    return cudaGetLastError();
+  }
   q_from_r_kernel<<<nrows, 256 / geo.b * geo.b, 0, s>>>(geo, n1_first, mapinv, R1, R2, Q, QN, QU);
   return cudaGetLastError();
 }

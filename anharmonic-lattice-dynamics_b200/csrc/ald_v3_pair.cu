@@ -313,6 +313,13 @@ cudaError_t launch_v3_rows_f32(const V3Args& a, cudaStream_t s) {
   return cudaGetLastError();
 }
 
+cudaError_t launch_v3_rows_f64(const V3Args& a, cudaStream_t s) {
+  const int n = a.ncls * 9 * a.geo.b;
+  dim3 rg((n + 255) / 256, a.nrows);
+  v3_row_kernel<double2><<<rg, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
 bool v3_pair_supported(int b, int precision) {
   (void)precision;
   return b == 3 || b == 6;

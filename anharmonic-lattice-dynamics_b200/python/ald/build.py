@@ -25,9 +25,11 @@ SOURCES = {
     "ald_capi.cpp": [],
     "ald_pipeline.cpp": [],
     "ald_phonon.cu": [],
+    "ald_heev.cu": [],
     "ald_v3.cu": [],
     "ald_v3_pair.cu": [],
     "ald_v3_tc.cu": [],
+    "ald_v3_dense.cu": [],
     # weight_tet's FP32/FP64 arithmetic must not be contracted into FMAs
     "ald_tetra.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
     "ald_iso.cu": ["-fmad=false", "--expt-relaxed-constexpr"],

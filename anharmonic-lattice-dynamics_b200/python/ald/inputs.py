@@ -401,9 +401,41 @@ def lj_superlattice(p: int, seed: int, a: float = 5.26, eps: float = 0.0104,
         pairs=[(1, 1, 0.1, rc_sigma * sigma, lennard_jones(eps, sigma))], atom_masses=masses)
 
 
-# configurations of the benchmark suite (seeded synthetic stand-ins)
+def rocksalt_supercell(seed: int, a: float = 5.64) -> Structure:
+    """The rock-salt Morse crystal in its 2x2x2 conventional supercell,
+    relabelled as one 64-atom cubic cell (192 bands), with the seeded
+    per-structure jitter of the batched benchmark: D +-20 %, alpha +-10 %
+    (uniform, per pair type), the two masses uniform in [10, 130] amu."""
+    rng = np.random.default_rng(seed)
+    mA, mB = (float(x) for x in rng.uniform(10.0, 130.0, size=2))
+    jit = lambda D, al, r0: (D * rng.uniform(0.8, 1.2), al * rng.uniform(0.9, 1.1), r0)
+    ab, aa, bb = jit(0.5, 1.2, 2.82), jit(0.1, 1.0, 3.99), jit(0.1, 1.0, 3.99)
+    fcc = [(0.0, 0.0, 0.0), (0.0, 0.5, 0.5), (0.5, 0.0, 0.5), (0.5, 0.5, 0.0)]
+    pos, types = [], []
+    for t, shift in ((1, (0.0, 0.0, 0.0)), (2, (0.5, 0.0, 0.0))):
+        for i in range(2):
+            for j in range(2):
+                for k in range(2):
+                    for f in fcc:
+                        pos.append(((f[0] + shift[0] + i) / 2.0 % 1.0, (f[1] + shift[1] + j) / 2.0 % 1.0,
+                                    (f[2] + shift[2] + k) / 2.0 % 1.0))
+                        types.append(t)
+    d1, d2 = a / 2.0, a / math.sqrt(2.0)
+    return Structure(
+        name="rocksalt-morse-2x2x2-s%d" % seed, conv_abc=(2.0, 2.0, 2.0), prim_in_conv=np.eye(3),
+        lattice_parameter=a, atom_types=types, atom_red_conv=pos, type_masses=[mA, mB], type_names=["Na", "Cl"],
+        pairs=[(1, 2, d1 - 0.01, d1 + 0.01, morse(*ab)),
+               (1, 1, d2 - 0.01, d2 + 0.01, morse(*aa)),
+               (2, 2, d2 - 0.01, d2 + 0.01, morse(*bb))])
+
+
+# configurations of the benchmark suite (seeded synthetic stand-ins); seeds
+# are 20261203 + structure index
+BASE_SEED = 20261203
+
+
 def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0,
-           rc_sigma: float = 2.5) -> Tuple[Structure, RunParams]:
+           rc_sigma: float = 2.5, p: int = 1, s: int = 0) -> Tuple[Structure, RunParams]:
     if n == 0:
         return lj_argon(), RunParams(mesh=tuple(mesh or (10, 10, 10)), tempk=tempk,
                                      width_cm=0.1 * THZ_TO_CM, delta="gauss")
@@ -414,10 +446,15 @@ def config(n: int, mesh: Optional[Sequence[int]] = None, tempk: float = 300.0,
                                      width_cm=0.05 * THZ_TO_CM, delta="gauss", cg_stop="residual",
                                      cg_tol=1e-8)
     if n == 3:
-        # one structure of the batched suite: superlattice p (default 1: the
-        # 4-atom conventional cell, 12 bands), mesh (ceil(12/p) >= 2) x 12 x 12
-        p = 1
+        # one structure of the batched suite: superlattice p (1: the 4-atom
+        # conventional cell, 12 bands; up to 8: 96 bands), structure s,
+        # mesh (ceil(12/p) >= 2) x 12 x 12
         m = mesh or (max(2, -(-12 // p)), 12, 12)
-        return (lj_superlattice(p, seed=20261203, rc_sigma=rc_sigma),
+        return (lj_superlattice(p, seed=BASE_SEED + s, rc_sigma=rc_sigma),
                 RunParams(mesh=tuple(m), tempk=tempk, width_cm=0.1 * THZ_TO_CM, delta="gauss"))
+    if n == 4:
+        # one structure of the batched mixed suite: the 64-atom rock-salt cell
+        # (192 bands), structure s, 8 x 8 x 8 mesh, tetrahedron delta
+        return (rocksalt_supercell(seed=BASE_SEED + s),
+                RunParams(mesh=tuple(mesh or (8, 8, 8)), tempk=tempk, delta="tetra"))
     raise ValueError("unknown configuration %r" % n)

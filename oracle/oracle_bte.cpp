@@ -47,7 +47,13 @@ void calculate_w3_ibz_split_sq(State& S, int k1, int k2, double* v33s8, int nthr
   int nsub = k2 - k1 + 1;
   int nb = ndn / 3;
   std::atomic<int> err{0};
-  parfor(k1, k2, nthreads, [&](int n1) {
+  // jobs: (row, l1, block of q2); each writes its own elements of v33s8, and
+  // the arithmetic of every element is the reference's whatever the split
+  const int q2blk = 256, nq2b = (nk + q2blk - 1) / q2blk;
+  parfor(0, nsub * ndn * nq2b - 1, nthreads, [&](int job) {
+    const int n1 = k1 + job / (ndn * nq2b);
+    const int l1 = 1 + (job / nq2b) % ndn;
+    const int n2lo = 1 + (job % nq2b) * q2blk, n2hi = std::min(nk, n2lo + q2blk - 1);
     int s = n1 - k1 + 1;
     std::vector<cplx> eivec3((size_t)27 * nb * nb * nb);
     double q1[3], q2[3], q3[3];
@@ -58,8 +64,8 @@ void calculate_w3_ibz_split_sq(State& S, int k1, int k2, double* v33s8, int nthr
       err = 1;
       return;
     }
-    for (int l1 = 1; l1 <= ndn; ++l1)
-      for (int n2 = 1; n2 <= nk; ++n2) {
+    {
+      for (int n2 = n2lo; n2 <= n2hi; ++n2) {
         for (int c = 0; c < 3; ++c) q2[c] = S.kpc[F2(c + 1, n2, 3)];
         int nk2, nk3;
         get_k_info(S, q2, nk2, i1, j1, kk1, inside);
@@ -120,6 +126,7 @@ void calculate_w3_ibz_split_sq(State& S, int k1, int k2, double* v33s8, int nthr
             v33s8[F5(s, n2, l1, l2, l3, nsub, nk, ndn, ndn)] = v;
           }
       }
+    }
   });
   if (err) throw std::runtime_error(err == 2 ? "MATRIX_ELT: den=0" : "V3: index mismatch");
 }

@@ -57,6 +57,21 @@ int orc_lattice(void* p, double* out) {
   return 0;
 }
 
+// fc3 terms and the atoms they refer to, as read by read_fc234 / read_lattice
+// (rest.f90:164-401): iat (3,nt3), ixyz (3,nt3), fcs (nt3), atompos
+// (3,natoms), iatomcell0 (natoms), mass0 (natoms0); 1-based indices
+int orc_fc3_terms(void* p, int* iat, int* ixyz, double* fcs, double* atompos, int* cell0, double* mass0) {
+  State& S = *(State*)p;
+  const int nt = S.nterms[2];
+  std::memcpy(iat, S.iatomterm_3.data(), sizeof(int) * 3 * nt);
+  std::memcpy(ixyz, S.ixyzterm_3.data(), sizeof(int) * 3 * nt);
+  std::memcpy(fcs, S.fcs_3.data(), sizeof(double) * nt);
+  std::memcpy(atompos, S.atompos.data(), sizeof(double) * 3 * S.natoms);
+  std::memcpy(cell0, S.iatomcell0.data(), sizeof(int) * S.natoms);
+  std::memcpy(mass0, S.mass0.data(), sizeof(double) * S.natoms0);
+  return nt;
+}
+
 int orc_op_kmatrix(void* p, double* out) {
   State& S = *(State*)p;
   for (int i = 0; i < S.lattpgcount; ++i) std::memcpy(out + 9 * i, S.op_kmatrix[i], 9 * sizeof(double));

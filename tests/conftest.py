@@ -38,7 +38,7 @@ def workdir(tmp_path_factory):
 def make_case(workdir, cfg, mesh, **kw):
     """Write one synthetic configuration into workdir and return its path."""
     from ald import inputs as I
-    skw = {"rc_sigma": kw.pop("rc_sigma")} if "rc_sigma" in kw else {}
+    skw = {k: kw.pop(k) for k in ("rc_sigma", "p", "s") if k in kw}
     st, rp = I.config(cfg, mesh=mesh, **skw)
     kw.update({"_" + k: v for k, v in skw.items()})  # part of the directory tag only
     for k, v in kw.items():

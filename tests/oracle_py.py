@@ -40,7 +40,7 @@ def lib():
                      "orc_tau", "orc_rta", "orc_collision", "orc_rhs", "orc_kappa_d", "orc_update_mpi",
                      "orc_iterative", "orc_giso", "orc_p_iso", "orc_collision_iso", "orc_mode_kappa_teff",
                      "orc_kappa_d_teff", "orc_make_kp_bs", "orc_frequencies_at", "orc_self_w",
-                     "orc_check_inside_bz"]:
+                     "orc_check_inside_bz", "orc_fc3_terms"]:
             getattr(L, name).restype = C.c_int
         L.orc_weight_tet_nonperm.restype = C.c_long
         _lib = L
@@ -149,6 +149,18 @@ class Oracle:
         vec = np.asfortranarray(vec, dtype=complex)
         vel = np.asfortranarray(vel, dtype=float)
         lib().orc_set_phonons(self.h, _p(ev), vec.ctypes.data_as(dp), _p(vel))
+
+    def fc3_terms(self):
+        """read_fc234's fc3 term list and the supercell atoms (1-based)."""
+        nt, na, n0 = self.nt3, self.natoms, self.nat0
+        iat = np.zeros((3, nt), dtype=np.int32, order="F")
+        ixyz = np.zeros((3, nt), dtype=np.int32, order="F")
+        fcs = np.zeros(nt)
+        pos = np.zeros((3, na), order="F")
+        cell0 = np.zeros(na, dtype=np.int32)
+        mass0 = np.zeros(n0)
+        lib().orc_fc3_terms(self.h, _p(iat, ip), _p(ixyz, ip), _p(fcs), _p(pos), _p(cell0, ip), _p(mass0))
+        return {"iat": iat, "ixyz": ixyz, "fcs": fcs, "atompos": pos, "cell0": cell0, "mass0": mass0}
 
     def tet(self):
         c = np.zeros((4, 6 * self.nkc), dtype=np.int32, order="F")

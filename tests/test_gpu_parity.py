@@ -135,7 +135,7 @@ def test_cg_quadratic(case, ald_lib):
     d, ref, ctx, _ = case
     x, fm, it, st = ald_lib.cg_quadratic(ref["CM"], ref["RHS"], ref["x0"])
     assert it == ref["cg_iters"]
-    ok, worst = close(x, ref["x"], rtol=1e-8, atol=1e-10)
+    ok, worst = close(x, ref["x"], atol=1e-10)
     assert ok, worst
 
 
@@ -155,7 +155,7 @@ def test_pipeline_injected_phonons(case):
     ok, worst = close(out["kappa_rta_modes"], ref["kappa_rta"], atol=1e-10)
     assert ok, worst
     assert out["cg_iters"] == ref["cg_iters"]
-    ok, worst = close(out["kappa_cg_modes"], ref["kappa_cg"], rtol=1e-8, atol=1e-10)
+    ok, worst = close(out["kappa_cg_modes"], ref["kappa_cg"], atol=1e-10)
     assert ok, worst
 
 
@@ -182,19 +182,19 @@ def test_update_mpi(case):
 def test_pipeline_iterative(case):
     """The job=3 sequence on the device against the oracle's mixing loop
     (kappa.f90:1390-1487) on the oracle's P1/P2: same iteration count, kappa
-    per mode to 1e-8 (the loop reuses its result 10-20 times)."""
+    per mode to 1e-10 (the FP64 bar; the loop reuses its result 10-20 times)."""
     d, ref, ctx, _ = case
     O = ref["O"]
     out = ctx.kappa_iterative(ref["tempk"])
     F, kap, iters, normk = O.iterative(ref["tempk"], ref["P1"], ref["P2"], ref["Q"], ref["FFF"])
     assert out["iters"] == iters
-    ok, worst = close(out["kappa_iter_modes"], kap, rtol=1e-8, atol=1e-10)
+    ok, worst = close(out["kappa_iter_modes"], kap, atol=1e-10)
     assert ok, worst
     # F of the acoustic modes at Gamma divides by a noise-level Q and carries no
     # weight in kappa (omega v = 0 there): compared elsewhere
     I = O.ibz()
     live = (ref["freq"][I["mapinv"] - 1] > 1e-6 * ref["freq"].max())[:, :, None] & np.ones(3, bool)
-    ok, worst = close(out["F"][live], F[live], rtol=1e-8, atol=1e-10)
+    ok, worst = close(out["F"][live], F[live], atol=1e-10)
     assert ok, worst
 
 
@@ -266,18 +266,58 @@ def test_e_minus_q_is_conjugate(phon):
         assert np.array_equal(vec_g[:, :, mk - 1], vec_g[:, :, n3 - 1].conj())
 
 
-def test_pipeline_own_eigensolver(phon, oracle_lib):
-    """End to end with each side's own eigensolver: kappa is basis dependent
-    only through degenerate subspaces; Q-weighted sums agree closely."""
-    O, ctx = phon
-    ctx.get_frequencies()
+def degenerate_groups(w, tol=1e-6):
+    """Index groups of modes whose eigenvalues agree to tol*max|w| (w sorted)."""
+    scale = max(np.abs(w).max(), 1e-300)
+    groups, cur = [], [0]
+    for l in range(1, len(w)):
+        if abs(w[l] - w[cur[-1]]) <= tol * scale:
+            cur.append(l)
+        else:
+            groups.append(cur)
+            cur = [l]
+    groups.append(cur)
+    return groups
+
+
+@pytest.mark.parametrize("cfg,mesh", [(1, (6, 6, 6)), (0, (10, 10, 10))], ids=["nacl6_gauss", "lj10_gauss"])
+def test_pipeline_own_eigensolver(oracle_lib, ald_lib, workdir, cfg, mesh):
+    """End to end with each side's own eigensolver (GPU Jacobi against the
+    oracle's), Gaussian delta.  Per-mode Q depends on the eigenvector basis
+    inside degenerate subspaces, but the sum of Q over a group of degenerate
+    modes l1 at q1 does not: P1 and P2 weight |V3(q1 l1, q2 l2, q3 l3)|^2 by
+    functions of the three frequencies only, so over whole degenerate groups
+    at q1, q2 and q3 the sum is the squared Frobenius norm of V3 restricted
+    to the three subspaces.  Bar: 1e-8 relative, floor 1e-10 max|Q|.  The
+    acoustic modes at Gamma (noise-level eigenvalues) are left out."""
+    d = make_case(workdir, cfg, mesh, delta="gauss")
+    ctx = ald_lib.Context(d)
+    ev_g, _, _ = ctx.get_frequencies()
     out = ctx.kappa_pipeline()
-    ref = oracle_lib.run_job1(ctx.dir)
-    for key, rk in (("kappa_rta", "kappa_rta"), ("kappa_cg", "kappa_cg")):
-        g = np.diag(out[key])
-        r = np.diag(ref[rk].sum(0))
+    ref = oracle_lib.run_job1(d)
+    O = ref["O"]
+    ev_o = O.get_phonons()[0]
+    scale = np.abs(ev_o).max()
+    assert np.all(np.abs(ev_g - ev_o) <= 1e-10 * np.abs(ev_o) + 1e-13 * scale)
+    mapinv = O.ibz()["mapinv"] - 1
+    Qg, Qo = out["Q"], ref["Q"]
+    qmax = np.abs(Qo).max()
+    worst, ngroups = 0.0, 0
+    for n in range(O.nibz):
+        w = ev_o[:, mapinv[n]]
+        for gr in degenerate_groups(w):
+            if abs(w[gr[0]]) < 1e-9 * scale:
+                continue
+            g, r = Qg[n, gr].sum(), Qo[n, gr].sum()
+            e = abs(g - r) / (abs(r) + 1e-10 * qmax)
+            worst = max(worst, e)
+            ngroups += 1
+    print("groups", ngroups, "worst relative difference of group sums of Q", worst)
+    assert worst <= 1e-8, worst
+    for key in ("kappa_rta", "kappa_cg"):  # basis dependent through 1/Q per mode: reported only
+        g, r = np.diag(out[key]), np.diag(ref[key].sum(0))
         print(key, g, r, np.abs(g / r - 1).max())
-        assert np.all(np.abs(g / r - 1) < 2e-2)
+    ctx.close()
 
 
 # ------------------------------------------------------------ golden pins
