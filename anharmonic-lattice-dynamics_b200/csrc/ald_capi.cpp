@@ -272,13 +272,34 @@ int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
   const int prec = c->opt.precision;
   V3Args a = a0;
   cudaError_t e;
-  if (v3_dense_supported(c->geo.b)) {
+  if (prec == ALD_MIXED && v3_dense_tc_supported(c->geo.b)) {
+    // more than 12 bands, mixed: split-FP16 tensor-core GEMMs per pair
+    const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, ALD_MIXED);
+    if (c->w_h.n < need) CKA(c->w_h.alloc(need));
+    a.hbuf = c->w_h.p;
+    const long long npairs = (long long)a.nrows * c->geo.nkc;
+    const long long P = v3_dense_tc_pairs(c->geo.b, npairs, (size_t)2 << 30);
+    const size_t wb = v3_dense_tc_work_bytes(c->geo.b, c->geo.nkc, a.nrows, P);
+    // GEMM 1 never writes the padding of the T2 operand: it is zeroed when the
+    // workspace is new or was last laid out for another (bands, pairs)
+    bool zeroed = c->w_v3work.n >= wb && c->v3work_tc_b == c->geo.b && c->v3work_tc_p == P;
+    if (c->w_v3work.n < wb) {
+      CKA(c->w_v3work.alloc(wb));
+      zeroed = false;
+    }
+    e = launch_v3_rows_f32(a, c->stream);
+    if (e == cudaSuccess) e = launch_v3_dense_tc(a, c->w_v3work.p, P, zeroed, c->stream);
+    c->v3work_tc_b = e == cudaSuccess ? c->geo.b : 0;
+    c->v3work_tc_p = P;
+    nl += 1 + v3_dense_tc_launches(npairs, P);
+  } else if (v3_dense_supported(c->geo.b)) {
     // more than 12 bands: batched GEMMs per pair (FP64)
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, ALD_FP64);
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
     const size_t wb = v3_dense_work_bytes(c->geo.b, (long long)a.nrows * c->geo.nkc, (size_t)2 << 30);
     if (c->w_v3work.n < wb) CKA(c->w_v3work.alloc(wb));
+    c->v3work_tc_b = 0;  // the FP64 GEMMs overwrite the workspace
     e = launch_v3_rows_f64(a, c->stream);
     if (e == cudaSuccess) e = launch_v3_dense(a, c->w_v3work.p, c->w_v3work.n, c->stream);
     const long long per = (long long)(c->w_v3work.n / (2 * (size_t)c->geo.b * c->geo.b * c->geo.b * 16));

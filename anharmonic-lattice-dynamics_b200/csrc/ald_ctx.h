@@ -33,6 +33,8 @@ struct ald_ctx {
   DevBuf<char> w_ptiles;              // phase tiles of the tensor-core V3 (mesh-only, built once)
   DevBuf<char> w_btiles;              // per-row B operands of the tensor-core V3
   DevBuf<char> w_v3work;              // T1/T2 of the large-cell V3 GEMMs
+  int v3work_tc_b = 0;                // its tensor-core T2 padding is zero for (bands, pairs)
+  long long v3work_tc_p = 0;
   bool ptiles_ok = false;
   // phonons and occupations
   DevBuf<double> w2_all, w2, evec, vel, freq, dist;

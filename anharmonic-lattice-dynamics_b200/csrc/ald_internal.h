@@ -271,6 +271,7 @@ struct V3Args {
   double const33;
   double* v3sq;              // v3_layout 0: [row][q2][l1][l2][l3] (the reference's order, per row)
   int v3_layout;             //           1: [row][l2][l3][l1][q2] (slices of the delta, q2 fastest)
+                             //           2: [row][l2][l3][q2][l1] (large cells, tensor-core V3)
   int* err;
   // phase classes (pair kernel)
   int ncls;
@@ -296,6 +297,18 @@ cudaError_t launch_v3_rows_f64(const V3Args& a, cudaStream_t s);
 bool v3_dense_supported(int b);
 size_t v3_dense_work_bytes(int b, long long npairs, size_t budget);
 cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s);
+// more than 12 bands, ALD_MIXED (ald_v3_dense_tc.cu): both mode products as
+// split-FP16 tcgen05 GEMMs; hbuf from launch_v3_rows_f32; work of
+// v3_dense_tc_work_bytes(b, nkc, nrows, pairs) bytes for batches of `pairs`
+// pairs; a2_zeroed: the workspace's T2 operand padding is already zero
+bool v3_dense_tc_supported(int b);
+long long v3_dense_tc_pairs(int b, long long npairs, size_t budget);
+size_t v3_dense_tc_work_bytes(int b, int nkc, int nrows, long long pairs);
+int v3_dense_tc_launches(long long npairs, long long pairs);
+cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long pairs, bool a2_zeroed, cudaStream_t s);
+// the |V3|^2 layout the pipeline asks V3 for and hands to the delta:
+// 0 [row][q2][l1][l2][l3], 1 [row][l2][l3][l1][q2], 2 [row][l2][l3][q2][l1]
+int v3_pipeline_layout(int b, int precision);
 // 3 bands, ALD_MIXED: class sums on tcgen05 (ald_v3_tc.cu); hbuf from launch_v3_rows_f32
 bool v3_tc_supported(int b, int ncls);
 // the row-independent phase tiles (split FP16, canonical layout), built once per context

@@ -89,7 +89,8 @@ static void shard_range(int nibz, int rank, int nranks, int& rb, int& re) {
 // rows; Q and the CG matrix-vector products are exchanged through `gather`
 struct ShardSpec {
   int rank, nranks;
-  ald_allgather_fn gather;
+  ald_allgather_fn gather;         // host buffers, or
+  ald_allgather_dev_fn gather_dev; // device buffers, ordered on the context's stream
   void* user;
 };
 
@@ -97,7 +98,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
                         double* kappa_rta_modes, double* kappa_cg_modes, double* xo, const IterSpec* it,
                         const ShardSpec* sh = nullptr) {
   if (!c || !res) return fail(ALD_ERR_ARG, "null argument");
-  if (sh && (sh->nranks < 1 || sh->rank < 0 || sh->rank >= sh->nranks || !sh->gather))
+  if (sh && (sh->nranks < 1 || sh->rank < 0 || sh->rank >= sh->nranks || (!sh->gather && !sh->gather_dev)))
     return fail(ALD_ERR_ARG, "sharded pipeline: bad rank, rank count or exchange function");
   if (sh && it) return fail(ALD_ERR_UNSUPPORTED, "the sharded pipeline runs job=1 only");
   if (it && !c->full_op_ok) return fail(ALD_ERR_UNSUPPORTED, "update_mpi: a mesh point is not a star arm of its IBZ point");
@@ -152,6 +153,11 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
       shard_range(nibz, k2, sh->nranks, a0, a1);
       counts[k2] = (long long)(a1 - a0) * (long long)unit;
     }
+    if (sh->gather_dev)  // device buffers: no staging, ordered on the stream
+      return sh->gather_dev(sh->user, mine, (long long)nloc * (long long)unit, all, counts.data(), sh->nranks,
+                            (void*)s) != 0
+                 ? ALD_ERR_ARG
+                 : ALD_OK;
     std::vector<double> hm((size_t)nloc * unit), ha((size_t)nibz * unit);
     if (!hm.empty() && cudaMemcpyAsync(hm.data(), mine, hm.size() * sizeof(double), cudaMemcpyDeviceToHost, s))
       return ALD_ERR_CUDA;
@@ -180,16 +186,17 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
-  const bool fused = !gauss && delta_fused_supported(c->geo);
-  // more than 16 bands: the band-generic delta kernels, straight into R1/R2
-  const bool any = !fused && b > kDeltaSmallBands;
-  if (!fused && !any) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
-  // class-form V3 kernels write that layout
-  const int v3_layout = v3_pair_supported(b, c->opt.precision) || v3_dense_supported(b) ? 1 : 0;
+  // class-form V3 kernels write that layout; the large-cell tensor-core V3
+  // writes runs of l1 instead (layout 2)
+  const int v3_layout = v3_pipeline_layout(b, c->opt.precision);
+  const bool fused = !gauss && v3_layout != 2 && delta_fused_supported(c->geo);
+  // more than 16 bands, or layout 2: the band-generic delta kernels, straight into R1/R2
+  const bool any = !fused && (b > kDeltaSmallBands || v3_layout == 2);
+  if (!fused && !any) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   ALD_CKA(c->w_brange.alloc((size_t)2 * b));
   ALD_CK(launch_band_range(c->geo, c->freq.p, c->w_brange.p, s));
-  res->launches[2] += 1;
+  res->launches[0] += 1;  // band ranges of the occupations, outside the timed delta stage
   for (int r0 = rb; r0 < re; r0 += K) {
     int nr = std::min(K, re - r0);
     ALD_CK(tm.begin(1));
@@ -218,23 +225,22 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     a.P1s = a.P2s = a.P1 = a.P2 = nullptr;
     a.R1p = it ? c->w_R1p.p + (size_t)r0 * nkc * b * b : nullptr;
     a.R2p = it ? c->w_R2p.p + (size_t)r0 * nkc * b * b : nullptr;
-    ALD_CK(tm.begin(2));
+    // the sums that the delta kernels add into start at zero; the zeroing
+    // runs outside the delta stage, so that stage times the kernel alone
     const size_t rbytes = (size_t)nr * nkc * b * b * sizeof(double);
     if (it) {
       ALD_CK(cudaMemsetAsync(a.R1p, 0, rbytes, s));
       ALD_CK(cudaMemsetAsync(a.R2p, 0, rbytes, s));
     }
+    if (fused || (any && !gauss)) {
+      ALD_CK(cudaMemsetAsync(a.R1, 0, rbytes, s));
+      ALD_CK(cudaMemsetAsync(a.R2, 0, rbytes, s));
+    }
+    ALD_CK(tm.begin(2));
     if (fused) {
-      const size_t n = rbytes;
-      ALD_CK(cudaMemsetAsync(a.R1, 0, n, s));
-      ALD_CK(cudaMemsetAsync(a.R2, 0, n, s));
       ALD_CK(launch_delta_fused(a, s));
       res->launches[2] += 1;
     } else if (any) {
-      if (!gauss) {  // the tetrahedron kernel adds into R1/R2
-        ALD_CK(cudaMemsetAsync(a.R1, 0, rbytes, s));
-        ALD_CK(cudaMemsetAsync(a.R2, 0, rbytes, s));
-      }
       ALD_CK(launch_delta_any(a, s));
       res->launches[2] += 1;
     } else {
@@ -518,7 +524,16 @@ extern "C" int ald_shard_rows(const ald_ctx* c, int rank, int nranks, int ksubse
 extern "C" int ald_kappa_pipeline_sharded(ald_ctx* c, double tempk, int rank, int nranks, ald_allgather_fn gather,
                                           void* user, ald_kappa_result* res, double* Qo, double* QNo, double* QUo,
                                           double* kappa_rta_modes, double* kappa_cg_modes, double* xo) {
-  ShardSpec sh{rank, nranks, gather, user};
+  ShardSpec sh{rank, nranks, gather, nullptr, user};
+  return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr, &sh);
+}
+
+extern "C" int ald_kappa_pipeline_sharded_dev(ald_ctx* c, double tempk, int rank, int nranks,
+                                              ald_allgather_dev_fn gather, void* user, ald_kappa_result* res,
+                                              double* Qo, double* QNo, double* QUo, double* kappa_rta_modes,
+                                              double* kappa_cg_modes, double* xo) {
+  if (!gather) return fail(ALD_ERR_ARG, "sharded pipeline: no exchange function");
+  ShardSpec sh{rank, nranks, nullptr, gather, user};
   return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr, &sh);
 }
 

@@ -778,12 +778,17 @@ __global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
   const int lend = lo2;
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   size_t sq, s1, s2, s3;
-  if (a.v3_layout == 1) {
+  if (a.v3_layout == 1) {  // [l2][l3][l1][q]
     sq = 1;
     s1 = nkc;
     s3 = (size_t)b * nkc;
     s2 = (size_t)b2 * nkc;
-  } else {
+  } else if (a.v3_layout == 2) {  // [l2][l3][q][l1]
+    s1 = 1;
+    sq = b;
+    s3 = (size_t)b * nkc;
+    s2 = (size_t)b2 * nkc;
+  } else {  // [q][l1][l2][l3]
     s3 = 1;
     s2 = b;
     s1 = (size_t)b2;
@@ -829,11 +834,22 @@ template <bool F32W>
 __global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
   const Geometry& g = a.geo;
   const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
-  // x: (l1, l2, block of w) with w blocks fastest; y: row
-  const int nwb = (nkc + blockDim.x - 1) / blockDim.x;
-  const int l12 = (int)(blockIdx.x / nwb), w = (int)(blockIdx.x % nwb) * blockDim.x + threadIdx.x, row = blockIdx.y;
-  const int l1 = l12 / b, l2 = l12 % b;
-  if (w >= nkc) return;
+  // x: (l1, l2, w), w fastest for layouts 0/1 (|V3|^2 runs of q2), l1
+  // fastest for layout 2 (runs of l1); y: row
+  const long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const int row = blockIdx.y;
+  int w, l1, l2;
+  if (a.v3_layout == 2) {
+    l1 = (int)(gid % b);
+    w = (int)((gid / b) % nkc);
+    l2 = (int)(gid / ((long long)b * nkc));
+  } else {
+    w = (int)(gid % nkc);
+    const long long l12 = gid / nkc;
+    l1 = (int)(l12 / b);
+    l2 = (int)(l12 % b);
+  }
+  if (l2 >= b || l1 >= b) return;
   const int q1 = a.mapinv[a.n1_first + row];
   int m1[3], mw[3], m3p[3], m3m[3], ins1, ins2;
   decompose(g, q1, m1);
@@ -846,8 +862,10 @@ __global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
   const double om1 = a.freq[(size_t)q1 * b + l1], nb1 = a.dist[(size_t)q1 * b + l1];
   const double n2 = a.dist[(size_t)w * b + l2], w2 = a.freq[(size_t)w * b + l2];
   const double* v3 = a.v3sq + (size_t)row * nkc * b3;
-  const size_t sq = a.v3_layout == 1 ? 1 : (size_t)b3, s1 = a.v3_layout == 1 ? (size_t)nkc : (size_t)b2;
-  const size_t s2 = a.v3_layout == 1 ? (size_t)b2 * nkc : (size_t)b, s3 = a.v3_layout == 1 ? (size_t)b * nkc : 1;
+  const int L = a.v3_layout;
+  const size_t sq = L == 1 ? 1 : (L == 2 ? (size_t)b : (size_t)b3);
+  const size_t s1 = L == 1 ? (size_t)nkc : (L == 2 ? 1 : (size_t)b2);
+  const size_t s2 = L == 0 ? (size_t)b : (size_t)b2 * nkc, s3 = L == 0 ? 1 : (size_t)b * nkc;
   const double gc1 = 0.5 / (a.sigma * a.sigma), gc2 = 1.0 / (sqrt(2 * PhysConst::pi) * a.sigma);
   const float fc1 = (float)gc1, fc2 = (float)gc2;
   double R[2] = {0.0, 0.0};
@@ -1016,7 +1034,7 @@ cudaError_t launch_delta_any(const CombineArgs& a, cudaStream_t s) {
   const Geometry& g = a.geo;
   if (g.b > 256) return cudaErrorInvalidValue;
   if (a.gauss) {
-    const long long nx = (long long)((g.nkc + 127) / 128) * g.b * g.b;
+    const long long nx = ((long long)g.nkc * g.b * g.b + 127) / 128;
     if (nx > 2147483647LL || a.nrows > 65535) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)nx, a.nrows);
     if (a.f32w) delta_gauss_any_kernel<true><<<grid, 128, 0, s>>>(a);

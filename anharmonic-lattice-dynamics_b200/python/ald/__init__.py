@@ -66,7 +66,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_rta_kappa", "ald_collision_matrix", "ald_rhs", "ald_cg_quadratic", "ald_mode_kappa_d",
            "ald_kappa_pipeline", "ald_set_stream", "ald_h2d_bytes", "ald_cg_quadratic_static", "ald_update_mpi",
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
-           "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_tau_eff", "ald_qandtau",
+           "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_kappa_pipeline_sharded_dev", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
            "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
@@ -445,14 +445,26 @@ class Context:
         _check(lib().ald_shard_rows(self.h, rank, nranks, k))
         return k[0], k[1]
 
-    def kappa_pipeline_sharded(self, rank: int, nranks: int, gather, tempk: Optional[float] = None):
+    def kappa_pipeline_sharded(self, rank: int, nranks: int, gather, tempk: Optional[float] = None,
+                               device: bool = False):
         """One rank of the row-sharded job=1 (ald_kappa_pipeline_sharded).
         `gather(mine, counts)` is the all-gather: it receives this rank's
         values (numpy) and the per-rank counts and returns every rank's values
-        concatenated in rank order (e.g. torch_allgather())."""
+        concatenated in rank order (e.g. torch_allgather()).  With device=True
+        the exchange stays on the GPU (ald_kappa_pipeline_sharded_dev):
+        `gather(mine_ptr, count, all_ptr, counts, stream)` gets device pointers
+        and the context's stream (e.g. torch_allgather_device())."""
         if tempk is None:
             tempk = self.info.tempk
         err = []
+
+        def cbd(user, mine, count, out, counts, nranks_, stream):
+            try:
+                gather(mine or 0, count, out or 0, [counts[k] for k in range(nranks_)], stream or 0)
+                return 0
+            except Exception as ex:  # reported after the call returns
+                err.append(ex)
+                return 1
 
         def cb(user, mine, count, out, counts, nranks_):
             try:
@@ -467,26 +479,35 @@ class Context:
                 err.append(ex)
                 return 1
 
-        fn = ALLGATHER_FN(cb)
+        fn = ALLGATHER_DEV_FN(cbd) if device else ALLGATHER_FN(cb)
+        entry = lib().ald_kappa_pipeline_sharded_dev if device else lib().ald_kappa_pipeline_sharded
         res = KappaResult()
         n, ni = self.ndyn, self.nibz
         Q, QN, QU = (np.zeros((ni, n), order="F") for _ in range(3))
         kr, kc = np.zeros((n, 3, 3), order="F"), np.zeros((n, 3, 3), order="F")
         x = np.zeros(ni * n * 3)
-        r = lib().ald_kappa_pipeline_sharded(self.h, C.c_double(tempk), rank, nranks, fn, None, C.byref(res), _p(Q),
-                                             _p(QN), _p(QU), _p(kr), _p(kc), _p(x))
+        r = entry(self.h, C.c_double(tempk), rank, nranks, fn, None, C.byref(res), _p(Q), _p(QN), _p(QU), _p(kr),
+                  _p(kc), _p(x))
         if err:
             raise err[0]
         _check(r)
         return {"kappa_rta": np.array(res.kappa_rta).reshape(3, 3, order="F"),
                 "kappa_cg": np.array(res.kappa_cg).reshape(3, 3, order="F"), "cg_iters": res.cg_iters,
                 "status_cg": res.status_cg, "stage_ms": dict(zip(STAGES, list(res.stage_ms))),
-                "Q": Q, "QN": QN, "QU": QU, "kappa_rta_modes": kr, "kappa_cg_modes": kc, "x": x}
+                "launches": dict(zip(STAGES, list(res.launches))), "triplet_bands": res.triplet_bands,
+                "d2h_bytes": res.d2h_bytes, "Q": Q, "QN": QN, "QU": QU, "kappa_rta_modes": kr,
+                "kappa_cg_modes": kc, "x": x}
 
 
 # int (*)(void* user, const double* mine, long long count, double* all, const long long* counts, int nranks)
 ALLGATHER_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(C.c_double), C.c_longlong, C.POINTER(C.c_double),
                            C.POINTER(C.c_longlong), C.c_int)
+
+
+# int (*)(void* user, const double* mine, long long count, double* all, const long long* counts, int nranks,
+#        void* stream), device pointers
+ALLGATHER_DEV_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_longlong, C.c_void_p, C.POINTER(C.c_longlong),
+                               C.c_int, C.c_void_p)
 
 
 def shard_rows(nibz: int, rank: int, nranks: int) -> Tuple[int, int]:
@@ -515,6 +536,49 @@ def torch_allgather(group=None):
         parts = [torch.empty_like(buf) for _ in counts]
         dist.all_gather(parts, buf, group=group)
         return np.concatenate([p[:c].cpu().numpy() for p, c in zip(parts, counts)])
+
+    return gather
+
+
+class _DeviceBuffer:
+    """A raw device pointer of float64 values seen by torch through the CUDA
+    array interface (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 2,
+                                         "strides": None}
+
+
+def torch_allgather_device(group=None):
+    """A device all-gather for kappa_pipeline_sharded(device=True) over
+    torch.distributed: the ranks' device values padded to the longest,
+    gathered with all_gather on the context's stream and copied into the
+    output in rank order -- on the GPU with NCCL; gloo (one GPU, tests) runs
+    its collective on host copies inside this adapter."""
+    import torch
+    import torch.distributed as dist
+
+    def gather(mine: int, count: int, out: int, counts: Sequence[int], stream: int) -> None:
+        dev = torch.device("cuda", torch.cuda.current_device())
+        m = max(counts)
+        st = torch.cuda.ExternalStream(stream, device=dev) if stream else torch.cuda.current_stream(dev)
+        with torch.cuda.stream(st):
+            buf = torch.zeros(m, dtype=torch.float64, device=dev)
+            if count > 0:
+                buf[:count] = torch.as_tensor(_DeviceBuffer(mine, count), device=dev)
+            if dist.get_backend(group) == "gloo":  # gloo collectives on host copies
+                cpu = buf.cpu()
+                parts = [torch.empty_like(cpu) for _ in counts]
+                dist.all_gather(parts, cpu, group=group)
+                parts = [p_.to(dev) for p_ in parts]
+            else:
+                parts = [torch.empty_like(buf) for _ in counts]
+                dist.all_gather(parts, buf, group=group)
+            dst = torch.as_tensor(_DeviceBuffer(out, sum(counts)), device=dev)
+            off = 0
+            for p_, c in zip(parts, counts):
+                dst[off:off + c] = p_[:c]
+                off += c
 
     return gather
 

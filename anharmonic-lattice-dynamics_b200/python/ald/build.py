@@ -30,6 +30,7 @@ SOURCES = {
     "ald_v3_pair.cu": [],
     "ald_v3_tc.cu": [],
     "ald_v3_dense.cu": [],
+    "ald_v3_dense_tc.cu": [],
     # weight_tet's FP32/FP64 arithmetic must not be contracted into FMAs
     "ald_tetra.cu": ["-fmad=false", "--expt-relaxed-constexpr"],
     "ald_iso.cu": ["-fmad=false", "--expt-relaxed-constexpr"],

@@ -23,8 +23,10 @@ between the two sit beside it.
 --impl reference times the reference algorithm's CPU implementation (the
 oracle restatement, all host threads) on a bounded sample of IBZ rows of
 the same workload and prints the same JSON line with "impl": "reference".
-With torchrun (N>1) every rank runs its own copy of the workload (weak
-scaling, no data-path collective); the reference arm runs on rank 0 only.
+With torchrun (N>1) the ranks split one job by IBZ rows, as the reference's
+MPI decomposition does (kappa.f90:418-431), and exchange Q and the CG
+matrix-vector products with NCCL all-gathers on device buffers (strong
+scaling); the reference arm runs on rank 0 only.
 """
 from __future__ import annotations
 
@@ -49,15 +51,22 @@ WORKLOADS = {
     "rocksalt": (16, "rocksalt-Morse NaCl-type, 2 atoms (6 bands), %dx%dx%d q-mesh, tetrahedron delta, T=300 K"),
     "lj-argon": (32, "fcc LJ argon, 1 atom (3 bands), %dx%dx%d q-mesh, Gaussian 0.05 THz, CG to residual 1e-8, "
                      "T=300 K"),
+    "rocksalt-192": (4, "rocksalt-Morse 2x2x2 conventional supercell as one 64-atom cell (192 bands), structure 0 "
+                        "of the batched suite, %dx%dx%d q-mesh, tetrahedron delta, T=300 K"),
 }
+CONFIG_OF = {"rocksalt": 1, "lj-argon": 2, "rocksalt-192": 4}
 
 
 def _peaks():
+    """Roofline denominators: MEASURED_PEAKS.json (written on this pool's
+    B200s) when present, else the pool's earlier measurement."""
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
         d = json.load(open(p))
-        return {"hbm_gbs": d.get("hbm_gbs", 6650.0), "src": "measured"}
-    return {"hbm_gbs": 6650.0, "src": "fallback"}
+        return {"hbm_gbs": float(d.get("hbm_gbs", 6650.0)), "bf16_tflops": float(d.get("bf16_tflops", 1590.0)),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d.get("bf16_tflops", 1400.0))),
+                "src": "measured"}
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0, "src": "fallback"}
 
 
 class ClockSampler:
@@ -120,7 +129,7 @@ class ClockSampler:
 
 def make_workload(d: str, mesh=(16, 16, 16), workload: str = "rocksalt"):
     from ald import inputs as I
-    st, rp = I.config(1 if workload == "rocksalt" else 2, mesh=mesh)
+    st, rp = I.config(CONFIG_OF[workload], mesh=mesh)
     I.write_inputs(st, rp, d)
     return rp
 
@@ -128,7 +137,7 @@ def make_workload(d: str, mesh=(16, 16, 16), workload: str = "rocksalt"):
 def workload_options(ald, rp, workload: str, **kw):
     """Library options of a workload: configuration 1 runs the defaults (tetrahedron delta, the
     reference's CG stop rule); configuration 2 the Gaussian delta and CG to a residual."""
-    if workload == "rocksalt":
+    if workload != "lj-argon":
         return ald.default_options(**kw)
     return ald.default_options(delta=ald.DELTA_GAUSS, cg_stop=ald.CG_RESIDUAL, cg_tol=rp.cg_tol,
                                width_cm=rp.width_cm, **kw)
@@ -161,39 +170,67 @@ def cpu_baseline(d: str, rows: int = 0, gauss: bool = False):
             "seconds": dt}
 
 
-def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8):
-    """Dominant device stage and its achieved HBM bandwidth from algorithmic bytes."""
+# DRAM bytes (read + write) of one launch from ncu captures of this workload
+# (profiles/), keyed by (stage, nkc, bands, rows per launch)
+NCU_TRAFFIC = {("delta", 4096, 6, 72): 452.72e6, ("v3", 4096, 6, 72): 477.53e6}
+
+
+def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8, rows_per_launch=None):
+    """The dominant device stage against its ceiling.
+
+    achieved = algorithmic bytes per launch / device time per launch (the
+    stage's CUDA events over the timed steps, divided by its launches).
+    Algorithmic bytes of the tetrahedron delta: R1/R2 written once,
+    2 nibz nkc b^2 8 bytes per step; `wide_bytes` adds the |V3|^2 read and
+    the R1/R2 read-modify-write of the fused kernel."""
     stages = {k: v for k, v in stage_ms.items() if k != "total"}
     dom = max(stages, key=stages.get)
     n = launches.get(dom, 1) or 1
     ms = stages[dom] / n
     N = 3 * b * nibz
     b3 = b ** 3
-    # algorithmic bytes per launch of the dominant stage
-    per = {
-        "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n,            # |V3|^2 out + e(q2), e(q3) in
-        "delta": nibz * nkc * (b3 * 8 + 2 * b * b * 8 * 2) / n,      # |V3|^2 in + R1/R2 out (read+write)
-        "collision": N * N * cm_bytes / n,                           # CM written once
-        "cg": None,
+    alg = {
+        "delta": 2 * nibz * nkc * b * b * 8 / n,
+        "v3": nibz * nkc * (b3 * 8) / n,
+        "collision": N * N * cm_bytes / n,
+        "cg": N * N * cm_bytes,
     }
-    bytes_ = per.get(dom)
+    wide = {"delta": nibz * nkc * (b3 * 8 + 2 * 2 * b * b * 8) / n,
+            "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n}
     if dom == "cg":
-        bytes_ = N * N * cm_bytes  # one matrix-vector product streams the matrix (per iteration)
         ms = stages[dom] / max(1, cg_iters)
-    if bytes_ is None or ms <= 0:
+    by = alg.get(dom)
+    if by is None or ms <= 0:
         return {"bound": "hbm", "achieved": None, "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": None,
                 "traffic": None, "kernel": dom}
-    ach = bytes_ / (ms * 1e-3) / 1e9
-    # DRAM bytes (read + write) per launch from one ncu capture of a 72-row chunk of this
-    # workload, scaled to the rows of a launch
-    ncu_bytes_72rows = {("delta", 4096, 6): 452.72e6, ("v3", 4096, 6): 477.53e6}
+    ach = by / (ms * 1e-3) / 1e9
     traffic = None
-    if (dom, nkc, b) in ncu_bytes_72rows:
-        traffic = ncu_bytes_72rows[(dom, nkc, b)] * (nibz / n) / 72
-    return {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
-            "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom, "ms_per_launch": ms,
-            "algorithmic_bytes": bytes_, "peak_source": peaks["src"],
-            "note": "the delta and V3 kernels are bound by instruction issue (ALU/FMA/FP64 pipes in ncu), not by HBM"}
+    rpl = rows_per_launch or max(1, nibz // n)
+    for (st, nk, bb, rows), t in NCU_TRAFFIC.items():
+        if st == dom and nk == nkc and bb == b:
+            traffic = t * rpl / rows  # DRAM traffic grows with the rows of a launch
+    out = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
+           "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom, "ms_per_launch": ms,
+           "launches_per_step": n, "algorithmic_bytes": by, "peak_source": peaks["src"] + " (copy bandwidth)"}
+    if dom in wide:
+        out["wide_bytes"] = wide[dom]
+        out["wide_frac"] = wide[dom] / (ms * 1e-3) / 1e9 / peaks["hbm_gbs"]
+    return out
+
+
+def v3_roofline(stage_ms, launches, nibz, nkc, b, peaks, where):
+    """V3 against the dense tensor-core peak: the algorithmic 24 b^4 real
+    flops per (q1, q2) pair of the three complex mode products, over the V3
+    stage's device time."""
+    ms = stage_ms.get("v3", 0.0)
+    flops = 24.0 * b ** 4 * nibz * nkc
+    if ms <= 0:
+        return None
+    ach = flops / (ms * 1e-3) / 1e12
+    pk = peaks["bf16_tflops"]
+    return {"bound": "tensor", "achieved": ach, "peak": pk, "unit": "TFLOP/s", "frac": ach / pk,
+            "kernel": "v3", "flops_per_step": flops, "ms_per_step": ms, "launches_per_step": launches.get("v3"),
+            "peak_source": peaks["src"] + " (dense bf16 GEMM, burst)", "where": where}
 
 
 def main():
@@ -208,6 +245,8 @@ def main():
                     help="rocksalt: the metric's configuration (default); lj-argon: the large single structure")
     ap.add_argument("--mesh", type=int, default=0, help="mesh edge (default: the workload's own)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the extra driver-timed workloads (32^3 argon, the 192-band cell)")
     args = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -224,11 +263,12 @@ def main():
             vals = []
             cb = None
             for _ in range(args.warmup + args.steps):
-                cb = cpu_baseline(d, gauss=args.workload == "lj-argon")
+                # two IBZ rows per step keep the whole run within a few minutes
+                cb = cpu_baseline(d, rows=2, gauss=args.workload == "lj-argon")
                 vals.append(cb["value"])
             v = sorted(vals[args.warmup:])[len(vals[args.warmup:]) // 2] if args.steps else vals[-1]
         line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
-                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+                "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (analytic %s FC2/FC3, reference file formats)" % (
                     "Morse" if args.workload == "rocksalt" else "Lennard-Jones"),
@@ -248,7 +288,7 @@ def main():
 
         import torch.distributed as dist
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     dev = local
     torch.cuda.set_device(dev)
     tmp = tempfile.TemporaryDirectory()
@@ -256,14 +296,17 @@ def main():
     rp = make_workload(d, mesh, args.workload)
     stream = torch.cuda.Stream(device=dev)
 
-    def timed_path(precision):
+    def timed_path(precision, d=d, rp=rp, workload=args.workload, steps=args.steps, warmup=args.warmup):
         """K timed steps of one precision path on a context whose tables are in HBM."""
-        opts = workload_options(ald, rp, args.workload, device=dev, precision=precision)
+        opts = workload_options(ald, rp, workload, device=dev, precision=precision)
         ctx = ald.Context(d, opts)
         ctx.set_stream(stream.cuda_stream)
         tempk = ctx.info.tempk
 
         ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        # several GPUs: the reference's MPI row split, one rank per GPU, with
+        # the Q and CG exchanges as NCCL all-gathers on device buffers
+        gdev = ald.torch_allgather_device() if world > 1 else None
 
         def step():
             # the eigensolve (get_frequencies) runs before the pipeline call;
@@ -271,12 +314,15 @@ def main():
             ev_a.record(stream)
             ctx.invalidate_phonons()
             ev_b.record(stream)
-            out = ctx.kappa_pipeline(tempk, want_modes=False)
+            if gdev is not None:
+                out = ctx.kappa_pipeline_sharded(rank, world, gdev, tempk, device=True)
+            else:
+                out = ctx.kappa_pipeline(tempk, want_modes=False)
             out["stage_ms"]["phonons"] += ev_a.elapsed_time(ev_b)
             out["stage_ms"]["total"] += ev_a.elapsed_time(ev_b)
             return out
 
-        for _ in range(args.warmup):
+        for _ in range(warmup):
             out = step()
         if world > 1:
             torch.distributed.barrier()
@@ -286,7 +332,7 @@ def main():
         with ClockSampler(dev) as clk:
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            for _ in range(args.steps):
+            for _ in range(steps):
                 out = step()
                 for k, v in out["stage_ms"].items():
                     stage_sum[k] += v
@@ -300,7 +346,7 @@ def main():
         if world > 1:
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms_max = float(t.item())
-        res = {"ms": ms_max, "stage": {k: v / args.steps for k, v in stage_sum.items()},
+        res = {"ms": ms_max, "steps": steps, "stage": {k: v / steps for k, v in stage_sum.items()},
                "launch_counts": dict(out["launches"]), "launches": launches, "out": out, "clocks": clk.summary(),
                "tempk": tempk, "nibz": ctx.nibz, "nkc": ctx.nkc, "b": ctx.ndyn, "opts": opts}
         ctx.close()
@@ -313,7 +359,9 @@ def main():
     out = head["out"]
     tb = out["triplet_bands"]
     ms_max = head["ms"]
-    value = world * tb * args.steps / (ms_max * 1e-3)
+    # one job split over the ranks (strong scaling): the job's triplet-bands
+    # per second of the slowest rank
+    value = tb * args.steps / (ms_max * 1e-3)
     per_step = head["stage"]
     per_launch_counts = head["launch_counts"]
     launches = head["launches"]
@@ -323,22 +371,62 @@ def main():
 
     # ---- end to end through the C ABI from the input files (headline path)
     e2e_times, h2d, d2h = [], 0.0, 0.0
+    gdev_e2e = ald.torch_allgather_device() if world > 1 else None
     for i in range(max(2, min(args.steps, 5)) + 1):
+        if world > 1:
+            torch.distributed.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         c2 = ald.Context(d, opts)
-        o2 = c2.kappa_pipeline(tempk, want_modes=True)
+        if gdev_e2e is not None:
+            c2.set_stream(stream.cuda_stream)
+            o2 = c2.kappa_pipeline_sharded(rank, world, gdev_e2e, tempk, device=True)
+        else:
+            o2 = c2.kappa_pipeline(tempk, want_modes=True)
         torch.cuda.synchronize()
         dt = time.perf_counter() - t0
         h2d, d2h = c2.h2d_bytes(), o2["d2h_bytes"] + 9 * 2 * 8
         c2.close()
         if i > 0:
             e2e_times.append(dt)
-    e2e = world * tb / (sorted(e2e_times)[len(e2e_times) // 2])
-    if world > 1:
-        te = torch.tensor([e2e / world], dtype=torch.float64, device="cuda")
+    e2e = tb / (sorted(e2e_times)[len(e2e_times) // 2])
+    if world > 1:  # the slowest rank's time
+        te = torch.tensor([e2e], dtype=torch.float64, device="cuda")
         torch.distributed.all_reduce(te, op=torch.distributed.ReduceOp.MIN)
-        e2e = float(te.item()) * world
+        e2e = float(te.item())
+
+    # ---- extra workloads, driver-timed beside the headline (single GPU only):
+    # the large single structure (32^3 argon, 3-band tensor-core class sums)
+    # and the 192-band cell (both mode products on the tensor cores)
+    extras = {}
+    if world == 1 and not args.no_extra:
+        peaks0 = _peaks()
+        for wl, st_, wu in (("lj-argon", 5, 3), ("rocksalt-192", 2, 1)):
+            try:
+                t2 = tempfile.TemporaryDirectory()
+                m2 = (WORKLOADS[wl][0],) * 3
+                rp2 = make_workload(t2.name, m2, wl)
+                rr = {pp: timed_path(pp, d=t2.name, rp=rp2, workload=wl, steps=st_, warmup=wu)
+                      for pp in (ald.FP64, ald.MIXED)}
+                f, m = rr[ald.FP64], rr[ald.MIXED]
+                tb2 = m["out"]["triplet_bands"]
+                kf, km = np.asarray(f["out"]["kappa_cg"]), np.asarray(m["out"]["kappa_cg"])
+                extras[wl] = {
+                    "workload": WORKLOADS[wl][1] % m2, "steps": st_, "warmup": wu,
+                    "nibz": m["nibz"], "nkc": m["nkc"], "ndyn": m["b"],
+                    "mixed": {"value": tb2 * st_ / (m["ms"] * 1e-3), "unit": UNIT, "ms_per_step": m["ms"] / st_,
+                              "stage_ms_per_step": {k: round(v, 4) for k, v in m["stage"].items()},
+                              "roofline_v3": v3_roofline(m["stage"], m["launch_counts"], m["nibz"], m["nkc"], m["b"],
+                                                         peaks0, "mixed path")},
+                    "fp64": {"value": tb2 * st_ / (f["ms"] * 1e-3), "unit": UNIT, "ms_per_step": f["ms"] / st_,
+                             "stage_ms_per_step": {k: round(v, 4) for k, v in f["stage"].items()}},
+                    "mixed_speedup_vs_fp64": f["ms"] / m["ms"],
+                    "mixed_v3_speedup_vs_fp64": f["stage"]["v3"] / max(m["stage"]["v3"], 1e-9),
+                    "kappa_rel_err_mixed_vs_fp64": float(np.abs(km - kf).max() / np.abs(kf).max()),
+                    "clocks": m["clocks"]}
+                t2.cleanup()
+            except Exception as ex:  # reported beside the headline, never required
+                extras[wl] = {"failed": str(ex)[:300]}
 
     line = None
     if rank == 0:
@@ -346,6 +434,8 @@ def main():
         mixed_head = precisions[-1] == ald.MIXED
         rf = roofline(per_step, per_launch_counts, nibz, nkc, b, peaks, cg_iters=max(1, out["cg_iters"]),
                       cm_bytes=4 if mixed_head else 8)
+        rf_v3 = v3_roofline(per_step, per_launch_counts, nibz, nkc, b, peaks,
+                            "mixed path" if mixed_head else "fp64 path")
         cb = None
         if world == 1 and not args.no_cpu_baseline:
             try:
@@ -355,7 +445,7 @@ def main():
                 cb = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port", "sample": "failed: %s" % ex}
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
-                "scaling": "weak", "vs_baseline": None,
+                "scaling": "strong", "vs_baseline": None,
                 "dtype": ("mixed: V3 class sums split-f16 on tensor cores (3 bands) or f32, mode products, delta "
                           "weights and CG matrix f32; eigensolve, sums, CG vectors and kappa f64")
                 if mixed_head else "f64",
@@ -365,19 +455,21 @@ def main():
                            "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
                            "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
                                2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * (4 if mixed_head else 8) / 1e6),
-                           "parallelism": "replicas" if world > 1 else "single GPU"},
+                           "parallelism": ("dp%d: IBZ rows sharded as the reference's MPI split, NCCL all-gathers "
+                                           "of Q and the CG products" % world) if world > 1 else "single GPU"},
                 "time_to_kappa_ms": ms_max / args.steps,
                 "stage_ms_per_step": {k: round(v, 4) for k, v in per_step.items()},
                 "kappa_cg_trace_over_3": float(np.trace(out["kappa_cg"]) / 3),
                 "cg_iters": out["cg_iters"],
                 "e2e": {"value": e2e, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                         "seconds_per_step": sorted(e2e_times)[len(e2e_times) // 2]},
-                "gpu_launches": launches, "roofline": rf, "cpu_baseline": cb, "clocks": clk_summary}
+                "gpu_launches": launches, "roofline": rf, "roofline_v3": rf_v3, "cpu_baseline": cb,
+                "clocks": clk_summary}
         if ald.FP64 in runs and ald.MIXED in runs:
             f, m = runs[ald.FP64], runs[ald.MIXED]
             kf, km = np.asarray(f["out"]["kappa_cg"]), np.asarray(m["out"]["kappa_cg"])
             krf, krm = np.asarray(f["out"]["kappa_rta"]), np.asarray(m["out"]["kappa_rta"])
-            line["fp64"] = {"value": world * tb * args.steps / (f["ms"] * 1e-3), "unit": UNIT,
+            line["fp64"] = {"value": tb * args.steps / (f["ms"] * 1e-3), "unit": UNIT,
                             "ms_per_step": f["ms"] / args.steps,
                             "stage_ms_per_step": {k: round(v, 4) for k, v in f["stage"].items()},
                             "clocks": f["clocks"]}
@@ -386,6 +478,8 @@ def main():
             line["kappa_rel_err_mixed_vs_fp64"] = {
                 "cg": float(np.abs(km - kf).max() / np.abs(kf).max()),
                 "rta": float(np.abs(krm - krf).max() / np.abs(krf).max())}
+        if extras:
+            line["extra_workloads"] = extras
         print(json.dumps(line))
     tmp.cleanup()
     if world > 1:

@@ -279,9 +279,23 @@ int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa
 typedef int (*ald_allgather_fn)(void* user, const double* mine, long long count, double* all,
                                 const long long* counts, int nranks);
 int ald_shard_rows(const ald_ctx* ctx, int rank, int nranks, int ksubset[2]);
+/* The same exchange on device buffers, for NCCL-style all-gathers that stay
+ * in GPU memory: `mine` (count values) and `all` are device pointers of this
+ * rank's GPU, and the gather must be ordered after the work already queued on
+ * `stream` (the context's cudaStream_t) and before the work queued after it
+ * returns -- e.g. enqueued on that stream; no host copy and no host
+ * synchronisation of the exchange is needed.  The CG still reads its stop
+ * flag on the host once per iteration, so every rank takes the same steps. */
+typedef int (*ald_allgather_dev_fn)(void* user, const double* mine, long long count, double* all,
+                                    const long long* counts, int nranks, void* stream);
 int ald_kappa_pipeline_sharded(ald_ctx* ctx, double tempk, int rank, int nranks, ald_allgather_fn gather,
                                void* user, ald_kappa_result* res, double* Q, double* QN, double* QU,
                                double* kappa_rta_modes, double* kappa_cg_modes, double* x);
+/* ald_kappa_pipeline_sharded with the device all-gather (replaces the same
+ * MPI_Allgatherv calls, kappa.f90:641-643, 790). */
+int ald_kappa_pipeline_sharded_dev(ald_ctx* ctx, double tempk, int rank, int nranks, ald_allgather_dev_fn gather,
+                                   void* user, ald_kappa_result* res, double* Q, double* QN, double* QU,
+                                   double* kappa_rta_modes, double* kappa_cg_modes, double* x);
 
 /* The job=3 sequence (kappa.f90:1046-1487): as ald_kappa_pipeline up to the
  * RTA kappa, then from FFF = F_RTA repeat FFF += update_mix (update_mpi(FFF)

@@ -170,3 +170,33 @@ def test_rocksalt192_v3_fgr_pipeline(rs192, ald_lib, oracle_lib):
     assert ok, ("pipeline Q", worst)
     assert np.all(np.isfinite(out["kappa_cg"]))
     ctx.close()
+
+
+@pytest.mark.parametrize("which", ["sl24", "rs192"])
+def test_large_mixed_tensor_cores(which, sl24, rs192, ald_lib):
+    """ALD_MIXED above 12 bands: both mode products as split-FP16 tcgen05
+    GEMMs (ald_v3_dense_tc.cu) against the FP64 oracle on the same
+    eigenpairs; |V3|^2 normwise within 1e-4, and the pipeline's Q per mode
+    within 1e-4 (+1e-8 max|Q|) of the FP64 pipeline's."""
+    d, O, ph = sl24 if which == "sl24" else rs192
+    rows = (2, 3) if which == "sl24" else (O.nibz, O.nibz)
+    v33 = O.v3(*rows) if which == "sl24" else oracle_dense.v3_factorised(O, *rows)
+    keep = ~gamma_acoustic_mask(O, ph[0], *rows)
+    delta = ald_lib.DELTA_TETRA
+    ctx = ald_lib.Context(d, ald_lib.default_options(precision=ald_lib.MIXED, delta=delta))
+    ctx.set_phonons(*ph)
+    v = ctx.calculate_w3_ibz_split_sq(list(rows))
+    err = np.linalg.norm(v[keep] - v33[keep]) / np.linalg.norm(v33[keep])
+    print(which, "tensor-core |V3|^2 normwise", err)
+    assert err <= 1e-4, err
+    out = ctx.kappa_pipeline(300.0)
+    ctx.close()
+    ref = ald_lib.Context(d, ald_lib.default_options(precision=ald_lib.FP64, delta=delta))
+    ref.set_phonons(*ph)
+    r = ref.kappa_pipeline(300.0)
+    ref.close()
+    eq = np.abs(out["Q"] - r["Q"]) / (np.abs(r["Q"]) + 1e-8 * np.abs(r["Q"]).max())
+    print(which, "mixed Q worst", eq.max())
+    assert eq.max() <= 1e-4
+    k, kr = out["kappa_cg"], r["kappa_cg"]
+    assert np.abs(k - kr).max() <= 1e-4 * np.abs(kr).max()
