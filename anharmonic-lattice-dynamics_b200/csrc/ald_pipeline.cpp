@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstring>
 #include <string>
@@ -481,6 +482,18 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
   return run_pipeline(c, tempk, res, Qo, QNo, QUo, kappa_rta_modes, kappa_cg_modes, xo, nullptr);
 }
 
+// the pipeline workspaces of a context (their blocks go to the library's
+// device-memory cache, where the next structure of the same sizes finds them)
+static void release_pipeline_workspaces(ald_ctx* c) {
+  for (DevBuf<double>* b : {&c->w_R1, &c->w_R2, &c->w_v3, &c->w_cm, &c->w_R1p, &c->w_R2p, &c->w_heev})
+    b->free();
+  c->w_h.free();
+  c->w_v3work.free();
+  c->v3work_tc_b = 0;
+  c->w_btiles.free();
+  c->w_scratch.free();
+}
+
 extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res,
                                  int* status) {
   if (n <= 0 || !ctx || !tempk || !res) return fail(ALD_ERR_ARG, "bad argument");
@@ -489,16 +502,38 @@ extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk
     for (int j = 0; j < i; ++j)
       if (ctx[j] == ctx[i]) return fail(ALD_ERR_ARG, "a context appears twice in the batch");
   }
-  // one host thread per structure: each context issues its work on its own
-  // stream, so the structures' kernels overlap on the device
+  // A pool of host threads, each issuing one structure at a time on that
+  // structure's own stream, so that structures overlap on the device; the
+  // largest (nibz nkc b^3) go first.  A batch larger than the pool keeps
+  // device memory bounded: after its run a structure's pipeline workspaces
+  // return to the library's device-memory cache for the next one.
+  const int pool = std::min(n, 8);
+  std::vector<int> order(n);
+  for (int i = 0; i < n; ++i) order[i] = i;
+  auto work = [&](int i) {
+    const ald_ctx* c = ctx[i];
+    return (double)c->T.nibz * c->T.nkc * (double)c->geo.b * c->geo.b * c->geo.b;
+  };
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
   std::vector<int> st(n, ALD_OK);
   std::vector<std::string> msg(n);
+  std::atomic<int> next{0};
   std::vector<std::thread> th;
-  th.reserve(n);
-  for (int i = 0; i < n; ++i)
-    th.emplace_back([&, i] {
-      st[i] = run_pipeline(ctx[i], tempk[i], &res[i], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
-      if (st[i] != ALD_OK) msg[i] = ald_last_error();
+  th.reserve(pool);
+  for (int t = 0; t < pool; ++t)
+    th.emplace_back([&] {
+      for (;;) {
+        const int k = next.fetch_add(1);
+        if (k >= n) break;
+        const int i = order[k];
+        st[i] = run_pipeline(ctx[i], tempk[i], &res[i], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                             nullptr);
+        if (st[i] != ALD_OK) msg[i] = ald_last_error();
+        if (n > pool) {
+          cudaSetDevice(ctx[i]->device);
+          release_pipeline_workspaces(ctx[i]);
+        }
+      }
     });
   for (auto& t : th) t.join();
   int first = ALD_OK;

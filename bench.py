@@ -55,6 +55,89 @@ WORKLOADS = {
                         "of the batched suite, %dx%dx%d q-mesh, tetrahedron delta, T=300 K"),
 }
 CONFIG_OF = {"rocksalt": 1, "lj-argon": 2, "rocksalt-192": 4}
+# the batched suites: many structures of uneven size in one ald_kappa_batched call
+SUITES = {
+    "suite3": "64 LJ argon mass superlattices, fcc conventional cell x p along x (p = 1..8, 8 structures each, "
+              "12-96 bands, layer masses U[20,80] amu from seed 20261203 + s), (ceil(12/p) >= 2) x 12 x 12 mesh, "
+              "lattice IBZ (none for the odd 3 x 12 x 12 meshes of p = 4, 5), Gaussian 0.1 THz, T=300 K",
+    "suite4": "rock-salt Morse 64-atom cells (192 bands) with seeded jitter (D +-20 %%, alpha +-10 %%, masses "
+              "U[10,130] amu), %d structures, %dx%dx%d mesh, tetrahedron delta, T=300 K",
+}
+
+
+def suite_dirs(root: str, suite: str, nstruct: int = 0, mesh_edge: int = 0):
+    """Input directories of a batched suite (written once under root)."""
+    from ald import inputs as I
+    out = []
+    if suite == "suite3":
+        k = 0
+        for p in range(1, 9):
+            for j in range(8):
+                st, rp = I.config(3, p=p, s=k)
+                if rp.mesh[0] % 2:
+                    rp.ibz = "none"
+                d = os.path.join(root, "s3_%02d" % k)
+                I.write_inputs(st, rp, d)
+                out.append(d)
+                k += 1
+    else:
+        n = nstruct or 2
+        m = mesh_edge or 4
+        for k in range(n):
+            st, rp = I.config(4, mesh=(m, m, m), s=k)
+            d = os.path.join(root, "s4_%02d" % k)
+            I.write_inputs(st, rp, d)
+            out.append(d)
+    return out
+
+
+def run_suite(args, suite: str):
+    """A batched suite: ald_kappa_batched over all structures (mixed and FP64)
+    against the same structures one after another; aggregate triplet-bands/s
+    of the whole batch, device time of the call (CUDA events bracket it on the
+    default stream after a device synchronize)."""
+    import numpy as np
+    import torch
+
+    import ald
+    tmp = tempfile.TemporaryDirectory()
+    dirs = suite_dirs(tmp.name, suite, args.suite_n, args.mesh)
+    res = {}
+    for prec, name in ((ald.MIXED, "mixed"), (ald.FP64, "fp64")):
+        ctxs = [ald.Context(d, ald.default_options(precision=prec, delta=ald.DELTA_TETRA if suite == "suite4"
+                                                   else ald.DELTA_GAUSS)) for d in dirs]
+        tempk = [c.info.tempk for c in ctxs]
+        out, st = ald.kappa_batched(ctxs, tempk)  # warm-up: phonons, workspaces, graphs
+        tb = sum(o["triplet_bands"] for o in out)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out, st = ald.kappa_batched(ctxs, tempk)
+        torch.cuda.synchronize()
+        tbat = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        seq = [c.kappa_pipeline(tk, want_modes=False) for c, tk in zip(ctxs, tempk)]
+        torch.cuda.synchronize()
+        tseq = time.perf_counter() - t0
+        res[name] = {"batched_s": tbat, "sequential_s": tseq, "batched_value": tb / tbat,
+                     "sequential_value": tb / tseq, "speedup_batched_vs_sequential": tseq / tbat,
+                     "status": st, "kappa_trace_over_3": [float(np.trace(o["kappa_cg"]) / 3) for o in out],
+                     "kappa_rel_diff_batched_vs_sequential": float(max(
+                         np.abs(o["kappa_cg"] - q["kappa_cg"]).max() / np.abs(q["kappa_cg"]).max()
+                         for o, q in zip(out, seq)))}
+        for c in ctxs:
+            c.close()
+        ald.release_cached_memory()
+    km, kf = np.array(res["mixed"]["kappa_trace_over_3"]), np.array(res["fp64"]["kappa_trace_over_3"])
+    desc = SUITES[suite] if suite == "suite3" else SUITES[suite] % (len(dirs), args.mesh or 4, args.mesh or 4,
+                                                                     args.mesh or 4)
+    line = {"metric": METRIC, "value": res["mixed"]["batched_value"], "unit": UNIT, "n_gpus": 1, "steps": 1,
+            "warmup": 1, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+            "dtype": "mixed (tensor-core V3 above 12 bands) and f64", "data": "synthetic (analytic FC2/FC3)",
+            "config": {"workload": desc, "structures": len(dirs), "triplet_bands": tb}, "mixed": res["mixed"],
+            "fp64": res["fp64"], "mixed_speedup_vs_fp64_batched": res["fp64"]["batched_s"] / res["mixed"]["batched_s"],
+            "kappa_rel_err_mixed_vs_fp64": float(np.abs(km - kf).max() / np.abs(kf).max())}
+    print(json.dumps(line))
+    tmp.cleanup()
 
 
 def _peaks():
@@ -241,13 +324,20 @@ def main():
     ap.add_argument("--impl", default="ald", choices=["ald", "reference"])
     ap.add_argument("--precision", default="both", choices=["fp64", "mixed", "both"],
                     help="both: time the FP64 and the mixed path; the line's value is the mixed path's")
-    ap.add_argument("--workload", default="rocksalt", choices=sorted(WORKLOADS),
+    ap.add_argument("--suite-n", type=int, default=0, help="suite4: number of structures (default 2)")
+    ap.add_argument("--workload", default="rocksalt", choices=sorted(WORKLOADS) + sorted(SUITES),
                     help="rocksalt: the metric's configuration (default); lj-argon: the large single structure")
     ap.add_argument("--mesh", type=int, default=0, help="mesh edge (default: the workload's own)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the extra driver-timed workloads (32^3 argon, the 192-band cell)")
     args = ap.parse_args()
+
+    if args.workload in SUITES:
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the batched suites are timed on the GPU only"}))
+            return
+        return run_suite(args, args.workload)
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

@@ -198,7 +198,8 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
  * stream) and the call returns after it finished.  Nothing is allocated: the
  * CG work vectors live in a fixed __device__ array of the library, so
  * n <= ALD_CG_STATIC_MAX_N (ALD_ERR_ARG otherwise).  The first call on a
- * device looks that array's address up; make it before any stream capture.
+ * device looks that array's address up and keeps it for the life of the
+ * process; make that first call before any stream capture.
  * Calls share the array: calls that overlap on one device race.  Returns
  * ALD_OK or ALD_WARN_CG_MAXITER like ald_cg_quadratic. */
 #define ALD_CG_STATIC_MAX_N 32768
@@ -253,12 +254,17 @@ int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double
                        double* kappa_rta_modes, double* kappa_cg_modes, double* x);
 
 /* ald_kappa_batched: ald_kappa_pipeline on n structures at once (the batched
- * configurations of many small cells), one host thread per context; each
- * context runs on its own stream, so the structures' kernels overlap on the
- * device.  tempk[n], res[n]; status[n] (may be NULL) receives each
- * structure's return code.  Returns ALD_OK, or the first structure's error
- * (ald_last_error names the structure).  The contexts must be distinct; each
- * structure's limits are those of ald_kappa_pipeline (at most 12 bands). */
+ * configurations of many cells of uneven size), no reference counterpart:
+ * the reference runs one structure per kappa_full run.  A pool of up to 8
+ * host threads takes the structures largest first (nibz nkc ndyn^3), each on
+ * its context's own stream, so the structures' kernels overlap on the
+ * device; when n exceeds the pool, a structure's pipeline workspaces are
+ * released after its run (to the library's device-memory cache), which
+ * bounds device memory by the pool.  tempk[n], res[n]; status[n] (may be
+ * NULL) receives each structure's return code.  Returns ALD_OK, or the first
+ * structure's error (ald_last_error names the structure).  The contexts must
+ * be distinct; each structure's limits are those of ald_kappa_pipeline (up
+ * to 256 bands). */
 int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res, int* status);
 
 /* Row-sharded job=1, one call per rank (one process per GPU): the MPI

@@ -62,3 +62,32 @@ def test_device_memory_cache_reuse_and_release(ald_lib, workdir):
         assert r["cg_iters"] == runs[0]["cg_iters"]
         for k in ("kappa_rta", "kappa_cg"):
             assert np.allclose(r[k], runs[0][k], rtol=1e-12, atol=1e-14 * np.abs(runs[0][k]).max())
+
+
+def test_batched_uneven_sizes_against_oracle(ald_lib, oracle_lib, workdir):
+    """Three structures of uneven size in one ald_kappa_batched call -- the
+    rock-salt cell (6 bands), the 4-atom LJ cell (12 bands) and the 8-atom
+    superlattice (24 bands, the large-cell kernels) -- each against the
+    oracle's job=1 run on the same eigenpairs: Q to 1e-10, kappa to 1e-10
+    (floor 1e-10 max|kappa|), the same CG iterations."""
+    from test_gpu_parity import close
+    cases = [(1, (4, 4, 4), {}), (3, (4, 4, 4), {"delta": "gauss", "width_cm": 5.0, "rc_sigma": 1.2}),
+             (3, (2, 4, 4), {"p": 2, "rc_sigma": 1.2, "delta": "gauss", "width_cm": 5.0})]
+    refs, ctxs = [], []
+    for cfg, mesh, kw in cases:
+        d = make_case(workdir, cfg, mesh, **kw)
+        ref = oracle_lib.run_job1(d)
+        ctx = ald_lib.Context(d)
+        ctx.set_phonons(*ref["O"].get_phonons())
+        refs.append(ref)
+        ctxs.append(ctx)
+    out, st = ald_lib.kappa_batched(ctxs, [r["tempk"] for r in refs])
+    assert st == [0] * len(cases)
+    for o, r, c in zip(out, refs, ctxs):
+        assert c.ndyn in (6, 12, 24)
+        assert o["cg_iters"] == r["cg_iters"]
+        for key, rk in (("kappa_rta", "kappa_rta"), ("kappa_cg", "kappa_cg")):
+            ok, worst = close(o[key], r[rk].sum(0), atol=1e-10)
+            assert ok, (c.ndyn, key, worst)
+    for c in ctxs:
+        c.close()

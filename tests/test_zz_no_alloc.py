@@ -6,9 +6,10 @@ inside another framework's allocator): they pass device buffers and the
 library allocates nothing, keeping its CG work vectors in a fixed __device__
 array.  Its results must equal those of the allocating entry point
 ald_cg_quadratic on the same system, within the CG tolerance of the other
-parity tests (rtol 1e-8, atol 1e-10 of the largest entry), on two calls in a
-row -- the second of a different size, so that a call never depends on what
-the previous one left in the shared array.
+parity tests (rtol 1e-10, atol 1e-10 of the largest entry), on two calls in
+a row -- the second of a different size, so that a call never depends on
+what the previous one left in the shared array -- and the second call must
+leave the device's free memory exactly as it found it.
 
 This file is collected last so that a run stopping at its first failure has
 already run every other test.
@@ -32,7 +33,7 @@ def _spd_system(n, seed):
     return A, b, x0
 
 
-def _close(g, r, rtol=1e-8, atol=1e-10):
+def _close(g, r, rtol=1e-10, atol=1e-10):
     scale = np.abs(r).max()
     return bool(np.all(np.abs(g - r) <= rtol * np.abs(r) + atol * scale))
 
@@ -49,8 +50,12 @@ def test_cg_static_matches_allocating_entry_point(ald_lib):
         dA = torch.from_numpy(np.ascontiguousarray(A.T)).to(dev)
         db = torch.from_numpy(b.copy()).to(dev)
         dx = torch.from_numpy(x0.copy()).to(dev)
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(dev)[0]
         fm, it, st = ald_lib.cg_quadratic_static(n, dA.data_ptr(), db.data_ptr(), dx.data_ptr(), max_iter=100,
                                                  n_dig_accur=ndig, stream=stream.cuda_stream)
+        if call == 1:  # the first call may load the library's module; later calls allocate nothing
+            assert torch.cuda.mem_get_info(dev)[0] == free0
         x = dx.cpu().numpy()
         assert st == st_ref, (call, st, st_ref)
         assert it == it_ref, (call, it, it_ref)
