@@ -79,8 +79,14 @@ __global__ void rta_F_kernel(KappaArgs a, const double* Q, double* F) {
   const double c = PhysConst::c_light, h = PhysConst::h_plank, kb = PhysConst::k_b;
   for (int x = 0; x < 3; ++x) {
     double v = a.vel[((size_t)n0 * b + l) * 3 + x];
-    F[(size_t)idx * 3 + x] = -((((((c * v) * h) * ((omega * c) * 100)) * nb) * (nb + 1)) / (kb * (a.tempk * a.tempk)) /
-                               ((Q[idx] * c) * 100));
+    // zero_q_f: a mode without scattering (Q = 0 exactly) gets F = 0 instead
+    // of a division by zero (the mixed path, where the FP32 weights of the
+    // acoustic modes at Gamma can vanish; those carry no heat, omega v = 0)
+    F[(size_t)idx * 3 + x] =
+        a.zero_q_f && Q[idx] == 0.0
+            ? 0.0
+            : -((((((c * v) * h) * ((omega * c) * 100)) * nb) * (nb + 1)) / (kb * (a.tempk * a.tempk)) /
+                ((Q[idx] * c) * 100));
   }
 }
 

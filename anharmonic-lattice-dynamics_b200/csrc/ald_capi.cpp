@@ -375,6 +375,7 @@ KappaArgs kappa_args(ald_ctx* c, double tempk) {
   k.arm_owner = c->arm_owner.p;
   k.narm = (int)c->T.arm_q.size();
   k.part = c->w_kpart.alloc(kappa_partial_doubles(c->geo.b, k.narm)) == cudaSuccess ? c->w_kpart.p : nullptr;
+  k.zero_q_f = c->opt.precision != ALD_FP64;
   return k;
 }
 

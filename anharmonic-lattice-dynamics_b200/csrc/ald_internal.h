@@ -272,6 +272,7 @@ struct V3Args {
   double* v3sq;              // v3_layout 0: [row][q2][l1][l2][l3] (the reference's order, per row)
   int v3_layout;             //           1: [row][l2][l3][l1][q2] (slices of the delta, q2 fastest)
                              //           2: [row][l2][l3][q2][l1] (large cells, tensor-core V3)
+  float* v3sq_f32 = nullptr; // the tensor-core V3 writes FP32 here instead of v3sq when set
   int* err;
   // phase classes (pair kernel)
   int ncls;
@@ -325,6 +326,7 @@ struct CombineArgs {
   const int* mapinv;
   const double* v3sq;        // v3_layout 0: [row][q2][l1][l2][l3]; 1: [row][l2][l3][l1][q2]
   int v3_layout;
+  const float* v3sq_f32 = nullptr;  // FP32 |V3|^2 in place of v3sq (band-generic kernels only)
   const double* freq;        // [q][l]
   const double* dist;        // [q][l]
   const int* tet_corner;
@@ -380,6 +382,7 @@ struct KappaArgs {
   const int* arm_owner;      // per arm (arm_q entry): its IBZ point
   int narm;                  // arm_off[nibz]
   double* part;              // scratch: kappa_partial_doubles(b, narm) (per-CTA partial sums)
+  int zero_q_f = 0;          // 1: F_RTA = 0 where Q = 0 (mixed path); 0: the reference's division
 };
 size_t kappa_partial_doubles(int b, int narm);
 cudaError_t launch_rta_F(const KappaArgs& a, const double* Q, double* FFF, cudaStream_t s);

@@ -183,9 +183,13 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     ALD_CKA(c->w_R2p.alloc(rsz));
   }
   ALD_CKA(Q.alloc((size_t)3 * nibz * b));
-  const int K = rows_per_chunk(c);
-  ALD_CKA(v3.alloc((size_t)K * nkc * b * b * b));
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
+  // the large-cell tensor-core V3 hands |V3|^2 to the delta in FP32 (layout
+  // 2): half the bytes, twice the rows per chunk
+  const bool v3f = v3_pipeline_layout(b, c->opt.precision) == 2;
+  const int K = v3f ? std::min(nibz, 2 * rows_per_chunk(c)) : rows_per_chunk(c);
+  const size_t v3n = (size_t)K * nkc * b * b * b;
+  ALD_CKA(v3.alloc(v3f ? (v3n + 1) / 2 : v3n));
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
   // class-form V3 kernels write that layout; the large-cell tensor-core V3
@@ -203,6 +207,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     ALD_CK(tm.begin(1));
     V3Args va = v3_args(c, r0, nr, v3.p);
     va.v3_layout = v3_layout;
+    if (v3f) va.v3sq_f32 = reinterpret_cast<float*>(v3.p);
     r = run_v3(c, va, &res->launches[1]);
     if (r) return r;
     ALD_CK(tm.end());
@@ -213,6 +218,7 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
     a.mapinv = c->mapinv.p;
     a.v3sq = v3.p;
     a.v3_layout = v3_layout;
+    a.v3sq_f32 = v3f ? reinterpret_cast<const float*>(v3.p) : nullptr;
     a.freq = c->freq.p;
     a.dist = c->dist.p;
     a.tet_corner = c->tet_corner.p;

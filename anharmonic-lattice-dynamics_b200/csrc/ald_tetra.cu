@@ -725,8 +725,8 @@ __global__ void __launch_bounds__(kFusedThreads) delta_fused_kernel(CombineArgs 
 //   R(row, w, l1, l2)           += that * n1 G(w)                       (if given)
 // with G and the Gamma-acoustic zeros of the fused kernel.  FP64 atomics:
 // the sums agree with the reference to FP64 rounding, not bitwise.
-template <bool F32W>
-__global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
+template <bool F32W, class VT>
+__global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a, const VT* __restrict__ v3sq) {
   extern __shared__ double s_any[];  // omega1[b], n1[b]
   const Geometry& g = a.geo;
   const int b = g.b, nkc = g.nkc, b2 = b * b;
@@ -794,7 +794,7 @@ __global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
     s1 = (size_t)b2;
     sq = (size_t)b2 * b;
   }
-  const double* v3 = a.v3sq + (size_t)row * nkc * b2 * b + l2 * s2 + l3 * s3;
+  const VT* v3 = v3sq + (size_t)row * nkc * b2 * b + l2 * s2 + l3 * s3;
   double* Ps = proc == 0 ? a.P1s : a.P2s;
   double* Rp = proc == 0 ? a.R1 : a.R2;
   double* Rpp = proc == 0 ? a.R1p : a.R2p;
@@ -815,7 +815,7 @@ __global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
     for (int k = 0; k < 4; ++k) {
       const double cw = cp[pos[k]];
       if (cw == 0.0 || G[k] < 0.0) continue;
-      const double ps = (cw / 6.0) * (__ldg(v3 + (size_t)src[k] * sq + l1 * s1) * fnorm);
+      const double ps = (cw / 6.0) * ((double)__ldg(v3 + (size_t)src[k] * sq + l1 * s1) * fnorm);
       const size_t w = (size_t)row * nkc + c[k];
       if (Ps) atomicAdd(Ps + (w * b + l1) * b2 + l2 * b + l3, ps);
       if (Rp) {
@@ -830,8 +830,8 @@ __global__ void __launch_bounds__(256) delta_tet_any_kernel(CombineArgs a) {
 // Gaussian: a thread per (row, w, l1, l2), w fastest; the sums over l3 of
 // both processes (R1, R2 at w) in registers, P1s/P2s written when given.
 // The Gaussian is delta_g of extratools.f90:239 as in delta_point_kernel.
-template <bool F32W>
-__global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
+template <bool F32W, class VT>
+__global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a, const VT* __restrict__ v3sq) {
   const Geometry& g = a.geo;
   const int b = g.b, nkc = g.nkc, b2 = b * b, b3 = b2 * b;
   // x: (l1, l2, w), w fastest for layouts 0/1 (|V3|^2 runs of q2), l1
@@ -861,7 +861,7 @@ __global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
   const double fnorm = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc;
   const double om1 = a.freq[(size_t)q1 * b + l1], nb1 = a.dist[(size_t)q1 * b + l1];
   const double n2 = a.dist[(size_t)w * b + l2], w2 = a.freq[(size_t)w * b + l2];
-  const double* v3 = a.v3sq + (size_t)row * nkc * b3;
+  const VT* v3 = v3sq + (size_t)row * nkc * b3;
   const int L = a.v3_layout;
   const size_t sq = L == 1 ? 1 : (L == 2 ? (size_t)b : (size_t)b3);
   const size_t s1 = L == 1 ? (size_t)nkc : (L == 2 ? 1 : (size_t)b2);
@@ -886,7 +886,7 @@ __global__ void __launch_bounds__(128) delta_gauss_any_kernel(CombineArgs a) {
         if (arg < 746.0) wl = exp(-arg) * gc2;
       }
       double ps = 0.0;
-      if (wl != 0.0 && !zero) ps = wl * (v3[(size_t)src * sq + l1 * s1 + l2 * s2 + l3 * s3] * fnorm);
+      if (wl != 0.0 && !zero) ps = wl * ((double)v3[(size_t)src * sq + l1 * s1 + l2 * s2 + l3 * s3] * fnorm);
       const double p = ps * (proc == 0 ? nb1 * n2 * (n3 + 1) : nb1 * (n2 + 1) * (n3 + 1));
       R[proc] += p;
       double* Rpm = proc == 0 ? a.R1p : a.R2p;
@@ -1037,16 +1037,26 @@ cudaError_t launch_delta_any(const CombineArgs& a, cudaStream_t s) {
     const long long nx = ((long long)g.nkc * g.b * g.b + 127) / 128;
     if (nx > 2147483647LL || a.nrows > 65535) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)nx, a.nrows);
-    if (a.f32w) delta_gauss_any_kernel<true><<<grid, 128, 0, s>>>(a);
-    else delta_gauss_any_kernel<false><<<grid, 128, 0, s>>>(a);
+    if (a.v3sq_f32) {
+      if (a.f32w) delta_gauss_any_kernel<true, float><<<grid, 128, 0, s>>>(a, a.v3sq_f32);
+      else delta_gauss_any_kernel<false, float><<<grid, 128, 0, s>>>(a, a.v3sq_f32);
+    } else {
+      if (a.f32w) delta_gauss_any_kernel<true, double><<<grid, 128, 0, s>>>(a, a.v3sq);
+      else delta_gauss_any_kernel<false, double><<<grid, 128, 0, s>>>(a, a.v3sq);
+    }
   } else {
     const long long nslice = (long long)a.nrows * g.b * g.b * 2;
     if (nslice > 2147483647LL) return cudaErrorInvalidValue;
     if ((6LL * g.nkc + 255) / 256 > 65535) return cudaErrorInvalidValue;
     const dim3 grid((unsigned)nslice, (6 * g.nkc + 255) / 256);
     const size_t smem = 2 * (size_t)g.b * sizeof(double);
-    if (a.f32w) delta_tet_any_kernel<true><<<grid, 256, smem, s>>>(a);
-    else delta_tet_any_kernel<false><<<grid, 256, smem, s>>>(a);
+    if (a.v3sq_f32) {
+      if (a.f32w) delta_tet_any_kernel<true, float><<<grid, 256, smem, s>>>(a, a.v3sq_f32);
+      else delta_tet_any_kernel<false, float><<<grid, 256, smem, s>>>(a, a.v3sq_f32);
+    } else {
+      if (a.f32w) delta_tet_any_kernel<true, double><<<grid, 256, smem, s>>>(a, a.v3sq);
+      else delta_tet_any_kernel<false, double><<<grid, 256, smem, s>>>(a, a.v3sq);
+    }
   }
   return cudaGetLastError();
 }

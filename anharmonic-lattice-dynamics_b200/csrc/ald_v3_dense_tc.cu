@@ -90,6 +90,7 @@ struct DenseTc {
   __half* a2;    // [pair][A operand] of GEMM 2 (T2); padding stays zero
   __half* bq;    // [q][B operand]: e(q) in real block form
   int* rexp;     // per row of the chunk: e1 (sum_c |H| <= 2^e1)
+  double* tq;    // [q][l]: 1/sqrt|lambda| of every mesh mode (+inf where lambda = 0)
   DenseTcShape sh;
 };
 
@@ -203,6 +204,13 @@ __global__ void v3tc_rowbound_kernel(V3Args a, unsigned* bound) {
   }
   for (int o = 16; o > 0; o >>= 1) mx = fmaxf(mx, __shfl_xor_sync(0xffffffffu, mx, o));
   if ((threadIdx.x & 31) == 0 && mx > 0.f) atomicMax(bound + row, __float_as_uint(mx));
+}
+
+__global__ void v3tc_modes_kernel(V3Args a, double* tq) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= a.geo.nkc * a.geo.b) return;
+  const double w = fabs(a.w2[i]);
+  tq[i] = w != 0.0 ? 1.0 / sqrt(w) : 1.0 / 0.0;
 }
 
 __global__ void v3tc_rowexp_kernel(int nrows, const unsigned* bound, int* rexp) {
@@ -458,7 +466,35 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
         const float f = ldexpf(1.f, -et - kSplitE);
         const int l1 = live ? m / b : 0, kc = live ? m % b : 0;
         __half* A2 = t.a2 + (size_t)p * s.a_pair_halves;
-        for (int cg = 0; cg < s.nh / 8; ++cg) {
+        // b a multiple of 8: every aligned group of 8 rows is 8 consecutive kc
+        // of one l1, i.e. one 16-byte K group of an A2 row.  The warp stages
+        // its 32 x 8 values in shared memory (the stages are free once the
+        // MMAs completed) and each lane stores one group of one column.
+        float* scr = reinterpret_cast<float*>(smraw) + (warp - 2) * 32 * 9;
+        const int grp = lane >> 3, gi = lane & 7;
+        const int mg = mt * kTM + quad * 32 + 8 * grp;
+        for (int cg = 0; cg < s.nh / 8 && (b & 7) == 0; ++cg) {
+          float vr[8], vi[8];
+          tmem_ld8(taddr + (uint32_t)(8 * cg), vr);
+          tmem_ld8(taddr + (uint32_t)(s.nh + 8 * cg), vi);
+#pragma unroll
+          for (int part = 0; part < 2; ++part) {
+            __syncwarp();
+#pragma unroll
+            for (int j = 0; j < 8; ++j) scr[lane * 9 + j] = (part ? vi[j] : vr[j]) * f;
+            __syncwarp();
+            float x[8];
+#pragma unroll
+            for (int jj = 0; jj < 8; ++jj) x[jj] = scr[(8 * grp + jj) * 9 + gi];
+            const int l2 = 8 * cg + gi;
+            if (mg < b * b && l2 < b) {
+              const int m2 = l2 * b + mg / b, kc0 = mg % b;
+              __half* dst = A2 + a_off(s, m2, (part ? s.kh : 0) + kc0);
+              split8(x, dst, dst + (size_t)kTM * kBK);
+            }
+          }
+        }
+        for (int cg = 0; cg < s.nh / 8 && (b & 7) != 0; ++cg) {
           float vr[8], vi[8];
           tmem_ld8(taddr + (uint32_t)(8 * cg), vr);
           tmem_ld8(taddr + (uint32_t)(s.nh + 8 * cg), vi);
@@ -478,11 +514,13 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
           }
         }
       } else {
-        // V = acc / (2^(13-e1-et) 2^13); |V|^2 const33^2 / (8 sqrt|l1 l2 l3|)
-        const double u = ldexp(1.0, e1 + et - 2 * kSplitE);
+        // V = acc / (2^(13-e1-et) 2^13), |V|^2 in FP32, then the FP64 factor
+        // const33^2 / (8 sqrt|l1 l2 l3|) from the per-mode 1/sqrt|l|
+        const float u = ldexpf(1.f, e1 + et - 2 * kSplitE);
         const int l2 = live ? m / b : 0, l1 = live ? m % b : 0;
-        const double c33 = a.const33 * a.const33 / 8;
-        const double w12 = live ? a.w2[(size_t)pi.q1 * b + l1] * a.w2[(size_t)pi.q2 * b + l2] : 0.0;
+        const double c12 = live ? a.const33 * a.const33 / 8 * t.tq[(size_t)pi.q1 * b + l1] * t.tq[(size_t)pi.q2 * b + l2]
+                                : 0.0;
+        const double* t3 = t.tq + (size_t)pi.q3 * b;
         const size_t nkc = g.nkc;
         for (int cg = 0; cg < s.nh / 8; ++cg) {
           float vr[8], vi[8];
@@ -493,15 +531,17 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
           for (int j = 0; j < 8; ++j) {
             const int l3 = 8 * cg + j;
             if (l3 >= b) break;
-            const double w123 = fabs(w12 * a.w2[(size_t)pi.q3 * b + l3]);
+            const double sc = c12 * t3[l3];
             double v = 0.0;
-            if (w123 != 0.0) {
-              const double re = vr[j] * u, im = vi[j] * u;
-              v = (re * re + im * im) * (c33 / sqrt(w123));
+            if (sc < 1.0 / 0.0) {
+              const float re = vr[j] * u, im = vi[j] * u;
+              v = (double)fmaf(re, re, im * im) * sc;
             } else {
               atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
             }
-            a.v3sq[v3_out_off(a.v3_layout, pi.row, pi.q2, l1, l2, l3, b, nkc)] = v;
+            const size_t o = v3_out_off(a.v3_layout, pi.row, pi.q2, l1, l2, l3, b, nkc);
+            if (a.v3sq_f32) a.v3sq_f32[o] = (float)v;
+            else a.v3sq[o] = v;
           }
         }
       }
@@ -539,10 +579,10 @@ long long v3_dense_tc_pairs(int b, long long npairs, size_t budget) {
 size_t v3_dense_tc_work_bytes(int b, int nkc, int nrows, long long pairs) {
   const DenseTcShape s = dense_tc_shape(b);
   return (size_t)pairs * 2 * s.a_pair_halves * sizeof(__half) + (size_t)nkc * s.bq_halves * sizeof(__half) +
-         (size_t)nrows * 2 * sizeof(int) + 512;
+         (size_t)nkc * b * sizeof(double) + (size_t)nrows * 2 * sizeof(int) + 512;
 }
 
-int v3_dense_tc_launches(long long npairs, long long pairs) { return 3 + 3 * (int)((npairs + pairs - 1) / pairs); }
+int v3_dense_tc_launches(long long npairs, long long pairs) { return 4 + 3 * (int)((npairs + pairs - 1) / pairs); }
 
 cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long P, bool a2_zeroed, cudaStream_t s) {
   const int b = a.geo.b;
@@ -555,7 +595,8 @@ cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long P, bool a2
   t.a1 = reinterpret_cast<__half*>(w);
   t.a2 = t.a1 + (size_t)P * sh.a_pair_halves;
   t.bq = t.a2 + (size_t)P * sh.a_pair_halves;
-  unsigned* bound = reinterpret_cast<unsigned*>(t.bq + (size_t)a.geo.nkc * sh.bq_halves);
+  t.tq = reinterpret_cast<double*>(t.bq + (size_t)a.geo.nkc * sh.bq_halves);
+  unsigned* bound = reinterpret_cast<unsigned*>(t.tq + (size_t)a.geo.nkc * b);
   t.rexp = reinterpret_cast<int*>(bound + a.nrows);
   cudaError_t e;
   if (!a2_zeroed) {  // GEMM 1's epilogue never writes the padding of A2
@@ -565,6 +606,7 @@ cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long P, bool a2
   e = cudaMemsetAsync(bound, 0, (size_t)a.nrows * sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
   v3tc_bq_kernel<<<a.geo.nkc, 256, 0, s>>>(a, t);
+  v3tc_modes_kernel<<<(a.geo.nkc * b + 255) / 256, 256, 0, s>>>(a, t.tq);
   v3tc_rowbound_kernel<<<dim3(64, a.nrows), 256, 0, s>>>(a, bound);
   v3tc_rowexp_kernel<<<(a.nrows + 127) / 128, 128, 0, s>>>(a.nrows, bound, t.rexp);
   const size_t t1_smem = (size_t)std::max(a.ncls, 1) * sizeof(float2);

@@ -361,7 +361,7 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "strong",
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (analytic %s FC2/FC3, reference file formats)" % (
-                    "Morse" if args.workload == "rocksalt" else "Lennard-Jones"),
+                    "Lennard-Jones" if args.workload == "lj-argon" else "Morse"),
                 "config": {"workload": workload_desc, "mesh": list(mesh)},
                 "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
@@ -540,7 +540,7 @@ def main():
                           "weights and CG matrix f32; eigensolve, sums, CG vectors and kappa f64")
                 if mixed_head else "f64",
                 "data": "synthetic (analytic %s FC2/FC3 written in the reference's file formats)" % (
-                    "Morse" if args.workload == "rocksalt" else "Lennard-Jones"),
+                    "Lennard-Jones" if args.workload == "lj-argon" else "Morse"),
                 "config": {"workload": workload_desc, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
                            "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
                            "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
