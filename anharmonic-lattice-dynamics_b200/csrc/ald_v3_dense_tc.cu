@@ -24,7 +24,8 @@
 // per mesh point B is [chunk][hi|lo][N' x 32].  One CTA computes one
 // 128 x N' tile of one pair: a producer warp streams (A, B) chunks through a
 // ring of shared-memory stages with bulk copies, one thread issues the MMAs
-// (N' <= 256: one accumulator; else two of N'/2 columns), and four epilogue
+// (N = the CTA's columns, one MMA into the Re and one into the Im accumulator per K
+// step and split term), and four epilogue
 // warps read the accumulator: GEMM 1 writes T2, scaled and split, as GEMM 2's
 // A operand; GEMM 2 forms |V|^2 in FP64 and stores the chunk's layout.
 //
@@ -50,12 +51,19 @@ constexpr int kThreads = 64 + 32 * kEpWarps;  // producer, MMA, epilogue warps
 constexpr unsigned kWaitLimit = 1u << 24;
 constexpr int kSplitE = 13;  // operands scaled below 2^14
 
+// Output columns: Nh = b rounded up to 16 (to 32 above 128 bands), in the
+// real block form N' = 2 Nh (Re | Im).  Each CTA takes a contiguous range of
+// `ncol` = Nh / nsplit columns of both parts (nsplit = 2 above 128 bands), as
+// two accumulators of ncol TMEM columns (Re, Im), so that the TMEM (at most
+// 256 columns) and the shared-memory stages of two CTAs fit one SM: one
+// CTA's epilogue then overlaps the other's MMAs.
 struct DenseTcShape {
-  int b, kh, nh, kp, np, nchunk, mtiles, nacc, nmma, tmem_cols, stages;
+  int b, kh, nh, kp, np, nchunk, mtiles, nsplit, ncol, tmem_cols, stages;
   size_t a_block_halves;  // one (M tile, chunk) block: hi + lo
   size_t a_pair_halves;   // one pair's A operand
-  size_t b_chunk_halves;  // one chunk of B: hi + lo
+  size_t b_chunk_halves;  // one chunk of B (global, all N' rows): hi + lo
   size_t bq_halves;       // one mesh point's B operand
+  size_t b_stage_bytes;   // one chunk of a CTA's B rows in shared memory
   size_t stage_bytes, smem;
 };
 
@@ -63,22 +71,23 @@ __host__ __device__ inline DenseTcShape dense_tc_shape(int b) {
   DenseTcShape s;
   s.b = b;
   s.kh = (b + 15) / 16 * 16;
-  s.nh = (b + 15) / 16 * 16;
+  s.nsplit = b > 128 ? 2 : 1;
+  s.nh = s.nsplit == 2 ? (b + 31) / 32 * 32 : (b + 15) / 16 * 16;
+  s.ncol = s.nh / s.nsplit;
   s.kp = 2 * s.kh;
   s.np = 2 * s.nh;
   s.nchunk = s.kp / kBK;
   s.mtiles = (b * b + kTM - 1) / kTM;
-  s.nacc = s.np <= 256 ? 1 : 2;
-  s.nmma = s.np / s.nacc;
   int tc = 32;
-  while (tc < s.np) tc *= 2;
+  while (tc < 2 * s.ncol) tc *= 2;
   s.tmem_cols = tc;
   s.a_block_halves = (size_t)2 * kTM * kBK;
   s.a_pair_halves = (size_t)s.mtiles * s.nchunk * s.a_block_halves;
   s.b_chunk_halves = (size_t)2 * s.np * kBK;
   s.bq_halves = (size_t)s.nchunk * s.b_chunk_halves;
-  s.stage_bytes = (s.a_block_halves + s.b_chunk_halves) * sizeof(__half);
-  int st = (int)((size_t)200 * 1024 / s.stage_bytes);
+  s.b_stage_bytes = (size_t)2 * (2 * s.ncol) * kBK * sizeof(__half);
+  s.stage_bytes = s.a_block_halves * sizeof(__half) + s.b_stage_bytes;
+  int st = (int)((size_t)104 * 1024 / s.stage_bytes);  // two CTAs per SM
   s.stages = st > 4 ? 4 : st;
   s.smem = (size_t)s.stages * s.stage_bytes;
   return s;
@@ -317,6 +326,16 @@ __device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity,
   }
   return false;
 }
+// the epilogue warps wait through the whole main loop: they back off between
+// polls so that the producer and MMA threads keep the issue slots
+__device__ __forceinline__ bool mbar_wait_idle(uint32_t bar, uint32_t parity, const volatile int* fail) {
+  for (unsigned it = 0; it < kWaitLimit / 64; ++it) {
+    if (mbar_try(bar, parity)) return true;
+    if (*fail) return false;
+    __nanosleep(256);
+  }
+  return false;
+}
 __device__ __forceinline__ void expect_tx(uint32_t bar, uint32_t bytes) {
   asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%1], %0;" ::"r"(bytes), "r"(bar) : "memory");
 }
@@ -331,14 +350,22 @@ __device__ __forceinline__ void bulk_copy(uint32_t dst, const void* src, uint32_
                  : "memory");
   }
 }
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float* v) {
-  uint32_t d[8];
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
-               : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7])
-               : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+
+// 16 accumulator columns at ta and 16 at tb (this warp's 32 lanes), one wait
+__device__ __forceinline__ void tmem_ld16x2(uint32_t ta, uint32_t tb, float* va, float* vb) {
+  uint32_t d[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%32];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%33];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]), "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]), "=r"(d[15]), "=r"(d[16]), "=r"(d[17]), "=r"(d[18]), "=r"(d[19]), "=r"(d[20]), "=r"(d[21]), "=r"(d[22]), "=r"(d[23]), "=r"(d[24]), "=r"(d[25]), "=r"(d[26]), "=r"(d[27]), "=r"(d[28]), "=r"(d[29]), "=r"(d[30]), "=r"(d[31])
+      : "r"(ta), "r"(tb)
+      : "memory");
 #pragma unroll
-  for (int i = 0; i < 8; ++i) v[i] = __uint_as_float(d[i]);
+  for (int i = 0; i < 16; ++i) {
+    va[i] = __uint_as_float(d[i]);
+    vb[i] = __uint_as_float(d[16 + i]);
+  }
 }
 
 // |V3|^2 element offset in the chunk's layout
@@ -352,7 +379,7 @@ __device__ __forceinline__ size_t v3_out_off(int layout, int row, int q2, int l1
 // One CTA = one 128-row tile of one pair.  KIND 1: A = T1, B = e(q2),
 // epilogue -> T2 as GEMM 2's A.  KIND 2: A = T2, B = e(q3), epilogue |V3|^2.
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseTc t, long long pair0) {
+__global__ void __launch_bounds__(kThreads, 2) v3tc_gemm_kernel(V3Args a, DenseTc t, long long pair0) {
   extern __shared__ __align__(1024) unsigned char smraw[];
   __shared__ uint32_t s_tmem;
   __shared__ __align__(8) uint64_t s_full[4], s_empty[4], s_accf;
@@ -360,7 +387,7 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
   const DenseTcShape& s = t.sh;
   const Geometry& g = a.geo;
   const int b = g.b, tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int mt = blockIdx.x, p = blockIdx.y, S = s.stages;
+  const int mt = blockIdx.x / s.nsplit, split = blockIdx.x % s.nsplit, p = blockIdx.y, S = s.stages;
   const PairIdx pi = pair_idx(a, pair0 + p);
   const uint32_t sm0 = (uint32_t)__cvta_generic_to_shared(smraw);
   const uint32_t full0 = (uint32_t)__cvta_generic_to_shared(&s_full[0]);
@@ -385,7 +412,8 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = s_tmem;
   const uint32_t a_bytes = (uint32_t)(s.a_block_halves * sizeof(__half));
-  const uint32_t b_bytes = (uint32_t)(s.b_chunk_halves * sizeof(__half));
+  const uint32_t b_bytes = (uint32_t)s.b_stage_bytes;
+  const int nh0 = split * s.ncol;  // this CTA's first output column of each part
   const __half* Asrc = (KIND == 1 ? t.a1 : t.a2) + (size_t)p * s.a_pair_halves + (size_t)mt * s.nchunk * s.a_block_halves;
   const __half* Bsrc = t.bq + (size_t)(KIND == 1 ? pi.q2 : pi.q3) * s.bq_halves;
 
@@ -403,7 +431,15 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
         const uint32_t dst = sm0 + (uint32_t)(st * s.stage_bytes);
         expect_tx(full0 + 8 * st, a_bytes + b_bytes);
         bulk_copy(dst, Asrc + (size_t)c * s.a_block_halves, a_bytes, full0 + 8 * st);
-        bulk_copy(dst + a_bytes, Bsrc + (size_t)c * s.b_chunk_halves, b_bytes, full0 + 8 * st);
+        // B: per hi/lo and K group, this CTA's Re rows then its Im rows
+        const uint32_t piece = (uint32_t)(s.ncol * 16);
+        for (int hl = 0; hl < 2; ++hl)
+          for (int kg = 0; kg < kBK / 8; ++kg) {
+            const __half* src = Bsrc + (size_t)c * s.b_chunk_halves + (size_t)hl * s.np * kBK + (size_t)kg * s.np * 8;
+            const uint32_t d = dst + a_bytes + (uint32_t)((hl * (kBK / 8) + kg) * 2) * piece;
+            bulk_copy(d, src + (size_t)nh0 * 8, piece, full0 + 8 * st);
+            bulk_copy(d + piece, src + (size_t)(s.nh + nh0) * 8, piece, full0 + 8 * st);
+          }
         issued = c + 1;
       }
       if (!ok) s_fail = 1;
@@ -416,22 +452,23 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
     if (lane == 0) {
       bool ok = true;
       int done = 0;
-      const uint32_t idesc = instr_desc(kTM, s.nmma);
+      const uint32_t idesc = instr_desc(kTM, s.ncol);
+      const uint32_t brows = (uint32_t)(2 * s.ncol);  // B rows of one K group in shared memory
       for (int c = 0; c < s.nchunk; ++c) {
         const int st = c % S;
         ok = mbar_wait_or_fail(full0 + 8 * st, (uint32_t)((c / S) & 1), &s_fail);
         if (!ok) break;
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t aH = sm0 + (uint32_t)(st * s.stage_bytes), aL = aH + (uint32_t)(kTM * kBK * 2);
-        const uint32_t bH = aH + a_bytes, bL = bH + (uint32_t)(s.np * kBK * 2);
+        const uint32_t bH = aH + a_bytes, bL = bH + (uint32_t)(brows * kBK * 2);
         for (int ks = 0; ks < kBK / 16; ++ks) {
-          const uint32_t oa = (uint32_t)(2 * ks * kTM * 16), ob = (uint32_t)(2 * ks * s.np * 16);
+          const uint32_t oa = (uint32_t)(2 * ks * kTM * 16), ob = (uint32_t)(2 * ks * brows * 16);
           const uint64_t dAh = smem_desc(aH + oa, kTM * 16, 128), dAl = smem_desc(aL + oa, kTM * 16, 128);
-          for (int h = 0; h < s.nacc; ++h) {
-            const uint32_t on = (uint32_t)(h * s.nmma * 16);
-            const uint64_t dBh = smem_desc(bH + ob + on, s.np * 16, 128);
-            const uint64_t dBl = smem_desc(bL + ob + on, s.np * 16, 128);
-            const uint32_t dt = tmem + (uint32_t)(h * s.nmma);
+          for (int h = 0; h < 2; ++h) {  // accumulator 0: the Re columns, 1: the Im columns
+            const uint32_t on = (uint32_t)(h * s.ncol * 16);
+            const uint64_t dBh = smem_desc(bH + ob + on, brows * 16, 128);
+            const uint64_t dBl = smem_desc(bL + ob + on, brows * 16, 128);
+            const uint32_t dt = tmem + (uint32_t)(h * s.ncol);
             mma_f16(dt, dAh, dBh, idesc, (c > 0 || ks > 0) ? 1u : 0u);
             mma_f16(dt, dAh, dBl, idesc, 1u);
             mma_f16(dt, dAl, dBh, idesc, 1u);
@@ -455,7 +492,7 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
     // ---------------- epilogue ----------------
     const int quad = warp & 3, r = quad * 32 + lane, m = mt * kTM + r;
     const uint32_t taddr = tmem + ((uint32_t)(32 * quad) << 16);
-    const bool w = mbar_wait_or_fail(accf, 0u, &s_fail);
+    const bool w = mbar_wait_idle(accf, 0u, &s_fail);
     if (__all_sync(0xffffffffu, w)) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const bool live = m < b * b;
@@ -473,44 +510,42 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
         float* scr = reinterpret_cast<float*>(smraw) + (warp - 2) * 32 * 9;
         const int grp = lane >> 3, gi = lane & 7;
         const int mg = mt * kTM + quad * 32 + 8 * grp;
-        for (int cg = 0; cg < s.nh / 8 && (b & 7) == 0; ++cg) {
-          float vr[8], vi[8];
-          tmem_ld8(taddr + (uint32_t)(8 * cg), vr);
-          tmem_ld8(taddr + (uint32_t)(s.nh + 8 * cg), vi);
+        for (int cg = 0; cg < s.ncol / 16; ++cg) {
+          float vr[16], vi[16];
+          tmem_ld16x2(taddr + (uint32_t)(16 * cg), taddr + (uint32_t)(s.ncol + 16 * cg), vr, vi);
+          if ((b & 7) == 0) {
 #pragma unroll
-          for (int part = 0; part < 2; ++part) {
-            __syncwarp();
+            for (int q8 = 0; q8 < 2; ++q8)
 #pragma unroll
-            for (int j = 0; j < 8; ++j) scr[lane * 9 + j] = (part ? vi[j] : vr[j]) * f;
-            __syncwarp();
-            float x[8];
+              for (int part = 0; part < 2; ++part) {
+                __syncwarp();
 #pragma unroll
-            for (int jj = 0; jj < 8; ++jj) x[jj] = scr[(8 * grp + jj) * 9 + gi];
-            const int l2 = 8 * cg + gi;
-            if (mg < b * b && l2 < b) {
-              const int m2 = l2 * b + mg / b, kc0 = mg % b;
-              __half* dst = A2 + a_off(s, m2, (part ? s.kh : 0) + kc0);
-              split8(x, dst, dst + (size_t)kTM * kBK);
+                for (int j = 0; j < 8; ++j) scr[lane * 9 + j] = (part ? vi[8 * q8 + j] : vr[8 * q8 + j]) * f;
+                __syncwarp();
+                float x[8];
+#pragma unroll
+                for (int jj = 0; jj < 8; ++jj) x[jj] = scr[(8 * grp + jj) * 9 + gi];
+                const int l2 = nh0 + 16 * cg + 8 * q8 + gi;
+                if (mg < b * b && l2 < b) {
+                  const int m2 = l2 * b + mg / b, kc0 = mg % b;
+                  __half* dst = A2 + a_off(s, m2, (part ? s.kh : 0) + kc0);
+                  split8(x, dst, dst + (size_t)kTM * kBK);
+                }
+              }
+          } else if (live) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+              const int l2 = nh0 + 16 * cg + j;
+              if (l2 >= b) break;
+              const int m2 = l2 * b + l1;
+              const float xr = vr[j] * f, xi = vi[j] * f;
+              const __half hr = __float2half_rn(xr), hi_ = __float2half_rn(xi);
+              const size_t o_r = a_off(s, m2, kc), o_i = a_off(s, m2, s.kh + kc);
+              A2[o_r] = hr;
+              A2[o_r + (size_t)kTM * kBK] = __float2half_rn(xr - __half2float(hr));
+              A2[o_i] = hi_;
+              A2[o_i + (size_t)kTM * kBK] = __float2half_rn(xi - __half2float(hi_));
             }
-          }
-        }
-        for (int cg = 0; cg < s.nh / 8 && (b & 7) != 0; ++cg) {
-          float vr[8], vi[8];
-          tmem_ld8(taddr + (uint32_t)(8 * cg), vr);
-          tmem_ld8(taddr + (uint32_t)(s.nh + 8 * cg), vi);
-          if (!live) continue;
-#pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l2 = 8 * cg + j;
-            if (l2 >= b) break;
-            const int m2 = l2 * b + l1;
-            const float xr = vr[j] * f, xi = vi[j] * f;
-            const __half hr = __float2half_rn(xr), hi_ = __float2half_rn(xi);
-            const size_t o_r = a_off(s, m2, kc), o_i = a_off(s, m2, s.kh + kc);
-            A2[o_r] = hr;
-            A2[o_r + (size_t)kTM * kBK] = __float2half_rn(xr - __half2float(hr));
-            A2[o_i] = hi_;
-            A2[o_i + (size_t)kTM * kBK] = __float2half_rn(xi - __half2float(hi_));
           }
         }
       } else {
@@ -522,14 +557,13 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
                                 : 0.0;
         const double* t3 = t.tq + (size_t)pi.q3 * b;
         const size_t nkc = g.nkc;
-        for (int cg = 0; cg < s.nh / 8; ++cg) {
-          float vr[8], vi[8];
-          tmem_ld8(taddr + (uint32_t)(8 * cg), vr);
-          tmem_ld8(taddr + (uint32_t)(s.nh + 8 * cg), vi);
+        for (int cg = 0; cg < s.ncol / 16; ++cg) {
+          float vr[16], vi[16];
+          tmem_ld16x2(taddr + (uint32_t)(16 * cg), taddr + (uint32_t)(s.ncol + 16 * cg), vr, vi);
           if (!live) continue;
 #pragma unroll
-          for (int j = 0; j < 8; ++j) {
-            const int l3 = 8 * cg + j;
+          for (int j = 0; j < 16; ++j) {
+            const int l3 = nh0 + 16 * cg + j;
             if (l3 >= b) break;
             const double sc = c12 * t3[l3];
             double v = 0.0;
@@ -561,7 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1) v3tc_gemm_kernel(V3Args a, DenseT
 bool v3_dense_tc_supported(int b) {
   if (b <= 12 || b > kHeevMaxBands) return false;
   const DenseTcShape s = dense_tc_shape(b);
-  return s.stages >= 2 && s.np <= 512;
+  return s.stages >= 2 && s.tmem_cols <= 256 && s.ncol % 16 == 0;
 }
 
 int v3_pipeline_layout(int b, int precision) {
@@ -614,16 +648,16 @@ cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long P, bool a2
     e = cudaFuncSetAttribute(v3tc_t1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1_smem);
     if (e != cudaSuccess) return e;
   }
-  e = cudaFuncSetAttribute(v3tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
+  e = cudaFuncSetAttribute(v3tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.sh.smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(v3tc_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sh.smem);
+  e = cudaFuncSetAttribute(v3tc_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.sh.smem);
   if (e != cudaSuccess) return e;
   for (long long p0 = 0; p0 < npairs; p0 += P) {
     const int np = (int)std::min<long long>(P, npairs - p0);
-    const dim3 grid(sh.mtiles, np);
-    v3tc_t1_kernel<<<grid, 256, t1_smem, s>>>(a, t, p0);
-    v3tc_gemm_kernel<1><<<grid, kThreads, sh.smem, s>>>(a, t, p0);
-    v3tc_gemm_kernel<2><<<grid, kThreads, sh.smem, s>>>(a, t, p0);
+    v3tc_t1_kernel<<<dim3(sh.mtiles, np), 256, t1_smem, s>>>(a, t, p0);
+    const dim3 gg(sh.mtiles * sh.nsplit, np);  // the column halves of one tile are neighbours
+    v3tc_gemm_kernel<1><<<gg, kThreads, t.sh.smem, s>>>(a, t, p0);
+    v3tc_gemm_kernel<2><<<gg, kThreads, t.sh.smem, s>>>(a, t, p0);
   }
   return cudaGetLastError();
 }
