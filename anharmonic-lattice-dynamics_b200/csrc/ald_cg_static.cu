@@ -240,14 +240,23 @@ extern "C" int ald_cg_quadratic_static(int n, const double* a, const double* b, 
 
   gemv_cm_kernel<<<nblk, kRows * kColGroups, 0, s>>>(n, a, vmin, aux, nullptr, nullptr);
   cg_start_kernel<<<1, kVecThreads, 0, s>>>(n, aux, b, grad, conj, st);
+  // every 8 iterations the host reads the stop flag (into a stack copy, no
+  // allocation) and stops launching once the stop rule has fired; the
+  // iterations launched past it return at once
+  CgState h;
   for (int it = 0; it < max_iter; ++it) {
     gemv_cm_kernel<<<nblk, kRows * kColGroups, 0, s>>>(n, a, conj, aux, part, st);
     cg_iter_kernel<<<1, kVecThreads, 0, s>>>(n, aux, part, nblk, grad, conj, vmin, st, tol);
+    if ((it & 7) == 7 && it + 1 < max_iter) {
+      e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+      if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("cg_static: ") + cudaGetErrorString(e));
+      if (h.done) break;
+    }
   }
   gemv_cm_kernel<<<nblk, kRows * kColGroups, 0, s>>>(n, a, vmin, aux, nullptr, nullptr);
   cg_value_kernel<<<1, kVecThreads, 0, s>>>(n, vmin, aux, b, st);
   e = cudaGetLastError();
-  CgState h;
   if (e == cudaSuccess) e = cudaMemcpyAsync(&h, st, sizeof h, cudaMemcpyDeviceToHost, s);
   if (e == cudaSuccess) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("cg_static: ") + cudaGetErrorString(e));

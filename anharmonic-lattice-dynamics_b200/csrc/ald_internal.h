@@ -298,7 +298,7 @@ cudaError_t launch_v3_rows_f64(const V3Args& a, cudaStream_t s);
 bool v3_dense_supported(int b);
 size_t v3_dense_work_bytes(int b, long long npairs, size_t budget);
 cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s);
-// more than 12 bands, ALD_MIXED (ald_v3_dense_tc.cu): both mode products as
+// more than 6 bands, ALD_MIXED (ald_v3_dense_tc.cu): both mode products as
 // split-FP16 tcgen05 GEMMs; hbuf from launch_v3_rows_f32; work of
 // v3_dense_tc_work_bytes(b, nkc, nrows, pairs) bytes for batches of `pairs`
 // pairs; a2_zeroed: the workspace's T2 operand padding is already zero

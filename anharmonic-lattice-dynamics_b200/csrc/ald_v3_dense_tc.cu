@@ -1,4 +1,4 @@
-// |V3|^2 for cells of more than 12 bands, mixed precision: the two
+// |V3|^2 for cells of more than 6 bands, mixed precision: the two
 // eigenvector mode products of every (q1, q2) pair as split-FP16 tcgen05
 // GEMMs with FP32 accumulation in TMEM (the ALD_MIXED path).
 //
@@ -593,13 +593,14 @@ __global__ void __launch_bounds__(kThreads, 2) v3tc_gemm_kernel(V3Args a, DenseT
 }  // namespace
 
 bool v3_dense_tc_supported(int b) {
-  if (b <= 12 || b > kHeevMaxBands) return false;
+  // every cell but the 3- and 6-band ones, which have their own kernels
+  if (b < 7 || b > kHeevMaxBands) return false;
   const DenseTcShape s = dense_tc_shape(b);
   return s.stages >= 2 && s.tmem_cols <= 256 && s.ncol % 16 == 0;
 }
 
 int v3_pipeline_layout(int b, int precision) {
-  if (b > 12 && precision == ALD_MIXED && v3_dense_tc_supported(b)) return 2;
+  if (precision == ALD_MIXED && v3_dense_tc_supported(b)) return 2;
   if (b == 3 || b == 6 || b > 12) return 1;
   return 0;
 }

@@ -193,15 +193,22 @@ def test_rocksalt192_v3_fgr_pipeline(rs192, ald_lib, oracle_lib):
     ctx.close()
 
 
-@pytest.mark.parametrize("which", ["sl24", "rs192"])
-def test_large_mixed_tensor_cores(which, sl24, rs192, ald_lib):
-    """ALD_MIXED above 12 bands: both mode products as split-FP16 tcgen05
+@pytest.fixture(scope="module")
+def lj12(oracle_lib, ald_lib, workdir):
+    d = make_case(workdir, 3, (4, 4, 4), rc_sigma=1.2, delta="tetra")
+    O, ph = _phonons(oracle_lib, d)
+    return d, O, ph
+
+
+@pytest.mark.parametrize("which", ["lj12", "sl24", "rs192"])
+def test_large_mixed_tensor_cores(which, lj12, sl24, rs192, ald_lib):
+    """ALD_MIXED from 9 bands up: both mode products as split-FP16 tcgen05
     GEMMs (ald_v3_dense_tc.cu) against the FP64 oracle on the same
     eigenpairs; |V3|^2 normwise within 1e-4, and the pipeline's Q per mode
     within 1e-4 (+1e-8 max|Q|) of the FP64 pipeline's."""
-    d, O, ph = sl24 if which == "sl24" else rs192
-    rows = (2, 3) if which == "sl24" else (O.nibz, O.nibz)
-    v33 = O.v3(*rows) if which == "sl24" else oracle_dense.v3_factorised(O, *rows)
+    d, O, ph = {"lj12": lj12, "sl24": sl24, "rs192": rs192}[which]
+    rows = (O.nibz, O.nibz) if which == "rs192" else (2, 3)
+    v33 = oracle_dense.v3_factorised(O, *rows) if which == "rs192" else O.v3(*rows)
     keep = ~gamma_acoustic_mask(O, ph[0], *rows)
     delta = ald_lib.DELTA_TETRA
     ctx = ald_lib.Context(d, ald_lib.default_options(precision=ald_lib.MIXED, delta=delta))
