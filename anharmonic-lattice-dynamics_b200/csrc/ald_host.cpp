@@ -1005,4 +1005,18 @@ std::string isotope_g_atoms(const System& S, std::vector<double>& g) {
   return "";
 }
 
+cudaError_t raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex m;
+  static std::map<std::pair<const void*, int>, size_t> done;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(m);
+  size_t& cur = done[{func, dev}];
+  if (bytes <= cur) return cudaSuccess;
+  e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) cur = bytes;
+  return e;
+}
+
 }  // namespace ald

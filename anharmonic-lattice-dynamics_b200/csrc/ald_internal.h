@@ -155,6 +155,13 @@ void dev_trim();
 // different host threads never synchronise the device during a capture.
 std::mutex& capture_mutex();
 
+// Raise a kernel's dynamic shared-memory limit on the current device to at
+// least `bytes`, never lowering it.  The limit is one process-wide attribute
+// per kernel, and contexts on different host threads (ald_kappa_batched)
+// launch the same kernels with different sizes: a plain set by one thread
+// could shrink the limit under another thread's launch.
+cudaError_t raise_smem_limit(const void* func, size_t bytes);
+
 template <class T>
 struct DevBuf {
   T* p = nullptr;

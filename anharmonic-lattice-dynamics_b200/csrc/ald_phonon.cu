@@ -639,7 +639,7 @@ cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
     cudaError_t e = cudaSuccess;
 #define ALD_PHW(GG)                                                                                            \
   if (smw > 48 * 1024)                                                                                         \
-    e = cudaFuncSetAttribute(phonon_warp_kernel<GG>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smw);    \
+    e = raise_smem_limit((const void*)phonon_warp_kernel<GG>, smw);                                            \
   if (e != cudaSuccess) return e;                                                                              \
   phonon_warp_kernel<GG><<<(nmat + per_cta - 1) / per_cta, kPhWarps * 32, smw, s>>>(a, nmat);
     if (G == 4) {
@@ -655,7 +655,7 @@ cudaError_t launch_phonons(const PhononArgs& a, cudaStream_t s) {
   size_t sm = 2 * (size_t)b * b * sizeof(double2);
   if (b > 64) return cudaErrorInvalidValue;
   if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(phonon_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = raise_smem_limit((const void*)phonon_kernel, sm);
     if (e != cudaSuccess) return e;
   }
   phonon_kernel<<<a.geo.nkc * a.ndisp, kThreads, sm, s>>>(a);

@@ -291,7 +291,7 @@ cudaError_t launch_self(const SelfArgs& a, double* out, cudaStream_t s) {
   const size_t sm = self_smem_bytes(a, &ppb);
   if (sm > 200 * 1024) return cudaErrorInvalidValue;
   if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(self_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = raise_smem_limit((const void*)self_kernel, sm);
     if (e != cudaSuccess) return e;
   }
   const int nblk = (a.nkc + ppb - 1) / ppb;

@@ -1007,7 +1007,7 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
   dim3 grid(g.nc[0] * f.nbj, a.nrows, 2 * g.b);
   cudaError_t e;
 #define ALD_FUSED1(BB, FW)                                                                                       \
-  e = cudaFuncSetAttribute(delta_fused_kernel<BB, FW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)f.smem); \
+  e = raise_smem_limit((const void*)delta_fused_kernel<BB, FW>, f.smem);                                       \
   if (e != cudaSuccess) return e;                                                                                \
   delta_fused_kernel<BB, FW><<<grid, kFusedThreads, f.smem, s>>>(a);
 #define ALD_FUSED(BB)     \

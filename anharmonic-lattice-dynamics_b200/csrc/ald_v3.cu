@@ -176,7 +176,7 @@ cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s) {
   size_t sm = (b2 + ppb * per_pair) * sizeof(double2) + (size_t)ppb * 2 * natoms * sizeof(int);
   if (sm > 200 * 1024) return cudaErrorInvalidValue;
   if (sm > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(v3_fp64_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = raise_smem_limit((const void*)v3_fp64_kernel, sm);
     if (e != cudaSuccess) return e;
   }
   dim3 grid((a.geo.nkc + ppb - 1) / ppb, a.nrows);

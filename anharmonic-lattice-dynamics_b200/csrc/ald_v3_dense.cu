@@ -68,7 +68,7 @@ __device__ __forceinline__ PairIdx pair_idx(const V3Args& a, long long pair) {
 
 // T1 of the batch's pairs: CTA (pair, jb), threads over (l1, kc)
 constexpr int kT1Threads = 256;
-__global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long pair0, double2* T1) {
+__global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long pair0, double2* T1, int table_ph) {
   extern __shared__ double2 s_ph[];  // P_c(q2) of every class
   const Geometry& g = a.geo;
   const int b = g.b, nat0 = g.nat0;
@@ -77,8 +77,10 @@ __global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long p
   int m2[3];
   decompose(g, pi.q2, m2);
   const double2* roots = reinterpret_cast<const double2*>(a.roots);
-  for (int c = threadIdx.x; c < a.ncls; c += blockDim.x)
-    s_ph[c] = roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
+  // the classes' phases in shared memory when they fit (table_ph), else
+  // read from the roots table where used
+  if (table_ph)
+    for (int c = threadIdx.x; c < a.ncls; c += blockDim.x) s_ph[c] = roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
   __syncthreads();
   const double2* H = static_cast<const double2*>(a.hbuf) + (size_t)pi.row * a.ncls * 9 * b;
   double2* out = T1 + ((size_t)p * b + jb) * b * b;
@@ -87,7 +89,8 @@ __global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long p
     const int grp = j0 * nat0 + k0;
     double2 acc = make_double2(0.0, 0.0);
     for (int c = a.cls_grp_off[grp]; c < a.cls_grp_off[grp + 1]; ++c) {
-      const double2 ph = s_ph[c], h = H[((size_t)c * 9 + be * 3 + ga) * b + l1];
+      const double2 ph = table_ph ? s_ph[c] : roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
+      const double2 h = H[((size_t)c * 9 + be * 3 + ga) * b + l1];
       acc.x = fma(ph.x, h.x, fma(-ph.y, h.y, acc.x));
       acc.y = fma(ph.x, h.y, fma(ph.y, h.x, acc.y));
     }
@@ -224,14 +227,16 @@ cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cuda
       std::min<long long>(65535, std::max<long long>(1, (long long)(work_bytes / (2 * b3 * sizeof(double2)))));
   double2* T1 = static_cast<double2*>(work);
   double2* T2 = T1 + (size_t)P * b3;
-  const size_t t1_smem = (size_t)std::max(a.ncls, 1) * sizeof(double2);
+  // phase table of every class in shared memory up to 96 KB (6 144 classes)
+  const int table_ph = (size_t)a.ncls * sizeof(double2) <= 96 * 1024;
+  const size_t t1_smem = table_ph ? (size_t)std::max(a.ncls, 1) * sizeof(double2) : 0;
   if (t1_smem > 48 * 1024) {
-    cudaError_t e = cudaFuncSetAttribute(v3_t1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1_smem);
+    cudaError_t e = raise_smem_limit((const void*)v3_t1_kernel, t1_smem);
     if (e != cudaSuccess) return e;
   }
   for (long long p0 = 0; p0 < npairs; p0 += P) {
     const int np = (int)std::min<long long>(P, npairs - p0);
-    v3_t1_kernel<<<dim3(np, b), kT1Threads, t1_smem, s>>>(a, p0, T1);
+    v3_t1_kernel<<<dim3(np, b), kT1Threads, t1_smem, s>>>(a, p0, T1, table_ph);
     const dim3 gg((b * b + kGM - 1) / kGM, (b + kGN - 1) / kGN, np);
     v3_zgemm_kernel<1><<<gg, kGThreads, 0, s>>>(a, p0, T1, T2);
     v3_zgemm_kernel<2><<<gg, kGThreads, 0, s>>>(a, p0, T2, nullptr);

@@ -233,7 +233,7 @@ __global__ void v3tc_rowexp_kernel(int nrows, const unsigned* bound, int* rexp) 
 
 // A operand of GEMM 1 for the batch's pairs: rows m = l1 b + kc, K' = (Re |
 // Im) jb; a thread per (row of the tile, K group of 8 jb)
-__global__ void __launch_bounds__(256) v3tc_t1_kernel(V3Args a, DenseTc t, long long pair0) {
+__global__ void __launch_bounds__(256) v3tc_t1_kernel(V3Args a, DenseTc t, long long pair0, int table_ph) {
   extern __shared__ float2 s_ph[];  // P_c(q2) of every class
   const DenseTcShape& s = t.sh;
   const Geometry& g = a.geo;
@@ -242,10 +242,13 @@ __global__ void __launch_bounds__(256) v3tc_t1_kernel(V3Args a, DenseTc t, long 
   int m2[3];
   decompose(g, pi.q2, m2);
   const double2* roots = reinterpret_cast<const double2*>(a.roots);
-  for (int c = threadIdx.x; c < a.ncls; c += blockDim.x) {
-    const double2 r = roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
-    s_ph[c] = make_float2((float)r.x, (float)r.y);
-  }
+  // the classes' phases in shared memory when they fit (table_ph), else
+  // read from the roots table where used
+  if (table_ph)
+    for (int c = threadIdx.x; c < a.ncls; c += blockDim.x) {
+      const double2 r = roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
+      s_ph[c] = make_float2((float)r.x, (float)r.y);
+    }
   __syncthreads();
   const float2* H = static_cast<const float2*>(a.hbuf) + (size_t)pi.row * a.ncls * 9 * b;
   const float sc = ldexpf(1.f, kSplitE - t.rexp[pi.row]);
@@ -263,7 +266,14 @@ __global__ void __launch_bounds__(256) v3tc_t1_kernel(V3Args a, DenseTc t, long 
       if (live && jb < b) {
         const int grp = (jb / 3) * nat0 + k0, be = jb % 3;
         for (int c = a.cls_grp_off[grp]; c < a.cls_grp_off[grp + 1]; ++c) {
-          const float2 ph = s_ph[c], h = H[((size_t)c * 9 + be * 3 + ga) * b + l1];
+          float2 ph;
+          if (table_ph) {
+            ph = s_ph[c];
+          } else {
+            const double2 r = roots[phase_index(a.cls_pc + 4 * c, m2, g.L, g.L32)];
+            ph = make_float2((float)r.x, (float)r.y);
+          }
+          const float2 h = H[((size_t)c * 9 + be * 3 + ga) * b + l1];
           acc.x = fmaf(ph.x, h.x, fmaf(-ph.y, h.y, acc.x));
           acc.y = fmaf(ph.x, h.y, fmaf(ph.y, h.x, acc.y));
         }
@@ -644,18 +654,20 @@ cudaError_t launch_v3_dense_tc(const V3Args& a, void* work, long long P, bool a2
   v3tc_modes_kernel<<<(a.geo.nkc * b + 255) / 256, 256, 0, s>>>(a, t.tq);
   v3tc_rowbound_kernel<<<dim3(64, a.nrows), 256, 0, s>>>(a, bound);
   v3tc_rowexp_kernel<<<(a.nrows + 127) / 128, 128, 0, s>>>(a.nrows, bound, t.rexp);
-  const size_t t1_smem = (size_t)std::max(a.ncls, 1) * sizeof(float2);
+  // phase table of every class in shared memory up to 96 KB (12 288 classes)
+  const int table_ph = (size_t)a.ncls * sizeof(float2) <= 96 * 1024;
+  const size_t t1_smem = table_ph ? (size_t)std::max(a.ncls, 1) * sizeof(float2) : 0;
   if (t1_smem > 48 * 1024) {
-    e = cudaFuncSetAttribute(v3tc_t1_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1_smem);
+    e = raise_smem_limit((const void*)v3tc_t1_kernel, t1_smem);
     if (e != cudaSuccess) return e;
   }
-  e = cudaFuncSetAttribute(v3tc_gemm_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.sh.smem);
+  e = raise_smem_limit((const void*)v3tc_gemm_kernel<1>, t.sh.smem);
   if (e != cudaSuccess) return e;
-  e = cudaFuncSetAttribute(v3tc_gemm_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t.sh.smem);
+  e = raise_smem_limit((const void*)v3tc_gemm_kernel<2>, t.sh.smem);
   if (e != cudaSuccess) return e;
   for (long long p0 = 0; p0 < npairs; p0 += P) {
     const int np = (int)std::min<long long>(P, npairs - p0);
-    v3tc_t1_kernel<<<dim3(sh.mtiles, np), 256, t1_smem, s>>>(a, t, p0);
+    v3tc_t1_kernel<<<dim3(sh.mtiles, np), 256, t1_smem, s>>>(a, t, p0, table_ph);
     const dim3 gg(sh.mtiles * sh.nsplit, np);  // the column halves of one tile are neighbours
     v3tc_gemm_kernel<1><<<gg, kThreads, t.sh.smem, s>>>(a, t, p0);
     v3tc_gemm_kernel<2><<<gg, kThreads, t.sh.smem, s>>>(a, t, p0);

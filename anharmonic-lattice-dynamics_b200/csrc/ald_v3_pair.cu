@@ -291,8 +291,7 @@ cudaError_t launch_pair_t(const V3Args& a, cudaStream_t s) {
   constexpr int B2 = B * B, B3 = B2 * B;
   const size_t smem = ((size_t)QT * ((B3 | 1) + 2 * (B2 | 1) + (a.ncls | 1))) * sizeof(C);
   if (smem > 220 * 1024) return cudaErrorInvalidValue;
-  cudaError_t e = cudaFuncSetAttribute(v3_pair_kernel<T, B, QT, S, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)smem);
+  cudaError_t e = raise_smem_limit((const void*)v3_pair_kernel<T, B, QT, S, NT>, smem);
   if (e != cudaSuccess) return e;
   // row stage
   const int n = a.ncls * 9 * B;

@@ -537,8 +537,7 @@ cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cuda
     const char* v = getenv("ALD_V3_TC_WG");
     return v && atoi(v) == 3 ? 3 : 2;
   }();
-  cudaError_t e = cudaFuncSetAttribute(ne == 3 ? v3_tc3_kernel<3> : v3_tc3_kernel<2>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  cudaError_t e = raise_smem_limit(ne == 3 ? (const void*)v3_tc3_kernel<3> : (const void*)v3_tc3_kernel<2>, smem);
   if (e != cudaSuccess) return e;
   const int ntiles = (a.geo.nkc + kTM - 1) / kTM;
   // rows per CTA: reuse the phase tile over several rows while the grid still fills the GPU twice
