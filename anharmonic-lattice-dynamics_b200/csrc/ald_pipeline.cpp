@@ -500,6 +500,13 @@ static void release_pipeline_workspaces(ald_ctx* c) {
   c->w_scratch.free();
 }
 
+extern "C" int ald_release_workspaces(ald_ctx* c) {
+  if (!c) return fail(ALD_ERR_ARG, "null context");
+  ALD_CK(cudaSetDevice(c->device));
+  release_pipeline_workspaces(c);
+  return ALD_OK;
+}
+
 extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res,
                                  int* status) {
   if (n <= 0 || !ctx || !tempk || !res) return fail(ALD_ERR_ARG, "bad argument");

@@ -68,7 +68,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_kappa_pipeline_sharded_dev", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
-           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched"]
+           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched", "ald_release_workspaces"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -416,6 +416,10 @@ class Context:
                                         _p(us), out_dir.encode() if out_dir else None))
         f = lambda a: (a[0::2] + 1j * a[1::2]).reshape(n, self.ndyn).T
         return {"kp_bs": kp, "dk_bs": dk, "omega0": om, "nself": f(ns), "uself": f(us)}
+
+    def release_workspaces(self):
+        """ald_release_workspaces: this context's pipeline workspaces back to the device-memory cache."""
+        _check(lib().ald_release_workspaces(self.h))
 
     def kappa_pipeline(self, tempk: Optional[float] = None, want_modes=True):
         if tempk is None:

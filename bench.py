@@ -115,7 +115,10 @@ def run_suite(args, suite: str):
         torch.cuda.synchronize()
         tbat = time.perf_counter() - t0
         t0 = time.perf_counter()
-        seq = [c.kappa_pipeline(tk, want_modes=False) for c, tk in zip(ctxs, tempk)]
+        seq = []
+        for c, tk in zip(ctxs, tempk):  # one after another, each keeping device memory only for its run
+            seq.append(c.kappa_pipeline(tk, want_modes=False))
+            c.release_workspaces()
         torch.cuda.synchronize()
         tseq = time.perf_counter() - t0
         res[name] = {"batched_s": tbat, "sequential_s": tseq, "batched_value": tb / tbat,

@@ -267,6 +267,13 @@ int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double
  * to 256 bands). */
 int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res, int* status);
 
+/* No counterpart in the reference: hands a context's pipeline workspaces
+ * (R1/R2, the |V3|^2 chunk, the V3 and eigensolver workspaces, the collision
+ * matrix) back to the library's device-memory cache; the next pipeline call
+ * of any context of the same sizes takes them from there.  For hosts that
+ * keep many contexts alive and run them one after another. */
+int ald_release_workspaces(ald_ctx* ctx);
+
 /* Row-sharded job=1, one call per rank (one process per GPU): the MPI
  * decomposition of kappa_full (kappa.f90:418-428: nibz/nranks IBZ rows per
  * rank, the last rank also takes the remainder; ald_shard_rows returns a

@@ -91,3 +91,17 @@ def test_batched_uneven_sizes_against_oracle(ald_lib, oracle_lib, workdir):
             assert ok, (c.ndyn, key, worst)
     for c in ctxs:
         c.close()
+
+
+def test_release_workspaces_then_rerun(ald_lib, workdir):
+    """ald_release_workspaces hands a context's workspaces back; its next
+    pipeline call takes new ones and gives the same results."""
+    d = make_case(workdir, 1, (6, 6, 6))
+    ctx = ald_lib.Context(d)
+    a = ctx.kappa_pipeline(want_modes=False)
+    ctx.release_workspaces()
+    b = ctx.kappa_pipeline(want_modes=False)
+    assert a["cg_iters"] == b["cg_iters"]
+    for k in ("kappa_rta", "kappa_cg"):
+        assert np.allclose(a[k], b[k], rtol=1e-12, atol=1e-14 * np.abs(a[k]).max())
+    ctx.close()
