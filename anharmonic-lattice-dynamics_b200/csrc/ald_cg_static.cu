@@ -15,8 +15,11 @@
 // The scratch array is sized for n <= ALD_CG_STATIC_MAX_N unknowns (about
 // 0.8 MB) and stays resident on every device that loads the library until the
 // process exits.  The first call on a device looks up the array's device
-// address (cudaGetSymbolAddress, with that device current); make that first
-// call before any stream capture.  All calls share the array: two calls whose
+// address (cudaGetSymbolAddress, with that device current) and keeps it for
+// the life of the process; make that first call before any stream capture.
+// A cudaDeviceReset by the host discards the module that holds the array, so
+// the kept address is no longer valid after one: do not reset a device
+// between calls.  All calls share the array: two calls whose
 // kernels overlap on the same device (different streams, or different host
 // threads) race on it.  Every value a call reads from it is written earlier in
 // the same call, so the contents left by a previous call never leak into a
@@ -208,6 +211,38 @@ bool on_device(const void* p, int dev) {
   return (at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged) && at.device == dev;
 }
 
+// The driver's cuMemGetAddressRange, reached through the runtime (the library
+// links only cudart): the allocation that holds a device address.  Declared
+// with plain types: CUdeviceptr is a 64-bit integer and CUresult an int.
+using AddrRangeFn = int (*)(unsigned long long* base, size_t* size, unsigned long long ptr);
+
+AddrRangeFn addr_range_fn() {
+  static AddrRangeFn fn = [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuMemGetAddressRange", &f, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess) {
+      cudaGetLastError();
+      f = nullptr;
+    }
+    return reinterpret_cast<AddrRangeFn>(f);
+  }();
+  return fn;
+}
+
+// false when the allocation holding p is known to end before p + bytes (a
+// caller's slice too short for what the call reads or writes); true when it
+// covers them or when its extent cannot be queried
+bool covers(const void* p, size_t bytes) {
+  AddrRangeFn fn = addr_range_fn();
+  if (!fn) return true;
+  unsigned long long base = 0;
+  size_t size = 0;
+  const unsigned long long q = reinterpret_cast<unsigned long long>(p);
+  if (fn(&base, &size, q) != 0) return true;
+  return q >= base && q - base <= size && bytes <= size - (size_t)(q - base);
+}
+
 using ald::capi::fail;
 
 }  // namespace
@@ -225,6 +260,9 @@ extern "C" int ald_cg_quadratic_static(int n, const double* a, const double* b, 
   if (dev < 0 || dev >= kMaxDevices) return fail(ALD_ERR_UNSUPPORTED, "cg_static: device ordinal out of range");
   if (!on_device(a, dev) || !on_device(b, dev) || !on_device(vmin, dev))
     return fail(ALD_ERR_ARG, "cg_static: a, b and vmin must be device memory of the current device");
+  if (!covers(a, (size_t)n * n * sizeof(double)) || !covers(b, (size_t)n * sizeof(double)) ||
+      !covers(vmin, (size_t)n * sizeof(double)))
+    return fail(ALD_ERR_ARG, "cg_static: a holds fewer than n*n doubles, or b or vmin fewer than n, in its allocation");
   double* base = nullptr;
   std::string msg;
   int r = scratch_address(dev, &base, msg);

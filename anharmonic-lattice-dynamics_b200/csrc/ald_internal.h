@@ -358,6 +358,11 @@ cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s);
 // R1/R2 of the chunk must be zero on entry
 bool delta_fused_supported(const Geometry& g);
 cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s);
+// the same deterministically: the mesh walked plane by plane, each R1/R2
+// entry written by one thread in a fixed order (no atomics, R1/R2 need no
+// zeroing); band marginals R1p/R2p are not produced
+bool delta_plane_supported(const Geometry& g, int f32w);
+cudaError_t launch_delta_plane(const CombineArgs& a, cudaStream_t s);
 // any number of bands (large cells): the tetrahedron or Gaussian delta into
 // R1/R2 and/or P1s/P2s straight from |V3|^2 of the chunk; for the tetrahedron
 // R1/R2/P1s/P2s (and R1p/R2p) must be zero on entry; P1/P2 are not produced

@@ -184,20 +184,26 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   }
   ALD_CKA(Q.alloc((size_t)3 * nibz * b));
   const int gauss = delta_mode(c) == ALD_DELTA_GAUSS;
-  // the large-cell tensor-core V3 hands |V3|^2 to the delta in FP32 (layout
-  // 2): half the bytes, twice the rows per chunk
-  const bool v3f = v3_pipeline_layout(b, c->opt.precision) == 2;
-  const int K = v3f ? std::min(nibz, 2 * rows_per_chunk(c)) : rows_per_chunk(c);
-  const size_t v3n = (size_t)K * nkc * b * b * b;
-  ALD_CKA(v3.alloc(v3f ? (v3n + 1) / 2 : v3n));
   // tetrahedron: weights straight into R1/R2 (no corner-energy/weight arrays)
   // the delta kernels read |V3|^2 slice by slice (coalesced over q2): the
   // class-form V3 kernels write that layout; the large-cell tensor-core V3
   // writes runs of l1 instead (layout 2)
   const int v3_layout = v3_pipeline_layout(b, c->opt.precision);
+  const bool mixed = c->opt.precision != ALD_FP64;
   const bool fused = !gauss && v3_layout != 2 && delta_fused_supported(c->geo);
+  // deterministic option: the plane-walking form of the fused delta where it
+  // applies (no band marginals)
+  const bool plane = fused && !it && v3_layout <= 1 && c->opt.deterministic && delta_plane_supported(c->geo, mixed);
   // more than 16 bands, or layout 2: the band-generic delta kernels, straight into R1/R2
   const bool any = !fused && (b > kDeltaSmallBands || v3_layout == 2);
+  // the mixed pipeline hands |V3|^2 to the delta in FP32 where the delta
+  // reads it so: the large-cell tensor-core V3 (layout 2), and the class-form
+  // V3 of 3 and 6 bands into the fused tetrahedron delta.  Half the bytes,
+  // twice the rows per chunk.
+  const bool v3f = v3_layout == 2 || (mixed && fused && v3_layout == 1 && (b == 3 || b == 6));
+  const int K = v3f ? std::min(nibz, 2 * rows_per_chunk(c)) : rows_per_chunk(c);
+  const size_t v3n = (size_t)K * nkc * b * b * b;
+  ALD_CKA(v3.alloc(v3f ? (v3n + 1) / 2 : v3n));
   if (!fused && !any) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   ALD_CKA(c->w_brange.alloc((size_t)2 * b));
   ALD_CK(launch_band_range(c->geo, c->freq.p, c->w_brange.p, s));
@@ -239,12 +245,15 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
       ALD_CK(cudaMemsetAsync(a.R1p, 0, rbytes, s));
       ALD_CK(cudaMemsetAsync(a.R2p, 0, rbytes, s));
     }
-    if (fused || (any && !gauss)) {
+    if ((fused && !plane) || (any && !gauss)) {
       ALD_CK(cudaMemsetAsync(a.R1, 0, rbytes, s));
       ALD_CK(cudaMemsetAsync(a.R2, 0, rbytes, s));
     }
     ALD_CK(tm.begin(2));
-    if (fused) {
+    if (plane) {
+      ALD_CK(launch_delta_plane(a, s));
+      res->launches[2] += 1;
+    } else if (fused) {
       ALD_CK(launch_delta_fused(a, s));
       res->launches[2] += 1;
     } else if (any) {

@@ -31,10 +31,15 @@ struct TetSorted {
   float e21, e31, e41, e32, e42, e43;
 };
 
+// |x| < small1 = 1e-10 is compared in double in the reference; for a float x
+// that is |x| <= the largest float below 1e-10 (0x1.b7cdfcp-34), the same test
+// without conversions.  Then x = +-(float)small2, small2 = 1e-10.
 ALD_TET_HD void tet_fix_small(float& x) {
-  const double small1 = 1e-10, small2 = 1e-10;
-  if (fabs((double)x) < small1 && x > 0.0f) x = (float)small2;
-  if (fabs((double)x) < small1 && x < 0.0f) x = (float)(-small2);
+  constexpr float kBelowSmall1 = 0x1.b7cdfcp-34f;
+  if (fabsf(x) <= kBelowSmall1) {
+    if (x > 0.0f) x = (float)1e-10;
+    else if (x < 0.0f) x = (float)(-1e-10);
+  }
 }
 
 ALD_TET_HD float fmax4(float a, float b) { return a > b ? a : b; }

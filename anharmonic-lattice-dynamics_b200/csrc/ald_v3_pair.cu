@@ -177,25 +177,38 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 2) v3_pair_kernel(V3A
   }
   __syncthreads();
 
-  // class sums: A[q][l1][j0 be][k0 ga]
+  // class sums: A[q][l1][j0 be][k0 ga]; in FP32 a thread per (column, q and
+  // q + QT/2), so that each H value it loads serves two pairs (FP64: one q,
+  // the registers of two would spill)
   const C* H = static_cast<const C*>(a.hbuf) + (size_t)row * a.ncls * 9 * B;
-  for (int task = tid; task < QT * NG * 9; task += NT) {
-    const int q = task % QT, col = task / QT;
+  constexpr int QB = sizeof(T) == 4 ? 2 : 1, QH = QT / QB;
+  for (int task = tid; task < QH * NG * 9; task += NT) {
+    const int q = task % QH, col = task / QH;
     const int grp = col / 9, bg = col % 9;
     const int j0 = grp / NAT, k0 = grp % NAT, be = bg / 3, ga = bg % 3;
-    C acc[B];
+    C acc[QB][B];
 #pragma unroll
-    for (int l = 0; l < B; ++l) acc[l] = C{0, 0};
+    for (int k = 0; k < QB; ++k)
+#pragma unroll
+      for (int l = 0; l < B; ++l) acc[k][l] = C{0, 0};
     const int c0 = a.cls_grp_off[grp], c1 = a.cls_grp_off[grp + 1];
     for (int c = c0; c < c1; ++c) {
-      const C p = P[q * PP + c];
+      C p[QB];
+#pragma unroll
+      for (int k = 0; k < QB; ++k) p[k] = P[(q + k * QH) * PP + c];
       const C* h = H + ((size_t)c * 9 + bg) * B;
 #pragma unroll
-      for (int l = 0; l < B; ++l) cmac(acc[l], p, h[l]);
+      for (int l = 0; l < B; ++l) {
+        const C hv = h[l];
+#pragma unroll
+        for (int k = 0; k < QB; ++k) cmac(acc[k][l], p[k], hv);
+      }
     }
     C* dst = At + q * AP + (3 * j0 + be) * B + 3 * k0 + ga;
 #pragma unroll
-    for (int l = 0; l < B; ++l) dst[l * B2] = acc[l];
+    for (int k = 0; k < QB; ++k)
+#pragma unroll
+      for (int l = 0; l < B; ++l) dst[k * QH * AP + l * B2] = acc[k][l];
   }
   __syncthreads();
 
@@ -258,8 +271,9 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 2) v3_pair_kernel(V3A
       const double c1 = a.const33 * a.const33 / 8 / sqrt(fabs(w2[(size_t)q1 * B + l1]));
       // layout 0: [row][q2][l1][l2][l3]; layout 1: [row][l2][l3][l1][q2]
       const size_t nk = g.nkc;
-      double* out = a.v3_layout == 1 ? a.v3sq + ((size_t)row * B3 + l2b * B2 + l1) * nk + q2
-                                     : a.v3sq + ((size_t)row * nk + q2) * B3 + l1 * B2 + l2b * B;
+      // FP64, or FP32 (a.v3sq_f32: the mixed pipeline) at the same index
+      const size_t o = a.v3_layout == 1 ? ((size_t)row * B3 + l2b * B2 + l1) * nk + q2
+                                        : ((size_t)row * nk + q2) * B3 + l1 * B2 + l2b * B;
       const size_t st_l2 = a.v3_layout == 1 ? (size_t)B2 * nk : B, st_l3 = a.v3_layout == 1 ? (size_t)B * nk : 1;
 #pragma unroll
       for (int i = 0; i < BS; ++i) {
@@ -274,7 +288,8 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 3 : 2) v3_pair_kernel(V3A
           } else {
             atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
           }
-          out[i * st_l2 + l * st_l3] = v;
+          if (a.v3sq_f32) a.v3sq_f32[o + i * st_l2 + l * st_l3] = (float)v;
+          else a.v3sq[o + i * st_l2 + l * st_l3] = v;
         }
       }
     }

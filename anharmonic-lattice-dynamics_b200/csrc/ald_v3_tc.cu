@@ -486,9 +486,10 @@ __global__ void __launch_bounds__(TcShape<NE>::threads, 1)
               double v = 0.0;
               if (sc < 1.0 / 0.0) v = (double)fmaf(sm.x, sm.x, sm.y * sm.y) * sc;
               else atomicOr(a.err, 2);  // matrix_elt_simplified: den = 0
-              double* out = a.v3_layout == 1 ? a.v3sq + (((size_t)row * 27 + l2 * 9 + l3 * 3 + l1) * nk + qg)
-                                             : a.v3sq + ((size_t)row * nk + qg) * 27 + l1 * 9 + l2 * 3 + l3;
-              *out = v;
+              const size_t o = a.v3_layout == 1 ? ((size_t)row * 27 + l2 * 9 + l3 * 3 + l1) * nk + qg
+                                                 : ((size_t)row * nk + qg) * 27 + l1 * 9 + l2 * 3 + l3;
+              if (a.v3sq_f32) a.v3sq_f32[o] = (float)v;  // the mixed pipeline's FP32 |V3|^2
+              else a.v3sq[o] = v;
             }
         }
       }

@@ -39,7 +39,7 @@ class AldError(RuntimeError):
 class Options(C.Structure):
     _fields_ = [("delta", C.c_int), ("precision", C.c_int), ("cg_stop", C.c_int), ("cg_max_iter", C.c_int),
                 ("cg_ndig", C.c_int), ("cg_tol", C.c_double), ("width_cm", C.c_double), ("device", C.c_int),
-                ("chunk_bytes", C.c_size_t)]
+                ("chunk_bytes", C.c_size_t), ("deterministic", C.c_int)]
 
 
 class Info(C.Structure):

@@ -59,6 +59,8 @@ typedef struct ald_options {
   double width_cm;   /* Gaussian width in cm^-1 for ALD_DELTA_GAUSS (<=0: latdyn width) */
   int device;        /* CUDA device ordinal                                             */
   size_t chunk_bytes;/* device bytes for one chunk of |V3|^2 rows (0 = automatic)      */
+  int deterministic; /* 1: the pipeline's tetrahedron delta sums R1/R2 in a fixed order
+                        (the same bits on every run; slower), 0: FP64 atomics         */
 } ald_options;
 
 typedef struct ald_ctx ald_ctx;
@@ -199,7 +201,11 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
  * CG work vectors live in a fixed __device__ array of the library, so
  * n <= ALD_CG_STATIC_MAX_N (ALD_ERR_ARG otherwise).  The first call on a
  * device looks that array's address up and keeps it for the life of the
- * process; make that first call before any stream capture.
+ * process; make that first call before any stream capture, and do not reset
+ * the device (cudaDeviceReset) between calls.  Every 8 iterations the call
+ * reads the stop flag back to the host, synchronising `stream`.  Buffers
+ * whose allocation is shorter than n*n (a) or n (b, vmin) doubles are
+ * refused with ALD_ERR_ARG.
  * Calls share the array: calls that overlap on one device race.  Returns
  * ALD_OK or ALD_WARN_CG_MAXITER like ald_cg_quadratic. */
 #define ALD_CG_STATIC_MAX_N 32768
