@@ -506,7 +506,9 @@ __host__ __device__ inline FusedShape fused_shape(const Geometry& g) {
   f.maxrec = 6 * f.R * N2;
   const size_t nw2 = (size_t)(f.NW + (f.NW & 1));
   // doubles: G; ushort4 records; ints: w, src, q3; floats: E; bytes: flags; ushorts: queue
-  f.smem = nw2 * 8 + (size_t)f.maxrec * 8 + (size_t)f.NW * 3 * 4 + (size_t)f.NW * 4 + (size_t)((f.NW + 3) & ~3) +
+  // doubles: G, omega(w, l2), n(w, l2); ushort4 records; ints: w, src, q3;
+  // floats: E; bytes: flags; ushorts: queue
+  f.smem = nw2 * 8 * 3 + (size_t)f.maxrec * 8 + (size_t)f.NW * 3 * 4 + (size_t)f.NW * 4 + (size_t)((f.NW + 3) & ~3) +
            (size_t)f.maxrec * g.b * 2;
   return f;
 }
@@ -528,7 +530,9 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
   // shared layout
   const int nw2 = NW + (NW & 1);
   double* s_G = reinterpret_cast<double*>(smraw);
-  ushort4* s_recp = reinterpret_cast<ushort4*>(s_G + nw2);
+  double* s_fw = s_G + nw2;  // omega(w, l2) and n(w, l2): the same for every slice
+  double* s_n2 = s_fw + nw2;
+  ushort4* s_recp = reinterpret_cast<ushort4*>(s_n2 + nw2);
   int* s_w = reinterpret_cast<int*>(s_recp + maxrec);
   int* s_src = s_w + NW;
   int* s_q3 = s_src + NW;
@@ -564,6 +568,8 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
     s_q3[p] = q3;
     s_src[p] = proc == 0 ? w : neg_index(g, mw);
     s_fl[p] = (unsigned char)((at_gamma_index(g, mw) ? 1 : 0) | (at_gamma_index(g, m3) ? 2 : 0));
+    s_fw[p] = a.freq[(size_t)w * b + l2];
+    s_n2[p] = a.dist[(size_t)w * b + l2];
   }
   // (2pi)^2/nkc and the 1/6 of the corner weights in one factor
   const double fnorm6 = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc / 6.0;
@@ -594,35 +600,37 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
     lp[c] = cell_ok ? (o0 * (R + 1) + cdj + o1) * N2 + kk : 0;
     s_lp[tid][c] = (unsigned short)lp[c];
   }
-  for (int l3 = 0; l3 < b; ++l3) {
-    __syncthreads();  // window staged / previous slice done
-    if (F32W && a.brange) {
-      // The energies of this slice, -+omega(w,l2) + omega(q3,l3), lie within
-      // the bands' ranges over the mesh; when that range misses every
-      // omega1 of the row (with a margin far above the FP32 rounding of E)
-      // no tetrahedron of the slice has weight: skip it (uniform branch).
-      // Measured on B200 (16^3 rock-salt): mixed delta 4.11 -> 4.01 ms, while
-      // the FP64 build of the kernel ran 6.85 -> 7.10 ms with it, so there it
-      // is left out.
+  // The energies of slice l3, -+omega(w,l2) + omega(q3,l3), lie within the
+  // bands' ranges over the mesh; when that range misses every omega1 of the
+  // row (with a margin far above the FP32 rounding of E) no tetrahedron of the
+  // slice has weight and the slice is skipped (the same for every thread).
+  unsigned live = 0xffffffffu;
+  if (a.brange) {
+    __syncthreads();  // s_om
+    double o1min = s_om[0], o1max = s_om[0];
+    for (int l = 1; l < b; ++l) {
+      o1min = fmin(o1min, s_om[l]);
+      o1max = fmax(o1max, s_om[l]);
+    }
+    for (int l3 = 0; l3 < b; ++l3) {
       const double lo2 = a.brange[l2], hi2 = a.brange[b + l2], lo3 = a.brange[l3], hi3 = a.brange[b + l3];
       const double emin = proc == 0 ? lo3 - hi2 : lo2 + lo3, emax = proc == 0 ? hi3 - lo2 : hi2 + hi3;
       const double tol = 1e-5 * (fabs(hi2) + fabs(hi3)) + 1e-10;
-      double o1min = s_om[0], o1max = s_om[0];
-      for (int l = 1; l < b; ++l) {
-        o1min = fmin(o1min, s_om[l]);
-        o1max = fmax(o1max, s_om[l]);
-      }
-      if (emax + tol < o1min || emin - tol > o1max) continue;
+      if (emax + tol < o1min || emin - tol > o1max) live &= ~(1u << l3);
     }
+  }
+  for (int l3 = 0; l3 < b; ++l3) {
+    if (!((live >> l3) & 1u)) continue;
+    __syncthreads();  // window staged / previous slice done
     if (tid == 0) {
       s_nrec = 0;
       s_nq = 0;
     }
     for (int p = tid; p < NW; p += blockDim.x) {
       const int q3 = s_q3[p];
-      const double fw = a.freq[(size_t)s_w[p] * b + l2], f3 = a.freq[(size_t)q3 * b + l3];
+      const double fw = s_fw[p], f3 = a.freq[(size_t)q3 * b + l3];
       s_E[p] = (float)(proc == 0 ? -fw + f3 : fw + f3);
-      const double n2 = a.dist[(size_t)s_w[p] * b + l2], n3 = a.dist[(size_t)q3 * b + l3];
+      const double n2 = s_n2[p], n3 = a.dist[(size_t)q3 * b + l3];
       const bool zero = (l2 < 3 && (s_fl[p] & 1)) || (l3 < 3 && (s_fl[p] & 2));
       s_G[p] = zero ? 0.0 : (proc == 0 ? n2 * (n3 + 1) : (n2 + 1) * (n3 + 1));
     }
