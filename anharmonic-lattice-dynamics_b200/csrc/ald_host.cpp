@@ -26,6 +26,7 @@
 #include <unordered_map>
 
 #include "ald_internal.h"
+#include "ald_pool.h"
 
 namespace ald {
 
@@ -631,8 +632,8 @@ std::string build_tables(const System& S, Tables& T) {
     for (int a = 0; a < 3; ++a) f[a] = Ginv[cm(a, 0)] * kc[0] + Ginv[cm(a, 1)] * kc[1] + Ginv[cm(a, 2)] * kc[2];
   };
   // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table.  They
-  // depend on the mesh only, so a host thread builds them while the IBZ and
-  // the stars are found.
+  // depend on the mesh only, so one worker builds them while the others find
+  // the stars of the mesh points.
   auto build_tet = [&]() -> std::string {
     static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
                                         {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
@@ -661,12 +662,6 @@ std::string build_tables(const System& S, Tables& T) {
     return std::string();
   };
   std::string tet_err;
-  struct Joiner {
-    std::thread t;
-    ~Joiner() {
-      if (t.joinable()) t.join();
-    }
-  } tet_thread{std::thread([&] { tet_err = build_tet(); })};
   // ---- IBZ (get_weights): first mesh point of each exact (unfolded) orbit
   T.mapibz.assign(T.nkc, 0);
   T.mapinv.clear();
@@ -678,27 +673,32 @@ std::string build_tables(const System& S, Tables& T) {
   // (-2: off the mesh or outside its cell, -1: end of the list); the pass
   // that assigns IBZ points is sequential, as in the reference.
   const int npg = T.npg;
+  // task 0 builds the tetrahedra (they depend on the mesh only); tasks 1..
+  // take stripes of mesh points, on the library's worker pool
   std::vector<int> cand((size_t)T.nkc * npg, -1);
   {
-    const int nthr = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthr; ++t)
-      pool.emplace_back([&, t] {
-        std::vector<std::array<double, 3>> ar;
-        std::vector<int> ao;
-        for (int n = t; n < T.nkc; n += nthr) {
-          star(&T.kpc32[3 * (size_t)n], ar, ao);
-          for (size_t c = 0; c < ar.size(); ++c) {
-            double f[3];
-            reduced(ar[c].data(), f);
-            bool in_cell;
-            const int idx = locate(f, in_cell);
-            cand[(size_t)n * npg + c] = idx >= 0 && in_cell ? idx : -2;
-          }
+    const int nthr = pool_width();
+    run_parallel(nthr + 1, [&](int task) {
+      if (task == 0) {
+        tet_err = build_tet();
+        return;
+      }
+      const int t = task - 1;
+      std::vector<std::array<double, 3>> ar;
+      std::vector<int> ao;
+      for (int n = t; n < T.nkc; n += nthr) {
+        star(&T.kpc32[3 * (size_t)n], ar, ao);
+        for (size_t c = 0; c < ar.size(); ++c) {
+          double f[3];
+          reduced(ar[c].data(), f);
+          bool in_cell;
+          const int idx = locate(f, in_cell);
+          cand[(size_t)n * npg + c] = idx >= 0 && in_cell ? idx : -2;
         }
-      });
-    for (auto& th : pool) th.join();
+      }
+    });
   }
+  if (!tet_err.empty()) return tet_err;
   for (int n = 0; n < T.nkc; ++n) {
     int found = -1;
     for (int c = 0; c < npg; ++c) {
@@ -747,26 +747,23 @@ std::string build_tables(const System& S, Tables& T) {
   {
     std::vector<int> aq((size_t)T.nibz * npg, -1), ao((size_t)T.nibz * npg, 0), ain((size_t)T.nibz * npg, 0),
         na(T.nibz, 0);
-    const int nthr = (int)std::max(1u, std::min(32u, std::thread::hardware_concurrency()));
-    std::vector<std::thread> pool;
-    for (int t = 0; t < nthr; ++t)
-      pool.emplace_back([&, t] {
-        std::vector<std::array<double, 3>> ar;
-        std::vector<int> op;
-        for (int i = t; i < T.nibz; i += nthr) {
-          star(&T.kibz[3 * (size_t)i], ar, op);
-          na[i] = (int)ar.size();
-          for (size_t c = 0; c < ar.size(); ++c) {
-            double f[3];
-            reduced(ar[c].data(), f);
-            bool in_cell;
-            aq[(size_t)i * npg + c] = locate(f, in_cell);
-            ao[(size_t)i * npg + c] = op[c];
-            ain[(size_t)i * npg + c] = in_cell ? 1 : 0;
-          }
+    const int nthr = pool_width();
+    run_parallel(nthr, [&](int t) {
+      std::vector<std::array<double, 3>> ar;
+      std::vector<int> op;
+      for (int i = t; i < T.nibz; i += nthr) {
+        star(&T.kibz[3 * (size_t)i], ar, op);
+        na[i] = (int)ar.size();
+        for (size_t c = 0; c < ar.size(); ++c) {
+          double f[3];
+          reduced(ar[c].data(), f);
+          bool in_cell;
+          aq[(size_t)i * npg + c] = locate(f, in_cell);
+          ao[(size_t)i * npg + c] = op[c];
+          ain[(size_t)i * npg + c] = in_cell ? 1 : 0;
         }
-      });
-    for (auto& th : pool) th.join();
+      }
+    });
     T.arm_off.assign(1, 0);
     T.star_off.assign(1, 0);
     for (int i = 0; i < T.nibz; ++i) {
@@ -784,8 +781,6 @@ std::string build_tables(const System& S, Tables& T) {
       T.star_off.push_back((int)T.star_q.size());
     }
   }
-  tet_thread.t.join();
-  if (!tet_err.empty()) return tet_err;
   // ---- exact phases: q(m).R_j = 2 pi sum_a (m_a/N_a - s/2) n_ja
   long L = 1;
   for (int a = 0; a < 3; ++a) L = std::lcm(L, (long)S.nc[a]);

@@ -22,6 +22,7 @@ COMMON = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler",
 
 SOURCES = {
     "ald_host.cpp": [],
+    "ald_pool.cpp": [],
     "ald_capi.cpp": [],
     "ald_pipeline.cpp": [],
     "ald_phonon.cu": [],
