@@ -258,31 +258,36 @@ def cpu_baseline(d: str, rows: int = 0, gauss: bool = False):
 
 # DRAM bytes (read + write) of one launch from ncu captures of this workload
 # (profiles/), keyed by (stage, nkc, bands, rows per launch)
-NCU_TRAFFIC = {("delta", 4096, 6, 72): 452.72e6, ("v3", 4096, 6, 72): 477.53e6}
+# (stage, nkc, bands, precision, rows per launch): DRAM read + write of one launch
+# (profiles/kappa_pipeline_nacl_morse_mesh16.md)
+NCU_TRAFFIC = {("delta", 4096, 6, "mixed", 150): 834.30e6, ("delta", 4096, 6, "fp64", 75): 587.54e6,
+               ("v3", 4096, 6, "mixed", 150): 481.57e6}
 
 
-def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8, rows_per_launch=None):
+def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8, rows_per_launch=None,
+             precision="mixed"):
     """The dominant device stage against its ceiling.
 
     achieved = algorithmic bytes per launch / device time per launch (the
     stage's CUDA events over the timed steps, divided by its launches).
     Algorithmic bytes of the tetrahedron delta: R1/R2 written once,
-    2 nibz nkc b^2 8 bytes per step; `wide_bytes` adds the |V3|^2 read and
-    the R1/R2 read-modify-write of the fused kernel."""
+    2 nibz nkc b^2 8 bytes per step; `wide_bytes` adds the |V3|^2 read (FP32
+    in the mixed path) and the R1/R2 read-modify-write of the fused kernel."""
     stages = {k: v for k, v in stage_ms.items() if k != "total"}
     dom = max(stages, key=stages.get)
     n = launches.get(dom, 1) or 1
     ms = stages[dom] / n
     N = 3 * b * nibz
     b3 = b ** 3
+    vb = 4 if precision == "mixed" else 8  # the mixed pipeline keeps |V3|^2 in FP32
     alg = {
         "delta": 2 * nibz * nkc * b * b * 8 / n,
-        "v3": nibz * nkc * (b3 * 8) / n,
+        "v3": nibz * nkc * (b3 * vb) / n,
         "collision": N * N * cm_bytes / n,
         "cg": N * N * cm_bytes,
     }
-    wide = {"delta": nibz * nkc * (b3 * 8 + 2 * 2 * b * b * 8) / n,
-            "v3": nibz * nkc * (b3 * 8 + 2 * b * b * 16) / n}
+    wide = {"delta": nibz * nkc * (b3 * vb + 2 * 2 * b * b * 8) / n,
+            "v3": nibz * nkc * (b3 * vb + 2 * b * b * 16) / n}
     if dom == "cg":
         ms = stages[dom] / max(1, cg_iters)
     by = alg.get(dom)
@@ -292,8 +297,8 @@ def roofline(stage_ms, launches, nibz, nkc, b, peaks, cg_iters=1, cm_bytes=8, ro
     ach = by / (ms * 1e-3) / 1e9
     traffic = None
     rpl = rows_per_launch or max(1, nibz // n)
-    for (st, nk, bb, rows), t in NCU_TRAFFIC.items():
-        if st == dom and nk == nkc and bb == b:
+    for (st, nk, bb, pr, rows), t in NCU_TRAFFIC.items():
+        if st == dom and nk == nkc and bb == b and pr == precision:
             traffic = t * rpl / rows  # DRAM traffic grows with the rows of a launch
     out = {"bound": "hbm", "achieved": ach, "peak": peaks["hbm_gbs"], "unit": "GB/s",
            "frac": ach / peaks["hbm_gbs"], "traffic": traffic, "kernel": dom, "ms_per_launch": ms,
@@ -526,7 +531,7 @@ def main():
         peaks = _peaks()
         mixed_head = precisions[-1] == ald.MIXED
         rf = roofline(per_step, per_launch_counts, nibz, nkc, b, peaks, cg_iters=max(1, out["cg_iters"]),
-                      cm_bytes=4 if mixed_head else 8)
+                      cm_bytes=4 if mixed_head else 8, precision="mixed" if mixed_head else "fp64")
         rf_v3 = v3_roofline(per_step, per_launch_counts, nibz, nkc, b, peaks,
                             "mixed path" if mixed_head else "fp64 path")
         cb = None
