@@ -408,7 +408,7 @@ void ald_default_options(ald_options* o) {
   o->width_cm = -1;
   o->device = 0;
   o->chunk_bytes = 0;
-  o->deterministic = 0;
+  o->deterministic = ALD_DET_AUTO;
 }
 
 const char* ald_last_error(void) { return g_err.c_str(); }

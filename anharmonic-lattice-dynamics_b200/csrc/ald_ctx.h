@@ -49,6 +49,7 @@ struct ald_ctx {
   DevBuf<double> w_brange;  // omega range of every band over the mesh
   DevBuf<char> w_scratch;
   DevBuf<double> w_heev;    // Householder eigensolver workspace (large cells)
+  DevBuf<double> w_rmax;    // deterministic delta: each R entry's largest term (FP64 bits)
   CgWork cg;
   bool have_phonons = false;
   double dist_tempk = -1;

@@ -346,6 +346,13 @@ struct CombineArgs {
   double* R2;
   double* R1p;               // optional [row][q][l1][l3] = sum_l2 P1 (update_mpi); nullptr = skip
   double* R2p;
+  // the two passes of the deterministic fused delta: per R1/R2/R1p/R2p entry
+  // the largest single term (its FP64 bits; every term is >= 0), then the
+  // terms as 62-bit fixed point scaled by that bound (delta_fused mode 1, 2)
+  unsigned long long* M1 = nullptr;
+  unsigned long long* M2 = nullptr;
+  unsigned long long* M1p = nullptr;
+  unsigned long long* M2p = nullptr;
   double* P1s;               // optional [row][q][l1][l2][l3] (P1smpi)
   double* P2s;
   double* P1;                // optional Bose-weighted
@@ -356,13 +363,15 @@ size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss);
 cudaError_t launch_combine(const CombineArgs& a, void* scratch, cudaStream_t s);
 // tetrahedron delta fused into R1/R2 (pipeline; P1s/P2s/P1/P2 not produced);
 // R1/R2 of the chunk must be zero on entry
+// mode 0: the terms added with FP64 atomics (arrival order);
+// mode 1 and 2 + launch_delta_finalize: the same sums with the same bits on
+// every run -- mode 1 records each entry's largest term in M1/M2 (M1p/M2p),
+// mode 2 adds every term as an integer, round(term * 2^(62 - e)), with
+// 2^e >= kDetTerms(b) x that largest term, and finalize converts the integer
+// sums back: R = sum * 2^(e - 62).  R must be zero and M zero on entry.
 bool delta_fused_supported(const Geometry& g);
-cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s);
-// the same deterministically: the mesh walked plane by plane, each R1/R2
-// entry written by one thread in a fixed order (no atomics, R1/R2 need no
-// zeroing); band marginals R1p/R2p are not produced
-bool delta_plane_supported(const Geometry& g, int f32w);
-cudaError_t launch_delta_plane(const CombineArgs& a, cudaStream_t s);
+cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s, int mode = 0);
+cudaError_t launch_delta_finalize(double* R, const unsigned long long* M, size_t n, int b, cudaStream_t s);
 // any number of bands (large cells): the tetrahedron or Gaussian delta into
 // R1/R2 and/or P1s/P2s straight from |V3|^2 of the chunk; for the tetrahedron
 // R1/R2/P1s/P2s (and R1p/R2p) must be zero on entry; P1/P2 are not produced

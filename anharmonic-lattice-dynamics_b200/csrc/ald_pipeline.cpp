@@ -191,9 +191,11 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   const int v3_layout = v3_pipeline_layout(b, c->opt.precision);
   const bool mixed = c->opt.precision != ALD_FP64;
   const bool fused = !gauss && v3_layout != 2 && delta_fused_supported(c->geo);
-  // deterministic option: the plane-walking form of the fused delta where it
-  // applies (no band marginals)
-  const bool plane = fused && !it && v3_layout <= 1 && c->opt.deterministic && delta_plane_supported(c->geo, mixed);
+  // deterministic option: the fused delta in two passes with fixed-point sums
+  // (the same bits on every run); its per-entry largest terms need a buffer
+  // of the chunk's R1/R2 (and R1p/R2p) size
+  const bool det = fused && (c->opt.deterministic > 0 ||
+                             (c->opt.deterministic == ALD_DET_AUTO && c->opt.precision == ALD_FP64));
   // more than 16 bands, or layout 2: the band-generic delta kernels, straight into R1/R2
   const bool any = !fused && (b > kDeltaSmallBands || v3_layout == 2);
   // the mixed pipeline hands |V3|^2 to the delta in FP32 where the delta
@@ -204,6 +206,8 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
   const int K = v3f ? std::min(nibz, 2 * rows_per_chunk(c)) : rows_per_chunk(c);
   const size_t v3n = (size_t)K * nkc * b * b * b;
   ALD_CKA(v3.alloc(v3f ? (v3n + 1) / 2 : v3n));
+  const size_t rchunk = (size_t)K * nkc * b * b;  // entries of one chunk's R1
+  if (det) ALD_CKA(c->w_rmax.alloc((it ? 4 : 2) * rchunk));
   if (!fused && !any) ALD_CKA(escratch.alloc(std::max<size_t>(256, combine_scratch_bytes(c->geo, K, gauss))));
   ALD_CKA(c->w_brange.alloc((size_t)2 * b));
   ALD_CK(launch_band_range(c->geo, c->freq.p, c->w_brange.p, s));
@@ -245,14 +249,31 @@ static int run_pipeline(ald_ctx* c, double tempk, ald_kappa_result* res, double*
       ALD_CK(cudaMemsetAsync(a.R1p, 0, rbytes, s));
       ALD_CK(cudaMemsetAsync(a.R2p, 0, rbytes, s));
     }
-    if ((fused && !plane) || (any && !gauss)) {
+    if (det) {
+      unsigned long long* M = reinterpret_cast<unsigned long long*>(c->w_rmax.p);
+      a.M1 = M;
+      a.M2 = M + rchunk;
+      a.M1p = it ? M + 2 * rchunk : nullptr;
+      a.M2p = it ? M + 3 * rchunk : nullptr;
+      ALD_CK(cudaMemsetAsync(M, 0, (it ? 4 : 2) * rchunk * sizeof(unsigned long long), s));
+    }
+    if (fused || (any && !gauss)) {
       ALD_CK(cudaMemsetAsync(a.R1, 0, rbytes, s));
       ALD_CK(cudaMemsetAsync(a.R2, 0, rbytes, s));
     }
     ALD_CK(tm.begin(2));
-    if (plane) {
-      ALD_CK(launch_delta_plane(a, s));
-      res->launches[2] += 1;
+    if (det) {
+      const size_t n = (size_t)nr * nkc * b * b;
+      ALD_CK(launch_delta_fused(a, s, 1));
+      ALD_CK(launch_delta_fused(a, s, 2));
+      ALD_CK(launch_delta_finalize(a.R1, a.M1, n, b, s));
+      ALD_CK(launch_delta_finalize(a.R2, a.M2, n, b, s));
+      res->launches[2] += 4;
+      if (it) {
+        ALD_CK(launch_delta_finalize(a.R1p, a.M1p, n, b, s));
+        ALD_CK(launch_delta_finalize(a.R2p, a.M2p, n, b, s));
+        res->launches[2] += 2;
+      }
     } else if (fused) {
       ALD_CK(launch_delta_fused(a, s));
       res->launches[2] += 1;
@@ -500,7 +521,7 @@ extern "C" int ald_kappa_pipeline(ald_ctx* c, double tempk, ald_kappa_result* re
 // the pipeline workspaces of a context (their blocks go to the library's
 // device-memory cache, where the next structure of the same sizes finds them)
 static void release_pipeline_workspaces(ald_ctx* c) {
-  for (DevBuf<double>* b : {&c->w_R1, &c->w_R2, &c->w_v3, &c->w_cm, &c->w_R1p, &c->w_R2p, &c->w_heev})
+  for (DevBuf<double>* b : {&c->w_R1, &c->w_R2, &c->w_v3, &c->w_cm, &c->w_R1p, &c->w_R2p, &c->w_heev, &c->w_rmax})
     b->free();
   c->w_h.free();
   c->w_v3work.free();

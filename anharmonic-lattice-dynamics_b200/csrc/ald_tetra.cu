@@ -465,8 +465,17 @@ __global__ void __launch_bounds__(256) q_from_r_kernel(Geometry g, int n1_first,
 //      (FP64 atomics in L2; FP64 atomics on shared memory would be CAS loops).
 //      |V3|^2(src(w), l1, l2, l3) is gathered where needed; in the slice-major
 //      layout the corners of one tetrahedron share sectors.
-// The sums run in atomic order (FP64 rounding, not bitwise, against the
-// reference's P1/P2 summed over l3).
+// MODE 0: the sums run in atomic order (FP64 rounding, not bitwise, against
+// the reference's P1/P2 summed over l3).  MODE 1 and 2 (the deterministic
+// option) run the kernel twice: first each entry's largest term (its FP64
+// bits, atomicMax: every term is >= 0 and the bit order of nonnegative
+// doubles is their numeric order), then every term as a 64-bit integer,
+// round(term * 2^(62 - e)) with 2^e >= kDetTerms(b) x the largest term, added
+// with integer atomics: integer sums do not depend on their order.  At most
+// kDetTerms(b) = 24 b terms reach an entry (24 tetrahedron corners at a
+// point, b slices l3 -- or b bands l2 for the marginals), so the sum stays
+// below 2^63 and each rounding is at most 2^-63 x 24 b of the entry.
+// launch_delta_finalize turns the integers back into doubles.
 // corners of make_kp_reg_tet's six tetrahedra (c = o0 + 2 o1 + 4 o2), 3 bits
 // each, tetrahedra 0..4 in one word; tetrahedron 5 is (2, 5, 6, 7)
 constexpr unsigned long long kTetCornerCode =
@@ -477,18 +486,20 @@ constexpr unsigned kTet5Code = 2u | 5u << 3 | 6u << 6 | 7u << 9;
 __device__ __forceinline__ unsigned tet_code(int t) {
   return t < 5 ? (unsigned)(kTetCornerCode >> (12 * t)) & 0xfffu : kTet5Code;
 }
-// slot (0..3) of corner c in tetrahedron t, plus one; 0 when c is not a corner
-// of t.  Three bits per tetrahedron.
-__host__ __device__ constexpr unsigned tet_slot_code(int c) {
-  unsigned code = 0;
-  constexpr int T[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
-  for (int t = 0; t < 6; ++t)
-    for (int k = 0; k < 4; ++k)
-      if (T[t][k] == c) code |= (unsigned)(k + 1) << (3 * t);
-  return code;
-}
 
 constexpr int kFusedThreads = 128;
+
+__host__ __device__ constexpr int kDetTerms(int b) { return 24 * b; }
+// exponent e of the fixed-point scale of an entry whose largest term has the
+// bits m: 2^e >= kDetTerms(b) * largest term
+__device__ __forceinline__ int det_exponent(unsigned long long m, int b) {
+  int e;
+  frexp(__longlong_as_double((long long)m) * (double)kDetTerms(b), &e);
+  return e;
+}
+__device__ __forceinline__ unsigned long long det_fixed(double v, unsigned long long m, int b) {
+  return (unsigned long long)llrint(ldexp(v, 62 - det_exponent(m, b)));
+}
 
 struct FusedShape {
   int R, nbj, NW, maxrec;
@@ -513,7 +524,7 @@ __host__ __device__ inline FusedShape fused_shape(const Geometry& g) {
   return f;
 }
 
-template <int B, bool F32W, class VT>
+template <int B, bool F32W, class VT, int MODE>
 __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT* __restrict__ v3sq) {
   extern __shared__ __align__(16) unsigned char smraw[];
   __shared__ double s_om[B], s_nb1[B];
@@ -575,6 +586,8 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
   const double fnorm6 = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc / 6.0;
   double* Rp = proc == 0 ? a.R1 : a.R2;
   double* Rpp = proc == 0 ? a.R1p : a.R2p;  // band marginal over l2 (optional)
+  unsigned long long* Mp = proc == 0 ? a.M1 : a.M2;  // largest terms (MODE 1, 2)
+  unsigned long long* Mpp = proc == 0 ? a.M1p : a.M2p;
   // |V3|^2 strides of (q, l1, l2, l3) in the chunk's layout
   size_t sq, s1, s2, s3;
   if (a.v3_layout == 1) {
@@ -796,8 +809,7 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
       }
       const int pos_pt[4] = {pp.x, pp.y, pp.z, pp.w};
       const double nb1 = s_nb1[l1];
-      double* Rrow = Rp + (size_t)row * nkc * b * b + l1 * b + l2;
-      double* Rrowp = Rpp ? Rpp + (size_t)row * nkc * b * b + l1 * b + l3 : nullptr;
+      const size_t o = (size_t)row * nkc * b * b + l1 * b + l2, op = (size_t)row * nkc * b * b + l1 * b + l3;
       const VT* vs = v3row + l2 * s2 + l3 * s3 + l1 * s1;
 #pragma unroll
       for (int k = 0; k < 4; ++k) {
@@ -805,8 +817,18 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
         const double G = s_G[p];
         if (cp[k] == 0.0 || G == 0.0) continue;
         const double val = cp[k] * ((double)__ldg(vs + (size_t)s_src[p] * sq) * fnorm6) * (nb1 * G);
-        atomicAdd(Rrow + (size_t)s_w[p] * b * b, val);
-        if (Rrowp) atomicAdd(Rrowp + (size_t)s_w[p] * b * b, val);
+        const size_t w = (size_t)s_w[p] * b * b;
+        if constexpr (MODE == 0) {
+          atomicAdd(Rp + o + w, val);
+          if (Rpp) atomicAdd(Rpp + op + w, val);
+        } else if constexpr (MODE == 1) {
+          const unsigned long long bits = (unsigned long long)__double_as_longlong(val);
+          atomicMax(Mp + o + w, bits);
+          if (Rpp) atomicMax(Mpp + op + w, bits);
+        } else {
+          atomicAdd(reinterpret_cast<unsigned long long*>(Rp + o + w), det_fixed(val, Mp[o + w], b));
+          if (Rpp) atomicAdd(reinterpret_cast<unsigned long long*>(Rpp + op + w), det_fixed(val, Mpp[op + w], b));
+        }
       }
     }
   }
@@ -815,437 +837,22 @@ __device__ __forceinline__ void delta_fused_body(const CombineArgs& a, const VT*
 // the kernels: the mixed one with the compiler's own register choice (55-62
 // registers at 6 bands, measured fastest), the FP64 one held to 64 registers
 // (8 CTAs per SM; measured fastest for it)
-template <int B, class VT>
+template <int B, class VT, int MODE>
 __global__ void __launch_bounds__(kFusedThreads) delta_fused_mixed_kernel(CombineArgs a, const VT* __restrict__ v3sq) {
-  delta_fused_body<B, true, VT>(a, v3sq);
+  delta_fused_body<B, true, VT, MODE>(a, v3sq);
 }
-template <int B>
+template <int B, int MODE>
 __global__ void __launch_bounds__(kFusedThreads, 8) delta_fused_fp64_kernel(CombineArgs a,
                                                                             const double* __restrict__ v3sq) {
-  delta_fused_body<B, false, double>(a, v3sq);
+  delta_fused_body<B, false, double, MODE>(a, v3sq);
 }
 
-// ---------------------------------------------------------------------------
-// Deterministic tetrahedron delta for the pipeline: the mesh walked plane by
-// plane, every R entry written by one thread in a fixed order.
-//
-// A CTA owns one IBZ row, one process and one band l2 and walks the cells of
-// the mesh along the first mesh axis (planes m0 = 0 .. N0-1).  Thread p owns
-// the in-plane position p = m1*N2 + m2: the cell with that base point in the
-// current plane, and the mesh points at p in the plane below (i) and above
-// (i+1) the cells.  When plane i starts, the energies of plane i+1 are staged
-// for every l3 (plane i's were staged one plane before).  Then per l3 (one
-// slice of the reference's loops):
-//   1. thread = cell: FP32 range tests of the cell's six tetrahedra against
-//      omega1 (as in delta_fused_kernel); the cell's (tetrahedron, l1) pairs,
-//      ordered by tetrahedron, then l1, go to a run of a shared queue (one
-//      reservation per warp); the run's start and length are kept per cell;
-//   2. thread = queue entry: weight_tet's four corner weights (bitwise
-//      ald_tet.h, ties broken in the tetrahedron's corner-list order);
-//   3. thread = position: for the point below and the point above, the
-//      weights of the runs of its four adjacent cells whose tetrahedron has
-//      that point as a corner, summed per l1 in (cell, run) order -- an order
-//      that does not depend on where the runs landed in the queue; then
-//      R += (sum/6) |V3|^2(src(w), l1, l2, l3) (2pi)^2/nkc n1 G(w).
-// Queues, run tables and weights are double-buffered by slice, so a slice
-// needs two barriers.  A slice whose pairs overflow the queue is redone in
-// windows of the queue's size over runs laid out by a block-wide scan in
-// thread order (the same order on every run).
-// A point's sum is complete after two planes: cells of plane i-1 (the point
-// as an upper corner) and of plane i (lower corner).  The upper part is
-// stored in R when plane i-1 ends; the same thread adds the lower part when
-// plane i ends (for plane 0, the upper part of the cells of plane N0-1 is
-// added after the last plane).  No atomics into R, no zeroing of R beforehand,
-// and the same bits on every run.
-constexpr int kPlaneQueue = 512;
-constexpr int kPlaneMaxPos = 256;  // positions per plane (threads per CTA)
-
-struct PlaneShape {
-  int P, threads;
-  size_t smem;
-};
-
-// up to 6 bands the R parts of a position stay in registers, above in shared memory
-template <int B>
-struct PlaneAccInRegs {
-  static constexpr bool value = B <= 6;
-};
-
-template <int B, bool F32W>
-__host__ __device__ inline PlaneShape plane_shape(const Geometry& g) {
-  PlaneShape s;
-  s.P = g.nc[1] * g.nc[2];
-  s.threads = (s.P + 31) / 32 * 32;
-  using WT = typename std::conditional<F32W, float, double>::type;
-  // weights [2][queue][4]; weight sums [2][B][P]; R parts [2][B][P] doubles
-  // (more than 6 bands); E [2][B][P] floats; run starts [2][P] ints; queue
-  // entries [2][queue] ushorts; run lengths [2][P] bytes
-  s.smem = (size_t)2 * kPlaneQueue * 4 * sizeof(WT) + (size_t)2 * B * s.P * sizeof(WT) +
-           (PlaneAccInRegs<B>::value ? 0 : (size_t)2 * B * s.P * sizeof(double)) + (size_t)2 * B * s.P * sizeof(float) +
-           (size_t)2 * s.P * sizeof(int) + (size_t)2 * kPlaneQueue * sizeof(unsigned short) + (size_t)2 * s.P + 16;
-  return s;
-}
-
-template <int B, bool F32W, class VT>
-__global__ void __launch_bounds__(kPlaneMaxPos, 2) delta_plane_kernel(CombineArgs a, const VT* __restrict__ v3sq) {
-  using WT = typename std::conditional<F32W, float, double>::type;
-  constexpr bool kAccReg = PlaneAccInRegs<B>::value;
-  extern __shared__ __align__(16) unsigned char smraw[];
-  __shared__ double s_om[B], s_nb1[B];
-  __shared__ int s_nq[3];   // queue fill of the slice, by slice number mod 3
-  __shared__ int s_ws[32];  // warp totals of the overflow scan
-  const Geometry& g = a.geo;
-  const PlaneShape S = plane_shape<B, F32W>(g);
-  const int P = S.P, N0 = g.nc[0], N1 = g.nc[1], N2 = g.nc[2], nkc = g.nkc, b = g.b;
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
-  const int l2 = blockIdx.x, proc = blockIdx.y, row = blockIdx.z;
-  WT* s_wt = reinterpret_cast<WT*>(smraw);                                    // [2][kPlaneQueue][4]
-  WT* s_ws2 = s_wt + (size_t)2 * kPlaneQueue * 4;                             // [2][B][P] weight sums
-  double* s_acc = reinterpret_cast<double*>(s_ws2 + (size_t)2 * B * P);       // [2][B][P] (B > 6)
-  float* s_E = reinterpret_cast<float*>(s_acc + (kAccReg ? 0 : (size_t)2 * B * P));  // [2][B][P]
-  int* s_qs = reinterpret_cast<int*>(s_E + (size_t)2 * B * P);                // [2][P] run starts
-  unsigned short* s_qe = reinterpret_cast<unsigned short*>(s_qs + 2 * P);     // [2][kPlaneQueue]
-  unsigned char* s_qn = reinterpret_cast<unsigned char*>(s_qe + 2 * kPlaneQueue);  // [2][P] run lengths
-
-  const int q1 = a.mapinv[a.n1_first + row];
-  int m1[3];
-  decompose(g, q1, m1);
-  if (tid < b) {
-    s_om[tid] = a.freq[(size_t)q1 * b + tid];
-    s_nb1[tid] = a.dist[(size_t)q1 * b + tid];
-  }
-  if (tid < 3) s_nq[tid] = 0;
-  float omlo[B], omhi[B];
-#pragma unroll
-  for (int l1 = 0; l1 < B; ++l1) {
-    const double om = l1 < b ? a.freq[(size_t)q1 * b + l1] : 0.0;
-    omlo[l1] = l1 < b ? __double2float_rd(om) : 3.4e38f;
-    omhi[l1] = l1 < b ? __double2float_ru(om) : 3.4e38f;
-  }
-  const int sign = proc == 0 ? 1 : -1;
-  const bool own = tid < P;
-  const int pj = own ? tid / N2 : 0, pk = own ? tid - (tid / N2) * N2 : 0;
-  const int pj1 = pj + 1 == N1 ? 0 : pj + 1, pk1 = pk + 1 == N2 ? 0 : pk + 1;
-  const int pjm = pj == 0 ? N1 - 1 : pj - 1, pkm = pk == 0 ? N2 - 1 : pk - 1;
-  const double fnorm6 = (2 * PhysConst::pi) * (2 * PhysConst::pi) / nkc / 6.0;
-  double* Rrow = (proc == 0 ? a.R1 : a.R2) + (size_t)row * nkc * b * b + l2;
-  // |V3|^2 of the row and band l2: strides of q2, l1, l3 in layout 1
-  // [row][l2][l3][l1][q2] (the pipeline's) or 0 [row][q2][l1][l2][l3]
-  const int b2 = b * b;
-  const int sq = a.v3_layout == 1 ? 1 : b2 * b, s1 = a.v3_layout == 1 ? nkc : b2, s3 = a.v3_layout == 1 ? b * nkc : 1;
-  const VT* v3l2 = v3sq + (size_t)row * nkc * b2 * b + (a.v3_layout == 1 ? (size_t)l2 * b2 * nkc : (size_t)l2 * b);
-  WT* wsum = s_ws2 + tid;  // this position's weight sums [h*B + l1] * P, h = 0 below, 1 above
-  double* accs = s_acc + tid;
-  double accr[kAccReg ? 2 * B : 1];
-  if (own) {
-#pragma unroll
-    for (int l = 0; l < 2 * B; ++l) wsum[l * P] = WT(0);
-  }
-
-  // the energies of plane pl, every l3, into ring slot `slot`
-  auto stage = [&](int pl, int slot) {
-    if (!own) return;
-    int mw[3] = {pl, pj, pk}, m3[3], ins;
-    const int w = compose(g, mw);
-    const int q3 = pm_index_m(g, m1, mw, sign, ins, m3);
-    const double fw = a.freq[(size_t)w * b + l2];
-#pragma unroll
-    for (int l3 = 0; l3 < B; ++l3)
-      if (l3 < b) s_E[(slot * B + l3) * P + tid] = (float)(proc == 0 ? -fw + a.freq[(size_t)q3 * b + l3]
-                                                                      : fw + a.freq[(size_t)q3 * b + l3]);
-  };
-  struct Pt {
-    int w, src, q3;
-    double n2;
-    bool gw, g3;
-  };
-  auto point = [&](int pl) {
-    Pt p;
-    int mw[3] = {pl, pj, pk}, m3[3], ins;
-    p.w = compose(g, mw);
-    p.src = proc == 0 ? p.w : neg_index(g, mw);
-    p.q3 = pm_index_m(g, m1, mw, sign, ins, m3);
-    p.gw = at_gamma_index(g, mw);
-    p.g3 = at_gamma_index(g, m3);
-    p.n2 = a.dist[(size_t)p.w * b + l2];
-    return p;
-  };
-
-  stage(0, 0);
-  __syncthreads();
-  // slices whose energies, -+omega(w,l2) + omega(q3,l3), can meet no omega1
-  // of the row (band ranges over the mesh, a margin far above the FP32
-  // rounding of E) are skipped
-  unsigned live = 0;
-  {
-    double o1min = s_om[0], o1max = s_om[0];
-    for (int l = 1; l < b; ++l) {
-      o1min = fmin(o1min, s_om[l]);
-      o1max = fmax(o1max, s_om[l]);
-    }
-    for (int l3 = 0; l3 < b; ++l3) {
-      bool keep = true;
-      if (a.brange) {
-        const double lo2 = a.brange[l2], hi2 = a.brange[b + l2], lo3 = a.brange[l3], hi3 = a.brange[b + l3];
-        const double emin = proc == 0 ? lo3 - hi2 : lo2 + lo3, emax = proc == 0 ? hi3 - lo2 : hi2 + hi3;
-        const double tol = 1e-5 * (fabs(hi2) + fabs(hi3)) + 1e-10;
-        keep = !(emax + tol < o1min || emin - tol > o1max);
-      }
-      live |= keep ? 1u << l3 : 0u;
-    }
-  }
-  int slice = 0;  // slices processed: picks the buffers
-  for (int i = 0; i < N0; ++i) {
-    const int ih = i + 1 == N0 ? 0 : i + 1;
-    const int slo = i & 1, shi = slo ^ 1;
-    stage(ih, shi);
-    const Pt plo = point(i), phi = point(ih);
-    if constexpr (kAccReg) {
-#pragma unroll
-      for (int l = 0; l < 2 * B; ++l) accr[l] = 0.0;
-    } else if (own) {
-#pragma unroll
-      for (int l = 0; l < 2 * B; ++l) accs[l * P] = 0.0;
-    }
-    __syncthreads();  // the staged plane is visible
-    for (int l3 = 0; l3 < b; ++l3) {
-      if (!((live >> l3) & 1u)) continue;  // uniform
-      const int u = slice & 1;
-      const int cnt_slot = slice % 3;
-      ++slice;
-      const float* Elo = s_E + (slo * B + l3) * P;
-      const float* Ehi = s_E + (shi * B + l3) * P;
-      int* qs = s_qs + u * P;
-      unsigned char* qn = s_qn + u * P;
-      unsigned short* qe = s_qe + u * kPlaneQueue;
-      WT* wt_all = s_wt + (size_t)u * kPlaneQueue * 4;
-      // n(q3, l3) of both points, requested early: used after phase 3
-      const double n3lo = own ? a.dist[(size_t)plo.q3 * b + l3] : 0.0;
-      const double n3hi = own ? a.dist[(size_t)phi.q3 * b + l3] : 0.0;
-      // ---- phase 1: the cell's (tetrahedron, l1) pairs; bands lo .. lo+cnt-1
-      // of tetrahedron t packed in 9 bits (lo: 4, cnt: 5)
-      constexpr int kTetOf[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5}, {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
-      unsigned long long tpack = 0;
-      int npair = 0;
-      {
-        float ec[8];
-        float emin = 3.4e38f, emax = -3.4e38f;
-        const int cpos[4] = {pj * N2 + pk, pj1 * N2 + pk, pj * N2 + pk1, pj1 * N2 + pk1};
-#pragma unroll
-        for (int c = 0; c < 8; ++c) {
-          ec[c] = own ? (c & 1 ? Ehi : Elo)[cpos[c >> 1]] : 0.0f;
-          emin = fminf(emin, ec[c]);
-          emax = fmaxf(emax, ec[c]);
-        }
-        int clo = 0, chi = 0;
-#pragma unroll
-        for (int l1 = 0; l1 < B; ++l1) {
-          clo += omhi[l1] < emin;
-          chi += omlo[l1] <= emax;
-        }
-        const bool any = own && chi > clo;
-        if (__any_sync(0xffffffffu, any)) {
-#pragma unroll
-          for (int t = 0; t < 6; ++t) {
-            const float e0 = ec[kTetOf[t][0]], e1 = ec[kTetOf[t][1]], e2 = ec[kTetOf[t][2]], e3 = ec[kTetOf[t][3]];
-            const float mn = fminf(fminf(e0, e1), fminf(e2, e3));
-            const float mx = fmaxf(fmaxf(e0, e1), fmaxf(e2, e3));
-            int lo = 0, hi = 0;
-#pragma unroll
-            for (int l1 = 0; l1 < B; ++l1) {
-              lo += omhi[l1] < mn;
-              hi += omlo[l1] <= mx;
-            }
-            const int cnt = any && hi > lo ? hi - lo : 0;
-            tpack |= (unsigned long long)(unsigned)((lo & 15) | cnt << 4) << (9 * t);
-            npair += cnt;
-          }
-        }
-      }
-      // the warp's runs, one reservation per warp
-      int incl = npair;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const int v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-      }
-      const int wtot = __shfl_sync(0xffffffffu, incl, 31);
-      int base = 0;
-      if (lane == 31 && wtot > 0) base = atomicAdd(&s_nq[cnt_slot], wtot);
-      base = __shfl_sync(0xffffffffu, base, 31);
-      int start = base + incl - npair;
-      const bool fits = start + npair <= kPlaneQueue;
-      if (own) {
-        qs[tid] = start;
-        qn[tid] = (unsigned char)npair;
-      }
-      auto write_runs = [&](int first, int w0, int nwin) {
-        int pos = first;
-#pragma unroll
-        for (int t = 0; t < 6; ++t) {
-          const unsigned f = (unsigned)(tpack >> (9 * t)) & 511u;
-          const int lo = (int)(f & 15u), cnt = (int)(f >> 4);
-          for (int l1 = lo; l1 < lo + cnt; ++l1, ++pos)
-            if (pos >= w0 && pos < w0 + nwin) qe[pos - w0] = (unsigned short)(tid | t << 8 | l1 << 11);
-        }
-      };
-      if (npair > 0 && fits) write_runs(start, 0, kPlaneQueue);
-      if (tid == 0) s_nq[(slice) % 3] = 0;  // the counter of the next slice
-      const int ovf = __syncthreads_or(npair > 0 && !fits);
-      const int total = s_nq[cnt_slot];
-      if (total == 0) continue;  // uniform: nothing to add in this slice
-      unsigned nzm = 0;          // (h, l1) sums of this position that are not zero
-      // phases 2 and 3 over the queue entries [w0, w0 + nwin) of the runs
-      auto weights_and_gather = [&](int w0, int nwin) {
-        // ---- phase 2: corner weights of the entries
-        for (int e = tid; e < nwin; e += blockDim.x) {
-          const unsigned v = qe[e];
-          const int cell = (int)(v & 255u), t = (int)((v >> 8) & 7u), l1 = (int)(v >> 11);
-          const int cj = cell / N2, ck = cell - cj * N2;
-          const int cj1 = cj + 1 == N1 ? 0 : cj + 1, ck1 = ck + 1 == N2 ? 0 : ck + 1;
-          const unsigned code = tet_code(t);
-          float en[4];
-#pragma unroll
-          for (int k = 0; k < 4; ++k) {
-            const int c = (int)((code >> (3 * k)) & 7u);
-            en[k] = ((c & 1) ? Ehi : Elo)[((c & 2) ? cj1 : cj) * N2 + ((c & 4) ? ck1 : ck)];
-          }
-          // sorted position of each corner slot (0 highest .. 3 lowest); ties
-          // by the slot order of the corner list
-          int ps[4];
-          ps[0] = tet_pos(en, 0);
-          ps[1] = tet_pos(en, 1);
-          ps[2] = tet_pos(en, 2);
-          ps[3] = 6 - ps[0] - ps[1] - ps[2];
-          const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
-          WT cw[4];
-          bool in;
-          if constexpr (F32W) {
-            in = tet_weights4_f32(ts, s_om[l1], cw);
-          } else {
-            in = tet_weights4(ts, s_om[l1], cw);
-          }
-          WT* wt = wt_all + (size_t)e * 4;
-#pragma unroll
-          for (int k = 0; k < 4; ++k) wt[k] = in ? cw[ps[k]] : WT(0);
-        }
-        __syncthreads();
-        // ---- phase 3: the position's two points gather the weights of the
-        // runs of its four adjacent cells.  Cell (pj - o1, pk - o2) has the
-        // point below as corner 2 o1 + 4 o2 and the point above as that + 1.
-        if (own) {
-          const int adj[4] = {pj * N2 + pk, pjm * N2 + pk, pj * N2 + pkm, pjm * N2 + pkm};
-          constexpr unsigned kLo[4] = {tet_slot_code(0), tet_slot_code(2), tet_slot_code(4), tet_slot_code(6)};
-          constexpr unsigned kHi[4] = {tet_slot_code(1), tet_slot_code(3), tet_slot_code(5), tet_slot_code(7)};
-#pragma unroll
-          for (int d = 0; d < 4; ++d) {
-            const int cell = adj[d];
-            const int r0 = qs[cell];
-            const int e0 = max(r0, w0), e1 = min(r0 + (int)qn[cell], w0 + nwin);
-            for (int e = e0; e < e1; ++e) {
-              const unsigned v = qe[e - w0];
-              const int t = (int)((v >> 8) & 7u), l1 = (int)(v >> 11);
-              const int kl = (int)((kLo[d] >> (3 * t)) & 7u), kh = (int)((kHi[d] >> (3 * t)) & 7u);
-              const WT* wt = wt_all + (size_t)(e - w0) * 4;
-              if (kl) {
-                wsum[l1 * P] += wt[kl - 1];
-                nzm |= 1u << l1;
-              }
-              if (kh) {
-                wsum[(B + l1) * P] += wt[kh - 1];
-                nzm |= 1u << (B + l1);
-              }
-            }
-          }
-        }
-      };
-      if (!ovf) {
-        weights_and_gather(0, total);
-      } else {
-        // overflow: runs laid out again by a block-wide scan in thread order,
-        // processed in windows of the queue's size
-        if (lane == 31) s_ws[warp] = incl;
-        __syncthreads();
-        int before = 0, all = 0;
-        for (int w = 0; w < nwarps; ++w) {
-          const int t = s_ws[w];
-          before += w < warp ? t : 0;
-          all += t;
-        }
-        start = before + incl - npair;
-        if (own) qs[tid] = start;
-        for (int w0 = 0; w0 < all; w0 += kPlaneQueue) {
-          const int nwin = min(kPlaneQueue, all - w0);
-          __syncthreads();  // the previous window is consumed; run starts visible
-          if (npair > 0 && start < w0 + nwin && start + npair > w0) write_runs(start, w0, nwin);
-          __syncthreads();
-          weights_and_gather(w0, nwin);
-        }
-        __syncthreads();  // the queue buffer may be reused two slices on
-      }
-      // R parts of this slice: (sum/6) |V3|^2 (2pi)^2/nkc n1 G, G = n2 (n3+1)
-      // [process 1] or (n2+1)(n3+1) [process 2], 0 at the reference's
-      // acoustic-at-Gamma points (sub.f90:7351-7356, 7412-7417).  Every
-      // |V3|^2 a point needs is requested at once (predicated loads).
-      if (own && nzm) {
-        const VT* v3s = v3l2 + l3 * s3;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-          const Pt& pt = h ? phi : plo;
-          const double n3 = h ? n3hi : n3lo;
-          const bool zero = (l2 < 3 && pt.gw) || (l3 < 3 && pt.g3);
-          const double G = proc == 0 ? pt.n2 * (n3 + 1) : (pt.n2 + 1) * (n3 + 1);
-          const VT* vp = v3s + pt.src * sq;
-          constexpr int LC = B < 6 ? B : 6;  // bands per batch of loads
-#pragma unroll
-          for (int l0 = 0; l0 < B; l0 += LC) {
-            WT x[LC];
-            VT v[LC];
-#pragma unroll
-            for (int k = 0; k < LC; ++k) {
-              const int l = l0 + k;
-              const bool nz = (nzm >> (h * B + l)) & 1u;
-              x[k] = nz ? wsum[(h * B + l) * P] : WT(0);
-              v[k] = nz && !zero ? __ldg(vp + l * s1) : VT(0);
-            }
-#pragma unroll
-            for (int k = 0; k < LC; ++k) {
-              const int l = l0 + k;
-              if ((nzm >> (h * B + l)) & 1u) {
-                wsum[(h * B + l) * P] = WT(0);
-                if (!zero) {
-                  const double r = (double)x[k] * ((double)v[k] * fnorm6) * (s_nb1[l] * G);
-                  if constexpr (kAccReg) accr[h * B + l] += r;
-                  else accs[(h * B + l) * P] += r;
-                }
-              }
-            }
-          }
-        }
-      }
-    }
-    // plane i ends: the point below is complete (plane 0: its lower part for
-    // now); the point above gets its upper part (plane 0: completed).  The
-    // stored parts are read first, all bands at once.
-    if (own) {
-      double* rl = Rrow + (size_t)plo.w * b * b;
-      double* rh = Rrow + (size_t)phi.w * b * b;
-      double old[B];
-#pragma unroll
-      for (int l = 0; l < B; ++l) old[l] = (l < b && i > 0) ? rl[l * b] : 0.0;
-#pragma unroll
-      for (int l = 0; l < B; ++l) {
-        const double al = kAccReg ? accr[kAccReg ? l : 0] : accs[l * P];
-        if (l < b) rl[l * b] = i == 0 ? al : old[l] + al;
-      }
-#pragma unroll
-      for (int l = 0; l < B; ++l) old[l] = (l < b && ih == 0) ? rh[l * b] : 0.0;
-#pragma unroll
-      for (int l = 0; l < B; ++l) {
-        const double ah = kAccReg ? accr[kAccReg ? B + l : 0] : accs[(B + l) * P];
-        if (l < b) rh[l * b] = ih == 0 ? old[l] + ah : ah;
-      }
-    }
+// the fixed-point sums of the deterministic passes back to FP64, in place
+__global__ void delta_finalize_kernel(double* R, const unsigned long long* __restrict__ M, size_t n, int b) {
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const unsigned long long m = M[i];
+    const unsigned long long acc = reinterpret_cast<const unsigned long long*>(R)[i];
+    R[i] = m == 0 ? 0.0 : ldexp((double)acc, det_exponent(m, b) - 62);
   }
 }
 
@@ -1538,9 +1145,9 @@ bool delta_fused_supported(const Geometry& g) {
 }
 
 #define ALD_COMMA ,
-cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
+template <int MODE>
+static cudaError_t launch_delta_fused_mode(const CombineArgs& a, cudaStream_t s) {
   const Geometry& g = a.geo;
-  if (!delta_fused_supported(g)) return cudaErrorInvalidValue;
   const FusedShape f = fused_shape(g);
   dim3 grid(g.nc[0] * f.nbj, a.nrows, 2 * g.b);
   cudaError_t e;
@@ -1551,13 +1158,13 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
     KERNEL<<<grid, kFusedThreads, f.smem, s>>>(a, PTR);                                  \
   }
   // FP32 |V3|^2 only comes with the FP32 weights of the mixed pipeline
-#define ALD_FUSED(BB)                                                \
-  if (a.v3sq_f32) {                                                  \
-    ALD_FUSED2(delta_fused_mixed_kernel<BB ALD_COMMA float>, a.v3sq_f32) \
-  } else if (a.f32w) {                                               \
-    ALD_FUSED2(delta_fused_mixed_kernel<BB ALD_COMMA double>, a.v3sq)    \
-  } else {                                                           \
-    ALD_FUSED2(delta_fused_fp64_kernel<BB>, a.v3sq)                  \
+#define ALD_FUSED(BB)                                                                  \
+  if (a.v3sq_f32) {                                                                    \
+    ALD_FUSED2(delta_fused_mixed_kernel<BB ALD_COMMA float ALD_COMMA MODE>, a.v3sq_f32) \
+  } else if (a.f32w) {                                                                 \
+    ALD_FUSED2(delta_fused_mixed_kernel<BB ALD_COMMA double ALD_COMMA MODE>, a.v3sq)    \
+  } else {                                                                             \
+    ALD_FUSED2(delta_fused_fp64_kernel<BB ALD_COMMA MODE>, a.v3sq)                      \
   }
   if (a.v3sq_f32 && !a.f32w) return cudaErrorInvalidValue;
   if (g.b <= 3) {
@@ -1571,58 +1178,23 @@ cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s) {
   }
 #undef ALD_FUSED
 #undef ALD_FUSED2
-#undef ALD_COMMA
   return cudaGetLastError();
 }
+#undef ALD_COMMA
 
-template <int B, bool FW>
-static bool plane_fits(const Geometry& g) {
-  const PlaneShape p = plane_shape<B, FW>(g);
-  return p.P <= kPlaneMaxPos && p.smem <= 200 * 1024;
+cudaError_t launch_delta_fused(const CombineArgs& a, cudaStream_t s, int mode) {
+  if (!delta_fused_supported(a.geo)) return cudaErrorInvalidValue;
+  if (mode == 0) return launch_delta_fused_mode<0>(a, s);
+  if (!a.M1 || !a.M2 || (a.R1p && !a.M1p) || (a.R2p && !a.M2p)) return cudaErrorInvalidValue;
+  if (mode == 1) return launch_delta_fused_mode<1>(a, s);
+  if (mode == 2) return launch_delta_fused_mode<2>(a, s);
+  return cudaErrorInvalidValue;
 }
 
-bool delta_plane_supported(const Geometry& g, int f32w) {
-  if (g.b > kMaxBandsTet || g.nc[1] * g.nc[2] > kPlaneMaxPos) return false;
-  if (g.b <= 3) return f32w ? plane_fits<3, true>(g) : plane_fits<3, false>(g);
-  if (g.b <= 6) return f32w ? plane_fits<6, true>(g) : plane_fits<6, false>(g);
-  if (g.b <= 12) return f32w ? plane_fits<12, true>(g) : plane_fits<12, false>(g);
-  return f32w ? plane_fits<16, true>(g) : plane_fits<16, false>(g);
-}
-
-cudaError_t launch_delta_plane(const CombineArgs& a, cudaStream_t s) {
-  const Geometry& g = a.geo;
-  if (!delta_plane_supported(g, a.f32w) || a.R1p || a.R2p || a.v3_layout > 1 || a.nrows > 65535)
-    return cudaErrorInvalidValue;
-  const dim3 grid(g.b, 2, a.nrows);
-  cudaError_t e;
-#define ALD_PLANE2(BB, FW, VT, PTR)                                                    \
-  {                                                                                     \
-    const PlaneShape p = plane_shape<BB, FW>(g);                                        \
-    e = raise_smem_limit((const void*)delta_plane_kernel<BB, FW, VT>, p.smem);          \
-    if (e != cudaSuccess) return e;                                                     \
-    delta_plane_kernel<BB, FW, VT><<<grid, p.threads, p.smem, s>>>(a, PTR);             \
-  }
-  // FP32 |V3|^2 only comes with the FP32 weights of the mixed pipeline
-#define ALD_PLANE(BB)                               \
-  if (a.v3sq_f32) {                                 \
-    ALD_PLANE2(BB, true, float, a.v3sq_f32)         \
-  } else if (a.f32w) {                              \
-    ALD_PLANE2(BB, true, double, a.v3sq)            \
-  } else {                                          \
-    ALD_PLANE2(BB, false, double, a.v3sq)           \
-  }
-  if (a.v3sq_f32 && !a.f32w) return cudaErrorInvalidValue;
-  if (g.b <= 3) {
-    ALD_PLANE(3)
-  } else if (g.b <= 6) {
-    ALD_PLANE(6)
-  } else if (g.b <= 12) {
-    ALD_PLANE(12)
-  } else {
-    ALD_PLANE(16)
-  }
-#undef ALD_PLANE
-#undef ALD_PLANE2
+cudaError_t launch_delta_finalize(double* R, const unsigned long long* M, size_t n, int b, cudaStream_t s) {
+  if (n == 0) return cudaSuccess;
+  const int blocks = (int)std::min<size_t>((n + 255) / 256, 148 * 16);
+  delta_finalize_kernel<<<blocks, 256, 0, s>>>(R, M, n, b);
   return cudaGetLastError();
 }
 

@@ -28,6 +28,7 @@ STATUS = {1: "ALD_ERR_ARG", 2: "ALD_ERR_IO", 3: "ALD_ERR_NOT_KPOINT", 4: "ALD_ER
 DELTA_TETRA, DELTA_GAUSS = 0, 1
 FP64, MIXED, MIXED_FP32 = 0, 1, 2
 CG_REFERENCE, CG_RESIDUAL = 0, 1
+DET_AUTO = -1  # Options.deterministic: FP64 deterministic, mixed with FP64 atomics
 
 
 class AldError(RuntimeError):

@@ -394,9 +394,13 @@ def main():
     rp = make_workload(d, mesh, args.workload)
     stream = torch.cuda.Stream(device=dev)
 
-    def timed_path(precision, d=d, rp=rp, workload=args.workload, steps=args.steps, warmup=args.warmup):
-        """K timed steps of one precision path on a context whose tables are in HBM."""
+    def timed_path(precision, d=d, rp=rp, workload=args.workload, steps=args.steps, warmup=args.warmup, det=None):
+        """K timed steps of one precision path on a context whose tables are in HBM.
+        det: the options' deterministic field (None: the library's default,
+        deterministic for FP64, FP64 atomics for the mixed path)."""
         opts = workload_options(ald, rp, workload, device=dev, precision=precision)
+        if det is not None:
+            opts.deterministic = det
         ctx = ald.Context(d, opts)
         ctx.set_stream(stream.cuda_stream)
         tempk = ctx.info.tempk
@@ -452,6 +456,8 @@ def main():
 
     precisions = {"fp64": [ald.FP64], "mixed": [ald.MIXED], "both": [ald.FP64, ald.MIXED]}[args.precision]
     runs = {p: timed_path(p) for p in precisions}
+    # the FP64 path with FP64 atomics in the delta (not bitwise repeatable), for comparison
+    fp64_atomic = timed_path(ald.FP64, steps=min(args.steps, 5), det=0) if world == 1 and ald.FP64 in runs else None
     head = runs[precisions[-1]]  # the mixed path when both run
     nibz, nkc, b = head["nibz"], head["nkc"], head["b"]
     out = head["out"]
@@ -570,7 +576,13 @@ def main():
             line["fp64"] = {"value": tb * args.steps / (f["ms"] * 1e-3), "unit": UNIT,
                             "ms_per_step": f["ms"] / args.steps,
                             "stage_ms_per_step": {k: round(v, 4) for k, v in f["stage"].items()},
-                            "clocks": f["clocks"]}
+                            "clocks": f["clocks"], "delta": "deterministic (the FP64 default)"}
+            if fp64_atomic is not None:
+                a_ = fp64_atomic
+                line["fp64"]["atomic_delta"] = {
+                    "ms_per_step": a_["ms"] / a_["steps"],
+                    "stage_ms_per_step": {k: round(v, 4) for k, v in a_["stage"].items()},
+                    "note": "ald_options.deterministic = 0: FP64 atomics, last bits vary between runs"}
             line["mixed_speedup_vs_fp64"] = f["ms"] / m["ms"]
             line["mixed_v3_speedup_vs_fp64"] = f["stage"]["v3"] / m["stage"]["v3"]
             line["kappa_rel_err_mixed_vs_fp64"] = {

@@ -47,6 +47,8 @@ enum ald_delta { ALD_DELTA_TETRA = 0, ALD_DELTA_GAUSS = 1 };
 enum ald_precision { ALD_FP64 = 0, ALD_MIXED = 1, ALD_MIXED_FP32 = 2 };
 enum ald_cg_stop { ALD_CG_REFERENCE = 0, ALD_CG_RESIDUAL = 1 };
 
+#define ALD_DET_AUTO (-1)
+
 typedef struct ald_options {
   int delta;         /* ALD_DELTA_TETRA (reference, calculate_FGR_mpi2) or ALD_DELTA_GAUSS
                         (extension: delta_g of width `width_cm`, extratools.f90:239)    */
@@ -59,8 +61,11 @@ typedef struct ald_options {
   double width_cm;   /* Gaussian width in cm^-1 for ALD_DELTA_GAUSS (<=0: latdyn width) */
   int device;        /* CUDA device ordinal                                             */
   size_t chunk_bytes;/* device bytes for one chunk of |V3|^2 rows (0 = automatic)      */
-  int deterministic; /* 1: the pipeline's tetrahedron delta sums R1/R2 in a fixed order
-                        (the same bits on every run; slower), 0: FP64 atomics         */
+  int deterministic; /* the pipeline's tetrahedron delta (up to 16 bands):
+                        1: sums with the same bits on every run (two passes, the second
+                        with fixed-point integer atomics; about 2.4x the delta's time),
+                        0: FP64 atomics in arrival order (last bits vary between runs),
+                        ALD_DET_AUTO (-1, the default): 1 for ALD_FP64, 0 otherwise    */
 } ald_options;
 
 typedef struct ald_ctx ald_ctx;

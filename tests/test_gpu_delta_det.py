@@ -1,16 +1,18 @@
 """The pipeline's tetrahedron delta with the deterministic option: run-to-run
-reproducibility and agreement with the default form (GPU).
+reproducibility and agreement with the atomic form (GPU).
 
-With ald_options.deterministic = 1 the pipeline's tetrahedron delta walks the
-mesh plane by plane and writes every R1/R2 entry from one thread in a fixed
-order, so repeated runs give the same bits (FP64 and mixed paths).  The
-default form adds the corner weights with FP64 atomics in arrival order;
+With ald_options.deterministic = 1 (the default for the FP64 path) the
+pipeline's tetrahedron delta runs twice: the first pass records each R1/R2
+entry's largest term, the second adds every term as a 62-bit fixed-point
+integer scaled by that bound, so the sums do not depend on the order of the
+additions and repeated runs give the same bits (FP64 and mixed paths).  With
+deterministic = 0 the terms are added with FP64 atomics in arrival order;
 both sum the same terms, so they agree to FP64 rounding:
   Q, Q_N, Q_U, the CG solution and kappa within 1e-12 relative (floor
   1e-14 of the largest value).
-Both forms are also held to the oracle at 1e-10 (the default form by the
-pipeline tests of test_gpu_parity.py and test_gpu_suite_sizes.py, the
-deterministic form by test_deterministic_matches_oracle below).
+Both forms are also held to the oracle at 1e-10 (the FP64 default by the
+pipeline tests of test_gpu_parity.py and test_gpu_suite_sizes.py, and
+test_deterministic_matches_oracle below).
 """
 import numpy as np
 import pytest
@@ -65,10 +67,9 @@ def test_deterministic_bitwise_repeatable(ald_lib, workdir, precision):
 
 
 def test_deterministic_mixed_matches_default(ald_lib, workdir):
-    """The FP32-weight forms: the same FP32 weights, summed per point in
-    FP32 by the deterministic form and added one by one in FP64 by the
-    default form; within the mixed path's own 1e-4 bars of each other, far
-    inside them."""
+    """The mixed path (FP32 weights and |V3|^2): the same FP64 terms, summed
+    in fixed point by the deterministic form and with FP64 atomics by the
+    default form; far inside the mixed path's own 1e-4 bars of each other."""
     d = make_case(workdir, 1, (6, 6, 6))
     a = run(ald_lib, d, ald_lib.MIXED, 1)
     r = run(ald_lib, d, ald_lib.MIXED)
