@@ -15,6 +15,7 @@
 #include <memory>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "ald_internal.h"
 
@@ -264,6 +265,115 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
   return a;
 }
 
+// The mixed path's |V3|^2 near zero frequencies.  Where a mode of q1, q2 or
+// q3 has |lambda| below 1e-9 of the largest (the acoustic modes at Gamma),
+// the matrix element before its 1/sqrt|lambda1 lambda2 lambda3| scaling is a
+// cancellation (translational invariance of the FC3 terms).  Split-FP16
+// products leave it at about 1e-7 of its terms instead of the 1e-16 of FP64,
+// and the scaling then blows that residue up by up to 1/sqrt|lambda|: on
+// meshes where the reference's Gamma test (loop indices nc/2 + 1,
+// sub.f90:7351-7356) misses Gamma, or at q1 = Gamma, those entries reached
+// kappa.  Such pairs are formed again in FP64 with the dense GEMMs of
+// ald_v3_dense.cu, over the chunk's output in its layout: every pair whose
+// q2 or q3 is such a point, and for a row whose q1 is one, every pair with
+// its soft bands l1 (the leading ones: bands are ordered by |lambda|).  The
+// linewidths of those soft modes are that residue in FP64 too, and through
+// the collision matrix they reach kappa: their row is formed with the
+// kernel the FP64 path uses for the cell (the direct form up to 12 bands),
+// so that both paths carry the same residue there.
+static int v3_soft_fp64(ald_ctx* c, const V3Args& a, int* nl) {
+  const int b = c->geo.b, nkc = c->T.nkc;
+  std::vector<double> w2((size_t)nkc * b);
+  CK(cudaMemcpyAsync(w2.data(), c->w2.p, w2.size() * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double mx = 0;
+  for (double v : w2) mx = std::max(mx, std::fabs(v));
+  const double thr = 1e-9 * mx;
+  std::vector<int> nsoft(nkc, 0), soft;
+  for (int q = 0; q < nkc; ++q) {
+    for (int l = 0; l < b; ++l)
+      if (std::fabs(w2[(size_t)q * b + l]) < thr) nsoft[q] = l + 1;
+    if (nsoft[q]) soft.push_back(q);
+  }
+  if (soft.empty()) return ALD_OK;
+  const int* nc = c->geo.nc;
+  auto dec = [&](int q, int* m) {
+    m[0] = q / (nc[1] * nc[2]);
+    m[1] = (q / nc[2]) % nc[1];
+    m[2] = q % nc[2];
+  };
+  std::vector<long long> all, part;
+  std::vector<int> soft_rows;  // rows of a soft q1 formed by the direct FP64 kernel
+  int nk1 = 0;
+  for (int r = 0; r < a.nrows; ++r) {
+    const int q1 = c->T.mapinv[a.n1_first + r] - 1;
+    int m1[3];
+    dec(q1, m1);
+    for (int sp : soft) {
+      int ms[3], m2[3];
+      dec(sp, ms);
+      all.push_back((long long)r * nkc + sp);  // q2 at the point
+      for (int x = 0; x < 3; ++x) {            // q3 = -q1 - q2 at the point
+        int v = (-m1[x] - ms[x] + (c->geo.shifted ? nc[x] / 2 : 0)) % nc[x];
+        m2[x] = v < 0 ? v + nc[x] : v;
+      }
+      all.push_back((long long)r * nkc + m2[2] + nc[2] * (m2[1] + nc[1] * m2[0]));
+    }
+    if (nsoft[q1]) {
+      nk1 = std::max(nk1, nsoft[q1]);
+      if (v3_dense_supported(b))
+        for (int q2 = 0; q2 < nkc; ++q2) part.push_back((long long)r * nkc + q2);
+      else
+        soft_rows.push_back(r);
+    }
+  }
+  std::sort(all.begin(), all.end());
+  all.erase(std::unique(all.begin(), all.end()), all.end());
+  const size_t nall = all.size(), npart = part.size();
+  all.insert(all.end(), part.begin(), part.end());
+  if (c->w_pairs.n < all.size()) CKA(c->w_pairs.alloc(all.size()));
+  // pageable source: the copy has left the vector when the call returns
+  CK(cudaMemcpyAsync(c->w_pairs.p, all.data(), all.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
+  V3Args f = a;
+  const size_t hneed = v3_hbuf_bytes(b, c->VC.ncls, a.nrows, ALD_FP64);
+  if (c->w_h64.n < hneed) CKA(c->w_h64.alloc(hneed));
+  f.hbuf = c->w_h64.p;
+  const size_t wb = v3_dense_work_bytes(b, (long long)std::max(nall, npart), (size_t)256 << 20);
+  if (c->w_v3fix.n < wb) CKA(c->w_v3fix.alloc(wb));
+  cudaError_t e = launch_v3_rows_f64(f, c->stream);
+  *nl += 1;
+  const long long per = (long long)(c->w_v3fix.n / (2 * (size_t)b * b * b * 16));
+  f.pair_list = c->w_pairs.p;
+  f.npairs_list = (long long)nall;
+  if (e == cudaSuccess) e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream);
+  *nl += 3 * (int)(((long long)nall + per - 1) / per);
+  if (npart && e == cudaSuccess) {
+    f.pair_list = c->w_pairs.p + nall;
+    f.npairs_list = (long long)npart;
+    e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream, nk1);
+    *nl += 3 * (int)(((long long)npart + per - 1) / per);
+  }
+  if (!soft_rows.empty() && e == cudaSuccess) {
+    const size_t rn = (size_t)nkc * b * b * b;
+    if (c->w_v3fix.n < rn * sizeof(double)) CKA(c->w_v3fix.alloc(rn * sizeof(double)));
+    for (int r : soft_rows) {
+      V3Args g = a;
+      g.n1_first = a.n1_first + r;
+      g.nrows = 1;
+      g.v3_layout = 0;
+      g.v3sq = reinterpret_cast<double*>(c->w_v3fix.p);
+      g.v3sq_f32 = nullptr;
+      g.pair_list = nullptr;
+      e = launch_v3_fp64(g, c->stream);
+      if (e == cudaSuccess) e = launch_v3_copy_row(a, r, g.v3sq, nk1, c->stream);
+      *nl += 2;
+      if (e != cudaSuccess) break;
+    }
+  }
+  if (e != cudaSuccess) return fail(ALD_ERR_CUDA, std::string("V3 near zero frequencies: ") + cudaGetErrorString(e));
+  return ALD_OK;
+}
+
 int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
   int nl = 0;
   if (c->S.include_fc[2] != 1) return fail(ALD_ERR_ARG, "fc3 terms are not included (include_fc(3) /= 1)");
@@ -292,6 +402,10 @@ int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
     c->v3work_tc_b = e == cudaSuccess ? c->geo.b : 0;
     c->v3work_tc_p = P;
     nl += 1 + v3_dense_tc_launches(npairs, P);
+    if (e == cudaSuccess) {
+      const int r = v3_soft_fp64(c, a, &nl);
+      if (r) return r;
+    }
   } else if (v3_dense_supported(c->geo.b)) {
     // more than 12 bands: batched GEMMs per pair (FP64)
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, ALD_FP64);

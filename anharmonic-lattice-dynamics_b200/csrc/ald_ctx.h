@@ -33,6 +33,8 @@ struct ald_ctx {
   DevBuf<char> w_ptiles;              // phase tiles of the tensor-core V3 (mesh-only, built once)
   DevBuf<char> w_btiles;              // per-row B operands of the tensor-core V3
   DevBuf<char> w_v3work;              // T1/T2 of the large-cell V3 GEMMs
+  DevBuf<char> w_h64, w_v3fix;        // mixed path, FP64 V3 near zero frequencies: H and T1/T2
+  DevBuf<long long> w_pairs;          // its (row, q2) pair list
   int v3work_tc_b = 0;                // its tensor-core T2 padding is zero for (bands, pairs)
   long long v3work_tc_p = 0;
   bool ptiles_ok = false;

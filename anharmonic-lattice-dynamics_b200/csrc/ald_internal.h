@@ -290,6 +290,10 @@ struct V3Args {
   const int* cls_trip_i0;
   const int* cls_trip_k;
   void* hbuf;                // row workspace: nrows*ncls*9*b complex (v3_hbuf_bytes)
+  // the FP64 GEMMs of ald_v3_dense.cu on a list of pairs (row * nkc + q2, row
+  // local to the chunk) instead of every pair of the chunk
+  const long long* pair_list = nullptr;
+  long long npairs_list = 0;
 };
 cudaError_t launch_v3_fp64(const V3Args& a, cudaStream_t s);
 // pair kernel: bands it handles and the row workspace it needs (0 = not handled)
@@ -304,7 +308,11 @@ cudaError_t launch_v3_rows_f64(const V3Args& a, cudaStream_t s);
 // work: v3_dense_work_bytes(b, pairs of the chunk, budget) bytes
 bool v3_dense_supported(int b);
 size_t v3_dense_work_bytes(int b, long long npairs, size_t budget);
-cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s);
+// l1_keep (0 = all): only bands l1 < l1_keep are formed and written
+cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s, int l1_keep = 0);
+// one row's |V3|^2 in the reference's order [q2][l1][l2][l3] (FP64) into row
+// `row` of the chunk of a, in a's layout and precision, bands l1 < l1_keep
+cudaError_t launch_v3_copy_row(const V3Args& a, int row, const double* src, int l1_keep, cudaStream_t s);
 // more than 6 bands, ALD_MIXED (ald_v3_dense_tc.cu): both mode products as
 // split-FP16 tcgen05 GEMMs; hbuf from launch_v3_rows_f32; work of
 // v3_dense_tc_work_bytes(b, nkc, nrows, pairs) bytes for batches of `pairs`

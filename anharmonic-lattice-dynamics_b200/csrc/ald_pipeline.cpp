@@ -16,9 +16,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <thread>
 #include <vector>
@@ -524,10 +526,32 @@ static void release_pipeline_workspaces(ald_ctx* c) {
   for (DevBuf<double>* b : {&c->w_R1, &c->w_R2, &c->w_v3, &c->w_cm, &c->w_R1p, &c->w_R2p, &c->w_heev, &c->w_rmax})
     b->free();
   c->w_h.free();
+  c->w_h64.free();
+  c->w_v3fix.free();
+  c->w_pairs.free();
   c->w_v3work.free();
   c->v3work_tc_b = 0;
   c->w_btiles.free();
   c->w_scratch.free();
+}
+
+// An upper estimate of the device bytes one pipeline call on c allocates
+// beyond the context's tables: R1/R2, |V3|^2 of one chunk, the collision
+// matrix, the fixed-point sums of the deterministic delta, and for large
+// cells the V3 GEMM workspace (2 GiB at most) and the Householder
+// eigensolver's slots.  The batched entry point admits structures by it.
+static size_t pipeline_bytes_estimate(const ald_ctx* c) {
+  const size_t nibz = c->T.nibz, nkc = c->T.nkc, b = c->geo.b;
+  const size_t rsz = nibz * nkc * b * b * sizeof(double);
+  const size_t per_row = nkc * b * b * b * sizeof(double);
+  const size_t budget = c->opt.chunk_bytes ? c->opt.chunk_bytes : (size_t)512 << 20;
+  const size_t k = std::max<size_t>(1, std::min<size_t>(budget / per_row, nibz));
+  const size_t N = 3 * b * nibz;
+  size_t s = 2 * rsz + k * per_row + N * N * sizeof(double);
+  s += 2 * (k * nkc * b * b) * sizeof(unsigned long long);  // deterministic delta
+  if (b > 12) s += (size_t)2 << 30;
+  if (b > 64) s += heev_work_doubles((int)b, heev_slots((int)nkc * 7)) * sizeof(double);
+  return s + ((size_t)256 << 20);
 }
 
 extern "C" int ald_release_workspaces(ald_ctx* c) {
@@ -547,9 +571,12 @@ extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk
   }
   // A pool of host threads, each issuing one structure at a time on that
   // structure's own stream, so that structures overlap on the device; the
-  // largest (nibz nkc b^3) go first.  A batch larger than the pool keeps
-  // device memory bounded: after its run a structure's pipeline workspaces
-  // return to the library's device-memory cache for the next one.
+  // largest (nibz nkc b^3) go first.  Admission is memory-aware: a structure
+  // starts only while the pipeline workspaces of the structures in flight on
+  // its device, plus its own (pipeline_bytes_estimate), stay within 85 % of
+  // the device memory free when the batch began; one structure always runs.
+  // When the batch is larger than what runs at once, a structure's pipeline
+  // workspaces return to the library's device-memory cache after its run.
   const int pool = std::min(n, 8);
   std::vector<int> order(n);
   for (int i = 0; i < n; ++i) order[i] = i;
@@ -558,24 +585,60 @@ extern "C" int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk
     return (double)c->T.nibz * c->T.nkc * (double)c->geo.b * c->geo.b * c->geo.b;
   };
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return work(a) > work(b); });
+  std::vector<size_t> est(n);
+  std::map<int, size_t> budget, inflight;
+  size_t total_est = 0;
+  for (int i = 0; i < n; ++i) {
+    est[i] = pipeline_bytes_estimate(ctx[i]);
+    total_est += est[i];
+    const int dev = ctx[i]->device;
+    if (!budget.count(dev)) {
+      size_t fr = 0, tot = 0;
+      cudaSetDevice(dev);
+      budget[dev] = cudaMemGetInfo(&fr, &tot) == cudaSuccess ? fr / 100 * 85 : (size_t)-1;
+      inflight[dev] = 0;
+    }
+  }
+  bool release_after = n > pool;
+  for (auto& kv : budget)
+    if (total_est > kv.second) release_after = n > 1;
+  std::mutex mu;
+  std::condition_variable cv;
   std::vector<int> st(n, ALD_OK);
   std::vector<std::string> msg(n);
-  std::atomic<int> next{0};
+  int next = 0;
   std::vector<std::thread> th;
   th.reserve(pool);
   for (int t = 0; t < pool; ++t)
     th.emplace_back([&] {
       for (;;) {
-        const int k = next.fetch_add(1);
-        if (k >= n) break;
-        const int i = order[k];
+        int i;
+        {
+          std::unique_lock<std::mutex> lk(mu);
+          if (next >= n) break;
+          const int dev = ctx[order[next]]->device;
+          // the next structure in order, once it fits (or nothing else runs)
+          cv.wait(lk, [&] {
+            return next >= n || inflight[ctx[order[next]]->device] == 0 ||
+                   inflight[ctx[order[next]]->device] + est[order[next]] <= budget[ctx[order[next]]->device];
+          });
+          (void)dev;
+          if (next >= n) break;
+          i = order[next++];
+          inflight[ctx[i]->device] += est[i];
+        }
         st[i] = run_pipeline(ctx[i], tempk[i], &res[i], nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                              nullptr);
         if (st[i] != ALD_OK) msg[i] = ald_last_error();
-        if (n > pool) {
+        if (release_after) {
           cudaSetDevice(ctx[i]->device);
           release_pipeline_workspaces(ctx[i]);
         }
+        {
+          std::lock_guard<std::mutex> lk(mu);
+          inflight[ctx[i]->device] -= est[i];
+        }
+        cv.notify_all();
       }
     });
   for (auto& t : th) t.join();

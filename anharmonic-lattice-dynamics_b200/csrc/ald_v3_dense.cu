@@ -56,6 +56,7 @@ struct PairIdx {
 __device__ __forceinline__ PairIdx pair_idx(const V3Args& a, long long pair) {
   PairIdx p;
   const int nkc = a.geo.nkc;
+  if (a.pair_list) pair = a.pair_list[pair];
   p.row = (int)(pair / nkc);
   p.q2 = (int)(pair % nkc);
   p.q1 = a.mapinv[a.n1_first + p.row];
@@ -105,16 +106,20 @@ __global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long p
 //                    B(k, n = l2) = e(q2)[n][k],  C -> T2[p][n][m]
 //   kind 2 (GEMM 2): A(m = l2 b + l1, k = kc) = T2[p][m][k]   (k contiguous)
 //                    B(k, n = l3) = e(q3)[n][k],  epilogue |V|^2 -> v3sq
+// With l1 < nk1 only (nk1 < b): GEMM 1 has the first nk1 b rows; GEMM 2 the
+// rows m' = l2 nk1 + l1 (A row l2 b + l1).
 constexpr int kGM = 64, kGN = 64, kGK = 8, kGThreads = 256;
 
 template <int KIND>
 __global__ void __launch_bounds__(kGThreads) v3_zgemm_kernel(V3Args a, long long pair0, const double2* Ain,
-                                                             double2* Cout) {
+                                                             double2* Cout, int nk1) {
   __shared__ double2 As[kGK][kGM + 1];
   __shared__ double2 Bs[kGK][kGN + 1];
   const Geometry& g = a.geo;
   const int b = g.b, b2 = b * b;
-  const int M = b2, N = b, K = b;
+  const int M = nk1 * b, N = b, K = b;
+  // A row of GEMM row m (GEMM 2 with a band subset: m = l2 nk1 + l1)
+  auto arow = [&](int m) { return KIND == 2 && nk1 < b ? (m / nk1) * b + m % nk1 : m; };
   const int p = blockIdx.z;
   const PairIdx pi = pair_idx(a, pair0 + p);
   const int m0 = blockIdx.x * kGM, n0 = blockIdx.y * kGN;
@@ -141,7 +146,7 @@ __global__ void __launch_bounds__(kGThreads) v3_zgemm_kernel(V3Args a, long long
       }
       const int m = m0 + mi, k = k0 + ki;
       double2 v = make_double2(0.0, 0.0);
-      if (m < M && k < K) v = KIND == 1 ? A[(size_t)k * b2 + m] : A[(size_t)m * b + k];
+      if (m < M && k < K) v = KIND == 1 ? A[(size_t)k * b2 + m] : A[(size_t)arow(m) * b + k];
       As[ki][mi] = v;
     }
     // B tile: 8 x 64, k contiguous in e(q)[n][k]
@@ -188,7 +193,7 @@ __global__ void __launch_bounds__(kGThreads) v3_zgemm_kernel(V3Args a, long long
       for (int j = 0; j < 4; ++j) {
         const int m = m0 + ty + 16 * i, l3 = n0 + tx + 16 * j;
         if (m >= M || l3 >= N) continue;
-        const int l2 = m / b, l1 = m % b;
+        const int l2 = m / nk1, l1 = m % nk1;
         const double den = sqrt(8 * sqrt(fabs(w2[(size_t)pi.q1 * b + l1] * w2[(size_t)pi.q2 * b + l2] *
                                               w2[(size_t)pi.q3 * b + l3])));
         double v = 0.0;
@@ -199,11 +204,35 @@ __global__ void __launch_bounds__(kGThreads) v3_zgemm_kernel(V3Args a, long long
           atomicOr(a.err, 2);
         }
         const size_t b3 = (size_t)b2 * b;
-        if (a.v3_layout == 1)  // [row][l2][l3][l1][q2]
-          a.v3sq[(size_t)pi.row * nkc * b3 + (((size_t)l2 * b + l3) * b + l1) * nkc + pi.q2] = v;
+        size_t o;
+        if (a.v3_layout == 2)  // [row][l2][l3][q2][l1]
+          o = (((size_t)pi.row * b + l2) * b + l3) * nkc * b + (size_t)pi.q2 * b + l1;
+        else if (a.v3_layout == 1)  // [row][l2][l3][l1][q2]
+          o = (size_t)pi.row * nkc * b3 + (((size_t)l2 * b + l3) * b + l1) * nkc + pi.q2;
         else  // [row][q2][l1][l2][l3]
-          a.v3sq[((size_t)pi.row * nkc + pi.q2) * b3 + ((size_t)l1 * b + l2) * b + l3] = v;
+          o = ((size_t)pi.row * nkc + pi.q2) * b3 + ((size_t)l1 * b + l2) * b + l3;
+        if (a.v3sq_f32) a.v3sq_f32[o] = (float)v;
+        else a.v3sq[o] = v;
       }
+  }
+}
+
+// |V3|^2 of one row in the reference's order, [q2][l1][l2][l3] FP64, into
+// row `row` of a chunk in its layout and precision, bands l1 < nk1 only
+__global__ void v3_copy_row_kernel(V3Args a, int row, const double* __restrict__ src, int nk1) {
+  const int b = a.geo.b, nkc = a.geo.nkc;
+  const long long n = (long long)nkc * nk1 * b * b;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int l3 = (int)(i % b), l2 = (int)((i / b) % b), l1 = (int)((i / ((long long)b * b)) % nk1);
+    const int q2 = (int)(i / ((long long)b * b * nk1));
+    const double v = src[(((size_t)q2 * b + l1) * b + l2) * b + l3];
+    const size_t b3 = (size_t)b * b * b;
+    size_t o;
+    if (a.v3_layout == 2) o = (((size_t)row * b + l2) * b + l3) * nkc * b + (size_t)q2 * b + l1;
+    else if (a.v3_layout == 1) o = (size_t)row * nkc * b3 + (((size_t)l2 * b + l3) * b + l1) * nkc + q2;
+    else o = ((size_t)row * nkc + q2) * b3 + ((size_t)l1 * b + l2) * b + l3;
+    if (a.v3sq_f32) a.v3sq_f32[o] = (float)v;
+    else a.v3sq[o] = v;
   }
 }
 
@@ -217,11 +246,13 @@ size_t v3_dense_work_bytes(int b, long long npairs, size_t budget) {
   return (size_t)p * per;
 }
 
-cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s) {
+cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cudaStream_t s, int l1_keep) {
   const int b = a.geo.b;
-  if (!v3_dense_supported(b) || !a.hbuf) return cudaErrorInvalidValue;
+  // any band count as the FP64 near-zero-mode pass of the mixed path (a pair list)
+  if (!a.hbuf || b > kHeevMaxBands || (!a.pair_list && !v3_dense_supported(b))) return cudaErrorInvalidValue;
+  const int nk1 = l1_keep > 0 && l1_keep < b ? l1_keep : b;
   const size_t b3 = (size_t)b * b * b;
-  const long long npairs = (long long)a.nrows * a.geo.nkc;
+  const long long npairs = a.pair_list ? a.npairs_list : (long long)a.nrows * a.geo.nkc;
   // pairs per batch: as many as the workspace holds, at most 65535 (grid z)
   const long long P =
       std::min<long long>(65535, std::max<long long>(1, (long long)(work_bytes / (2 * b3 * sizeof(double2)))));
@@ -237,10 +268,19 @@ cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cuda
   for (long long p0 = 0; p0 < npairs; p0 += P) {
     const int np = (int)std::min<long long>(P, npairs - p0);
     v3_t1_kernel<<<dim3(np, b), kT1Threads, t1_smem, s>>>(a, p0, T1, table_ph);
-    const dim3 gg((b * b + kGM - 1) / kGM, (b + kGN - 1) / kGN, np);
-    v3_zgemm_kernel<1><<<gg, kGThreads, 0, s>>>(a, p0, T1, T2);
-    v3_zgemm_kernel<2><<<gg, kGThreads, 0, s>>>(a, p0, T2, nullptr);
+    const dim3 gg((nk1 * b + kGM - 1) / kGM, (b + kGN - 1) / kGN, np);
+    v3_zgemm_kernel<1><<<gg, kGThreads, 0, s>>>(a, p0, T1, T2, nk1);
+    v3_zgemm_kernel<2><<<gg, kGThreads, 0, s>>>(a, p0, T2, nullptr, nk1);
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_v3_copy_row(const V3Args& a, int row, const double* src, int l1_keep, cudaStream_t s) {
+  const int b = a.geo.b;
+  const int nk1 = l1_keep > 0 && l1_keep < b ? l1_keep : b;
+  const long long n = (long long)a.geo.nkc * nk1 * b * b;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 148 * 8);
+  v3_copy_row_kernel<<<blocks, 256, 0, s>>>(a, row, src, nk1);
   return cudaGetLastError();
 }
 

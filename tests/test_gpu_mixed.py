@@ -42,3 +42,33 @@ def test_mixed_precision_errors(oracle_lib, ald_lib, workdir, cfg, mesh, kw):
         k, kr = out[key], ref[rk].sum(0)
         assert np.abs(k - kr).max() <= 1e-4 * np.abs(kr).max(), (key, k, kr)
     ctx.close()
+
+
+@pytest.mark.parametrize("cfg,mesh,kw", [
+    (3, (3, 4, 4), {"p": 2, "rc_sigma": 1.2, "ibz": "none", "delta": "gauss"}),
+    (3, (4, 4, 4), {"p": 1, "rc_sigma": 1.2, "delta": "gauss"}),
+    (3, (4, 4, 4), {"p": 1, "rc_sigma": 1.2, "delta": "tetra"})],
+    ids=["sl24_odd_mesh", "sl12_gauss", "sl12_tetra"])
+def test_mixed_near_zero_modes(ald_lib, workdir, cfg, mesh, kw):
+    """The mixed path against the FP64 path where modes of vanishing frequency
+    enter: on the odd 3x4x4 mesh the reference's Gamma test (indices nc/2+1)
+    misses Gamma, so the pairs with q2 or q3 at Gamma carry the acoustic modes'
+    cancellation residue into the sums; at q1 = Gamma the acoustic linewidths
+    are that residue.  The mixed path forms those pairs in FP64, so the linewidths
+    of every other mode and kappa stay within the mixed bars of the FP64 path."""
+    d = make_case(workdir, cfg, mesh, **kw)
+    delta = ald_lib.DELTA_GAUSS if kw.get("delta") == "gauss" else ald_lib.DELTA_TETRA
+    out = {}
+    for prec in (ald_lib.FP64, ald_lib.MIXED):
+        with ald_lib.Context(d, ald_lib.default_options(precision=prec, delta=delta)) as ctx:
+            ev = ctx.get_frequencies()[0]
+            mapinv = ctx.get_mesh()["mapinv"] - 1
+            out[prec] = ctx.kappa_pipeline(ctx.info.tempk)
+    f, m = out[ald_lib.FP64], out[ald_lib.MIXED]
+    # linewidths of the IBZ modes whose frequency is not rounding noise
+    soft = np.abs(ev[:, mapinv].T) < 1e-9 * np.abs(ev).max()
+    Qf, Qm = f["Q"][~soft], m["Q"][~soft]
+    assert np.all(np.abs(Qm - Qf) <= 1e-4 * np.abs(Qf) + 1e-8 * np.abs(Qf).max()), np.abs(Qm - Qf).max()
+    for key in ("kappa_rta", "kappa_cg"):
+        k, kr = m[key], f[key]
+        assert np.abs(k - kr).max() <= 1e-4 * np.abs(kr).max(), (key, k, kr)
