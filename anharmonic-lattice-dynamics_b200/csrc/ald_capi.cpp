@@ -388,7 +388,7 @@ int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
     if (c->w_h.n < need) CKA(c->w_h.alloc(need));
     a.hbuf = c->w_h.p;
     const long long npairs = (long long)a.nrows * c->geo.nkc;
-    const long long P = v3_dense_tc_pairs(c->geo.b, npairs, (size_t)2 << 30);
+    const long long P = v3_dense_tc_pairs(c->geo.b, npairs, c->tune_gemm_bytes ? c->tune_gemm_bytes : (size_t)2 << 30);
     const size_t wb = v3_dense_tc_work_bytes(c->geo.b, c->geo.nkc, a.nrows, P);
     // GEMM 1 never writes the padding of the T2 operand: it is zeroed when the
     // workspace is new or was last laid out for another (bands, pairs)
@@ -432,7 +432,7 @@ int run_v3(ald_ctx* c, const V3Args& a0, int* nlaunch) {
     const size_t bneed = v3_tc_btile_bytes(a.nrows, c->VC.ncls, c->geo.nkc);
     if (c->w_btiles.n < bneed) CKA(c->w_btiles.alloc(bneed));
     e = launch_v3_rows_f32(a, c->stream);
-    if (e == cudaSuccess) e = launch_v3_tc(a, c->w_ptiles.p, c->w_btiles.p, c->stream);
+    if (e == cudaSuccess) e = launch_v3_tc(a, c->w_ptiles.p, c->w_btiles.p, c->stream, c->tune_v3_rpc, c->tune_v3_wg);
     nl += 4;  // class sums H, mode factors, B tiles, the MMA kernel
   } else if (v3_pair_supported(c->geo.b, prec)) {
     const size_t need = v3_hbuf_bytes(c->geo.b, c->VC.ncls, a.nrows, prec);

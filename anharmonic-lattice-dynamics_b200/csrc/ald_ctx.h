@@ -52,6 +52,9 @@ struct ald_ctx {
   DevBuf<char> w_scratch;
   DevBuf<double> w_heev;    // Householder eigensolver workspace (large cells)
   DevBuf<double> w_rmax;    // deterministic delta: each R entry's largest term (FP64 bits)
+  // launch shapes chosen by ald_autotune (0 = the built-in choices)
+  int tune_v3_rpc = 0, tune_v3_wg = 0;
+  size_t tune_gemm_bytes = 0;
   CgWork cg;
   bool have_phonons = false;
   double dist_tempk = -1;

@@ -333,7 +333,10 @@ cudaError_t launch_v3_tc_ptiles(const V3Args& a, void* ptiles, cudaStream_t s);
 // btiles: scratch of v3_tc_btile_bytes(nrows, ncls, nkc) (B operands and row data of the
 // chunk's rows, per-mode factors and FP32 eigenvectors of the mesh)
 size_t v3_tc_btile_bytes(int nrows, int ncls, int nkc);
-cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s);
+// rows_per_cta, epilogue_wg: 0 = the built-in choice (up to 16 rows while the
+// grid fills the GPU twice; 2 warpgroups), else 1..16 rows and 2 or 3
+cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s, int rows_per_cta = 0,
+                         int epilogue_wg = 0);
 
 struct CombineArgs {
   Geometry geo;

@@ -549,7 +549,7 @@ static size_t pipeline_bytes_estimate(const ald_ctx* c) {
   const size_t N = 3 * b * nibz;
   size_t s = 2 * rsz + k * per_row + N * N * sizeof(double);
   s += 2 * (k * nkc * b * b) * sizeof(unsigned long long);  // deterministic delta
-  if (b > 12) s += (size_t)2 << 30;
+  if (b > 12) s += c->tune_gemm_bytes ? c->tune_gemm_bytes : (size_t)2 << 30;
   if (b > 64) s += heev_work_doubles((int)b, heev_slots((int)nkc * 7)) * sizeof(double);
   return s + ((size_t)256 << 20);
 }

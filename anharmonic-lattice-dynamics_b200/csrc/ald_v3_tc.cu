@@ -526,24 +526,27 @@ size_t v3_tc_btile_bytes(int nrows, int ncls, int nkc) {
   return total;
 }
 
-cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s) {
+cudaError_t launch_v3_tc(const V3Args& a, const void* ptiles, void* btiles, cudaStream_t s, int rows_per_cta,
+                         int epilogue_wg) {
   if (!v3_tc_supported(a.geo.b, a.ncls)) return cudaErrorInvalidValue;
   const int kp = (2 * a.ncls + 15) / 16 * 16;
   const TcScratch ts = tc_carve(btiles, a.nrows, kp, a.geo.nkc, nullptr);
   v3_tc_modes_kernel<<<(a.geo.nkc + 127) / 128, 128, 0, s>>>(a, ts);
   v3_btile_kernel<<<a.nrows, 256, 0, s>>>(a, kp, ts);
   const size_t smem = (size_t)(2 * kTM + 4 * kNP) * kp * sizeof(__half);
-  // epilogue warpgroups: 2 by default; ALD_V3_TC_WG=3 selects three
-  static const int ne = [] {
+  // epilogue warpgroups: 2 unless the caller (the autotuner) or ALD_V3_TC_WG=3 selects three
+  static const int ne_env = [] {
     const char* v = getenv("ALD_V3_TC_WG");
     return v && atoi(v) == 3 ? 3 : 2;
   }();
+  const int ne = epilogue_wg == 2 || epilogue_wg == 3 ? epilogue_wg : ne_env;
   cudaError_t e = raise_smem_limit(ne == 3 ? (const void*)v3_tc3_kernel<3> : (const void*)v3_tc3_kernel<2>, smem);
   if (e != cudaSuccess) return e;
   const int ntiles = (a.geo.nkc + kTM - 1) / kTM;
   // rows per CTA: reuse the phase tile over several rows while the grid still fills the GPU twice
   int rpc = 16;
   while (rpc > 1 && (long)ntiles * ((a.nrows + rpc - 1) / rpc) < 2 * 148) rpc /= 2;
+  if (rows_per_cta >= 1 && rows_per_cta <= 16) rpc = rows_per_cta;
   dim3 grid(ntiles, (a.nrows + rpc - 1) / rpc);
   if (ne == 3)
     v3_tc3_kernel<3><<<grid, TcShape<3>::threads, smem, s>>>(a, kp, static_cast<const __half*>(ptiles), ts, rpc);

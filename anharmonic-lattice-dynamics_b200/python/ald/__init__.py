@@ -55,6 +55,11 @@ class KappaResult(C.Structure):
                 ("launches", C.c_int * 10), ("triplet_bands", C.c_double), ("d2h_bytes", C.c_double)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("chunk_bytes", C.c_size_t), ("v3_rows_per_cta", C.c_int), ("v3_epilogue_wg", C.c_int),
+                ("v3_gemm_bytes", C.c_size_t), ("ms", C.c_double), ("from_cache", C.c_int), ("candidates", C.c_int)]
+
+
 STAGES = ["phonons", "v3", "delta", "q_reduce", "rta", "collision", "rhs", "cg", "kappa_cg", "total"]
 
 
@@ -69,7 +74,8 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_kappa_iterative", "ald_collision_matrix_iso", "ald_p_iso_split", "ald_set_isotope_g",
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_kappa_pipeline_sharded_dev", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
-           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched", "ald_release_workspaces"]
+           "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched", "ald_release_workspaces",
+           "ald_autotune", "ald_set_tuning"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -92,6 +98,8 @@ def lib():
                                               C.c_int, C.c_int, C.POINTER(C.c_int), C.c_void_p]
         L.ald_format_value.argtypes = [C.c_char_p, C.c_double, C.c_char_p, C.c_int]
         L.ald_release_cached_memory.restype = None
+        L.ald_autotune.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.POINTER(Tuning)]
+        L.ald_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
         for n in EXPORTS[2:]:
             if n not in ("ald_destroy", "ald_h2d_bytes", "ald_release_cached_memory"):
                 getattr(L, n).restype = C.c_int
@@ -199,6 +207,22 @@ class Context:
 
     def h2d_bytes(self) -> float:
         return lib().ald_h2d_bytes(self.h)
+
+    def autotune(self, cache_path=None, budget_s=0.0):
+        """ald_autotune: time candidate launch shapes of the pipeline (or read
+        them from the cache file), keep the fastest on this context; returns
+        the choice as a dict."""
+        t = Tuning()
+        _check(lib().ald_autotune(self.h, cache_path.encode() if cache_path else None, float(budget_s), C.byref(t)))
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
+
+    def set_tuning(self, **kw):
+        """ald_set_tuning: apply a choice (chunk_bytes, v3_rows_per_cta,
+        v3_epilogue_wg, v3_gemm_bytes; missing fields = the built-in choice)."""
+        t = Tuning()
+        for k, v in kw.items():
+            setattr(t, k, v)
+        _check(lib().ald_set_tuning(self.h, C.byref(t)))
 
     def invalidate_phonons(self):
         """Make the next pipeline call recompute eigenpairs (get_frequencies)."""

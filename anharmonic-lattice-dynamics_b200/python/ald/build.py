@@ -25,6 +25,7 @@ SOURCES = {
     "ald_pool.cpp": [],
     "ald_capi.cpp": [],
     "ald_pipeline.cpp": [],
+    "ald_tune.cpp": [],
     "ald_phonon.cu": [],
     "ald_heev.cu": [],
     "ald_v3.cu": [],

@@ -269,14 +269,43 @@ int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double
  * the reference runs one structure per kappa_full run.  A pool of up to 8
  * host threads takes the structures largest first (nibz nkc ndyn^3), each on
  * its context's own stream, so the structures' kernels overlap on the
- * device; when n exceeds the pool, a structure's pipeline workspaces are
- * released after its run (to the library's device-memory cache), which
- * bounds device memory by the pool.  tempk[n], res[n]; status[n] (may be
+ * device.  A structure starts only while the estimated pipeline workspaces
+ * of the structures running on its device, plus its own, stay within 85 %
+ * of the device memory free when the call began (one structure always
+ * runs).  When not every structure runs at once, a structure's pipeline
+ * workspaces are released after its run (to the library's device-memory
+ * cache).  tempk[n], res[n]; status[n] (may be
  * NULL) receives each structure's return code.  Returns ALD_OK, or the first
  * structure's error (ald_last_error names the structure).  The contexts must
  * be distinct; each structure's limits are those of ald_kappa_pipeline (up
  * to 256 bands). */
 int ald_kappa_batched(int n, ald_ctx* const* ctx, const double* tempk, ald_kappa_result* res, int* status);
+
+/* No counterpart in the reference (one code path per routine there): the
+ * pipeline's autotuner.  ald_autotune times whole ald_kappa_pipeline calls
+ * (device time, at the tmin of latdyn.params) over candidate launch shapes,
+ * one knob at a time: the |V3|^2 chunk (IBZ rows per V3 and delta launch),
+ * for 3-band mixed cells the tensor-core V3's rows per CTA and epilogue
+ * warpgroups, for mixed cells of 9 bands and up the pair-batch workspace of
+ * the tensor-core mode-product GEMMs.  It keeps the fastest on the context
+ * and in the cache file (cache_path; NULL or "": $ALD_TUNE_CACHE; neither:
+ * no file), one text line per shape (device, bands, mesh, IBZ rows,
+ * precision, delta, deterministic option).  When the file already holds the
+ * context's shape, the choice is read from it and nothing is timed.
+ * budget_s (<= 0: 10 s) bounds the timing; the knobs change launch shapes
+ * only, not results.  ald_set_tuning applies a choice directly (0 fields =
+ * the built-in choices). */
+typedef struct ald_tuning {
+  size_t chunk_bytes;   /* as ald_options.chunk_bytes (0 = automatic)                    */
+  int v3_rows_per_cta;  /* 3-band tensor-core V3: IBZ rows per CTA, 1..16 (0 = built-in) */
+  int v3_epilogue_wg;   /* 3-band tensor-core V3: epilogue warpgroups, 2 or 3 (0 = 2)    */
+  size_t v3_gemm_bytes; /* tensor-core mode-product GEMMs: pair-batch workspace (0 = 2 GiB) */
+  double ms;            /* device time of one pipeline call with this choice             */
+  int from_cache;       /* 1: read from the cache file, 0: timed by this call            */
+  int candidates;       /* pipeline choices timed                                        */
+} ald_tuning;
+int ald_autotune(ald_ctx* ctx, const char* cache_path, double budget_s, ald_tuning* out);
+int ald_set_tuning(ald_ctx* ctx, const ald_tuning* t);
 
 /* No counterpart in the reference: hands a context's pipeline workspaces
  * (R1/R2, the |V3|^2 chunk, the V3 and eigensolver workspaces, the collision
