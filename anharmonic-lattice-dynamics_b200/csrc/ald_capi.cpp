@@ -275,8 +275,10 @@ V3Args v3_args(ald_ctx* c, int first, int nrows, double* out) {
 // sub.f90:7351-7356) misses Gamma, or at q1 = Gamma, those entries reached
 // kappa.  Such pairs are formed again in FP64 with the dense GEMMs of
 // ald_v3_dense.cu, over the chunk's output in its layout: every pair whose
-// q2 or q3 is such a point, and for a row whose q1 is one, every pair with
-// its soft bands l1 (the leading ones: bands are ordered by |lambda|).  The
+// q2 or q3 is such a point (unless the delta zeroes every soft band there:
+// at most 3 of them, at the point of the Gamma test), and for a row whose q1
+// is one, every pair with its soft bands l1 (the leading ones: bands are
+// ordered by |lambda|).  The
 // linewidths of those soft modes are that residue in FP64 too, and through
 // the collision matrix they reach kappa: their row is formed with the
 // kernel the FP64 path uses for the cell (the direct form up to 12 bands),
@@ -312,6 +314,9 @@ static int v3_soft_fp64(ald_ctx* c, const V3Args& a, int* nl) {
     for (int sp : soft) {
       int ms[3], m2[3];
       dec(sp, ms);
+      // the delta zeroes bands l < 3 at the point with indices nc/2 (the
+      // reference's Gamma test): there nothing of a soft mode reaches the sums
+      if (ms[0] == nc[0] / 2 && ms[1] == nc[1] / 2 && ms[2] == nc[2] / 2 && nsoft[sp] <= 3) continue;
       all.push_back((long long)r * nkc + sp);  // q2 at the point
       for (int x = 0; x < 3; ++x) {            // q3 = -q1 - q2 at the point
         int v = (-m1[x] - ms[x] + (c->geo.shifted ? nc[x] / 2 : 0)) % nc[x];
@@ -331,27 +336,34 @@ static int v3_soft_fp64(ald_ctx* c, const V3Args& a, int* nl) {
   all.erase(std::unique(all.begin(), all.end()), all.end());
   const size_t nall = all.size(), npart = part.size();
   all.insert(all.end(), part.begin(), part.end());
-  if (c->w_pairs.n < all.size()) CKA(c->w_pairs.alloc(all.size()));
-  // pageable source: the copy has left the vector when the call returns
-  CK(cudaMemcpyAsync(c->w_pairs.p, all.data(), all.size() * sizeof(long long), cudaMemcpyHostToDevice, c->stream));
-  V3Args f = a;
-  const size_t hneed = v3_hbuf_bytes(b, c->VC.ncls, a.nrows, ALD_FP64);
-  if (c->w_h64.n < hneed) CKA(c->w_h64.alloc(hneed));
-  f.hbuf = c->w_h64.p;
-  const size_t wb = v3_dense_work_bytes(b, (long long)std::max(nall, npart), (size_t)256 << 20);
-  if (c->w_v3fix.n < wb) CKA(c->w_v3fix.alloc(wb));
-  cudaError_t e = launch_v3_rows_f64(f, c->stream);
-  *nl += 1;
-  const long long per = (long long)(c->w_v3fix.n / (2 * (size_t)b * b * b * 16));
-  f.pair_list = c->w_pairs.p;
-  f.npairs_list = (long long)nall;
-  if (e == cudaSuccess) e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream);
-  *nl += 3 * (int)(((long long)nall + per - 1) / per);
-  if (npart && e == cudaSuccess) {
-    f.pair_list = c->w_pairs.p + nall;
-    f.npairs_list = (long long)npart;
-    e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream, nk1);
-    *nl += 3 * (int)(((long long)npart + per - 1) / per);
+  if (all.empty() && soft_rows.empty()) return ALD_OK;
+  if (!all.empty()) {
+    if (c->w_pairs.n < all.size()) CKA(c->w_pairs.alloc(all.size()));
+    // pageable source: the copy has left the vector when the call returns
+    CK(cudaMemcpyAsync(c->w_pairs.p, all.data(), all.size() * sizeof(long long), cudaMemcpyHostToDevice,
+                       c->stream));
+  }
+  cudaError_t e = cudaSuccess;
+  if (nall || npart) {  // the dense FP64 GEMMs over the pair lists
+    V3Args f = a;
+    const size_t hneed = v3_hbuf_bytes(b, c->VC.ncls, a.nrows, ALD_FP64);
+    if (c->w_h64.n < hneed) CKA(c->w_h64.alloc(hneed));
+    f.hbuf = c->w_h64.p;
+    const size_t wb = v3_dense_work_bytes(b, (long long)std::max(nall, npart), (size_t)256 << 20);
+    if (c->w_v3fix.n < wb) CKA(c->w_v3fix.alloc(wb));
+    e = launch_v3_rows_f64(f, c->stream);
+    *nl += 1;
+    const long long per = (long long)(c->w_v3fix.n / (2 * (size_t)b * b * b * 16));
+    f.pair_list = c->w_pairs.p;
+    f.npairs_list = (long long)nall;
+    if (nall && e == cudaSuccess) e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream);
+    *nl += 3 * (int)(((long long)nall + per - 1) / per);
+    if (npart && e == cudaSuccess) {
+      f.pair_list = c->w_pairs.p + nall;
+      f.npairs_list = (long long)npart;
+      e = launch_v3_dense(f, c->w_v3fix.p, c->w_v3fix.n, c->stream, nk1);
+      *nl += 3 * (int)(((long long)npart + per - 1) / per);
+    }
   }
   if (!soft_rows.empty() && e == cudaSuccess) {
     const size_t rn = (size_t)nkc * b * b * b;

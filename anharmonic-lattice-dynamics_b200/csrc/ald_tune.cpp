@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <map>
 #include <mutex>
 #include <sstream>
 #include <string>
@@ -48,15 +49,28 @@ struct Choice {
 
 std::mutex g_tune_mu;  // one tuner per process touches the cache file at a time
 
-std::string shape_key(const ald_ctx* c) {
+// the device's name and compute capability, looked up once per device
+// (cudaGetDeviceProperties takes milliseconds)
+std::string device_tag(int device) {
+  static std::mutex mu;
+  static std::map<int, std::string> tags;
+  std::lock_guard<std::mutex> lk(mu);
+  auto it = tags.find(device);
+  if (it != tags.end()) return it->second;
   cudaDeviceProp p;
   std::string dev = "device";
-  if (cudaGetDeviceProperties(&p, c->device) == cudaSuccess) {
+  if (cudaGetDeviceProperties(&p, device) == cudaSuccess) {
     dev = p.name;
     dev += "-sm" + std::to_string(p.major) + std::to_string(p.minor);
   }
   for (char& ch : dev)
     if (ch == ' ' || ch == '\t') ch = '_';
+  tags[device] = dev;
+  return dev;
+}
+
+std::string shape_key(const ald_ctx* c) {
+  const std::string dev = device_tag(c->device);
   std::ostringstream k;
   k << dev << "|b" << c->geo.b << "|mesh" << c->geo.nc[0] << "x" << c->geo.nc[1] << "x" << c->geo.nc[2] << "|nibz"
     << c->T.nibz << "|prec" << c->opt.precision << "|delta" << delta_mode(const_cast<ald_ctx*>(c)) << "|det"

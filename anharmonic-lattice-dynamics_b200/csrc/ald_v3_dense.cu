@@ -69,7 +69,8 @@ __device__ __forceinline__ PairIdx pair_idx(const V3Args& a, long long pair) {
 
 // T1 of the batch's pairs: CTA (pair, jb), threads over (l1, kc)
 constexpr int kT1Threads = 256;
-__global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long pair0, double2* T1, int table_ph) {
+__global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long pair0, double2* T1, int table_ph,
+                                                             int nk1) {
   extern __shared__ double2 s_ph[];  // P_c(q2) of every class
   const Geometry& g = a.geo;
   const int b = g.b, nat0 = g.nat0;
@@ -85,7 +86,7 @@ __global__ void __launch_bounds__(kT1Threads) v3_t1_kernel(V3Args a, long long p
   __syncthreads();
   const double2* H = static_cast<const double2*>(a.hbuf) + (size_t)pi.row * a.ncls * 9 * b;
   double2* out = T1 + ((size_t)p * b + jb) * b * b;
-  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+  for (int e = threadIdx.x; e < nk1 * b; e += blockDim.x) {  // bands l1 < nk1
     const int l1 = e / b, kc = e % b, k0 = kc / 3, ga = kc % 3;
     const int grp = j0 * nat0 + k0;
     double2 acc = make_double2(0.0, 0.0);
@@ -267,7 +268,7 @@ cudaError_t launch_v3_dense(const V3Args& a, void* work, size_t work_bytes, cuda
   }
   for (long long p0 = 0; p0 < npairs; p0 += P) {
     const int np = (int)std::min<long long>(P, npairs - p0);
-    v3_t1_kernel<<<dim3(np, b), kT1Threads, t1_smem, s>>>(a, p0, T1, table_ph);
+    v3_t1_kernel<<<dim3(np, b), kT1Threads, t1_smem, s>>>(a, p0, T1, table_ph, nk1);
     const dim3 gg((nk1 * b + kGM - 1) / kGM, (b + kGN - 1) / kGN, np);
     v3_zgemm_kernel<1><<<gg, kGThreads, 0, s>>>(a, p0, T1, T2, nk1);
     v3_zgemm_kernel<2><<<gg, kGThreads, 0, s>>>(a, p0, T2, nullptr, nk1);

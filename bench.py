@@ -346,6 +346,8 @@ def main():
                     help="rocksalt: the metric's configuration (default); lj-argon: the large single structure")
     ap.add_argument("--mesh", type=int, default=0, help="mesh edge (default: the workload's own)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--tune-cache", default="",
+                    help="the autotuner's cache file (default: a fresh one in the workload's directory)")
     ap.add_argument("--no-extra", action="store_true",
                     help="skip the extra driver-timed workloads (32^3 argon, the 192-band cell)")
     args = ap.parse_args()
@@ -415,7 +417,7 @@ def main():
         tempk = ctx.info.tempk
         # the library's autotuner picks the launch shapes (outside the timed
         # region; its cache file lives in the workload's directory)
-        tuning = ctx.autotune(os.path.join(d, "ald_tune.txt"), budget_s=30) if world == 1 else None
+        tuning = ctx.autotune(args.tune_cache or os.path.join(d, "ald_tune.txt"), budget_s=30) if world == 1 else None
 
         ev_a, ev_b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         # several GPUs: the reference's MPI row split, one rank per GPU, with
@@ -495,7 +497,7 @@ def main():
         t0 = time.perf_counter()
         c2 = ald.Context(d, opts)
         if world == 1:  # the tuned launch shapes, read from the cache file
-            c2.autotune(os.path.join(d, "ald_tune.txt"))
+            c2.autotune(args.tune_cache or os.path.join(d, "ald_tune.txt"))
         if gdev_e2e is not None:
             c2.set_stream(stream.cuda_stream)
             o2 = c2.kappa_pipeline_sharded(rank, world, gdev_e2e, tempk, device=True)
