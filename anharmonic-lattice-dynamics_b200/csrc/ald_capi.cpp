@@ -215,6 +215,7 @@ int ensure_phonons(ald_ctx* c) {
   CK(launch_phonon_post(c->geo, c->w2_all.p, a.dq, PhysConst::cnst(), c->vel.p, c->stream));
   CK(launch_subst_eivecs(c->geo, c->neg_src.p, c->neg_dst.p, (int)c->T.neg_src.size(), c->evec.p, c->stream));
   c->have_phonons = true;
+  ++c->phonon_epoch;
   c->dist_tempk = -1;
   return ALD_OK;
 }
@@ -820,6 +821,7 @@ int ald_set_phonons(ald_ctx* c, const double* eigenval, const double* eigenvec, 
   CK(cudaMemcpyAsync(c->vel.p, veloc, nkc * b * 3 * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   c->have_phonons = true;
+  ++c->phonon_epoch;
   c->dist_tempk = -1;
   return ALD_OK;
 }

@@ -57,6 +57,15 @@ struct ald_ctx {
   size_t tune_gemm_bytes = 0;
   CgWork cg;
   bool have_phonons = false;
+  unsigned long long phonon_epoch = 0;  // advanced whenever the eigenpairs change
+  // |V3|^2 of every row of [v3c_rb, v3c_re) in w_v3 from one chunk, valid for
+  // the eigenpairs of v3c_epoch (0 = nothing kept): a later pipeline call
+  // with the same eigenpairs and rows reuses it (|V3|^2 does not depend on T)
+  unsigned long long v3c_epoch = 0;
+  int v3c_rb = -1, v3c_re = -1, v3c_layout = -1;
+  bool v3c_f32 = false;
+  const void* v3c_ptr = nullptr;
+  size_t v3c_n = 0;
   double dist_tempk = -1;
 };
 

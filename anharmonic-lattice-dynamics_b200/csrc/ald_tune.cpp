@@ -136,6 +136,7 @@ int time_choice(ald_ctx* c, const Choice& ch, double tempk, double& ms) {
   apply(c, ch);
   ms = 1e300;
   for (int rep = 0; rep < 2; ++rep) {
+    c->v3c_epoch = 0;  // time V3 too, not the kept |V3|^2
     ald_kappa_result r;
     const int st = ald_kappa_pipeline(c, tempk, &r, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     if (st != ALD_OK && st != ALD_WARN_CG_MAXITER) return st;
