@@ -260,7 +260,12 @@ int ald_set_stream(ald_ctx* ctx, void* stream);
 double ald_h2d_bytes(ald_ctx* ctx);
 
 /* Q, QN, QU (nibz,ndyn), kappa_rta_modes / kappa_cg_modes (ndyn,3,3),
- * x (nibz*ndyn*3, the CG solution) may be NULL. */
+ * x (nibz*ndyn*3, the CG solution) may be NULL.  When one |V3|^2 chunk
+ * (ald_options.chunk_bytes, or the autotuner's choice) holds every IBZ row,
+ * the context keeps it after the call; a later call with the same eigenpairs
+ * (another temperature, as kappa_full's tmin..tmax) reuses it and launches no
+ * V3 kernel (res->launches[1] = 0).  New eigenpairs (ald_get_frequencies,
+ * ald_set_phonons) or ald_release_workspaces drop it. */
 int ald_kappa_pipeline(ald_ctx* ctx, double tempk, ald_kappa_result* res, double* Q, double* QN, double* QU,
                        double* kappa_rta_modes, double* kappa_cg_modes, double* x);
 
