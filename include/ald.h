@@ -41,9 +41,13 @@ enum ald_status {
 
 enum ald_delta { ALD_DELTA_TETRA = 0, ALD_DELTA_GAUSS = 1 };
 /* ALD_MIXED: the V3 contraction in reduced precision with FP32 accumulation --
- * for 3 bands the phase-class sums run on the tensor cores (split-FP16
- * tcgen05 MMAs), otherwise in FP32 on the CUDA cores; ALD_MIXED_FP32 always
- * uses the FP32 CUDA-core form.  Everything outside V3 stays FP64. */
+ * for 3 bands the phase-class sums, from 9 bands up both eigenvector mode
+ * products run on the tensor cores (split-FP16 tcgen05 MMAs), 6 bands in FP32
+ * on the CUDA cores; from 9 bands up the pairs that involve a mode of
+ * vanishing frequency are formed again in FP64.  ALD_MIXED_FP32 uses the FP32
+ * CUDA-core form where one exists.  Inside the pipeline the delta weights and
+ * the stored collision matrix are FP32 too; eigensolve, Bose factors, the sums
+ * into Q, CG vectors and kappa stay FP64. */
 enum ald_precision { ALD_FP64 = 0, ALD_MIXED = 1, ALD_MIXED_FP32 = 2 };
 enum ald_cg_stop { ALD_CG_REFERENCE = 0, ALD_CG_RESIDUAL = 1 };
 
