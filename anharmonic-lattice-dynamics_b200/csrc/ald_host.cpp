@@ -673,6 +673,66 @@ std::string build_tables(const System& S, Tables& T) {
   // (-2: off the mesh or outside its cell, -1: end of the list); the pass
   // that assigns IBZ points is sequential, as in the reference.
   const int npg = T.npg;
+  // getstar + locate for one mesh point, as star() and the reduced/locate
+  // steps above, with each op's two products folded into one matrix per
+  // frame: v2 = (primlatt^T opk) k for the duplicate test, f = (G^-1 opk) k
+  // for the mesh index (reordered sums: the 1e-6 duplicate tolerance and the
+  // 1e-3 mesh tolerance are far above their rounding).  out[c] is the mesh
+  // index of the c-th distinct arm, -2 where it is off the mesh or outside
+  // its cell; the list ends at -1.
+  std::vector<std::array<double, 9>> opv2(npg), opf(npg);
+  for (int o = 0; o < npg; ++o)
+    for (int a = 0; a < 3; ++a)
+      for (int b2 = 0; b2 < 3; ++b2) {
+        double sv = 0, sf = 0;
+        for (int k = 0; k < 3; ++k) {
+          sv += S.primlatt[cm(k, a)] * T.opk[o][cm(k, b2)];
+          sf += Ginv[cm(a, k)] * T.opk[o][cm(k, b2)];
+        }
+        opv2[o][3 * a + b2] = sv;
+        opf[o][3 * a + b2] = sf;
+      }
+  auto mesh_star_cands = [&](const double* kc, int* out) {
+    constexpr int kBuckets = 1 << 16, kSlots = 128;
+    double key[48][3];
+    int head[kSlots], nxt[48], kb[48], nkey = 0;
+    std::fill(head, head + kSlots, -1);
+    for (int o = 0; o < npg; ++o) {
+      const double* A = opv2[o].data();
+      double fr[3];
+      for (int a = 0; a < 3; ++a) {
+        const double v2 = A[3 * a] * kc[0] + A[3 * a + 1] * kc[1] + A[3 * a + 2] * kc[2];
+        fr[a] = v2 - std::floor(v2);
+      }
+      const int bk = std::min(kBuckets - 1, (int)(fr[0] * kBuckets));
+      bool dup = false;
+      for (int db = -1; db <= 1 && !dup; ++db) {
+        const int bb = (bk + db + kBuckets) % kBuckets;
+        for (int q = head[bb % kSlots]; q >= 0 && !dup; q = nxt[q]) {
+          if (kb[q] != bb) continue;
+          int c;
+          for (c = 0; c < 3; ++c) {
+            const double d = std::fabs(fr[c] - key[q][c]);
+            if (d > 1e-6 && d < 1 - 1e-6) break;
+          }
+          if (c == 3) dup = true;
+        }
+      }
+      if (dup) continue;
+      kb[nkey] = bk;
+      nxt[nkey] = head[bk % kSlots];
+      head[bk % kSlots] = nkey;
+      key[nkey][0] = fr[0];
+      key[nkey][1] = fr[1];
+      key[nkey][2] = fr[2];
+      const double* B = opf[o].data();
+      double f[3];
+      for (int a = 0; a < 3; ++a) f[a] = B[3 * a] * kc[0] + B[3 * a + 1] * kc[1] + B[3 * a + 2] * kc[2];
+      bool in_cell;
+      const int idx = locate(f, in_cell);
+      out[nkey++] = idx >= 0 && in_cell ? idx : -2;
+    }
+  };
   // task 0 builds the tetrahedra (they depend on the mesh only); tasks 1..
   // take stripes of mesh points, on the library's worker pool
   std::vector<int> cand((size_t)T.nkc * npg, -1);
@@ -684,18 +744,7 @@ std::string build_tables(const System& S, Tables& T) {
         return;
       }
       const int t = task - 1;
-      std::vector<std::array<double, 3>> ar;
-      std::vector<int> ao;
-      for (int n = t; n < T.nkc; n += nthr) {
-        star(&T.kpc32[3 * (size_t)n], ar, ao);
-        for (size_t c = 0; c < ar.size(); ++c) {
-          double f[3];
-          reduced(ar[c].data(), f);
-          bool in_cell;
-          const int idx = locate(f, in_cell);
-          cand[(size_t)n * npg + c] = idx >= 0 && in_cell ? idx : -2;
-        }
-      }
+      for (int n = t; n < T.nkc; n += nthr) mesh_star_cands(&T.kpc32[3 * (size_t)n], &cand[(size_t)n * npg]);
     });
   }
   if (!tet_err.empty()) return tet_err;
