@@ -1081,6 +1081,26 @@ int ald_cg_quadratic(int n, const double* a, const double* b, double* vmin, doub
   return r;
 }
 
+int ald_weight_tet(int ntet, const double* w, double e, int fp32, double* c) {
+  if (ntet < 0 || (ntet > 0 && (!w || !c))) return fail(ALD_ERR_ARG, "bad argument");
+  if (ntet == 0) return ALD_OK;
+  cudaStream_t s;
+  CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  struct SG {
+    cudaStream_t s;
+    ~SG() { cudaStreamDestroy(s); }
+  } guard{s};
+  const size_t n = (size_t)4 * ntet;
+  DevBuf<double> dw, dc;
+  CKA(dw.alloc(n));
+  CKA(dc.alloc(n));
+  CK(cudaMemcpyAsync(dw.p, w, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(launch_weight_tet(ntet, dw.p, e, fp32 ? 1 : 0, dc.p, s));
+  CK(cudaMemcpyAsync(c, dc.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return ALD_OK;
+}
+
 int ald_set_isotope_g(ald_ctx* c, const double* g) {
   if (!c || !g) return fail(ALD_ERR_ARG, "null argument");
   c->giso.assign(g, g + c->S.nat0);

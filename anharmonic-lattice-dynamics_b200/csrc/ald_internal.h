@@ -441,6 +441,8 @@ cudaError_t launch_piso(const Geometry& geo, int n1_first, int nrows, const int*
 cudaError_t launch_add(size_t n, double* y, const double* x, cudaStream_t s);
 // brange[l] = min_q omega(q,l), brange[b+l] = max_q omega(q,l)
 cudaError_t launch_band_range(const Geometry& geo, const double* freq, double* brange, cudaStream_t s);
+// weight_tet on a list of tetrahedra (device arrays w, c of 4 doubles each), fp32: the mixed form
+cudaError_t launch_weight_tet(int ntet, const double* w, double e, int fp32, double* c, cudaStream_t s);
 // the g of cal_g for an element name (false: no isotope data for it), and
 // of every primitive atom (cal_giso)
 bool isotope_g(const std::string& element, double& g);

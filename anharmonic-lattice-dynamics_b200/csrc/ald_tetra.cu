@@ -1086,7 +1086,37 @@ __global__ void __launch_bounds__(256) q_from_r_any_kernel(Geometry g, int n1_fi
   }
 }
 
+// weight_tet over a list of tetrahedra at one energy e, one thread each:
+// w[4 t + k] corner energies, c[4 t + k] corner weights (0 outside the
+// tetrahedron's energy range).  fp32 = 0: the FP64 form the FP64 pipeline
+// uses (bit for bit the reference's arithmetic); 1: the FP32 form of the
+// mixed pipeline.
+__global__ void __launch_bounds__(256) weight_tet_kernel(int ntet, const double* __restrict__ w, double e, int fp32,
+                                                         double* __restrict__ c) {
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntet; t += gridDim.x * blockDim.x) {
+    float en[4];
+    for (int k = 0; k < 4; ++k) en[k] = (float)w[4 * (size_t)t + k];
+    const TetSorted ts = tet_sort(en[0], en[1], en[2], en[3]);
+    double cp[4] = {0.0, 0.0, 0.0, 0.0};
+    if (fp32) {
+      float cf[4];
+      if (tet_weights4_f32(ts, e, cf))
+        for (int k = 0; k < 4; ++k) cp[k] = (double)cf[k];
+    } else if (!tet_weights4(ts, e, cp)) {
+      cp[0] = cp[1] = cp[2] = cp[3] = 0.0;
+    }
+    for (int k = 0; k < 4; ++k) c[4 * (size_t)t + k] = cp[tet_pos(en, k)];
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_weight_tet(int ntet, const double* w, double e, int fp32, double* c, cudaStream_t s) {
+  if (ntet <= 0) return cudaSuccess;
+  const int blocks = std::min((ntet + 255) / 256, 148 * 8);
+  weight_tet_kernel<<<blocks, 256, 0, s>>>(ntet, w, e, fp32, c);
+  return cudaGetLastError();
+}
 
 size_t combine_scratch_bytes(const Geometry& geo, int nrows, int gauss) {
   if (gauss) return 0;

@@ -75,7 +75,7 @@ EXPORTS = ["ald_default_options", "ald_last_error", "ald_create_from_dir", "ald_
            "ald_get_isotope_g", "ald_shard_rows", "ald_kappa_pipeline_sharded", "ald_kappa_pipeline_sharded_dev", "ald_tau_eff", "ald_qandtau",
            "ald_write_kappa", "ald_write_job1_files", "ald_format_value", "ald_make_kp_bs",
            "ald_function_self_w", "ald_self_energy_bs", "ald_release_cached_memory", "ald_kappa_batched", "ald_release_workspaces",
-           "ald_autotune", "ald_set_tuning"]
+           "ald_autotune", "ald_set_tuning", "ald_weight_tet"]
 CG_STATIC_MAX_N = 32768  # ALD_CG_STATIC_MAX_N of include/ald.h
 
 
@@ -100,6 +100,7 @@ def lib():
         L.ald_release_cached_memory.restype = None
         L.ald_autotune.argtypes = [C.c_void_p, C.c_char_p, C.c_double, C.POINTER(Tuning)]
         L.ald_set_tuning.argtypes = [C.c_void_p, C.POINTER(Tuning)]
+        L.ald_weight_tet.argtypes = [C.c_int, dp, C.c_double, C.c_int, dp]
         for n in EXPORTS[2:]:
             if n not in ("ald_destroy", "ald_h2d_bytes", "ald_release_cached_memory"):
                 getattr(L, n).restype = C.c_int
@@ -610,6 +611,16 @@ def torch_allgather_device(group=None):
                 off += c
 
     return gather
+
+
+def weight_tet(w, e: float, fp32: bool = False):
+    """weight_tet (tetrahedron.f90:188) on the GPU: w(ntet, 4) corner
+    energies of each tetrahedron -> c(ntet, 4) corner weights at energy e.
+    fp32: the mixed pipeline's FP32 weights instead of the FP64 pipeline's."""
+    W = np.ascontiguousarray(w, dtype=float).reshape(-1, 4)
+    c = np.zeros_like(W)
+    _check(lib().ald_weight_tet(W.shape[0], _p(W), float(e), 1 if fp32 else 0, _p(c)))
+    return c
 
 
 def cg_quadratic(a, b, vmin, max_iter=100, n_dig_accur=2):

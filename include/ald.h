@@ -149,6 +149,16 @@ int ald_calculate_w3_ibz_split_sq(ald_ctx* ctx, const int ksubset[2], double* v3
  * ald_calculate_w3_ibz_split_sq for the same ksubset. */
 int ald_calculate_fgr(ald_ctx* ctx, const int ksubset[2], const double* v33s8, double* P1smpi, double* P2smpi);
 
+/* weight_tet (tetrahedron.f90:188-384, with SSORT tetrahedron.f90:716-738):
+ * the linear-tetrahedron weights of every tetrahedron at one energy e, on
+ * the device.  The module array tet(:) of the reference becomes two host
+ * arrays: w(4,ntet) = tet(i)%p(k)%w (corner energies, REAL(8); rounded to
+ * REAL as the reference does) and c(4,ntet) = tet(i)%p(k)%c (out).  fp32 = 0
+ * is the arithmetic of the FP64 pipeline, bit for bit the reference's;
+ * fp32 = 1 the FP32 weights of the mixed pipeline (a few FP32 ulps per
+ * weight).  Synchronous; needs no context. */
+int ald_weight_tet(int ntet, const double* w, double e, int fp32, double* c);
+
 /* distribution (sub.f90:1955): frequency(nkc,ndyn) cm^-1, dist(nkc,ndyn). */
 int ald_distribution(ald_ctx* ctx, double tempk, double* frequency, double* dist);
 
