@@ -15,6 +15,7 @@
 //   make_kp_reg_tet tetrahedron.f90:2-142.
 #include <algorithm>
 #include <array>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -22,6 +23,7 @@
 #include <fstream>
 #include <map>
 #include <numeric>
+#include <string_view>
 #include <thread>
 #include <unordered_map>
 
@@ -46,49 +48,55 @@ class Records {
   bool load(const std::string& path) {
     FILE* f = std::fopen(path.c_str(), "rb");
     if (!f) return false;
-    std::string buf;
     char chunk[1 << 16];
     size_t n;
-    while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) buf.append(chunk, n);
+    while ((n = std::fread(chunk, 1, sizeof chunk, f)) > 0) buf_.append(chunk, n);
     std::fclose(f);
     size_t b = 0;
-    while (b < buf.size()) {  // lines as getline gives them
-      size_t e = buf.find('\n', b);
-      if (e == std::string::npos) e = buf.size();
-      rec_.emplace_back(buf, b, e - b);
+    while (b < buf_.size()) {  // lines as getline gives them
+      size_t e = buf_.find('\n', b);
+      if (e == std::string::npos) e = buf_.size();
+      rec_.push_back({b, e - b});
       b = e + 1;
     }
     return true;
   }
-  bool next(size_t n, std::vector<std::string>& out) {
+  bool next(size_t n, std::vector<std::string_view>& out) {
     out.clear();
     while (out.size() < n) {
       if (at_ >= rec_.size()) return false;
-      split(rec_[at_++], out, n);
+      split(record(at_++), out, n);
     }
     return true;
   }
   bool line(std::string& s) {
     if (at_ >= rec_.size()) return false;
-    s = rec_[at_++];
+    s.assign(record(at_++));
     return true;
   }
-  size_t remaining_nonblank() const {
-    size_t c = 0;
+  // the records from the current one on that hold a value before any '/'
+  std::vector<size_t> nonblank_records() const {
+    std::vector<size_t> r;
     for (size_t i = at_; i < rec_.size(); ++i)
-      for (char ch : rec_[i]) {
+      for (char ch : record(i)) {
         if (ch == '/') break;
         if (!is_sep(ch)) {
-          ++c;
+          r.push_back(i);
           break;
         }
       }
-    return c;
+    return r;
+  }
+  // the values of record i alone (at most cap)
+  void values(size_t i, std::vector<std::string_view>& out, size_t cap) const {
+    out.clear();
+    split(record(i), out, cap);
   }
 
  private:
+  std::string_view record(size_t i) const { return std::string_view(buf_.data() + rec_[i].first, rec_[i].second); }
   static bool is_sep(char c) { return c == ' ' || c == '\t' || c == ',' || c == '\r'; }
-  static void split(const std::string& l, std::vector<std::string>& out, size_t cap) {
+  static void split(std::string_view l, std::vector<std::string_view>& out, size_t cap) {
     const char* p = l.data();
     const size_t n = l.size();
     size_t i = 0;
@@ -105,17 +113,31 @@ class Records {
       i = j;
     }
   }
-  std::vector<std::string> rec_;
+  std::string buf_;
+  std::vector<std::pair<size_t, size_t>> rec_;  // (offset, length) of each line in buf_
   size_t at_ = 0;
 };
 
-double dval(const std::string& s) {
-  std::string t(s);
-  for (char& c : t)
-    if (c == 'd' || c == 'D') c = 'e';
-  return std::strtod(t.c_str(), nullptr);
+// a value as strtod / strtol read it (Fortran's D exponent read as E)
+double dval(std::string_view s) {
+  char b[64];
+  if (s.size() >= sizeof b) {
+    std::string t(s);
+    for (char& c : t)
+      if (c == 'd' || c == 'D') c = 'e';
+    return std::strtod(t.c_str(), nullptr);
+  }
+  for (size_t i = 0; i < s.size(); ++i) b[i] = (s[i] == 'd' || s[i] == 'D') ? 'e' : s[i];
+  b[s.size()] = 0;
+  return std::strtod(b, nullptr);
 }
-int ival(const std::string& s) { return (int)std::strtol(s.c_str(), nullptr, 10); }
+int ival(std::string_view s) {
+  char b[64];
+  if (s.size() >= sizeof b) return (int)std::strtol(std::string(s).c_str(), nullptr, 10);
+  std::memcpy(b, s.data(), s.size());
+  b[s.size()] = 0;
+  return (int)std::strtol(b, nullptr, 10);
+}
 
 inline int cm(int i, int j) { return i + 3 * j; }  // 0-based column-major 3x3
 
@@ -261,7 +283,7 @@ std::string lattice_point_group(const double* prim_to_cart, std::vector<std::arr
 
 // ======================================================================
 std::string read_system(const std::string& dir, System& S) {
-  std::vector<std::string> t;
+  std::vector<std::string_view> t;
   {  // ------------------------------------------------- latdyn.params
     Records R;
     if (!R.load(dir + "/latdyn.params")) return "cannot open latdyn.params";
@@ -323,7 +345,7 @@ std::string read_system(const std::string& dir, System& S) {
       for (int i = 0; i < ntype; ++i) S.mas.push_back(dval(t[i]));
     ok = ok && R.next(ntype, t);
     if (ok)
-      for (int i = 0; i < ntype; ++i) S.atname.push_back(t[i]);
+      for (int i = 0; i < ntype; ++i) S.atname.emplace_back(t[i]);
     ok = ok && R.next(1, t);
     if (ok) S.nat0 = ival(t[0]);
     if (ok && (S.nat0 < 1 || S.nat0 > 4096)) return "structure.params: bad natoms0";
@@ -414,22 +436,47 @@ std::string read_system(const std::string& dir, System& S) {
     if (!R.load(fn)) return "READ_FC234: file " + std::string(rank == 2 ? "fc2.dat" : "fc3.dat") + " does not exist";
     std::string hdr;
     R.line(hdr);
-    size_t mx = R.remaining_nonblank();
+    const std::vector<size_t> lines = R.nonblank_records();
+    const size_t mx = lines.size();
     if ((int)mx != S.nterms[rank - 1])
       return "READ_FC" + std::to_string(rank) + ": number of lines read inconsistent with lat_fc.dat";
-    int nv = 2 + 2 * rank + 1;
+    const int nv = 2 + 2 * rank + 1;
     auto& idx = rank == 2 ? S.t2 : S.t3;
     auto& val = rank == 2 ? S.f2 : S.f3;
     idx.resize(mx * 2 * rank);
     val.resize(mx);
-    for (size_t j = 0; j < mx; ++j) {
-      if (!R.next(nv, t)) return "fc file truncated";
-      for (int c = 0; c < 2 * rank; ++c) idx[j * 2 * rank + c] = ival(t[2 + c]);
-      val[j] = dval(t[nv - 1]);
+    auto term = [&](size_t j, const std::vector<std::string_view>& v) {
+      for (int c = 0; c < 2 * rank; ++c) idx[j * 2 * rank + c] = ival(v[2 + c]);
+      val[j] = dval(v[nv - 1]);
       for (int c = 0; c < rank; ++c) {
         int at = idx[j * 2 * rank + 2 * c], xyz = idx[j * 2 * rank + 2 * c + 1];
-        if (at < 1 || at > S.natoms || xyz < 1 || xyz > 3) return "fc file: atom or xyz index out of range";
+        if (at < 1 || at > S.natoms || xyz < 1 || xyz > 3) return false;
       }
+      return true;
+    };
+    // Each READ of a term takes at least one record and there are as many
+    // nonblank records as terms, so in a file the reference accepts term j
+    // is nonblank record j: the records are parsed on the worker pool.  A
+    // record with fewer than nv values (a READ that would span records)
+    // sends the file through the sequential reader, which fails where the
+    // reference's READ does.
+    std::atomic<bool> short_rec{false}, bad_index{false};
+    const int nthr = (int)std::min<size_t>(pool_width(), mx / 256 + 1);
+    run_parallel(nthr, [&](int w) {
+      std::vector<std::string_view> v;
+      for (size_t j = w; j < mx && !short_rec.load(std::memory_order_relaxed); j += nthr) {
+        R.values(lines[j], v, nv);
+        if ((int)v.size() < nv) short_rec = true;
+        else if (!term(j, v)) bad_index = true;
+      }
+    });
+    if (short_rec) {
+      for (size_t j = 0; j < mx; ++j) {
+        if (!R.next(nv, t)) return "fc file truncated";
+        if (!term(j, t)) return "fc file: atom or xyz index out of range";
+      }
+    } else if (bad_index) {
+      return "fc file: atom or xyz index out of range";
     }
   }
   {  // ------------------------------------------------ dielectric.params
@@ -679,7 +726,8 @@ std::string build_tables(const System& S, Tables& T) {
   // for the mesh index (reordered sums: the 1e-6 duplicate tolerance and the
   // 1e-3 mesh tolerance are far above their rounding).  out[c] is the mesh
   // index of the c-th distinct arm, -2 where it is off the mesh or outside
-  // its cell; the list ends at -1.
+  // its cell; the list ends at -1, or at the first arm on a mesh point
+  // before n (the point's own index).
   std::vector<std::array<double, 9>> opv2(npg), opf(npg);
   for (int o = 0; o < npg; ++o)
     for (int a = 0; a < 3; ++a)
@@ -692,7 +740,7 @@ std::string build_tables(const System& S, Tables& T) {
         opv2[o][3 * a + b2] = sv;
         opf[o][3 * a + b2] = sf;
       }
-  auto mesh_star_cands = [&](const double* kc, int* out) {
+  auto mesh_star_cands = [&](const double* kc, int n, int* out) {
     constexpr int kBuckets = 1 << 16, kSlots = 128;
     double key[48][3];
     int head[kSlots], nxt[48], kb[48], nkey = 0;
@@ -731,6 +779,9 @@ std::string build_tables(const System& S, Tables& T) {
       bool in_cell;
       const int idx = locate(f, in_cell);
       out[nkey++] = idx >= 0 && in_cell ? idx : -2;
+      // the pass below takes the first arm on an earlier mesh point (every
+      // earlier point is assigned by then): nothing after it is read
+      if (idx >= 0 && in_cell && idx < n) return;
     }
   };
   // task 0 builds the tetrahedra (they depend on the mesh only); tasks 1..
@@ -744,7 +795,7 @@ std::string build_tables(const System& S, Tables& T) {
         return;
       }
       const int t = task - 1;
-      for (int n = t; n < T.nkc; n += nthr) mesh_star_cands(&T.kpc32[3 * (size_t)n], &cand[(size_t)n * npg]);
+      for (int n = t; n < T.nkc; n += nthr) mesh_star_cands(&T.kpc32[3 * (size_t)n], n, &cand[(size_t)n * npg]);
     });
   }
   if (!tet_err.empty()) return tet_err;
