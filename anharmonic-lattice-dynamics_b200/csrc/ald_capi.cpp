@@ -145,14 +145,50 @@ int fail(int code, const std::string& msg) {
 
 double g_h2d = 0;  // bytes uploaded by the create call in progress
 
-template <class T>
-cudaError_t upload(DevBuf<T>& d, const std::vector<T>& h, cudaStream_t s) {
-  cudaError_t e = d.alloc(std::max<size_t>(h.size(), 1));
-  if (e != cudaSuccess) return e;
-  if (h.empty()) return cudaSuccess;
-  g_h2d += (double)h.size() * sizeof(T);
-  return cudaMemcpyAsync(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, s);
-}
+// The context's tables go to the device as one block: staged back to back
+// (256-byte aligned) in one host buffer, copied with one H2D copy into one
+// device allocation (a size the device-memory cache keeps, so a context of
+// the same shape reuses it), each table's DevBuf a view into the block.  One
+// allocation and one copy instead of one of each per table: about forty
+// small cudaMalloc calls and pageable copies per context otherwise.
+class TableStager {
+ public:
+  template <class T>
+  void add(DevBuf<T>& d, const std::vector<T>& h) {
+    const size_t n = std::max<size_t>(h.size(), 1);
+    off_ = (off_ + 255) / 256 * 256;
+    host_.resize(off_ + n * sizeof(T), 0);
+    if (!h.empty()) std::memcpy(host_.data() + off_, h.data(), h.size() * sizeof(T));
+    views_.push_back({&d, off_, n, [](void* dv, char* q, size_t cnt) {
+                        static_cast<DevBuf<T>*>(dv)->view_of(reinterpret_cast<T*>(q), cnt);
+                      }});
+    off_ += n * sizeof(T);
+    bytes_ += (double)h.size() * sizeof(T);
+  }
+  // the block (whole MiB, at least one), the copy, then the views
+  cudaError_t commit(DevBuf<char>& block, cudaStream_t s) {
+    const size_t mib = (size_t)1 << 20;
+    const size_t total = std::max(mib, (off_ + mib - 1) / mib * mib);
+    cudaError_t e = block.alloc(total);
+    if (e != cudaSuccess) return e;
+    if (off_) e = cudaMemcpyAsync(block.p, host_.data(), off_, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return e;
+    for (auto& v : views_) v.bind(v.buf, block.p + v.off, v.n);
+    g_h2d += bytes_;
+    return cudaSuccess;
+  }
+
+ private:
+  struct View {
+    void* buf;
+    size_t off, n;
+    void (*bind)(void*, char*, size_t);
+  };
+  std::vector<char> host_;
+  std::vector<View> views_;
+  size_t off_ = 0;
+  double bytes_ = 0;
+};
 
 double temp_cm(double tempk) {
   return tempk * PhysConst::k_b / (100 * PhysConst::h_plank * PhysConst::c_light);
@@ -587,19 +623,20 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
   cudaStream_t s = c->stream;
   g_h2d = 0;
   // tables
-  CKA(upload(c->kpc32, c->T.kpc32, s));
+  TableStager st;
+  st.add(c->kpc32, c->T.kpc32);
   std::vector<double> rr(3 * (size_t)c->S.natoms);
   for (int j = 0; j < c->S.natoms; ++j) {
     int j0 = c->S.cell0[j] - 1;
     for (int x = 0; x < 3; ++x) rr[3 * j + x] = c->S.atompos[3 * j + x] - c->S.atompos[3 * j0 + x];
   }
-  CKA(upload(c->rr, rr, s));
-  CKA(upload(c->fc2_off, c->F2.off, s));
-  CKA(upload(c->fc2_atom, c->F2.atom, s));
-  CKA(upload(c->fc2_val, c->F2.val, s));
-  CKA(upload(c->fc2_sqm, c->F2.sqm, s));
-  CKA(upload(c->fc2_uatom, c->F2.uatom, s));
-  CKA(upload(c->fc2_uidx, c->F2.uidx, s));
+  st.add(c->rr, rr);
+  st.add(c->fc2_off, c->F2.off);
+  st.add(c->fc2_atom, c->F2.atom);
+  st.add(c->fc2_val, c->F2.val);
+  st.add(c->fc2_sqm, c->F2.sqm);
+  st.add(c->fc2_uatom, c->F2.uatom);
+  st.add(c->fc2_uidx, c->F2.uidx);
   {
     // epsil(9), charge(9*nat0), masses(nat0), eps_scale, rho2, om0
     std::vector<double> bo(9 + 10 * c->S.nat0 + 4, 0.0);
@@ -613,19 +650,19 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
     sc[0] = 8.8541878176e-12 / 1e10 / PhysConst::ee;
     sc[1] = rho * rho;
     sc[2] = c->S.volume_r;
-    CKA(upload(c->born, bo, s));
+    st.add(c->born, bo);
   }
   if (c->S.include_fc[2] == 1) {
-    CKA(upload(c->blk_off, c->F3.blk_off, s));
-    CKA(upload(c->trip_j, c->F3.trip_j, s));
-    CKA(upload(c->trip_k, c->F3.trip_k, s));
-    CKA(upload(c->fc3w, c->F3.w, s));
-    CKA(upload(c->cls_grp_off, c->VC.grp_off, s));
-    CKA(upload(c->cls_pc, c->VC.pc, s));
-    CKA(upload(c->cls_trip_off, c->VC.trip_off, s));
-    CKA(upload(c->cls_trip, c->VC.trip, s));
-    CKA(upload(c->cls_trip_i0, c->VC.trip_i0, s));
-    CKA(upload(c->cls_trip_k, c->VC.trip_k, s));
+    st.add(c->blk_off, c->F3.blk_off);
+    st.add(c->trip_j, c->F3.trip_j);
+    st.add(c->trip_k, c->F3.trip_k);
+    st.add(c->fc3w, c->F3.w);
+    st.add(c->cls_grp_off, c->VC.grp_off);
+    st.add(c->cls_pc, c->VC.pc);
+    st.add(c->cls_trip_off, c->VC.trip_off);
+    st.add(c->cls_trip, c->VC.trip);
+    st.add(c->cls_trip_i0, c->VC.trip_i0);
+    st.add(c->cls_trip_k, c->VC.trip_k);
   }
   {
     std::vector<double> rt(2 * (size_t)c->T.L);
@@ -642,22 +679,22 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
         rt[2 * t + 1] = k == 1 ? 1.0 : (k == 3 ? -1.0 : 0.0);
       }
     }
-    CKA(upload(c->roots, rt, s));
+    st.add(c->roots, rt);
   }
-  CKA(upload(c->phase_coef, c->T.phase_coef, s));
+  st.add(c->phase_coef, c->T.phase_coef);
   std::vector<int> mi(c->T.nibz);
   for (int i = 0; i < c->T.nibz; ++i) mi[i] = c->T.mapinv[i] - 1;
-  CKA(upload(c->mapinv, mi, s));
-  CKA(upload(c->neg_src, c->T.neg_src, s));
-  CKA(upload(c->neg_dst, c->T.neg_dst, s));
-  CKA(upload(c->arm_off, c->T.arm_off, s));
-  CKA(upload(c->arm_q, c->T.arm_q, s));
-  CKA(upload(c->arm_op, c->T.arm_op, s));
-  CKA(upload(c->star_off, c->T.star_off, s));
-  CKA(upload(c->star_q, c->T.star_q, s));
-  CKA(upload(c->star_op, c->T.star_op, s));
-  CKA(upload(c->tet_corner, c->T.tet_corner, s));
-  CKA(upload(c->tet_inc, c->T.tet_inc, s));
+  st.add(c->mapinv, mi);
+  st.add(c->neg_src, c->T.neg_src);
+  st.add(c->neg_dst, c->T.neg_dst);
+  st.add(c->arm_off, c->T.arm_off);
+  st.add(c->arm_q, c->T.arm_q);
+  st.add(c->arm_op, c->T.arm_op);
+  st.add(c->star_off, c->T.star_off);
+  st.add(c->star_q, c->T.star_q);
+  st.add(c->star_op, c->T.star_op);
+  st.add(c->tet_corner, c->T.tet_corner);
+  st.add(c->tet_inc, c->T.tet_inc);
   {
     // update_mpi's rotation of F to every mesh point: the op of the point's
     // arm in kstarsinfbz1 of its IBZ point (every mesh point is such an arm
@@ -669,8 +706,8 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
         if (fop[c->T.arm_q[a]] < 0 && m0[c->T.arm_q[a]] == i) fop[c->T.arm_q[a]] = c->T.arm_op[a];
     c->full_op_ok = std::all_of(fop.begin(), fop.end(), [](int v) { return v >= 0; });
     for (int& v : fop) v = std::max(v, 0);
-    CKA(upload(c->mapibz0, m0, s));
-    CKA(upload(c->full_op, fop, s));
+    st.add(c->mapibz0, m0);
+    st.add(c->full_op, fop);
     // mesh integers of every point, 4 ints each (the collision kernel's arm lookups)
     std::vector<int> mm(4 * (size_t)c->T.nkc, 0);
     const int N1 = c->S.nc[1], N2 = c->S.nc[2];
@@ -679,11 +716,11 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
       mm[4 * (size_t)q + 1] = (q / N2) % N1;
       mm[4 * (size_t)q + 2] = q % N2;
     }
-    CKA(upload(c->mesh_m, mm, s));
+    st.add(c->mesh_m, mm);
     std::vector<int> own(c->T.arm_q.size());
     for (int i = 0; i < c->T.nibz; ++i)
       for (int a = c->T.arm_off[i]; a < c->T.arm_off[i + 1]; ++a) own[a] = i;
-    CKA(upload(c->arm_owner, own, s));
+    st.add(c->arm_owner, own);
   }
   {
     std::vector<double> op(48 * 9, 0.0), opi(48 * 9, 0.0);
@@ -705,11 +742,11 @@ int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out) 
       r[2 + 3 * 1] = (M(0, 1) * M(2, 0) - M(0, 0) * M(2, 1)) / det;
       r[2 + 3 * 2] = (M(0, 0) * M(1, 1) - M(0, 1) * M(1, 0)) / det;
     }
-    CKA(upload(c->opk, op, s));
-    CKA(upload(c->opk_inv, opi, s));
+    st.add(c->opk, op);
+    st.add(c->opk_inv, opi);
   }
-  CKA(c->err.alloc(4));
-  CK(cudaMemsetAsync(c->err.p, 0, 4 * sizeof(int), s));
+  st.add(c->err, std::vector<int>(4, 0));  // the kernels' error flags, cleared
+  CKA(st.commit(c->tables, s));
   CK(cudaStreamSynchronize(s));
   c->h2d_bytes = g_h2d;
   *out = c.release();

@@ -19,7 +19,8 @@ struct ald_ctx {
   cudaStream_t own_stream = nullptr;  // the context's own stream
   double h2d_bytes = 0;
   Geometry geo;
-  // device tables
+  // device tables: views into one block (`tables`), uploaded with one copy
+  DevBuf<char> tables;
   DevBuf<double> kpc32, rr, fc2_val, fc2_sqm, born, fc3w, roots, opk, opk_inv;
   DevBuf<int> fc2_uatom, fc2_uidx;
   DevBuf<int> fc2_off, fc2_atom, blk_off, trip_j, trip_k, phase_coef, mapinv, neg_src, neg_dst, arm_off, arm_q,

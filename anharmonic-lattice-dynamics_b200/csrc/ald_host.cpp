@@ -678,37 +678,59 @@ std::string build_tables(const System& S, Tables& T) {
   auto reduced = [&](const double* kc, double* f) {
     for (int a = 0; a < 3; ++a) f[a] = Ginv[cm(a, 0)] * kc[0] + Ginv[cm(a, 1)] * kc[1] + Ginv[cm(a, 2)] * kc[2];
   };
-  // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table.  They
-  // depend on the mesh only, so one worker builds them while the others find
-  // the stars of the mesh points.
-  auto build_tet = [&]() -> std::string {
-    static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
-                                        {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
-    static const int off8[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
-                                    {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
-    T.tet_corner.assign(24 * (size_t)T.nkc, 0);
-    // incidences (tetrahedron corner (6n+l)*4+k at point p) are generated in
-    // increasing order, so each point's list of 24 comes out sorted
-    T.tet_inc.assign(24 * (size_t)T.nkc, 0);
-    std::vector<int> ninc(T.nkc, 0);
-    for (int n = 0; n < T.nkc; ++n) {
-      int m[3] = {n / (N1 * N2), (n / N2) % N1, n % N2};
-      int pt[8];
-      for (int c = 0; c < 8; ++c)
-        pt[c] = mesh_index(wrap(m[0] + off8[c][0], N0), wrap(m[1] + off8[c][1], N1), wrap(m[2] + off8[c][2], N2));
-      for (int l = 0; l < 6; ++l)
-        for (int k = 0; k < 4; ++k) {
-          int p = pt[corner_of[l][k]];
-          T.tet_corner[4 * (6 * (size_t)n + l) + k] = p;
-          if (ninc[p] >= 24) return std::string("tetrahedron incidence count");
-          T.tet_inc[24 * (size_t)p + ninc[p]++] = (6 * n + l) * 4 + k;
-        }
+  // ---- tetrahedra (make_kp_reg_tet): six per mesh cell, corner table, and
+  // per mesh point its 24 incidences (tetrahedron corner (6n+l)*4+k at the
+  // point) in increasing order.  Both depend on the mesh only: two workers
+  // build them (tet_corner, tet_inc) while the others find the stars of the
+  // mesh points.  A point is corner c of cell point - offset(c) for each of
+  // the 8 corner numbers c (offset bits x, y, z = c & 1, c & 2, c & 4).
+  static const int corner_of[6][4] = {{0, 1, 2, 5}, {1, 2, 3, 5}, {0, 2, 4, 5},
+                                      {2, 3, 5, 7}, {2, 4, 5, 6}, {2, 5, 6, 7}};
+  // corner slots 4l + k of the six tetrahedra at each corner number, ascending
+  int slots[8][6], nslot[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  for (int l = 0; l < 6; ++l)
+    for (int k = 0; k < 4; ++k) {
+      const int c = corner_of[l][k];
+      slots[c][nslot[c]++] = 4 * l + k;
     }
-    for (int p = 0; p < T.nkc; ++p)
-      if (ninc[p] != 24) return std::string("tetrahedron incidence count");
-    return std::string();
+  auto up = [](int v, int n) { return v + 1 == n ? 0 : v + 1; };
+  auto down = [](int v, int n) { return v == 0 ? n - 1 : v - 1; };
+  auto build_tet_corner = [&]() {
+    T.tet_corner.assign(24 * (size_t)T.nkc, 0);
+    for (int n = 0; n < T.nkc; ++n) {
+      const int m0 = n / (N1 * N2), m1 = (n / N2) % N1, m2 = n % N2;
+      const int a[2] = {m0, up(m0, N0)}, b[2] = {m1, up(m1, N1)}, c2[2] = {m2, up(m2, N2)};
+      int pt[8];
+      for (int c = 0; c < 8; ++c) pt[c] = mesh_index(a[c & 1], b[(c >> 1) & 1], c2[c >> 2]);
+      for (int l = 0; l < 6; ++l)
+        for (int k = 0; k < 4; ++k) T.tet_corner[4 * (6 * (size_t)n + l) + k] = pt[corner_of[l][k]];
+    }
   };
-  std::string tet_err;
+  // incidence (6n + l) * 4 + k = 24 n + slot: the runs of the 8 cells,
+  // each ascending, concatenated in increasing cell order
+  auto build_tet_inc = [&]() {
+    T.tet_inc.assign(24 * (size_t)T.nkc, 0);
+    for (int p = 0; p < T.nkc; ++p) {
+      const int m0 = p / (N1 * N2), m1 = (p / N2) % N1, m2 = p % N2;
+      const int a[2] = {m0, down(m0, N0)}, b[2] = {m1, down(m1, N1)}, c2[2] = {m2, down(m2, N2)};
+      int cell[8], ord[8];
+      for (int c = 0; c < 8; ++c) {
+        cell[c] = mesh_index(a[c & 1], b[(c >> 1) & 1], c2[c >> 2]);
+        ord[c] = c;
+      }
+      for (int i = 1; i < 8; ++i)
+        for (int j = i; j > 0 && cell[ord[j - 1]] > cell[ord[j]]; --j) std::swap(ord[j - 1], ord[j]);
+      int* v = &T.tet_inc[24 * (size_t)p];
+      int nv = 0;
+      bool dup = false;
+      for (int i = 0; i < 8; ++i) {
+        const int c = ord[i];
+        dup |= i > 0 && cell[ord[i - 1]] == cell[c];
+        for (int s2 = 0; s2 < nslot[c]; ++s2) v[nv++] = 24 * cell[c] + slots[c][s2];
+      }
+      if (dup) std::sort(v, v + nv);  // an edge of 1 or 2 points: one cell at several corners
+    }
+  };
   // ---- IBZ (get_weights): first mesh point of each exact (unfolded) orbit
   T.mapibz.assign(T.nkc, 0);
   T.mapinv.clear();
@@ -784,21 +806,18 @@ std::string build_tables(const System& S, Tables& T) {
       if (idx >= 0 && in_cell && idx < n) return;
     }
   };
-  // task 0 builds the tetrahedra (they depend on the mesh only); tasks 1..
-  // take stripes of mesh points, on the library's worker pool
+  // on the library's worker pool: task 0 and 1 build the tetrahedron tables,
+  // tasks 2.. take stripes of mesh points
   std::vector<int> cand((size_t)T.nkc * npg, -1);
   {
     const int nthr = pool_width();
-    run_parallel(nthr + 1, [&](int task) {
-      if (task == 0) {
-        tet_err = build_tet();
-        return;
-      }
-      const int t = task - 1;
+    run_parallel(nthr + 2, [&](int task) {
+      if (task == 0) return build_tet_corner();
+      if (task == 1) return build_tet_inc();
+      const int t = task - 2;
       for (int n = t; n < T.nkc; n += nthr) mesh_star_cands(&T.kpc32[3 * (size_t)n], n, &cand[(size_t)n * npg]);
     });
   }
-  if (!tet_err.empty()) return tet_err;
   for (int n = 0; n < T.nkc; ++n) {
     int found = -1;
     for (int c = 0; c < npg; ++c) {

@@ -166,17 +166,26 @@ template <class T>
 struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
+  bool view = false;  // p points into a block another DevBuf owns
   cudaError_t alloc(size_t count) {
-    if (count == n && p) return cudaSuccess;
+    if (count == n && p && !view) return cudaSuccess;
     free();
     n = count;
     if (count == 0) return cudaSuccess;
     return dev_alloc((void**)&p, count * sizeof(T));
   }
+  // count elements at q, owned elsewhere (never freed through this DevBuf)
+  void view_of(T* q, size_t count) {
+    free();
+    p = q;
+    n = count;
+    view = true;
+  }
   void free() {
-    if (p) dev_free(p, n * sizeof(T));
+    if (p && !view) dev_free(p, n * sizeof(T));
     p = nullptr;
     n = 0;
+    view = false;
   }
   ~DevBuf() { free(); }
 };
