@@ -90,3 +90,72 @@ def test_create_without_device_fails_cleanly(ald_lib, workdir):
     with pytest.raises(ald_lib.AldError) as e:
         ald_lib.Context(d)
     assert e.value.code == 7
+
+
+@pytest.mark.parametrize("cfg,mesh,kw", [(3, (6, 12, 12), {"p": 2}), (3, (3, 12, 12), {"p": 5}),
+                                         (4, (4, 4, 4), {}), (1, (5, 5, 5), {})])
+def test_host_tables_equal_oracle_large_cells(ald_lib, oracle_lib, workdir, cfg, mesh, kw):
+    """The superlattices (point group of 16 ops, an odd mesh edge) and the
+    192-band cell (an FC3 file of the size the worker pool parses in
+    parallel): mesh, IBZ and weights against the oracle."""
+    d = make_case(workdir, cfg, mesh, **kw)
+    info, M = ald_lib.read_mesh(d)
+    O = oracle_lib.Oracle(d)
+    O.mesh()
+    R = O.ibz()
+    assert info.nibz == O.nibz and info.lattpgcount == O.npg
+    assert np.array_equal(M["kpc"], O.kpc())
+    assert np.array_equal(M["mapinv"], R["mapinv"])
+    assert np.array_equal(M["mapibz"], R["mapibz"])
+    assert np.allclose(M["wibz"], R["wibz"], rtol=0, atol=1e-15)
+
+
+def _fc3_variant(workdir, tag, edit):
+    d = make_case(workdir, 1, (4, 4, 4))
+    bad = os.path.join(str(workdir), tag)
+    shutil.copytree(d, bad, dirs_exist_ok=True)
+    p = os.path.join(bad, "fc3.dat")
+    lines = open(p).read().splitlines()
+    open(p, "w").write("\n".join(edit(lines)) + "\n")
+    return bad
+
+
+def test_fc3_blank_records_are_skipped(ald_lib, workdir):
+    """Blank records between terms: a list-directed READ passes over them,
+    so the file reads as without them (the same mesh and IBZ)."""
+    d = make_case(workdir, 1, (4, 4, 4))
+    spaced = _fc3_variant(workdir, "fc3_blank", lambda L: L[:1] + [x for l in L[1:] for x in (l, "   ")])
+    a, Ma = ald_lib.read_mesh(d)
+    b, Mb = ald_lib.read_mesh(spaced)
+    assert (a.nterms3, a.nibz) == (b.nterms3, b.nibz)
+    assert np.array_equal(Ma["mapibz"], Mb["mapibz"])
+
+
+def test_fc3_short_record_is_truncated(ald_lib, workdir):
+    """A term record with a value missing: the READ takes the next record's
+    values, and the file ends before the last term (the sequential reader's
+    error, whichever worker met the short record)."""
+    def drop_value(L):
+        j = len(L) // 2
+        L = list(L)
+        L[j] = " ".join(L[j].split()[:-1])
+        return L
+    bad = _fc3_variant(workdir, "fc3_short", drop_value)
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.read_mesh(bad)
+    assert e.value.code == 2
+    assert "truncated" in str(e.value)
+
+
+def test_fc3_index_out_of_range(ald_lib, workdir):
+    def bad_xyz(L):
+        L = list(L)
+        t = L[-1].split()
+        t[3] = "4"  # the first xyz index of the last term
+        L[-1] = " ".join(t)
+        return L
+    bad = _fc3_variant(workdir, "fc3_xyz", bad_xyz)
+    with pytest.raises(ald_lib.AldError) as e:
+        ald_lib.read_mesh(bad)
+    assert e.value.code == 2
+    assert "out of range" in str(e.value)
