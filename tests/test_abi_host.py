@@ -159,3 +159,30 @@ def test_fc3_index_out_of_range(ald_lib, workdir):
         ald_lib.read_mesh(bad)
     assert e.value.code == 2
     assert "out of range" in str(e.value)
+
+
+def test_host_tables_from_concurrent_threads(ald_lib, workdir):
+    """Several host threads reading input directories at once (as contexts
+    created on different threads do): every thread shares the library's one
+    worker pool, and each gets the tables a lone call gives."""
+    import threading
+    dirs = [make_case(workdir, 1, (6, 6, 6)), make_case(workdir, 0, (10, 10, 10)),
+            make_case(workdir, 3, (6, 12, 12), p=2), make_case(workdir, 1, (16, 16, 16))]
+    want = [ald_lib.read_mesh(d)[1] for d in dirs]
+    got, errs = {}, []
+
+    def work(i, d):
+        try:
+            for _ in range(3):
+                got[(i, _)] = ald_lib.read_mesh(d)[1]
+        except Exception as e:  # reported below
+            errs.append(e)
+    th = [threading.Thread(target=work, args=(i, d)) for i, d in enumerate(dirs * 2)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errs, errs
+    for (i, _), M in got.items():
+        for k in ("mapibz", "mapinv", "kpc", "wibz"):
+            assert np.array_equal(M[k], want[i % len(dirs)][k])
