@@ -27,7 +27,11 @@ using namespace ald;
 namespace ald {
 
 namespace {
-constexpr size_t kCacheMin = (size_t)1 << 20, kCacheMax = (size_t)32 << 30;
+// every freed block is kept, whatever its size: a fresh context's first
+// pipeline call allocates its small workspaces (Q, the CG vectors, kappa
+// partials) next to the large ones, and a driver allocation there lands
+// between kernel launches
+constexpr size_t kCacheMin = 1, kCacheMax = (size_t)32 << 30;
 struct DevCache {
   std::mutex m;
   std::map<std::pair<int, size_t>, std::vector<void*>> blocks;  // (device, bytes) -> free blocks

@@ -140,7 +140,7 @@ struct Fc2Csr {
 std::string build_fc2(const System& S, Fc2Csr& F);
 
 // ------------------------------------------------------------ device side
-// Device memory of the library.  Blocks of 1 MiB or more that are freed are
+// Device memory of the library.  Blocks that are freed (of any size) are
 // kept per device (after a device synchronisation, so no queued work still
 // uses them) and handed out again to an allocation of the same byte size:
 // contexts created one after another reuse their workspaces without

@@ -105,7 +105,7 @@ const char* ald_last_error(void);
  * (make_kp_reg_tet tetrahedron.f90:2), and uploads the tables. */
 int ald_create_from_dir(const char* dir, const ald_options* opt, ald_ctx** out);
 void ald_destroy(ald_ctx* ctx);
-/* Device blocks of 1 MiB or more freed by the library (ald_destroy, workspace
+/* Device blocks of any size freed by the library (ald_destroy, workspace
  * resizes) stay reserved in a per-device cache, up to 32 GiB per device, and
  * are reused by later allocations of the same size: a context created after
  * another one skips cudaMalloc.  The cache gives its blocks back when
