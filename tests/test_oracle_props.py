@@ -120,3 +120,97 @@ def test_get_k_info_has_no_state_across_oracles(oracle_lib, workdir):
         idx = [O.get_k_info(kpc[:, n])[0] for n in range(kpc.shape[1])]
         assert idx == list(range(1, kpc.shape[1] + 1))
         del O
+
+
+def _v3_case(oracle_lib, workdir, cfg, mesh, **kw):
+    d = make_case(workdir, cfg, mesh, **kw)
+    O = oracle_lib.Oracle(d)
+    O.mesh()
+    R = O.ibz()
+    O.phonons()
+    ev, _, _ = O.get_phonons()
+    v = O.v3(1, O.nibz)
+    kpc = O.kpc()
+    gam = {q for q in range(O.nkc) if np.abs(kpc[:, q]).max() < 1e-9}
+    q3 = np.array([[O.get_k_info(-kpc[:, R["mapinv"][n1] - 1] - kpc[:, q2])[0] - 1 for q2 in range(O.nkc)]
+                   for n1 in range(O.nibz)])
+    return O, R, ev, v, kpc, gam, q3
+
+
+def _gamma_acoustic(b, gam, qs):
+    """Mask (l1, l2, l3) of the entries with an acoustic mode at Gamma: 0/0
+    in exact arithmetic (the reference zeroes them downstream)."""
+    m = np.ones((b, b, b), bool)
+    for ax, q in enumerate(qs):
+        if q in gam:
+            idx = [slice(None)] * 3
+            idx[ax] = slice(0, 3)
+            m[tuple(idx)] = False
+    return m
+
+
+@pytest.mark.parametrize("cfg,mesh", [(1, (4, 4, 4)), (0, (5, 5, 5))])
+def test_v3_symmetric_in_q2_q3(oracle_lib, workdir, cfg, mesh):
+    """matrix_elt_simplified (sub.f90:5888-6011) with FC3 symmetric in its
+    atom/direction pairs gives V3(q1l1, q2l2, q3l3) = V3(q1l1, q3l3, q2l2):
+    the oracle's |V3|^2 at (q2, l2, l3) equals that at (q3, l3, l2)."""
+    O, R, ev, v, kpc, gam, q3 = _v3_case(oracle_lib, workdir, cfg, mesh)
+    b, scale = O.ndyn, np.abs(v).max()
+    for n1 in range(O.nibz):
+        q1 = R["mapinv"][n1] - 1
+        for q2 in range(O.nkc):
+            a, c = v[n1, q2], v[n1, q3[n1, q2]].transpose(0, 2, 1)
+            m = _gamma_acoustic(b, gam, (q1, q2, q3[n1, q2]))
+            assert np.all(np.abs(a - c)[m] <= 1e-9 * np.abs(a)[m] + 1e-12 * scale), (n1, q2)
+
+
+@pytest.mark.parametrize("cfg", [1, 0])
+def test_v3_invariant_under_the_little_group_of_q1(oracle_lib, workdir, cfg):
+    """|V3|^2 summed over degenerate groups of modes is a scalar of the
+    lattice point group: for every op S with S q1 = q1 (mod G), the group
+    sums at (q2, q3) and at (S q2, S q3) agree.  On a 4^3 mesh the reference's
+    default-REAL mesh fractions m/4 are exact, so the mesh is exactly
+    symmetric and the sums agree to rounding (on meshes such as 6^3 the
+    fractions m/6 carry FP32 noise and the sums agree to about 1e-5 only)."""
+    O, R, ev, v, kpc, gam, q3 = _v3_case(oracle_lib, workdir, cfg, (4, 4, 4))
+    b, scale = O.ndyn, np.abs(v).max()
+    tol = 1e-8 * np.abs(ev).max()
+
+    def group_matrix(q):
+        w, g, cur = ev[:, q], [], [0]
+        for l in range(1, b):
+            if abs(w[l] - w[cur[-1]]) <= tol:
+                cur.append(l)
+            else:
+                g.append(cur)
+                cur = [l]
+        g.append(cur)
+        P = np.zeros((len(g), b))
+        for i, gg in enumerate(g):
+            P[i, gg] = 1.0
+        return P, np.array([(q in gam) and gg[0] < 3 for gg in g])
+
+    GM = [group_matrix(q) for q in range(O.nkc)]
+    ops = O.op_kmatrix()
+    checked = 0
+    for n1 in range(O.nibz):
+        q1 = R["mapinv"][n1] - 1
+        for S in ops:
+            if O.get_k_info(S @ kpc[:, q1])[0] - 1 != q1:
+                continue
+            for q2 in range(O.nkc):
+                s2 = O.get_k_info(S @ kpc[:, q2])[0] - 1
+                sums = []
+                for qa, qb in ((q2, q3[n1, q2]), (s2, q3[n1, s2])):
+                    (P1, a1), (P2, a2), (P3, a3) = GM[q1], GM[qa], GM[qb]
+                    t = np.einsum("ai,bj,ck,ijk->abc", P1, P2, P3, v[n1, qa])
+                    t[a1] = np.nan
+                    t[:, a2] = np.nan
+                    t[:, :, a3] = np.nan
+                    sums.append(t)
+                a, c = sums
+                m = ~np.isnan(a)
+                assert np.array_equal(m, ~np.isnan(c))
+                assert np.all(np.abs(a - c)[m] <= 1e-9 * np.abs(a)[m] + 1e-12 * scale), (n1, q2, s2)
+                checked += 1
+    assert checked > O.nkc * O.nibz  # every row has ops beyond the identity
