@@ -214,3 +214,24 @@ def test_v3_invariant_under_the_little_group_of_q1(oracle_lib, workdir, cfg):
                 assert np.all(np.abs(a - c)[m] <= 1e-9 * np.abs(a)[m] + 1e-12 * scale), (n1, q2, s2)
                 checked += 1
     assert checked > O.nkc * O.nibz  # every row has ops beyond the identity
+
+
+@pytest.mark.parametrize("cfg", [1, 0])
+def test_rta_kappa_diagonal_is_isotropic(oracle_lib, workdir, cfg):
+    """Cubic crystals: mode_kappa (sub.f90:1292-1401) sums every IBZ mode over
+    its star arms with op_kmatrix, so the three diagonal entries of the RTA
+    kappa tensor (summed over bands) agree to rounding.  With the Gaussian
+    delta (argon) the off-diagonal entries vanish to rounding too; with the
+    tetrahedron delta (rock-salt) they are about 2e-3 of the diagonal, since
+    make_kp_reg_tet cuts every mesh cell into six tetrahedra around one cell
+    diagonal, which breaks the cubic symmetry of Q.  (The CG kappa is not
+    isotropic either way: the reference's stop rule, (num/den)^2 |p|^2/|x|^2
+    < 1e-4, leaves the solution about 1 % from converged.)"""
+    d = make_case(workdir, cfg, (4, 4, 4))
+    r = oracle_lib.run_job1(d)
+    K = r["kappa_rta"].sum(0)
+    diag = np.diag(K)
+    assert np.all(diag > 0)
+    assert (diag.max() - diag.min()) <= 1e-12 * diag.mean()
+    if cfg == 0:
+        assert np.abs(K - np.diag(diag)).max() <= 1e-12 * diag.mean()
