@@ -70,3 +70,54 @@ def test_torch_allgather_gloo_two_ranks():
     assert all(p.exitcode == 0 for p in procs), [p.exitcode for p in procs]
     res = [q.get(timeout=5) for _ in range(4)]
     assert all(ok for _, ok in res), res
+
+
+def _failing_worker(rank, world, port, out):
+    """Rank 1 fails before the exchange (a shard lost between steps); rank 0
+    must get an error from its all-gather within the process group's
+    timeout instead of waiting for good."""
+    import datetime
+    import time
+    import torch.distributed as dist
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=10))
+    counts = [4, 4]
+    if rank == 1:
+        dist.barrier()  # both ranks are up
+        out.put((rank, "left"))
+        out.close()
+        out.join_thread()  # the message is out before the process ends
+        os._exit(3)  # no destroy_process_group: the peer sees the rank vanish
+    dist.barrier()
+    t0 = time.time()
+    try:
+        ald.torch_allgather()(np.ones(4), counts)
+        out.put((rank, "no error"))
+    except Exception as e:  # the expected path
+        out.put((rank, "error after %.1f s: %s" % (time.time() - t0, type(e).__name__)))
+    out.close()
+    out.join_thread()
+    os._exit(0)
+
+
+def test_torch_allgather_reports_a_lost_rank():
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_failing_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    for p in procs:
+        p.join(timeout=90)
+    alive = [p for p in procs if p.is_alive()]
+    for p in alive:
+        p.kill()
+    assert not alive, "a rank hung on the lost peer"
+    res = dict(q.get(timeout=5) for _ in range(2))
+    assert res[1] == "left"
+    assert res[0].startswith("error after"), res[0]
+    assert procs[0].exitcode == 0 and procs[1].exitcode == 3
