@@ -16,6 +16,7 @@
 #include <algorithm>
 #include <array>
 #include <atomic>
+#include <charconv>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -118,7 +119,11 @@ class Records {
   size_t at_ = 0;
 };
 
-// a value as strtod / strtol read it (Fortran's D exponent read as E)
+// a value as strtod / strtol read it (Fortran's D exponent read as E).
+// std::from_chars (correctly rounded, as strtod is) takes the tokens it reads
+// whole; anything else -- a leading '+', an out-of-range value, a token with
+// trailing characters -- goes to strtod / strtol, so every token reads as
+// strtod / strtol read it.
 double dval(std::string_view s) {
   char b[64];
   if (s.size() >= sizeof b) {
@@ -129,9 +134,15 @@ double dval(std::string_view s) {
   }
   for (size_t i = 0; i < s.size(); ++i) b[i] = (s[i] == 'd' || s[i] == 'D') ? 'e' : s[i];
   b[s.size()] = 0;
+  double v;
+  const auto r = std::from_chars(b, b + s.size(), v);
+  if (r.ec == std::errc() && r.ptr == b + s.size()) return v;
   return std::strtod(b, nullptr);
 }
 int ival(std::string_view s) {
+  int v;
+  const auto r = std::from_chars(s.data(), s.data() + s.size(), v);
+  if (r.ec == std::errc() && r.ptr == s.data() + s.size()) return v;
   char b[64];
   if (s.size() >= sizeof b) return (int)std::strtol(std::string(s).c_str(), nullptr, 10);
   std::memcpy(b, s.data(), s.size());
