@@ -818,15 +818,16 @@ std::string build_tables(const System& S, Tables& T) {
     }
   };
   // on the library's worker pool: task 0 and 1 build the tetrahedron tables,
-  // tasks 2.. take stripes of mesh points
+  // tasks 2.. take stripes of mesh points (four per worker, handed out as
+  // workers come free: an IBZ point costs all npg arms, the others a few)
   std::vector<int> cand((size_t)T.nkc * npg, -1);
   {
-    const int nthr = pool_width();
-    run_parallel(nthr + 2, [&](int task) {
+    const int nstripe = 4 * pool_width();
+    run_parallel(nstripe + 2, [&](int task) {
       if (task == 0) return build_tet_corner();
       if (task == 1) return build_tet_inc();
       const int t = task - 2;
-      for (int n = t; n < T.nkc; n += nthr) mesh_star_cands(&T.kpc32[3 * (size_t)n], n, &cand[(size_t)n * npg]);
+      for (int n = t; n < T.nkc; n += nstripe) mesh_star_cands(&T.kpc32[3 * (size_t)n], n, &cand[(size_t)n * npg]);
     });
   }
   for (int n = 0; n < T.nkc; ++n) {
