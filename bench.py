@@ -260,7 +260,18 @@ def cpu_baseline(d: str, rows: int = 0, gauss: bool = False):
             "sample": "%d of %d IBZ rows of the same workload: V3 + %s FGR + tauRTA (%.1f s); "
                       "mesh/IBZ/phonon setup %.1f s not counted" % (rows, O.nibz, "Gaussian" if gauss else
                                                                     "tetrahedron", dt, t_setup),
-            "seconds": dt}
+            "seconds": dt, "nibz": O.nibz, "nkc": O.nkc, "ndyn": O.ndyn}
+
+
+def arm_config(workload_desc, mesh, nibz, nkc, b, tb, world, mixed_head):
+    """The workload of the bench line: both arms (the GPU path and the
+    reference's CPU path) print this same dict for the same arguments."""
+    return {"workload": workload_desc, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
+            "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
+            "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
+                2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * (4 if mixed_head else 8) / 1e6),
+            "parallelism": ("dp%d: IBZ rows sharded as the reference's MPI split, NCCL all-gathers "
+                            "of Q and the CG products" % world) if world > 1 else "single GPU"}
 
 
 # DRAM bytes (read + write) of one launch from ncu captures of this workload
@@ -381,7 +392,9 @@ def main():
                 "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic (analytic %s FC2/FC3, reference file formats)" % (
                     "Lennard-Jones" if args.workload == "lj-argon" else "Morse"),
-                "config": {"workload": workload_desc, "mesh": list(mesh)},
+                "config": arm_config(workload_desc, mesh, cb["nibz"], cb["nkc"], cb["ndyn"],
+                                     float(cb["nibz"] * cb["nkc"] * cb["ndyn"] ** 3), world,
+                                     args.precision != "fp64"),
                 "cpu_baseline": {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")},
                 "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
         print(json.dumps(line))
@@ -593,12 +606,7 @@ def main():
                 if mixed_head else "f64",
                 "data": "synthetic (analytic %s FC2/FC3 written in the reference's file formats)" % (
                     "Lennard-Jones" if args.workload == "lj-argon" else "Morse"),
-                "config": {"workload": workload_desc, "mesh": list(mesh), "nibz": nibz, "nkc": nkc, "ndyn": b,
-                           "triplet_bands_per_step": tb, "precision": "mixed" if mixed_head else "fp64",
-                           "l2": "working set > L2 (R1/R2 %.0f MB, collision matrix %.0f MB)" % (
-                               2 * nibz * nkc * b * b * 8 / 1e6, (3 * b * nibz) ** 2 * (4 if mixed_head else 8) / 1e6),
-                           "parallelism": ("dp%d: IBZ rows sharded as the reference's MPI split, NCCL all-gathers "
-                                           "of Q and the CG products" % world) if world > 1 else "single GPU"},
+                "config": arm_config(workload_desc, mesh, nibz, nkc, b, tb, world, mixed_head),
                 "time_to_kappa_ms": ms_max / args.steps,
                 "stage_ms_per_step": {k: round(v, 4) for k, v in per_step.items()},
                 "kappa_cg_trace_over_3": float(np.trace(out["kappa_cg"]) / 3),
