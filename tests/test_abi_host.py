@@ -186,3 +186,50 @@ def test_host_tables_from_concurrent_threads(ald_lib, workdir):
     for (i, _), M in got.items():
         for k in ("mapibz", "mapinv", "kpc", "wibz"):
             assert np.array_equal(M[k], want[i % len(dirs)][k])
+
+
+@pytest.fixture(scope="module")
+def fc_reader(tmp_path_factory):
+    """The library's reader (ald_host.cpp) built into a small program that
+    prints the FC values it read."""
+    import subprocess
+    exe = str(tmp_path_factory.mktemp("fcread") / "fc_read")
+    src = os.path.join(ROOT, "anharmonic-lattice-dynamics_b200", "csrc")
+    subprocess.check_call(["g++", "-std=c++17", "-O2", "-I/usr/local/cuda/include", "-o", exe,
+                           os.path.join(ROOT, "tests", "fc_read_harness.cpp"), os.path.join(src, "ald_host.cpp"),
+                           os.path.join(src, "ald_pool.cpp"), "-L/usr/local/cuda/lib64", "-lcudart", "-lpthread",
+                           "-Wl,-rpath,/usr/local/cuda/lib64"])
+    return exe
+
+
+def test_fc_values_read_as_strtod_reads_them(fc_reader, workdir):
+    """Every FC3 value written in another Fortran-readable form -- a D
+    exponent, a leading '+', no leading digit, a subnormal, a long token --
+    reads to the double that strtod gives for it (Python's float is the same
+    correctly rounded conversion), in the records the worker pool parses."""
+    import subprocess
+    rng = np.random.default_rng(17)
+    forms = [lambda v: "%.17E" % v, lambda v: ("%.15E" % v).replace("E", "D"), lambda v: "%+.12e" % v,
+             lambda v: ("%.9f" % v).replace("0.", ".", 1) if abs(v) < 1 else "%.9f" % v,
+             lambda v: "%.40e" % v, lambda v: "%.6g" % (v * 1e-310), lambda v: "%.17g" % v]
+    expect = []
+
+    def edit(lines):
+        out = lines[:1]
+        for j, l in enumerate(lines[1:]):
+            t = l.split()
+            v = rng.standard_normal() * 10.0 ** rng.integers(-6, 4)
+            tok = forms[j % len(forms)](v)
+            expect.append(float(tok.replace("D", "e")))
+            out.append(" ".join(t[:-1] + [tok]))
+        return out
+    d = _fc3_variant(workdir, "fc3_forms", edit)
+    txt = subprocess.run([fc_reader, d], capture_output=True, text=True, check=True).stdout.split("\n")
+    f3 = [float.fromhex(l.split()[1]) for l in txt if l.startswith("f3 ")]
+    assert len(f3) == len(expect) > 256
+    assert all(a == b for a, b in zip(f3, expect)), next((i, a, b) for i, (a, b) in enumerate(zip(f3, expect))
+                                                         if a != b)
+    # the index tuples are those of the file
+    lines = open(os.path.join(d, "fc3.dat")).read().split("\n")[1:]
+    t3 = [tuple(int(x) for x in l.split()[2:8]) for l in txt if l.startswith("f3 ")]
+    assert t3 == [tuple(int(x) for x in l.split()[2:8]) for l in lines if l.strip()]
